@@ -1,0 +1,280 @@
+"""Throughput of the TV/TGV primal-dual reconstruction on B200, in megapixel-iterations per second.
+
+The workload is the reconstruction of a 4032x3024 YCbCr 4:2:0 picture (seeded synthetic
+piecewise-smooth picture per RGB channel with Gaussian noise sigma 3, quality 75 standard
+tables) by TGV with alpha0 = 2, alpha1 = 1, 500 iterations, all three planes, binary32 state.
+A step is one full solve of it (500 iterations).
+
+  value  the iteration loop alone with the state resident in HBM: device time of K steps by CUDA
+         events on the solve's stream (unround_b200_measure), max over ranks; the state (~3 GB)
+         is larger than L2, so no flush is needed between iterations.
+  e2e    the same metric through the drop-in call (unround.native.solve -> unround_solve) with
+         host arrays: levels copied in, the binary64 result copied out, every step.
+
+With --gpus N (under torchrun) each rank solves its own picture (images are independent units,
+no data-path collective): weak scaling, value = all ranks' pixel-iterations / max time.
+--impl reference times the reference's own C++ solver (oracle/_ref) on the host cores instead.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+HEIGHT, WIDTH, ITERATIONS = 3024, 4032, 500
+OPTIONS = ["--method", "tgv", "--alpha1", "1", "--alpha0", "2", "--iterations", str(ITERATIONS), "--tolerance", "0",
+           "--record-every", "0"]
+METRIC = "TGV PDHG Mpx*iter/s on 1 B200 (4032x3024 YCbCr 4:2:0, 500 iterations)"
+UNIT = "Mpx*iter/s"
+# Algorithmic bytes per sample-iteration of the fused TGV iteration in binary32, 4:2:0
+# (8 fields read and written, 4 B each, and the int16 levels: (2 + 2*2/4) / 3 = 1 B per sample).
+ALGORITHMIC_BYTES = 65.0
+# The dual kernel alone: x~, x, w(2), p(2), r(3) read and x, w, p, r written.
+DUAL_BYTES = 17 * 4.0
+
+
+def _rank() -> tuple[int, int, int]:
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def _peaks() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int) -> None:
+        self.device = device
+        self.samples: list[list[str]] = []
+        self._process: subprocess.Popen | None = None
+        self._thread: threading.Thread | None = None
+
+    def __enter__(self) -> Clocks:
+        try:
+            self._process = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._thread = threading.Thread(target=self._read, daemon=True)
+            self._thread.start()
+        except OSError:
+            self._process = None
+        return self
+
+    def _read(self) -> None:
+        assert self._process is not None and self._process.stdout is not None
+        for line in self._process.stdout:
+            self.samples.append([part.strip() for part in line.split(",")])
+
+    def __exit__(self, *_: object) -> None:
+        if self._process is not None:
+            self._process.terminate()
+            self._process.wait(timeout=5)
+        if self._thread is not None:
+            self._thread.join(timeout=2)
+
+    def summary(self) -> dict:
+        mhz = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        top = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples if len(s) >= 9 for k in range(4) if s[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": max(top) if top else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def _workload(seed: int):
+    from unround import synthetic
+
+    return synthetic.colour(HEIGHT, WIDTH, quality=75, seed=seed, noise=3.0).image
+
+
+def _reference_arm(args: argparse.Namespace, rank: int) -> None:
+    """The reference's own C++ solver on the host cores: each step a bounded sample of the
+    workload (two iterations of the same picture, setup excluded by differencing)."""
+    if rank != 0:
+        return
+    from oracle import reference
+
+    if not reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libunround_ref.so is not built"}))
+        return
+    image = _workload(seed=0)
+    components = [(c.coefficients, c.quant_table.reshape(64), c.h_samp_factor, c.v_samp_factor)
+                  for c in image.components]
+    threads = os.cpu_count() or 1
+
+    def run(iterations: int) -> float:
+        options = [*OPTIONS[:6], "--iterations", str(iterations), "--tolerance", "0", "--record-every", "0",
+                   "--threads", str(threads)]
+        began = time.perf_counter()
+        reference.solve(image.height, image.width, int(image.color_space), components, options)
+        return time.perf_counter() - began
+
+    sample = 2
+    for _ in range(args.warmup):
+        run(1)
+    seconds = []
+    for _ in range(args.steps):
+        seconds.append(max(run(1 + sample) - run(1), 1e-9))
+    per_step = statistics.median(seconds)
+    pixels = HEIGHT * WIDTH
+    value = pixels * sample / per_step / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded piecewise-smooth + noise sigma 3)",
+        "config": {"workload": "tgv-colour-4032x3024-420", "iterations_per_step": sample,
+                   "sample": f"{sample} iterations of the full picture per step (setup differenced out)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{sample} iterations of the 4032x3024 4:2:0 TGV workload, {threads} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def _cpu_baseline(image) -> dict | None:
+    """The reference's solver on the host cores, a bounded sample (two iterations, differenced)."""
+    from oracle import reference
+
+    if not reference.available():
+        return None
+    components = [(c.coefficients, c.quant_table.reshape(64), c.h_samp_factor, c.v_samp_factor)
+                  for c in image.components]
+    threads = os.cpu_count() or 1
+
+    def run(iterations: int) -> float:
+        options = [*OPTIONS[:6], "--iterations", str(iterations), "--tolerance", "0", "--record-every", "0",
+                   "--threads", str(threads)]
+        began = time.perf_counter()
+        reference.solve(image.height, image.width, int(image.color_space), components, options)
+        return time.perf_counter() - began
+
+    sample = 2
+    seconds = max(run(1 + sample) - run(1), 1e-9)
+    return {"value": HEIGHT * WIDTH * sample / seconds / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{sample} iterations of the 4032x3024 4:2:0 TGV workload (setup differenced out), {threads} threads"}
+
+
+def _traffic() -> float | None:
+    """DRAM bytes per launch of the dual kernel at this workload, from the committed ncu summary."""
+    path = ROOT / "profiles" / "traffic.json"
+    try:
+        return float(json.loads(path.read_text())["dual_kernel_bytes_per_launch_4032x3024_420"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=3)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    args = parser.parse_args()
+    rank, local_rank, world = _rank()
+    if world > 1:
+        # One GPU per rank, made the process's only visible device before any CUDA call.
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local_rank)
+    for path in (ROOT / "jpeg-unround_b200", ROOT):
+        sys.path.insert(0, str(path))
+    group = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        group = dist
+    if args.impl == "reference":
+        _reference_arm(args, rank)
+        if group is not None:
+            group.destroy_process_group()
+        return
+
+    import numpy as np
+
+    from unround import native
+
+    image = _workload(seed=rank)
+    # Warm-up steps and timed steps of the device-resident loop.
+    if group is not None:
+        group.barrier()
+    with Clocks(local_rank if world == 1 else 0) as clocks:
+        timing, _ = native.measure(image, OPTIONS, warmup=args.warmup * ITERATIONS, iterations=args.steps * ITERATIONS)
+    seconds = timing.milliseconds / 1e3
+    if group is not None:
+        import torch
+
+        worst = torch.tensor([seconds], dtype=torch.float64)
+        group.all_reduce(worst, op=group.ReduceOp.MAX)
+        seconds = float(worst.item())
+    pixels = timing.pixels
+    value = world * pixels * args.steps * ITERATIONS / seconds / 1e6
+    # End to end through the drop-in call, host arrays in and out.
+    if group is not None:
+        group.barrier()
+    levels_bytes = sum(c.coefficients.nbytes for c in image.components)
+    native.solve(image, OPTIONS)  # warm the call path
+    began = time.perf_counter()
+    for _ in range(args.steps):
+        decoded = native.solve(image, OPTIONS)
+    e2e_seconds = time.perf_counter() - began
+    if group is not None:
+        import torch
+
+        worst = torch.tensor([e2e_seconds], dtype=torch.float64)
+        group.all_reduce(worst, op=group.ReduceOp.MAX)
+        e2e_seconds = float(worst.item())
+    d2h = decoded.canvas.nbytes + sum(c.nbytes for c in decoded.coefficients)
+    e2e = world * pixels * args.steps * ITERATIONS / e2e_seconds / 1e6
+    peak, peak_kind = _peaks()
+    samples = timing.samples
+    dual_achieved = DUAL_BYTES * samples / (timing.dual_milliseconds / 1e3) / 1e9
+    iteration_seconds = seconds / (args.steps * ITERATIONS)
+    iteration_achieved = ALGORITHMIC_BYTES * samples / iteration_seconds / 1e9
+    traffic = _traffic()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": seconds / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded piecewise-smooth per RGB channel + noise sigma 3, quality 75)",
+            "config": {"workload": "tgv-colour-4032x3024-420", "iterations_per_step": ITERATIONS,
+                       "alpha1": 1.0, "alpha0": 2.0, "samples": samples, "pixels": pixels,
+                       "l2": "state larger than L2 (~3 GB), no flush", "parallelism": f"{world} independent images"},
+            "roofline": {"bound": "hbm", "kernel": "dual_kernel<tgv,3,coupled>", "achieved": dual_achieved,
+                         "peak": peak, "unit": "GB/s", "frac": dual_achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_sample": DUAL_BYTES,
+                         "iteration_achieved": iteration_achieved, "iteration_frac": iteration_achieved / peak,
+                         "iteration_bytes_per_sample": ALGORITHMIC_BYTES,
+                         "dual_ms": timing.dual_milliseconds, "primal_ms": timing.primal_milliseconds},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": levels_bytes, "d2h_bytes_per_step": d2h},
+            "gpu_launches": timing.launches_per_iteration * args.steps * ITERATIONS,
+            "clocks": clocks.summary(),
+        }
+        if world == 1:
+            line["cpu_baseline"] = _cpu_baseline(image)
+        print(json.dumps(line))
+    if group is not None:
+        group.destroy_process_group()
+    del np
+
+
+if __name__ == "__main__":
+    main()

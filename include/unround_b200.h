@@ -1,0 +1,61 @@
+/* Extensions of this build beside the reference's C interface (unround.h). They have no
+ * counterpart in unround.h of the reference unless a comment names one; the reference's
+ * callers need none of them.
+ *
+ * Plain pointers and sizes only. Host arrays are binary64 unless named otherwise. */
+#ifndef UNROUND_B200_H
+#define UNROUND_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "unround.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A state to start from (the reference library's pdhg::Start, cpp/include/unround/pdhg.hpp:124-133,
+ * which its C interface does not expose): every component's coefficients, all components'
+ * blocks one after another, which are clipped to their intervals; and each channel's dual
+ * fields p (2 planes), w (2 planes, TGV) and r (3 planes, TGV) of canvas rows x columns,
+ * channel after channel, which are projected onto their balls. A null pointer leaves that
+ * part at the default start (docs/math.md 5). */
+typedef struct unround_b200_start {
+  const double* coefficients;
+  const double* p;
+  const double* w;
+  const double* r;
+} unround_b200_start;
+
+/* unround_solve from a given start. */
+unround_status unround_b200_solve_from(const unround_input* input, const unround_settings* settings,
+                                       const unround_b200_start* start, unround_observer observer, void* user,
+                                       unround_result** result, char* message, size_t message_size);
+
+/* Measurement of the iteration loop alone (no records, no host copies): the settings' method
+ * on the input, `warmup` iterations untimed, then `iterations` timed with CUDA events on the
+ * solve's stream. Writes the device milliseconds of the timed iterations, the kernels
+ * launched per iteration, the canvas's samples and the device bytes held, and each kernel
+ * group's average time from 20 further iterations with events around every launch. With `result`
+ * non-null, the binary64 result of the last iterate is made as unround_solve makes it. */
+typedef struct unround_b200_timing {
+  double milliseconds;
+  double dual_milliseconds;   /* one iteration's dual-step kernel, averaged over 20 timed apart */
+  double primal_milliseconds; /* one iteration's primal-step kernels (every component), likewise */
+  uint64_t iterations;
+  uint64_t launches_per_iteration;
+  uint64_t samples;
+  uint64_t pixels;
+  uint64_t device_bytes;
+} unround_b200_timing;
+
+unround_status unround_b200_measure(const unround_input* input, const unround_settings* settings, uint64_t warmup,
+                                    uint64_t iterations, unround_b200_timing* timing, unround_result** result,
+                                    char* message, size_t message_size);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,580 @@
+// The C interface (include/unround.h, include/unround_b200.h): the reference's unround_capi
+// entry points (rust/capi/src/lib.rs) over the device solver. Inputs are copied for the call
+// (rust/capi/src/lib.rs:617-660), results are owned by the library until unround_result_free,
+// and no exception crosses the interface: each entry point catches everything and returns a
+// status with its message (rust/capi/src/lib.rs:99-115, `guarded`).
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "model.hpp"
+#include "settings.hpp"
+#include "solver.hpp"
+#include "unround.h"
+#include "unround_b200.h"
+
+struct unround_settings {
+  urb::Settings settings;
+};
+
+struct unround_result {
+  urb::Frame frame;
+  urb::Outcome outcome;
+  std::vector<double> picture;
+  std::uint64_t height = 0, width = 0, channels = 0;
+  std::vector<double> planes;
+  std::vector<std::uint64_t> record_iterations;
+  std::vector<double> record_values[5];
+  // What the model holds, made when first asked for (rust/capi/src/lib.rs:888-930).
+  mutable std::once_flag problem_once;
+  mutable std::vector<std::vector<double>> problem[3];
+  std::vector<std::vector<double>> steps, weights;
+};
+
+namespace {
+
+const char kVersion[] = "unround 0.1.0 (B200: CUDA sm_100a, C interface)";
+
+// Writes text into the caller's buffer, NUL-terminated, cut at a UTF-8 character's boundary.
+void say(char* buffer, std::size_t size, const std::string& text) {
+  if (buffer == nullptr || size == 0) return;
+  std::size_t end = std::min(text.size(), size - 1);
+  while (end > 0 && end < text.size() && (static_cast<unsigned char>(text[end]) & 0xC0u) == 0x80u) --end;
+  std::memcpy(buffer, text.data(), end);
+  buffer[end] = 0;
+}
+
+template <typename Body>
+std::int32_t guarded(char* message, std::size_t size, Body&& body) {
+  try {
+    urb::Failure failure;
+    if (body(failure)) return urb::kOk;
+    say(message, size, failure.message);
+    return failure.status;
+  } catch (const std::bad_alloc&) {
+    say(message, size, "an internal error of JPEG-Unround: out of host memory");
+    return urb::kInternal;
+  } catch (const std::exception& error) {
+    say(message, size, std::string("an internal error of JPEG-Unround: ") + error.what());
+    return urb::kInternal;
+  } catch (...) {
+    say(message, size, "an internal error of JPEG-Unround");
+    return urb::kInternal;
+  }
+}
+
+bool have_device(urb::Failure& failure) {
+  int count = 0;
+  const cudaError_t error = cudaGetDeviceCount(&count);
+  if (error != cudaSuccess || count == 0) {
+    failure = {urb::kInternal, std::string("no CUDA device for the solver: ") +
+                                   (error != cudaSuccess ? cudaGetErrorString(error) : "none found")};
+    return false;
+  }
+  return true;
+}
+
+// A CUDA stream of the call's own.
+struct Stream {
+  cudaStream_t stream = nullptr;
+  cudaError_t error = cudaSuccess;
+  Stream() { error = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking); }
+  ~Stream() {
+    if (stream != nullptr) cudaStreamDestroy(stream);
+  }
+};
+
+bool inputs_of(const unround_input* input, std::vector<urb::ComponentInput>& out, urb::Failure& failure) {
+  if (input->components == nullptr || input->count == 0) {
+    failure = {urb::kArgument, "components are given"};
+    return false;
+  }
+  for (std::uint32_t c = 0; c < input->count; ++c) {
+    const unround_component& given = input->components[c];
+    if (given.levels == nullptr) {
+      failure = {urb::kArgument, "a component's levels are a null pointer"};
+      return false;
+    }
+    urb::ComponentInput in;
+    in.levels = given.levels;
+    in.rows = given.rows;
+    in.columns = given.columns;
+    in.h = given.h_samp_factor;
+    in.v = given.v_samp_factor;
+    for (int k = 0; k < 64; ++k) in.table[k] = given.quant_table[k];
+    out.push_back(in);
+  }
+  return true;
+}
+
+// JFIF's RGB of Y, Cb and Cr (docs/math.md 8; rust/unround/src/colour.rs:45-70): the doubles
+// nearest to 701/500, 443/250, 25251/73375 and 209599/293500.
+constexpr double kCr = 0x1.66e978d4fdf3bp+0;
+constexpr double kCb = 0x1.c5a1cac083127p+0;
+constexpr double kGb = 0x1.6065433a66b17p-2;
+constexpr double kGr = 0x1.6da345743d962p-1;
+// And back: the doubles nearest to 0.299, 0.587, 0.114, 250/443 and 500/701.
+constexpr double kR = 0x1.322d0e5604189p-2;
+constexpr double kG = 0x1.2c8b439581062p-1;
+constexpr double kB = 0x1.d2f1a9fbe76c9p-4;
+constexpr double kToCb = 0x1.20f065b4e0378p-1;
+constexpr double kToCr = 0x1.6d314d0e3e153p-1;
+
+void to_rgb(const double* planes, std::size_t size, double* picture) {
+  for (std::size_t k = 0; k < size; ++k) {
+    const double y = planes[k], cb = planes[size + k] - 128.0, cr = planes[2 * size + k] - 128.0;
+    picture[3 * k] = y + kCr * cr;
+    picture[3 * k + 1] = (y - kGb * cb) - kGr * cr;
+    picture[3 * k + 2] = y + kCb * cb;
+  }
+}
+
+void to_ycbcr(const double* picture, std::size_t size, double* planes) {
+  for (std::size_t k = 0; k < size; ++k) {
+    const double r = picture[3 * k], g = picture[3 * k + 1], b = picture[3 * k + 2];
+    const double y = (kR * r + kG * g) + kB * b;
+    planes[k] = y;
+    planes[size + k] = 128.0 + kToCb * (b - y);
+    planes[2 * size + k] = 128.0 + kToCr * (r - y);
+  }
+}
+
+// The result of a solve (rust/unround/src/decode.rs:306-364): the canvas cut to the picture,
+// and of YCbCr its JFIF RGB, interleaved.
+unround_result* result_of(urb::Frame&& frame, urb::Outcome&& outcome) {
+  auto* made = new unround_result;
+  made->frame = std::move(frame);
+  made->outcome = std::move(outcome);
+  const urb::Frame& f = made->frame;
+  const std::size_t h = f.height, w = f.width, count = f.channels();
+  made->height = h;
+  made->width = w;
+  made->planes.resize(count * h * w);
+  for (std::size_t c = 0; c < count; ++c) {
+    for (std::size_t i = 0; i < h; ++i) {
+      const double* from = made->outcome.canvas.data() + (c * f.rows + i) * f.columns;
+      std::copy(from, from + w, made->planes.begin() + static_cast<std::ptrdiff_t>((c * h + i) * w));
+    }
+  }
+  if (f.color_space == 2) {
+    made->channels = 3;
+    made->picture.resize(3 * h * w);
+    to_rgb(made->planes.data(), h * w, made->picture.data());
+  } else if (count == 1) {
+    made->channels = 1;
+    made->picture = made->planes;
+  } else {
+    made->channels = count;
+    made->picture.resize(count * h * w);
+    for (std::size_t k = 0; k < h * w; ++k) {
+      for (std::size_t c = 0; c < count; ++c) made->picture[k * count + c] = made->planes[c * h * w + k];
+    }
+  }
+  for (const urb::Record& r : made->outcome.records) {
+    made->record_iterations.push_back(r.iteration);
+    made->record_values[0].push_back(r.seconds);
+    made->record_values[1].push_back(r.primal);
+    made->record_values[2].push_back(r.dual);
+    made->record_values[3].push_back(r.scaling);
+    made->record_values[4].push_back(r.partial_gap);
+  }
+  for (const urb::Component& c : f.components) {
+    made->steps.emplace_back(c.steps.begin(), c.steps.end());
+    made->weights.emplace_back(c.weights.begin(), c.weights.end());
+  }
+  return made;
+}
+
+bool solve_input(const unround_input* input, const unround_settings* settings, const urb::Start* start,
+                 unround_observer observer, void* user, unround_result** result, urb::Failure& failure,
+                 const unround_b200_start* given) {
+  if (input == nullptr || settings == nullptr || result == nullptr) {
+    failure = {urb::kArgument, "the input, the settings and the result are not null pointers"};
+    return false;
+  }
+  std::vector<urb::ComponentInput> inputs;
+  if (!inputs_of(input, inputs, failure)) return false;
+  const urb::Settings& s = settings->settings;
+  auto frame = urb::make_frame(input->height, input->width, input->color_space, inputs, s, failure);
+  if (!frame) return false;
+  if (s.method == urb::Method::subgradient) {
+    failure = {urb::kUnsupported,
+               "the subgradient method (docs/math.md 7) is not on this build's path: use mmse, tv or tgv"};
+    return false;
+  }
+  std::optional<urb::Plan> plan;
+  if (s.method != urb::Method::mmse) {
+    plan = urb::make_plan(s, frame->channels(), failure);
+    if (!plan) return false;
+  }
+  urb::Start owned_start;
+  if (given != nullptr) {
+    const std::size_t plane = frame->plane(), channels = frame->channels();
+    if (given->coefficients != nullptr) {
+      std::size_t offset = 0;
+      for (const urb::Component& c : frame->components) {
+        owned_start.coefficients.emplace_back(given->coefficients + offset,
+                                              given->coefficients + offset + c.coefficient_count());
+        offset += c.coefficient_count();
+      }
+    }
+    if (given->p != nullptr) owned_start.p.assign(given->p, given->p + 2 * channels * plane);
+    if (given->w != nullptr) owned_start.w.assign(given->w, given->w + 2 * channels * plane);
+    if (given->r != nullptr) owned_start.r.assign(given->r, given->r + 3 * channels * plane);
+    start = &owned_start;
+  }
+  if (!have_device(failure)) return false;
+  Stream stream;
+  if (stream.error != cudaSuccess) {
+    failure = {urb::kInternal, std::string("a CUDA stream: ") + cudaGetErrorString(stream.error)};
+    return false;
+  }
+  urb::Outcome outcome;
+  {
+    urb::Solver solver(*frame, stream.stream);
+    urb::Observer watch;
+    if (observer != nullptr) {
+      const std::uint64_t channels = frame->channels(), rows = frame->rows, columns = frame->columns;
+      watch = [&](const urb::Record& r, double gap, const double* canvas) {
+        unround_record raw{r.iteration, gap, r.primal, r.dual, channels, rows, columns, canvas};
+        return observer(user, &raw) != 0;
+      };
+    }
+    if (!solver.solve(s.method, plan ? &*plan : nullptr, start, watch, outcome, failure)) return false;
+  }
+  *result = result_of(std::move(*frame), std::move(outcome));
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t unround_abi_version(void) { return UNROUND_ABI_VERSION; }
+
+const char* unround_version(void) { return kVersion; }
+
+unround_settings* unround_settings_new(size_t count, const char* const* options, char* message, size_t message_size) {
+  unround_settings* made = nullptr;
+  guarded(message, message_size, [&](urb::Failure& failure) {
+    std::vector<std::string> arguments;
+    if (count > 0 && options == nullptr) {
+      failure = {urb::kArgument, "the strings are a null pointer"};
+      return false;
+    }
+    for (std::size_t i = 0; i < count; ++i) {
+      if (options[i] == nullptr) {
+        failure = {urb::kArgument, "a string is a null pointer"};
+        return false;
+      }
+      arguments.emplace_back(options[i]);
+    }
+    auto* settings = new unround_settings;
+    std::string errors;
+    if (!urb::parse_settings(arguments, settings->settings, errors)) {
+      delete settings;
+      failure = {urb::kOptions, errors};
+      return false;
+    }
+    made = settings;
+    return true;
+  });
+  return made;
+}
+
+void unround_settings_free(unround_settings* settings) { delete settings; }
+
+size_t unround_settings_options(const unround_settings* settings, char* buffer, size_t size) {
+  if (settings == nullptr) return 0;
+  try {
+    std::string text;
+    for (const std::string& option : urb::options_of(settings->settings)) text += (text.empty() ? "" : " ") + option;
+    say(buffer, size, text);
+    return text.size();
+  } catch (...) {
+    return 0;
+  }
+}
+
+unround_status unround_decode(const uint8_t*, size_t, const unround_settings*, unround_observer, void*,
+                              unround_result**, char* message, size_t message_size) {
+  say(message, message_size,
+      "reading a JPEG file needs libjpeg-turbo, which this build does not carry: give the components as arrays "
+      "to unround_solve");
+  return UNROUND_ERROR_UNSUPPORTED;
+}
+
+unround_status unround_solve(const unround_input* input, const unround_settings* settings, unround_observer observer,
+                             void* user, unround_result** result, char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    return solve_input(input, settings, nullptr, observer, user, result, failure, nullptr);
+  });
+}
+
+unround_status unround_b200_solve_from(const unround_input* input, const unround_settings* settings,
+                                       const unround_b200_start* start, unround_observer observer, void* user,
+                                       unround_result** result, char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    return solve_input(input, settings, nullptr, observer, user, result, failure, start);
+  });
+}
+
+unround_status unround_b200_measure(const unround_input* input, const unround_settings* settings, uint64_t warmup,
+                                    uint64_t iterations, unround_b200_timing* timing, unround_result** result,
+                                    char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (input == nullptr || settings == nullptr || timing == nullptr) {
+      failure = {urb::kArgument, "the input, the settings and the timing are not null pointers"};
+      return false;
+    }
+    std::vector<urb::ComponentInput> inputs;
+    if (!inputs_of(input, inputs, failure)) return false;
+    const urb::Settings& s = settings->settings;
+    if (s.method != urb::Method::tv && s.method != urb::Method::tgv) {
+      failure = {urb::kOptions, "the measurement is of the primal-dual methods, tv or tgv"};
+      return false;
+    }
+    auto frame = urb::make_frame(input->height, input->width, input->color_space, inputs, s, failure);
+    if (!frame) return false;
+    auto plan = urb::make_plan(s, frame->channels(), failure);
+    if (!plan) return false;
+    if (!have_device(failure)) return false;
+    Stream stream;
+    urb::Outcome outcome;
+    {
+      urb::Solver solver(*frame, stream.stream);
+      if (!solver.prepare(*plan, failure)) return false;
+      if (warmup > 0 && !solver.iterate(warmup, failure)) return false;
+      cudaEvent_t begin, end;
+      cudaEventCreate(&begin);
+      cudaEventCreate(&end);
+      cudaStreamSynchronize(stream.stream);
+      cudaEventRecord(begin, stream.stream);
+      const bool ok = solver.iterate(iterations, failure);
+      cudaEventRecord(end, stream.stream);
+      cudaEventSynchronize(end);
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, begin, end);
+      cudaEventDestroy(begin);
+      cudaEventDestroy(end);
+      if (!ok) return false;
+      double dual_ms = 0.0, primal_ms = 0.0;
+      if (!solver.breakdown(20, dual_ms, primal_ms, failure)) return false;
+      timing->milliseconds = ms;
+      timing->dual_milliseconds = dual_ms;
+      timing->primal_milliseconds = primal_ms;
+      timing->iterations = iterations;
+      timing->launches_per_iteration = static_cast<std::uint64_t>(solver.launches_per_iteration());
+      timing->samples = static_cast<std::uint64_t>(frame->channels()) * frame->rows * frame->columns;
+      timing->pixels = static_cast<std::uint64_t>(frame->rows) * frame->columns;
+      timing->device_bytes = solver.device_bytes();
+      if (result != nullptr) {
+        if (!solver.finish(outcome, failure)) return false;
+        outcome.solved = true;
+        outcome.iterations = warmup + iterations + 20;
+        outcome.stop = 2;
+        outcome.tau = plan->tau;
+        outcome.sigma = plan->sigma;
+      }
+    }
+    if (result != nullptr) *result = result_of(std::move(*frame), std::move(outcome));
+    return true;
+  });
+}
+
+unround_status unround_project(const uint8_t*, size_t, const unround_settings*, const double*, uint64_t, uint64_t,
+                               uint64_t, unround_result**, char* message, size_t message_size) {
+  say(message, message_size, "projecting onto a JPEG file's intervals needs libjpeg-turbo, which this build does "
+                             "not carry");
+  return UNROUND_ERROR_UNSUPPORTED;
+}
+
+void unround_result_free(unround_result* result) { delete result; }
+
+static void put(uint64_t* target, uint64_t value) {
+  if (target != nullptr) *target = value;
+}
+
+const double* unround_result_picture(const unround_result* result, uint64_t* height, uint64_t* width,
+                                     uint64_t* channels) {
+  if (result == nullptr) return nullptr;
+  put(height, result->height);
+  put(width, result->width);
+  put(channels, result->channels);
+  return result->picture.data();
+}
+
+const double* unround_result_planes(const unround_result* result, uint64_t* count) {
+  if (result == nullptr) return nullptr;
+  put(count, result->planes.size());
+  return result->planes.data();
+}
+
+int32_t unround_result_color_space(const unround_result* result) {
+  return result == nullptr ? 0 : result->frame.color_space;
+}
+
+const double* unround_result_canvas(const unround_result* result, uint64_t* channels, uint64_t* height,
+                                    uint64_t* width) {
+  if (result == nullptr) return nullptr;
+  put(channels, result->frame.channels());
+  put(height, result->frame.rows);
+  put(width, result->frame.columns);
+  return result->outcome.canvas.data();
+}
+
+uint64_t unround_result_components(const unround_result* result) {
+  return result == nullptr ? 0 : result->frame.channels();
+}
+
+const double* unround_result_coefficients(const unround_result* result, uint64_t component, uint64_t* count) {
+  if (result == nullptr || component >= result->outcome.coefficients.size()) return nullptr;
+  put(count, result->outcome.coefficients[component].size());
+  return result->outcome.coefficients[component].data();
+}
+
+const double* unround_result_problem(const unround_result* result, uint64_t component, int32_t which, uint64_t* count) {
+  if (result == nullptr || component >= result->frame.channels() || which < 0 || which > 4) return nullptr;
+  if (which == 3) {
+    put(count, 64);
+    return result->steps[component].data();
+  }
+  if (which == 4) {
+    put(count, 64);
+    return result->weights[component].data();
+  }
+  try {
+    std::call_once(result->problem_once, [result] {
+      for (const urb::Component& c : result->frame.components) {
+        const std::size_t n = c.coefficient_count();
+        std::vector<double> lower(n), upper(n), centres(n);
+        for (std::size_t at = 0; at < n; ++at) {
+          const int k = static_cast<int>(at % 64);
+          lower[at] = c.lower(c.levels[at], k);
+          upper[at] = c.upper(c.levels[at], k);
+          centres[at] = c.centre(c.levels[at], k);
+        }
+        result->problem[0].push_back(std::move(lower));
+        result->problem[1].push_back(std::move(upper));
+        result->problem[2].push_back(std::move(centres));
+      }
+    });
+  } catch (...) {
+    return nullptr;
+  }
+  const std::vector<double>& values = result->problem[which][component];
+  put(count, values.size());
+  return values.data();
+}
+
+unround_status unround_result_component(const unround_result* result, uint64_t component, uint64_t* rows,
+                                        uint64_t* columns, uint64_t* down, uint64_t* across) {
+  if (result == nullptr || component >= result->frame.channels()) return UNROUND_ERROR_ARGUMENT;
+  const urb::Component& c = result->frame.components[component];
+  put(rows, c.block_rows);
+  put(columns, c.block_columns);
+  put(down, c.cell_rows);
+  put(across, c.cell_columns);
+  return UNROUND_OK;
+}
+
+int32_t unround_result_solver(const unround_result* result, uint64_t* iterations, int32_t* stop) {
+  if (result == nullptr || !result->outcome.solved) return 0;
+  put(iterations, result->outcome.iterations);
+  if (stop != nullptr) *stop = result->outcome.stop;
+  return 1;
+}
+
+const uint64_t* unround_result_record_iterations(const unround_result* result, uint64_t* count) {
+  if (result == nullptr || !result->outcome.solved) return nullptr;
+  put(count, result->record_iterations.size());
+  return result->record_iterations.data();
+}
+
+const double* unround_result_record_values(const unround_result* result, int32_t which, uint64_t* count) {
+  if (result == nullptr || !result->outcome.solved || which < 0 || which > 4) return nullptr;
+  put(count, result->record_values[which].size());
+  return result->record_values[which].data();
+}
+
+int32_t unround_result_alpha_solver(const unround_result*, uint64_t*, int32_t*) { return 0; }
+const uint64_t* unround_result_alpha_record_iterations(const unround_result*, uint64_t*) { return nullptr; }
+const double* unround_result_alpha_record_values(const unround_result*, int32_t, uint64_t*) { return nullptr; }
+const uint8_t* unround_result_icc_profile(const unround_result*, uint64_t*) { return nullptr; }
+int32_t unround_result_exif_orientation(const unround_result*) { return 0; }
+int32_t unround_result_format(const unround_result* result) { return result == nullptr ? 0 : UNROUND_FORMAT_JPEG; }
+int32_t unround_result_bits(const unround_result* result) { return result == nullptr ? 0 : 8; }
+const char* unround_result_warning(const unround_result* result) { return result == nullptr ? nullptr : ""; }
+const double* unround_result_excess(const unround_result*, uint64_t, uint64_t*) { return nullptr; }
+
+unround_status unround_tiff(const double*, uint64_t, uint64_t, uint64_t, int32_t, const uint8_t*, uint64_t, uint8_t**,
+                            uint64_t*, char* message, size_t message_size) {
+  say(message, message_size, "the TIFF writer is host output outside this build's path");
+  return UNROUND_ERROR_UNSUPPORTED;
+}
+
+unround_status unround_png(const double*, uint64_t, uint64_t, uint64_t, int32_t, int32_t, int32_t, const uint8_t*,
+                           uint64_t, uint8_t**, uint64_t*, char* message, size_t message_size) {
+  say(message, message_size, "writing PNG needs libpng, which this build does not carry");
+  return UNROUND_ERROR_UNSUPPORTED;
+}
+
+unround_status unround_pnm(const double*, uint64_t, uint64_t, uint64_t, int32_t, int32_t, uint8_t**, uint64_t*,
+                           char* message, size_t message_size) {
+  say(message, message_size, "the PNM writer is host output outside this build's path");
+  return UNROUND_ERROR_UNSUPPORTED;
+}
+
+void unround_bytes_free(uint8_t* bytes, uint64_t) { delete[] bytes; }
+
+unround_status unround_orient(const double*, uint64_t, uint64_t, uint64_t, int32_t, double*, uint64_t*, uint64_t*,
+                              char* message, size_t message_size) {
+  say(message, message_size, "turning a picture upright is host output outside this build's path");
+  return UNROUND_ERROR_UNSUPPORTED;
+}
+
+unround_status unround_to_rgb(const double* planes, uint64_t height, uint64_t width, double* picture) {
+  if (planes == nullptr || picture == nullptr) return UNROUND_ERROR_ARGUMENT;
+  to_rgb(planes, static_cast<std::size_t>(height * width), picture);
+  return UNROUND_OK;
+}
+
+unround_status unround_to_ycbcr(const double* picture, uint64_t height, uint64_t width, double* planes) {
+  if (planes == nullptr || picture == nullptr) return UNROUND_ERROR_ARGUMENT;
+  to_ycbcr(picture, static_cast<std::size_t>(height * width), planes);
+  return UNROUND_OK;
+}
+
+int32_t unround_main(size_t, const char* const*) { return 3; }
+
+int32_t unround_jpeg_abi_version(void) { return UNROUND_JPEGIO_ABI_VERSION; }
+const char* unround_jpeg_libjpeg_version(void) { return "none (this build reads no JPEG files)"; }
+const char* unround_jpeg_libpng_version(void) { return "none (this build writes no PNG files)"; }
+
+int32_t unround_jpeg_check_icc(const uint8_t*, uint64_t, int32_t, char* reason, size_t reason_size) {
+  say(reason, reason_size, "this build carries no libpng to check a profile");
+  return 0;
+}
+
+unround_jpegio_status unround_jpeg_read(const uint8_t*, size_t, const unround_jpegio_options*, unround_jpegio_image*,
+                                        char* message, size_t message_size) {
+  say(message, message_size, "reading a JPEG file needs libjpeg-turbo, which this build does not carry");
+  return 3;
+}
+
+void unround_jpeg_image_free(unround_jpegio_image*) {}
+
+unround_jpegio_status unround_jpeg_decode_planes(const uint8_t*, size_t, const unround_jpegio_options*,
+                                                 unround_jpegio_planes*, char* message, size_t message_size) {
+  say(message, message_size, "decoding a JPEG file needs libjpeg-turbo, which this build does not carry");
+  return 3;
+}
+
+void unround_jpeg_planes_free(unround_jpegio_planes*) {}
+
+}  // extern "C"

@@ -1,0 +1,988 @@
+// The kernels of the solver, sm_100a, binary32 iterations with binary64 records, start and
+// result. See kernels.hpp for the layout. The formulas and their order of operations follow
+// the reference's iteration (cpp/src/primal_dual.hpp:525-735; rust/unround/src/kernels.rs),
+// a pixel or a block at a time instead of a row at a time:
+//
+//   dual_kernel    x- = 2x~ - x, w~ = w + tau g (p + div2 r), w- = 2w~ - w,
+//                  p~ = proj_a1(p + sigma g (grad x- - w-)), r~ = proj_a0(r + sigma g E w-),
+//                  and every field relaxed, x <- rho x~ + (1 - rho) x   (docs/math.md 5)
+//   primal_kernel  v = x + tau g div p, then per block of the component: the means of the
+//                  cells, the DCT, the clip of the proximal map, the inverse DCT, and the
+//                  change spread back over the cells (docs/math.md 4.1, 4.4)
+//
+// The finite differences are those of docs/math.md 3.1-3.2 with Neumann ends: forward
+// differences are 0 in the last column/row, backward differences drop the sample of the last
+// column/row and the neighbour before the first.
+#include "kernels.hpp"
+
+#include <cfloat>
+#include <cstdint>
+
+#include "dct.cuh"
+
+namespace urb {
+
+namespace {
+
+constexpr int kWarps = 8;
+
+__device__ __forceinline__ float ld(const float* base, std::size_t at) { return __ldg(base + at); }
+
+// radius / |p| beyond the ball, 1 within it (cpp/include/unround/operators.hpp:112-116).
+template <typename T>
+__device__ __forceinline__ T ball_scale(T square, T radius) {
+  const T norm = sqrt(square);
+  return norm > radius ? radius / norm : T(1);
+}
+
+template <typename T>
+__device__ __forceinline__ T clamp_to(T value, T low, T high) {
+  return fmin(fmax(value, low), high);
+}
+
+// The sum (or the largest) over the CTA of one double per thread, in a fixed order: warp
+// by warp with shuffles, then the warps' in order. Thread 0 holds the result.
+template <bool MAX>
+__device__ double cta_reduce(double value) {
+  __shared__ double partial[32];
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int warps = (blockDim.x * blockDim.y * blockDim.z + 31) / 32;
+  for (int offset = 16; offset > 0; offset >>= 1) {
+    const double other = __shfl_down_sync(0xffffffffu, value, offset);
+    value = MAX ? fmax(value, other) : value + other;
+  }
+  if ((tid & 31) == 0) partial[tid >> 5] = value;
+  __syncthreads();
+  double total = 0.0;
+  if (tid < 32) {
+    total = tid < warps ? partial[tid] : 0.0;
+    for (int offset = 16; offset > 0; offset >>= 1) {
+      const double other = __shfl_down_sync(0xffffffffu, total, offset);
+      total = MAX ? fmax(total, other) : total + other;
+    }
+  }
+  __syncthreads();
+  return total;
+}
+
+__device__ __forceinline__ int cta_index() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+
+__device__ __forceinline__ bool cta_leader() { return threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0; }
+
+// One double per CTA into out[cta].
+__device__ __forceinline__ void cta_sum(double value, double* out) {
+  const double total = cta_reduce<false>(value);
+  if (cta_leader()) out[cta_index()] = total;
+}
+
+// ---------------------------------------------------------------------------------------
+// The dual step (one thread per pixel, every channel of it).
+
+struct Wt {
+  float w1, w2;  // w of s_{n-1}
+  float t1, t2;  // w~
+};
+
+// w~ = w + tau g (p + div2 r) at (i, j) of one channel (cpp/src/primal_dual.hpp:547-557):
+// div2 r = (dx r11 + dy r12, dx r12 + dy r22), forward differences, 0 at the ends.
+__device__ __forceinline__ Wt w_tilde(const Fields& in, std::size_t base, std::size_t at, int i, int j, int rows,
+                                      int columns, int pitch, float tau) {
+  const float r11 = ld(in.r11 + base, at), r12 = ld(in.r12 + base, at), r22 = ld(in.r22 + base, at);
+  float d1 = 0.0f, d2 = 0.0f;
+  if (j + 1 < columns) {
+    d1 = ld(in.r11 + base, at + 1) - r11;
+    d2 = ld(in.r12 + base, at + 1) - r12;
+  }
+  if (i + 1 < rows) {
+    d1 = d1 + (ld(in.r12 + base, at + pitch) - r12);
+    d2 = d2 + (ld(in.r22 + base, at + pitch) - r22);
+  }
+  Wt w;
+  w.w1 = ld(in.w1 + base, at);
+  w.w2 = ld(in.w2 + base, at);
+  w.t1 = w.w1 + tau * (ld(in.p1 + base, at) + d1);
+  w.t2 = w.w2 + tau * (ld(in.p2 + base, at) + d2);
+  return w;
+}
+
+template <bool TGV, int C, bool COUPLED, bool KEEP>
+__global__ void __launch_bounds__(256) dual_kernel(const DualParams P) {
+  const int j = blockIdx.x * 32 + threadIdx.x;
+  const int i = blockIdx.y * 8 + threadIdx.y;
+  const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+  if (i >= rows || j >= columns) return;
+  const std::size_t at = static_cast<std::size_t>(i) * pitch + j;
+  const bool has_right = j + 1 < columns, has_down = i + 1 < rows;
+  const bool has_left = j > 0, has_up = i > 0;
+  const float rho = P.rho, rest = P.rest;
+
+  float step_p1[C], step_p2[C], old_p1[C], old_p2[C];
+  float step_r11[C], step_r22[C], step_r12[C], old_r11[C], old_r22[C], old_r12[C];
+  float square_p = 0.0f, square_r = 0.0f;
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const std::size_t base = c * P.g.plane;
+    const float* xt = P.xt + base;
+    const float* x = P.in.x + base;
+    const float xt0 = ld(xt, at), x0 = ld(x, at);
+    const float bar = 2.0f * xt0 - x0;
+    const float gx = has_right ? (2.0f * ld(xt, at + 1) - ld(x, at + 1)) - bar : 0.0f;
+    const float gy = has_down ? (2.0f * ld(xt, at + pitch) - ld(x, at + pitch)) - bar : 0.0f;
+    P.out.x[base + at] = rho * xt0 + rest * x0;
+    const float p1 = ld(P.in.p1 + base, at), p2 = ld(P.in.p2 + base, at);
+    old_p1[c] = p1;
+    old_p2[c] = p2;
+    const float sigma = P.sigma[c];
+    if constexpr (!TGV) {
+      step_p1[c] = p1 + sigma * gx;
+      step_p2[c] = p2 + sigma * gy;
+    } else {
+      const float tau = P.tau[c];
+      const Wt w0 = w_tilde(P.in, base, at, i, j, rows, columns, pitch, tau);
+      const float wb1 = 2.0f * w0.t1 - w0.w1, wb2 = 2.0f * w0.t2 - w0.w2;
+      float wl1 = 0.0f, wl2 = 0.0f, wu1 = 0.0f, wu2 = 0.0f;
+      if (has_left) {
+        const Wt w = w_tilde(P.in, base, at - 1, i, j - 1, rows, columns, pitch, tau);
+        wl1 = 2.0f * w.t1 - w.w1;
+        wl2 = 2.0f * w.t2 - w.w2;
+      }
+      if (has_up) {
+        const Wt w = w_tilde(P.in, base, at - pitch, i - 1, j, rows, columns, pitch, tau);
+        wu1 = 2.0f * w.t1 - w.w1;
+        wu2 = 2.0f * w.t2 - w.w2;
+      }
+      P.out.w1[base + at] = rho * w0.t1 + rest * w0.w1;
+      P.out.w2[base + at] = rho * w0.t2 + rest * w0.w2;
+      if constexpr (KEEP) {
+        P.tilde.w1[base + at] = w0.t1;
+        P.tilde.w2[base + at] = w0.t2;
+      }
+      step_p1[c] = p1 + sigma * (gx - wb1);
+      step_p2[c] = p2 + sigma * (gy - wb2);
+      // E w- = (dx' w1, dy' w2, (dy' w1 + dx' w2) / 2), backward differences.
+      const float own1x = has_right ? wb1 : 0.0f, own2x = has_right ? wb2 : 0.0f;
+      const float own1y = has_down ? wb1 : 0.0f, own2y = has_down ? wb2 : 0.0f;
+      const float exx = own1x - wl1;
+      const float eyy = own2y - wu2;
+      const float exy = 0.5f * ((own1y - wu1) + (own2x - wl2));
+      const float r11 = ld(P.in.r11 + base, at), r22 = ld(P.in.r22 + base, at), r12 = ld(P.in.r12 + base, at);
+      old_r11[c] = r11;
+      old_r22[c] = r22;
+      old_r12[c] = r12;
+      step_r11[c] = r11 + sigma * exx;
+      step_r22[c] = r22 + sigma * eyy;
+      step_r12[c] = r12 + sigma * exy;
+    }
+    if constexpr (COUPLED) {
+      square_p += step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c];
+      if constexpr (TGV) {
+        square_r += step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]);
+      }
+    }
+  }
+  float scale_p = 1.0f, scale_r = 1.0f;
+  if constexpr (COUPLED) {
+    scale_p = ball_scale(square_p, P.radius);
+    if constexpr (TGV) scale_r = ball_scale(square_r, P.radius0);
+  }
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const std::size_t base = c * P.g.plane;
+    float sp = scale_p;
+    if constexpr (!COUPLED) sp = ball_scale(step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c], P.radius);
+    const float q1 = step_p1[c] * sp, q2 = step_p2[c] * sp;
+    P.out.p1[base + at] = rho * q1 + rest * old_p1[c];
+    P.out.p2[base + at] = rho * q2 + rest * old_p2[c];
+    if constexpr (KEEP) {
+      P.tilde.p1[base + at] = q1;
+      P.tilde.p2[base + at] = q2;
+    }
+    if constexpr (TGV) {
+      float sr = scale_r;
+      if constexpr (!COUPLED) {
+        sr = ball_scale(step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]),
+                        P.radius0);
+      }
+      const float t11 = step_r11[c] * sr, t22 = step_r22[c] * sr, t12 = step_r12[c] * sr;
+      P.out.r11[base + at] = rho * t11 + rest * old_r11[c];
+      P.out.r22[base + at] = rho * t22 + rest * old_r22[c];
+      P.out.r12[base + at] = rho * t12 + rest * old_r12[c];
+      if constexpr (KEEP) {
+        P.tilde.r11[base + at] = t11;
+        P.tilde.r22[base + at] = t22;
+        P.tilde.r12[base + at] = t12;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// The primal step and the proximal map. A CTA is 8 warps; a warp takes 4 of the component's
+// blocks side by side, a lane one column of the block's 8 x 8 (cell) means: the lane computes
+// v for the CR x CC samples of each of its cells, the column DCT in registers, and a
+// transpose through shared memory gives each lane one row of coefficients (v = lane, u = 0..7)
+// for the row DCT, the clip, and the inverse row DCT; a second transpose returns the columns.
+
+// The interval and the centre of a coefficient in binary32, from its level
+// (cpp/src/model.cpp:41-46, 237-247; laplace.hpp:51-56).
+struct Coefficient {
+  float low, high, centre, own_low, own_high;
+};
+
+__device__ __forceinline__ Coefficient coefficient_of(int q, int k, const ProxFactors& F) {
+  const float level = static_cast<float>(q);
+  const float step = F.step[k];
+  const float shift = k == 0 ? 1024.0f : 0.0f;
+  Coefficient c;
+  c.low = ((level - 0.5f) - F.slack) * step + shift;
+  c.high = ((level + 0.5f) + F.slack) * step + shift;
+  if (F.mmse && k != 0) {
+    const float size = (fabsf(level) - F.shrink[k]) * step;
+    c.centre = q == 0 ? 0.0f : (q < 0 ? -size : size);
+  } else {
+    c.centre = level * step + shift;
+  }
+  c.own_low = (level - 0.5f) * step + shift;
+  c.own_high = (level + 0.5f) * step + shift;
+  return c;
+}
+
+// prox of a coefficient (cpp/src/model.cpp:57-72): z = (e + t c) r clipped, and with a
+// slack's cost moved back by h beyond the file's own interval, not past its end.
+__device__ __forceinline__ float prox_of(float e, float t, float r, float h, const Coefficient& c, bool costed) {
+  const float z = (e + t * c.centre) * r;
+  if (!costed) return clamp_to(z, c.low, c.high);
+  const float above = fmaxf(c.own_high, z - h);
+  const float below = fminf(c.own_low, z + h);
+  const float inside = z < c.own_low ? below : z;
+  return clamp_to(z > c.own_high ? above : inside, c.low, c.high);
+}
+
+// G's terms at a coefficient in binary64 (cpp/src/model.cpp:384-392): m/2 (c - centre)^2, and
+// the cost of lying beyond the file's own interval.
+__device__ __forceinline__ double value_term(double zeta, int q, int k, bool flat, const Constants64& K) {
+  const double level = static_cast<double>(q);
+  const double step = K.step[k];
+  const double shift = k == 0 ? 1024.0 : 0.0;
+  double centre;
+  if (K.mmse && k != 0) {
+    const double size = (fabs(level) - K.shrink[k]) * step;
+    centre = q == 0 ? 0.0 : (q < 0 ? -size : size);
+  } else {
+    centre = level * step + shift;
+  }
+  const double m = flat ? K.flat_weight[k] : K.weight[k];
+  const double away = zeta - centre;
+  double term = 0.5 * m * (away * away);
+  if (K.costed) {
+    const double own_low = (level - 0.5) * step + shift;
+    const double own_high = (level + 0.5) * step + shift;
+    term = term + K.cost[k] * fmax(fmax(zeta - own_high, own_low - zeta), 0.0);
+  }
+  return term;
+}
+
+template <int CR, int CC, bool KEEP>
+__global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
+  __shared__ ProxFactors F;
+  __shared__ float tile[kWarps][4][72];
+  {
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    const float* from = reinterpret_cast<const float*>(P.component.factors);
+    float* to = reinterpret_cast<float*>(&F);
+    for (int k = tid; k < static_cast<int>(sizeof(ProxFactors) / 4); k += 256) to[k] = from[k];
+  }
+  __syncthreads();
+  constexpr int BH = 8 * CR, BW = 8 * CC;
+  const int lane = threadIdx.x, b = lane >> 3, m = lane & 7;
+  const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+  const int vbx = blockIdx.x * 4 + b;
+  const int vby = blockIdx.y * kWarps + threadIdx.y;
+  const bool active = vbx * BW < columns && vby * BH < rows;
+  const int j0 = vbx * BW + m * CC;
+  const int i0 = vby * BH;
+  const bool in_blocks = active && vby < P.component.block_rows && vbx < P.component.block_columns;
+  const float descent = P.descent;
+
+  // v = x + tau g div p over the lane's CR x CC cells of each mean row.
+  float v[BH][CC];
+  float p2_above[CC];
+#pragma unroll
+  for (int c = 0; c < CC; ++c) {
+    const int j = j0 + c;
+    p2_above[c] = (active && i0 > 0) ? ld(P.p2, static_cast<std::size_t>(i0 - 1) * pitch + j) : 0.0f;
+  }
+#pragma unroll
+  for (int r = 0; r < BH; ++r) {
+    const int i = i0 + r;
+    const std::size_t row = static_cast<std::size_t>(i) * pitch;
+    float p1[CC], p2[CC], x[CC];
+#pragma unroll
+    for (int c = 0; c < CC; ++c) {
+      p1[c] = active ? ld(P.p1, row + j0 + c) : 0.0f;
+      p2[c] = active ? ld(P.p2, row + j0 + c) : 0.0f;
+      x[c] = active ? ld(P.x, row + j0 + c) : 0.0f;
+    }
+    float left = __shfl_up_sync(0xffffffffu, p1[CC - 1], 1);
+    if (lane == 0) left = (active && j0 > 0) ? ld(P.p1, row + j0 - 1) : 0.0f;
+#pragma unroll
+    for (int c = 0; c < CC; ++c) {
+      const int j = j0 + c;
+      const float before = c == 0 ? left : p1[c - 1];
+      // div p = dy' p2 + dx' p1, backward differences.
+      const float dy = (i + 1 < rows ? p2[c] : 0.0f) - (i > 0 ? p2_above[c] : 0.0f);
+      const float dx = (j + 1 < columns ? p1[c] : 0.0f) - (j > 0 ? before : 0.0f);
+      v[r][c] = x[c] + descent * (dy + dx);
+      p2_above[c] = p2[c];
+    }
+  }
+
+  float out[BH][CC];
+  float zeta[8];
+  int levels[8];
+  bool flat = false;
+  if constexpr (CR == 1 && CC == 1) {
+    // The means are v itself.
+  }
+  float mean[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    if constexpr (CR == 1 && CC == 1) {
+      mean[r] = v[r][0];
+    } else {
+      float sum = 0.0f;
+#pragma unroll
+      for (int c = 0; c < CC; ++c) {
+        float column = v[CR * r][c];
+#pragma unroll
+        for (int a = 1; a < CR; ++a) column += v[CR * r + a][c];
+        sum = c == 0 ? column : sum + column;
+      }
+      mean[r] = sum / static_cast<float>(CR * CC);
+    }
+  }
+  // Column DCT, transpose, row DCT: the lane holds coefficients (v = m, u = 0..7).
+  float col[8], coef[8];
+  forward8(mean, col);
+  float* t = tile[threadIdx.y][b];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) t[k * 9 + m] = col[k];
+  __syncwarp();
+  float row[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) row[u] = t[m * 9 + u];
+  forward8(row, coef);
+  // The clip of the proximal map.
+  {
+    const std::size_t block = static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns +
+                              (in_blocks ? vbx : 0);
+    const int4 packed = in_blocks ? __ldg(reinterpret_cast<const int4*>(P.component.levels + block * 64 + m * 8))
+                                  : make_int4(0, 0, 0, 0);
+    const int words[4] = {packed.x, packed.y, packed.z, packed.w};
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const unsigned word = static_cast<unsigned>(words[u >> 1]);
+      levels[u] = static_cast<int>(static_cast<std::int16_t>((u & 1) ? (word >> 16) : (word & 0xffffu)));
+    }
+    flat = in_blocks && P.component.flat[block] != 0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = m * 8 + u;
+      const Coefficient c = coefficient_of(levels[u], k, F);
+      const float tk = flat ? F.t_flat[k] : F.t[k];
+      const float rk = flat ? F.r_flat[k] : F.r[k];
+      const float hk = flat ? F.h_flat[k] : F.h[k];
+      zeta[u] = prox_of(coef[u], tk, rk, hk, c, F.costed != 0);
+    }
+    if constexpr (KEEP) {
+      if (in_blocks) {
+        float4* to = reinterpret_cast<float4*>(P.component.zeta + block * 64 + m * 8);
+        to[0] = make_float4(zeta[0], zeta[1], zeta[2], zeta[3]);
+        to[1] = make_float4(zeta[4], zeta[5], zeta[6], zeta[7]);
+      }
+    }
+  }
+  // Inverse row DCT, transpose back, inverse column DCT.
+  inverse8(zeta, row);
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < 8; ++c) t[m * 9 + c] = row[c];
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 8; ++k) col[k] = t[k * 9 + m];
+  float back[8];
+  inverse8(col, back);
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    if constexpr (CR == 1 && CC == 1) {
+      out[r][0] = in_blocks ? back[r] : v[r][0];
+    } else {
+      const float change = back[r] - mean[r];
+#pragma unroll
+      for (int a = 0; a < CR; ++a) {
+#pragma unroll
+        for (int c = 0; c < CC; ++c) out[CR * r + a][c] = in_blocks ? v[CR * r + a][c] + change : v[CR * r + a][c];
+      }
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (int r = 0; r < BH; ++r) {
+      const std::size_t at = static_cast<std::size_t>(i0 + r) * pitch + j0;
+#pragma unroll
+      for (int c = 0; c < CC; ++c) {
+        P.xt[at + c] = out[r][c];
+        if constexpr (KEEP) P.v[at + c] = v[r][c];
+      }
+    }
+  }
+  if constexpr (KEEP) {
+    double sum = 0.0;
+    if (in_blocks) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) sum += value_term(zeta[u], levels[u], m * 8 + u, flat, *P.component.constants);
+    }
+    cta_sum(sum, P.partials);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Binary64: the start's coefficients, and canvases of coefficients.
+
+__global__ void __launch_bounds__(256) start_kernel(const StartParams P) {
+  const int thread = blockIdx.x * 256 + threadIdx.x;
+  const int blocks = P.component.block_rows * P.component.block_columns;
+  const int block = thread >> 3, m = thread & 7;
+  double sum = 0.0;
+  if (block < blocks) {
+    const Constants64& K = *P.component.constants;
+    const bool flat = P.component.flat[block] != 0;
+    for (int u = 0; u < 8; ++u) {
+      const int k = m * 8 + u;
+      const std::size_t at = static_cast<std::size_t>(block) * 64 + k;
+      const int q = P.component.levels[at];
+      const double level = static_cast<double>(q);
+      const double step = K.step[k];
+      const double shift = k == 0 ? 1024.0 : 0.0;
+      const double low = ((level - 0.5) - K.slack) * step + shift;
+      const double high = ((level + 0.5) + K.slack) * step + shift;
+      double centre;
+      if (K.mmse && k != 0) {
+        const double size = (fabs(level) - K.shrink[k]) * step;
+        centre = q == 0 ? 0.0 : (q < 0 ? -size : size);
+      } else {
+        centre = level * step + shift;
+      }
+      const double from = P.given != nullptr ? P.given[at] : centre;
+      const double zeta = clamp_to(from, low, high);
+      P.coefficients[at] = zeta;
+      sum += value_term(zeta, q, k, flat, K);
+    }
+  }
+  cta_sum(sum, P.partials);
+}
+
+template <int CR, int CC>
+__global__ void __launch_bounds__(256) canvas_kernel(const CanvasParams P) {
+  __shared__ double tile[kWarps][4][72];
+  constexpr int BH = 8 * CR, BW = 8 * CC;
+  const int lane = threadIdx.x, b = lane >> 3, m = lane & 7;
+  const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+  const int vbx = blockIdx.x * 4 + b;
+  const int vby = blockIdx.y * kWarps + threadIdx.y;
+  const bool active = vbx * BW < columns && vby * BH < rows;
+  const bool in_blocks = active && vby < P.component.block_rows && vbx < P.component.block_columns;
+  const int j0 = vbx * BW + m * CC, i0 = vby * BH;
+  const std::size_t block =
+      static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
+  // The lane's row of coefficients, the inverse row DCT, transpose, inverse column DCT.
+  double zeta[8], row[8], col[8], back[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) zeta[u] = in_blocks ? P.coefficients[block * 64 + m * 8 + u] : 0.0;
+  inverse8(zeta, row);
+  double* t = tile[threadIdx.y][b];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) t[m * 9 + c] = row[c];
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 8; ++k) col[k] = t[k * 9 + m];
+  inverse8(col, back);
+  if (!active) return;
+  double* canvas = P.canvas;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    double vs[CR][CC];
+    double mean = 0.0;
+    if (P.mode == 1) {
+      double sum = 0.0;
+#pragma unroll
+      for (int c = 0; c < CC; ++c) {
+        double column = 0.0;
+#pragma unroll
+        for (int a = 0; a < CR; ++a) {
+          vs[a][c] = static_cast<double>(P.v[static_cast<std::size_t>(i0 + CR * r + a) * pitch + j0 + c]);
+          column = a == 0 ? vs[a][c] : column + vs[a][c];
+        }
+        sum = c == 0 ? column : sum + column;
+      }
+      mean = sum / static_cast<double>(CR * CC);
+    }
+#pragma unroll
+    for (int a = 0; a < CR; ++a) {
+#pragma unroll
+      for (int c = 0; c < CC; ++c) {
+        const int i = i0 + CR * r + a, j = j0 + c;
+        double value;
+        if (P.mode == 0) {
+          value = in_blocks ? back[r] : P.beyond;
+        } else if (CR * CC == 1) {
+          value = in_blocks ? back[r] : vs[a][c];
+        } else {
+          value = in_blocks ? vs[a][c] + (back[r] - mean) : vs[a][c];
+        }
+        canvas[static_cast<std::size_t>(i) * columns + j] = value;
+        if (P.mode == 0 && P.x != nullptr) P.x[static_cast<std::size_t>(i) * pitch + j] = static_cast<float>(value);
+      }
+    }
+  }
+}
+
+__global__ void gradient_kernel(const float* x, float* w1, float* w2, Geometry g) {
+  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y;
+  if (i >= g.rows || j >= g.columns) return;
+  for (int c = 0; c < g.channels; ++c) {
+    const std::size_t base = c * g.plane, at = static_cast<std::size_t>(i) * g.pitch + j;
+    const float here = x[base + at];
+    w1[base + at] = j + 1 < g.columns ? x[base + at + 1] - here : 0.0f;
+    w2[base + at] = i + 1 < g.rows ? x[base + at + g.pitch] - here : 0.0f;
+  }
+}
+
+// Projects a start's duals onto their balls (cpp/src/operators.cpp project; 4.4, 5).
+__global__ void project_kernel(Fields f, Geometry g, int tgv, int coupled, float radius, float radius0) {
+  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y;
+  if (i >= g.rows || j >= g.columns) return;
+  const std::size_t at = static_cast<std::size_t>(i) * g.pitch + j;
+  if (coupled) {
+    float sp = 0.0f, sr = 0.0f;
+    for (int c = 0; c < g.channels; ++c) {
+      const std::size_t k = c * g.plane + at;
+      sp += f.p1[k] * f.p1[k] + f.p2[k] * f.p2[k];
+      if (tgv) sr += f.r11[k] * f.r11[k] + f.r22[k] * f.r22[k] + 2.0f * (f.r12[k] * f.r12[k]);
+    }
+    const float ap = ball_scale(sp, radius), ar = ball_scale(sr, radius0);
+    for (int c = 0; c < g.channels; ++c) {
+      const std::size_t k = c * g.plane + at;
+      f.p1[k] *= ap;
+      f.p2[k] *= ap;
+      if (tgv) {
+        f.r11[k] *= ar;
+        f.r22[k] *= ar;
+        f.r12[k] *= ar;
+      }
+    }
+  } else {
+    for (int c = 0; c < g.channels; ++c) {
+      const std::size_t k = c * g.plane + at;
+      const float ap = ball_scale(f.p1[k] * f.p1[k] + f.p2[k] * f.p2[k], radius);
+      f.p1[k] *= ap;
+      f.p2[k] *= ap;
+      if (tgv) {
+        const float ar =
+            ball_scale(f.r11[k] * f.r11[k] + f.r22[k] * f.r22[k] + 2.0f * (f.r12[k] * f.r12[k]), radius0);
+        f.r11[k] *= ar;
+        f.r22[k] *= ar;
+        f.r12[k] *= ar;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Records, binary64 sums from the binary32 tilde point (cpp/src/primal_dual.hpp:446-501,
+// 791-895): the norms of the pixels, TGV's div2 r~ and its largest norm; G* of a field
+// (cpp/src/frames.cpp:428-487, model.cpp:74-111); the residual of the partial gap.
+
+template <bool TGV, int C, bool COUPLED>
+__global__ void __launch_bounds__(256) norms_kernel(const NormParams P) {
+  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y;
+  const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+  double first = 0.0, second = 0.0, most = 0.0;
+  if (i < rows && j < columns) {
+    const std::size_t at = static_cast<std::size_t>(i) * pitch + j;
+    double square = 0.0;
+    for (int c = 0; c < C; ++c) {
+      const std::size_t base = c * P.g.plane;
+      const double gamma = P.weight[c];
+      const double here = P.xt[base + at];
+      double gx = j + 1 < columns ? static_cast<double>(P.xt[base + at + 1]) - here : 0.0;
+      double gy = i + 1 < rows ? static_cast<double>(P.xt[base + at + pitch]) - here : 0.0;
+      if constexpr (TGV) {
+        gx = gx - static_cast<double>(P.tilde.w1[base + at]);
+        gy = gy - static_cast<double>(P.tilde.w2[base + at]);
+      }
+      square += (COUPLED ? gamma * gamma : 1.0) * (gx * gx + gy * gy);
+      if constexpr (!COUPLED) {
+        first += gamma * sqrt(square);
+        square = 0.0;
+      }
+    }
+    if constexpr (COUPLED) first = sqrt(square);
+    if constexpr (TGV) {
+      square = 0.0;
+      for (int c = 0; c < C; ++c) {
+        const std::size_t base = c * P.g.plane;
+        const double gamma = P.weight[c];
+        const float* w1 = P.tilde.w1 + base;
+        const float* w2 = P.tilde.w2 + base;
+        const bool last_c = j + 1 == columns, last_r = i + 1 == rows;
+        const double a1 = last_c ? 0.0 : w1[at], a2 = last_r ? 0.0 : w2[at];
+        const double b1 = last_r ? 0.0 : w1[at], b2 = last_c ? 0.0 : w2[at];
+        const double l1 = j > 0 ? w1[at - 1] : 0.0, l2 = j > 0 ? w2[at - 1] : 0.0;
+        const double u1 = i > 0 ? w1[at - pitch] : 0.0, u2 = i > 0 ? w2[at - pitch] : 0.0;
+        const double exx = a1 - l1, eyy = a2 - u2, exy = 0.5 * ((b1 - u1) + (b2 - l2));
+        square += (COUPLED ? gamma * gamma : 1.0) * (exx * exx + eyy * eyy + 2.0 * (exy * exy));
+        if constexpr (!COUPLED) {
+          second += gamma * sqrt(square);
+          square = 0.0;
+        }
+      }
+      if constexpr (COUPLED) second = sqrt(square);
+      square = 0.0;
+      for (int c = 0; c < C; ++c) {
+        const std::size_t base = c * P.g.plane;
+        const float* r11 = P.tilde.r11 + base;
+        const float* r22 = P.tilde.r22 + base;
+        const float* r12 = P.tilde.r12 + base;
+        double d1 = j + 1 < columns ? static_cast<double>(r11[at + 1]) - r11[at] : 0.0;
+        double d2 = j + 1 < columns ? static_cast<double>(r12[at + 1]) - r12[at] : 0.0;
+        if (i + 1 < rows) {
+          d1 += static_cast<double>(r12[at + pitch]) - r12[at];
+          d2 += static_cast<double>(r22[at + pitch]) - r22[at];
+        }
+        P.div2[(2 * c) * P.g.plane + at] = static_cast<float>(d1);
+        P.div2[(2 * c + 1) * P.g.plane + at] = static_cast<float>(d2);
+        square += d1 * d1 + d2 * d2;
+        if constexpr (!COUPLED) {
+          most = fmax(most, sqrt(square));
+          square = 0.0;
+        }
+      }
+      if constexpr (COUPLED) most = fmax(most, sqrt(square));
+    }
+  }
+  const double sum_first = cta_reduce<false>(first);
+  const double sum_second = cta_reduce<false>(second);
+  const double largest = cta_reduce<true>(most);
+  if (cta_leader()) {
+    const int count = gridDim.x * gridDim.y;
+    const int cta = cta_index();
+    P.partials[cta] = sum_first;
+    P.partials[count + cta] = sum_second;
+    P.partials[2 * count + cta] = largest;
+  }
+}
+
+// g*(s) of a coefficient (cpp/src/model.cpp:74-111, docs/math.md 4.1).
+__device__ __forceinline__ double conjugate_term(double s, int q, int k, bool flat, const Constants64& K) {
+  const double level = static_cast<double>(q);
+  const double step = K.step[k];
+  const double shift = k == 0 ? 1024.0 : 0.0;
+  const double low = ((level - 0.5) - K.slack) * step + shift;
+  const double high = ((level + 0.5) + K.slack) * step + shift;
+  double centre;
+  if (K.mmse && k != 0) {
+    const double size = (fabs(level) - K.shrink[k]) * step;
+    centre = q == 0 ? 0.0 : (q < 0 ? -size : size);
+  } else {
+    centre = level * step + shift;
+  }
+  const double m = flat ? K.flat_weight[k] : K.weight[k];
+  if (!K.costed) {
+    const double best = clamp_to(centre + s / m, low, high);
+    const double away = best - centre;
+    const double weighted = s * best - 0.5 * m * (away * away);
+    const double support = fmax(s * low, s * high);
+    return m > 0.0 ? weighted : support;
+  }
+  const double lambda = K.cost[k];
+  const double own_low = (level - 0.5) * step + shift;
+  const double own_high = (level + 0.5) * step + shift;
+  const double free = centre + s / m;
+  const double upward = clamp_to(centre + (s - lambda) / m, own_high, high);
+  const double downward = clamp_to(centre + (s + lambda) / m, low, own_low);
+  const double within = free < own_low ? downward : free;
+  const double weighted = free > own_high ? upward : within;
+  const double lower_end = s < -lambda ? low : own_low;
+  const double upper_end = s > lambda ? high : own_high;
+  const double flat_best = s > 0.0 ? upper_end : lower_end;
+  const double best = m > 0.0 ? weighted : flat_best;
+  const double away = best - centre;
+  const double beyond = fmax(fmax(best - own_high, own_low - best), 0.0);
+  return s * best - 0.5 * m * (away * away) - lambda * beyond;
+}
+
+template <int CR, int CC>
+__global__ void __launch_bounds__(256) conjugate_kernel(const ConjugateParams P) {
+  __shared__ double tile[kWarps][4][72];
+  constexpr int BH = 8 * CR, BW = 8 * CC;
+  const int lane = threadIdx.x, b = lane >> 3, m = lane & 7;
+  const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+  const int vbx = blockIdx.x * 4 + b;
+  const int vby = blockIdx.y * kWarps + threadIdx.y;
+  const bool active = vbx * BW < columns && vby * BH < rows;
+  const bool in_blocks = active && vby < P.component.block_rows && vbx < P.component.block_columns;
+  const int j0 = vbx * BW + m * CC, i0 = vby * BH;
+  // xi = gamma div q at the lane's samples, q = scale (q1, q2).
+  auto q_at = [&](const float* f, int i, int j) -> double { return P.scale * static_cast<double>(f[static_cast<std::size_t>(i) * pitch + j]); };
+  double xi[BH][CC];
+  double sums[8], means[8];
+  double total = 0.0;
+#pragma unroll
+  for (int r = 0; r < BH; ++r) {
+#pragma unroll
+    for (int c = 0; c < CC; ++c) {
+      const int i = i0 + r, j = j0 + c;
+      double value = 0.0;
+      if (active) {
+        const double dy = (i + 1 < rows ? q_at(P.q2, i, j) : 0.0) - (i > 0 ? q_at(P.q2, i - 1, j) : 0.0);
+        const double dx = (j + 1 < columns ? q_at(P.q1, i, j) : 0.0) - (j > 0 ? q_at(P.q1, i, j - 1) : 0.0);
+        value = P.gamma * (dy + dx);
+      }
+      xi[r][c] = value;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    double sum = 0.0;
+#pragma unroll
+    for (int c = 0; c < CC; ++c) {
+      double column = xi[CR * r][c];
+#pragma unroll
+      for (int a = 1; a < CR; ++a) column += xi[CR * r + a][c];
+      sum = c == 0 ? column : sum + column;
+    }
+    sums[r] = sum;
+    means[r] = sum / static_cast<double>(CR * CC);
+  }
+  if (P.free && active) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+#pragma unroll
+      for (int a = 0; a < CR; ++a) {
+#pragma unroll
+        for (int c = 0; c < CC; ++c) {
+          const double s = xi[CR * r + a][c];
+          total += in_blocks ? P.radius * fabs(s - means[r]) : 128.0 * s + P.radius * fabs(s);
+        }
+      }
+    }
+  }
+  // The DCT of the cell sums, and g* of each coefficient of the lane's row.
+  double col[8], row[8], coef[8];
+  forward8(sums, col);
+  double* t = tile[threadIdx.y][b];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) t[k * 9 + m] = col[k];
+  __syncwarp();
+#pragma unroll
+  for (int u = 0; u < 8; ++u) row[u] = t[m * 9 + u];
+  forward8(row, coef);
+  if (in_blocks) {
+    const std::size_t block = static_cast<std::size_t>(vby) * P.component.block_columns + vbx;
+    const bool flat = P.component.flat[block] != 0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = m * 8 + u;
+      total += conjugate_term(coef[u], P.component.levels[block * 64 + k], k, flat, *P.component.constants);
+    }
+  }
+  cta_sum(total, P.partials);
+}
+
+__global__ void __launch_bounds__(256) residual_kernel(const ResidualParams P) {
+  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y;
+  double value = 0.0;
+  if (i < P.g.rows && j < P.g.columns) {
+    const std::size_t at = static_cast<std::size_t>(i) * P.g.pitch + j;
+    const double a = static_cast<double>(P.p1[at]) + 1.0 * P.d1[at];
+    const double b = static_cast<double>(P.p2[at]) + 1.0 * P.d2[at];
+    value = sqrt(a * a + b * b);
+  }
+  cta_sum(value, P.partials);
+}
+
+__global__ void widen_kernel(const float* from, double* to, Geometry g) {
+  const std::size_t n = static_cast<std::size_t>(g.rows) * g.columns * g.channels;
+  for (std::size_t k = blockIdx.x * 256ull + threadIdx.x; k < n; k += static_cast<std::size_t>(gridDim.x) * 256) {
+    const std::size_t c = k / (static_cast<std::size_t>(g.rows) * g.columns);
+    const std::size_t rest = k % (static_cast<std::size_t>(g.rows) * g.columns);
+    const std::size_t i = rest / g.columns, j = rest % g.columns;
+    to[k] = from[c * g.plane + i * g.pitch + j];
+  }
+}
+
+__global__ void narrow_kernel(const double* from, float* to, Geometry g) {
+  const std::size_t n = static_cast<std::size_t>(g.rows) * g.columns * g.channels;
+  for (std::size_t k = blockIdx.x * 256ull + threadIdx.x; k < n; k += static_cast<std::size_t>(gridDim.x) * 256) {
+    const std::size_t c = k / (static_cast<std::size_t>(g.rows) * g.columns);
+    const std::size_t rest = k % (static_cast<std::size_t>(g.rows) * g.columns);
+    const std::size_t i = rest / g.columns, j = rest % g.columns;
+    to[c * g.plane + i * g.pitch + j] = static_cast<float>(from[k]);
+  }
+}
+
+dim3 pixel_grid(const Geometry& g) { return dim3((g.columns + 31) / 32, (g.rows + 7) / 8, 1); }
+
+dim3 block_grid(const Geometry& g, const ComponentDevice& c) {
+  const int vbc = (g.columns + 8 * c.cell_columns - 1) / (8 * c.cell_columns);
+  const int vbr = (g.rows + 8 * c.cell_rows - 1) / (8 * c.cell_rows);
+  return dim3((vbc + 3) / 4, (vbr + kWarps - 1) / kWarps, 1);
+}
+
+template <template <int, int> class Launch, typename... A>
+cudaError_t by_cells(int cr, int cc, A&&... args) {
+#define URB_CELL(R, C) \
+  if (cr == R && cc == C) return Launch<R, C>::run(args...);
+  URB_CELL(1, 1) URB_CELL(1, 2) URB_CELL(2, 1) URB_CELL(2, 2) URB_CELL(1, 3) URB_CELL(3, 1) URB_CELL(3, 3)
+  URB_CELL(1, 4) URB_CELL(4, 1) URB_CELL(2, 4) URB_CELL(4, 2) URB_CELL(4, 4) URB_CELL(2, 3) URB_CELL(3, 2)
+  URB_CELL(3, 4) URB_CELL(4, 3)
+#undef URB_CELL
+  return cudaErrorInvalidValue;
+}
+
+template <int CR, int CC>
+struct PrimalLaunch {
+  static cudaError_t run(const PrimalParams& p, bool keep, cudaStream_t s) {
+    const dim3 grid = block_grid(p.g, p.component);
+    if (keep) {
+      primal_kernel<CR, CC, true><<<grid, dim3(32, kWarps), 0, s>>>(p);
+    } else {
+      primal_kernel<CR, CC, false><<<grid, dim3(32, kWarps), 0, s>>>(p);
+    }
+    return cudaGetLastError();
+  }
+};
+
+template <int CR, int CC>
+struct CanvasLaunch {
+  static cudaError_t run(const CanvasParams& p, cudaStream_t s) {
+    canvas_kernel<CR, CC><<<block_grid(p.g, p.component), dim3(32, kWarps), 0, s>>>(p);
+    return cudaGetLastError();
+  }
+};
+
+template <int CR, int CC>
+struct ConjugateLaunch {
+  static cudaError_t run(const ConjugateParams& p, cudaStream_t s) {
+    conjugate_kernel<CR, CC><<<block_grid(p.g, p.component), dim3(32, kWarps), 0, s>>>(p);
+    return cudaGetLastError();
+  }
+};
+
+template <bool TGV, int C, bool COUPLED>
+cudaError_t dual_keep(const DualParams& p, bool keep, cudaStream_t s) {
+  if (keep) {
+    dual_kernel<TGV, C, COUPLED, true><<<pixel_grid(p.g), dim3(32, 8), 0, s>>>(p);
+  } else {
+    dual_kernel<TGV, C, COUPLED, false><<<pixel_grid(p.g), dim3(32, 8), 0, s>>>(p);
+  }
+  return cudaGetLastError();
+}
+
+template <bool TGV>
+cudaError_t dual_channels(const DualParams& p, bool coupled, bool keep, cudaStream_t s) {
+  switch (p.g.channels) {
+    case 1: return dual_keep<TGV, 1, false>(p, keep, s);
+    case 2: return coupled ? dual_keep<TGV, 2, true>(p, keep, s) : dual_keep<TGV, 2, false>(p, keep, s);
+    case 3: return coupled ? dual_keep<TGV, 3, true>(p, keep, s) : dual_keep<TGV, 3, false>(p, keep, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <bool TGV>
+cudaError_t norms_channels(const NormParams& p, bool coupled, cudaStream_t s) {
+  const dim3 grid = pixel_grid(p.g);
+  switch (p.g.channels) {
+    case 1: norms_kernel<TGV, 1, false><<<grid, dim3(32, 8), 0, s>>>(p); break;
+    case 2:
+      if (coupled) norms_kernel<TGV, 2, true><<<grid, dim3(32, 8), 0, s>>>(p);
+      else norms_kernel<TGV, 2, false><<<grid, dim3(32, 8), 0, s>>>(p);
+      break;
+    case 3:
+      if (coupled) norms_kernel<TGV, 3, true><<<grid, dim3(32, 8), 0, s>>>(p);
+      else norms_kernel<TGV, 3, false><<<grid, dim3(32, 8), 0, s>>>(p);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int dual_grid_blocks(const Geometry& g) {
+  const dim3 d = pixel_grid(g);
+  return static_cast<int>(d.x * d.y);
+}
+int norms_grid_blocks(const Geometry& g) { return dual_grid_blocks(g); }
+int primal_grid_blocks(const Geometry& g, const ComponentDevice& c) {
+  const dim3 d = block_grid(g, c);
+  return static_cast<int>(d.x * d.y);
+}
+int conjugate_grid_blocks(const Geometry& g, const ComponentDevice& c) { return primal_grid_blocks(g, c); }
+int start_grid_blocks(const ComponentDevice& c) { return (c.block_rows * c.block_columns * 8 + 255) / 256; }
+
+cudaError_t launch_dual(const DualParams& p, bool tgv, bool coupled, bool keep, cudaStream_t stream) {
+  return tgv ? dual_channels<true>(p, coupled, keep, stream) : dual_channels<false>(p, coupled, keep, stream);
+}
+
+cudaError_t launch_primal(const PrimalParams& p, bool keep, cudaStream_t stream) {
+  return by_cells<PrimalLaunch>(p.component.cell_rows, p.component.cell_columns, p, keep, stream);
+}
+
+cudaError_t launch_start_coefficients(const StartParams& p, cudaStream_t stream) {
+  const int blocks = start_grid_blocks(p.component);
+  if (blocks == 0) return cudaSuccess;
+  start_kernel<<<blocks, 256, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_canvas(const CanvasParams& p, cudaStream_t stream) {
+  return by_cells<CanvasLaunch>(p.component.cell_rows, p.component.cell_columns, p, stream);
+}
+
+cudaError_t launch_gradient(const float* x, float* w1, float* w2, const Geometry& g, cudaStream_t stream) {
+  gradient_kernel<<<pixel_grid(g), dim3(32, 8), 0, stream>>>(x, w1, w2, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_project(Fields f, const Geometry& g, bool tgv, bool coupled, float radius, float radius0,
+                           cudaStream_t stream) {
+  project_kernel<<<pixel_grid(g), dim3(32, 8), 0, stream>>>(f, g, tgv ? 1 : 0, coupled ? 1 : 0, radius, radius0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_norms(const NormParams& p, bool tgv, bool coupled, cudaStream_t stream) {
+  return tgv ? norms_channels<true>(p, coupled, stream) : norms_channels<false>(p, coupled, stream);
+}
+
+cudaError_t launch_conjugate(const ConjugateParams& p, cudaStream_t stream) {
+  return by_cells<ConjugateLaunch>(p.component.cell_rows, p.component.cell_columns, p, stream);
+}
+
+cudaError_t launch_residual(const ResidualParams& p, cudaStream_t stream) {
+  residual_kernel<<<pixel_grid(p.g), dim3(32, 8), 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_widen(const float* from, double* to, const Geometry& g, cudaStream_t stream) {
+  widen_kernel<<<1184, 256, 0, stream>>>(from, to, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_narrow(const double* from, float* to, const Geometry& g, cudaStream_t stream) {
+  narrow_kernel<<<1184, 256, 0, stream>>>(from, to, g);
+  return cudaGetLastError();
+}
+
+}  // namespace urb

@@ -1,0 +1,186 @@
+// The device side of the solver: plain structures of device pointers and constants that the
+// host driver fills, and the launchers of the kernels (kernels.cu). The canvas fields are
+// binary32 planes in HBM, channel after channel, each rows x pitch with the pitch a multiple
+// of 32 samples (128-byte rows); the levels are int16 in block order, 64 to a block in
+// natural order, as the file gives them.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace urb {
+
+constexpr int kMaxChannels = 3;
+
+// The per-frequency factors of a component's proximal map in binary32, for one step tau
+// (docs/math.md 4.1, 4.4; cpp/src/model.cpp:483-497): t = (tau / n_c) m, r = 1 / (1 + t),
+// and with a slack's cost h = (tau / n_c) lambda r, in a block that is not flat and in one
+// that is; the steps Q; delta / Q of the MMSE centres.
+struct ProxFactors {
+  float step[64];
+  float t[64];
+  float r[64];
+  float t_flat[64];
+  float r_flat[64];
+  float h[64];
+  float h_flat[64];
+  float shrink[64];
+  float slack;
+  int mmse;
+  int costed;
+  int pad;
+};
+
+// The same constants in binary64 for the records and the start (G, G*, the centres).
+struct Constants64 {
+  double step[64];
+  double weight[64];
+  double flat_weight[64];
+  double shrink[64];
+  double cost[64];
+  double slack;
+  int mmse;
+  int costed;
+};
+
+struct ComponentDevice {
+  const std::int16_t* levels = nullptr;  // [by][bx][64]
+  const std::uint8_t* flat = nullptr;    // [by][bx]
+  int block_rows = 0;
+  int block_columns = 0;
+  int cell_rows = 1;
+  int cell_columns = 1;
+  const ProxFactors* factors = nullptr;
+  const Constants64* constants = nullptr;
+  float* zeta = nullptr;  // kept coefficients, [by][bx][64]
+};
+
+struct Geometry {
+  int rows = 0;
+  int columns = 0;
+  int pitch = 0;
+  int channels = 1;
+  std::size_t plane = 0;  // rows * pitch
+};
+
+// A state of the method (docs/math.md 5): x, p and for TGV w and r, each channels planes.
+struct Fields {
+  float* x = nullptr;
+  float* p1 = nullptr;
+  float* p2 = nullptr;
+  float* w1 = nullptr;
+  float* w2 = nullptr;
+  float* r11 = nullptr;
+  float* r22 = nullptr;
+  float* r12 = nullptr;
+};
+
+// The dual step of iteration n and the relaxation (docs/math.md 5): from x~_n and the state
+// s_{n-1} (in) to s_n (out); with keep, the tilde point's p~, r~ and w~ into `tilde`.
+struct DualParams {
+  Geometry g;
+  const float* xt = nullptr;
+  Fields in;
+  Fields out;
+  Fields tilde;
+  float sigma[kMaxChannels] = {};  // sigma gamma_c
+  float tau[kMaxChannels] = {};    // tau gamma_c
+  float rho = 1.9f;
+  float rest = -0.9f;
+  float radius = 1.0f;   // alpha of TV, alpha1 of TGV
+  float radius0 = 2.0f;  // alpha0
+};
+
+// The primal step of iteration n+1 for one channel: v = x + tau gamma div p and its proximal
+// map x~ (docs/math.md 4.4, 5); with keep, the coefficients zeta, v, and each CTA's sum of
+// the data term's terms at zeta.
+struct PrimalParams {
+  Geometry g;
+  ComponentDevice component;
+  const float* x = nullptr;
+  const float* p1 = nullptr;
+  const float* p2 = nullptr;
+  float* xt = nullptr;
+  float* v = nullptr;
+  double* partials = nullptr;
+  float descent = 0.0f;  // tau gamma_c
+};
+
+// The records (docs/math.md 6): sums over the canvas in binary64 from the binary32 tilde
+// point, each CTA's into `partials`.
+struct NormParams {
+  Geometry g;
+  const float* xt = nullptr;
+  Fields tilde;          // p~, w~, r~
+  float* div2 = nullptr;  // div_2 r~ of each channel: 2 planes per channel
+  double weight[kMaxChannels] = {};
+  double* partials = nullptr;  // 3 per CTA: first-order norms, second-order norms, max |div_2 r~|
+};
+
+struct ConjugateParams {
+  Geometry g;
+  ComponentDevice component;
+  const float* q1 = nullptr;  // the field whose divergence xi is: p~, or div_2 r~ scaled
+  const float* q2 = nullptr;
+  double scale = 1.0;   // q = scale * (q1, q2): 1 for p~, -theta for div_2 r~
+  double gamma = 1.0;   // xi = gamma div q
+  double radius = 255.0;  // R of the free samples (docs/math.md 6.6)
+  int free = 0;
+  double* partials = nullptr;  // 1 per CTA
+};
+
+struct ResidualParams {
+  Geometry g;
+  const float* p1 = nullptr;
+  const float* p2 = nullptr;
+  const float* d1 = nullptr;
+  const float* d2 = nullptr;
+  double* partials = nullptr;
+};
+
+// The FP64 canvas of coefficients (docs/math.md 1.3): mode 0, the start, their inverse DCT
+// spread over the cells and `beyond` past the blocks; mode 1, a result, v plus the change of
+// each cell (its inverse DCT less the mean of v), and v past the blocks (n_c = 1: the inverse
+// DCT itself).
+struct CanvasParams {
+  Geometry g;
+  ComponentDevice component;
+  const double* coefficients = nullptr;  // [by][bx][64]
+  const float* v = nullptr;              // mode 1
+  double* canvas = nullptr;              // rows x columns (unpadded), this channel's
+  float* x = nullptr;                    // mode 0: the binary32 start, pitched
+  double beyond = 128.0;
+  int mode = 0;
+};
+
+// The start's coefficients: the centres, or given ones, clipped to their intervals; with
+// sums of the data term's terms there into `partials`.
+struct StartParams {
+  ComponentDevice component;
+  const double* given = nullptr;  // null: the centres
+  double* coefficients = nullptr;
+  double* partials = nullptr;
+};
+
+int dual_grid_blocks(const Geometry& g);
+int primal_grid_blocks(const Geometry& g, const ComponentDevice& c);
+int conjugate_grid_blocks(const Geometry& g, const ComponentDevice& c);
+int norms_grid_blocks(const Geometry& g);
+int start_grid_blocks(const ComponentDevice& c);
+
+cudaError_t launch_dual(const DualParams& p, bool tgv, bool coupled, bool keep, cudaStream_t stream);
+cudaError_t launch_primal(const PrimalParams& p, bool keep, cudaStream_t stream);
+cudaError_t launch_start_coefficients(const StartParams& p, cudaStream_t stream);
+cudaError_t launch_canvas(const CanvasParams& p, cudaStream_t stream);
+cudaError_t launch_gradient(const float* x, float* w1, float* w2, const Geometry& g, cudaStream_t stream);
+cudaError_t launch_project(Fields f, const Geometry& g, bool tgv, bool coupled, float radius, float radius0,
+                           cudaStream_t stream);
+cudaError_t launch_norms(const NormParams& p, bool tgv, bool coupled, cudaStream_t stream);
+cudaError_t launch_conjugate(const ConjugateParams& p, cudaStream_t stream);
+cudaError_t launch_residual(const ResidualParams& p, cudaStream_t stream);
+cudaError_t launch_widen(const float* from, double* to, const Geometry& g, cudaStream_t stream);
+cudaError_t launch_narrow(const double* from, float* to, const Geometry& g, cudaStream_t stream);
+
+}  // namespace urb

@@ -1,0 +1,618 @@
+// The device solve. See solver.hpp.
+#include "solver.hpp"
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+
+namespace urb {
+
+namespace {
+
+constexpr double kNaN = std::numeric_limits<double>::quiet_NaN();
+
+std::string describe(cudaError_t error) {
+  return std::string(cudaGetErrorName(error)) + ": " + cudaGetErrorString(error);
+}
+
+}  // namespace
+
+struct Solver::Impl {
+  const Frame& frame;
+  cudaStream_t stream;
+  Geometry g;
+  std::vector<void*> owned;
+  std::size_t bytes = 0;
+  cudaError_t error = cudaSuccess;
+
+  std::vector<ComponentDevice> components;
+  std::vector<double*> coefficients;  // binary64, per component
+  std::vector<ProxFactors*> factors;
+  Fields state[2];
+  Fields tilde;
+  float* xt = nullptr;
+  float* v = nullptr;
+  float* div2 = nullptr;
+  double* canvas = nullptr;
+  double* partials = nullptr;        // record reductions
+  double* value_partials = nullptr;  // the data term of the last kept primal step, per component
+  std::size_t partial_count = 0;
+  std::vector<int> value_counts;
+  std::vector<int> value_written;
+  bool tgv = false;
+  int current = 0;  // which state holds s_n
+  Plan plan;
+  bool planned = false;
+  std::vector<double> host_partials;
+
+  Impl(const Frame& f, cudaStream_t s) : frame(f), stream(s) {}
+
+  ~Impl() {
+    for (void* p : owned) cudaFreeAsync(p, stream);
+    cudaStreamSynchronize(stream);
+  }
+
+  template <typename T>
+  T* allocate(std::size_t count) {
+    if (error != cudaSuccess) return nullptr;
+    void* p = nullptr;
+    const std::size_t size = std::max<std::size_t>(count * sizeof(T), 16);
+    error = cudaMallocAsync(&p, size, stream);
+    if (error != cudaSuccess) return nullptr;
+    owned.push_back(p);
+    bytes += size;
+    return static_cast<T*>(p);
+  }
+
+  template <typename T>
+  T* upload(const T* from, std::size_t count) {
+    T* p = allocate<T>(count);
+    if (p != nullptr && count > 0) error = cudaMemcpyAsync(p, from, count * sizeof(T), cudaMemcpyHostToDevice, stream);
+    return p;
+  }
+
+  Fields fields(bool with_tgv) {
+    const std::size_t n = g.plane * g.channels;
+    Fields f;
+    f.x = allocate<float>(n);
+    f.p1 = allocate<float>(n);
+    f.p2 = allocate<float>(n);
+    if (with_tgv) {
+      f.w1 = allocate<float>(n);
+      f.w2 = allocate<float>(n);
+      f.r11 = allocate<float>(n);
+      f.r22 = allocate<float>(n);
+      f.r12 = allocate<float>(n);
+    }
+    return f;
+  }
+
+  bool check(Failure& failure, const char* where) {
+    if (error == cudaSuccess) error = cudaGetLastError();
+    if (error == cudaSuccess) return true;
+    failure.status = kInternal;
+    failure.message = std::string("the device failed in ") + where + ": " + describe(error);
+    return false;
+  }
+
+  // Device copies of the model: levels, flat blocks, binary64 constants.
+  void setup(bool with_tgv) {
+    tgv = with_tgv;
+    const std::size_t n = g.plane * g.channels;
+    for (const Component& c : frame.components) {
+      ComponentDevice d;
+      d.block_rows = static_cast<int>(c.block_rows);
+      d.block_columns = static_cast<int>(c.block_columns);
+      d.cell_rows = static_cast<int>(c.cell_rows);
+      d.cell_columns = static_cast<int>(c.cell_columns);
+      d.levels = upload(c.levels.data(), c.levels.size());
+      d.flat = upload(c.flat.data(), c.flat.size());
+      Constants64 k{};
+      for (int i = 0; i < 64; ++i) {
+        k.step[i] = c.steps[i];
+        k.weight[i] = c.weights[i];
+        k.flat_weight[i] = c.flat_weights[i];
+        k.shrink[i] = c.shrink[i];
+        k.cost[i] = c.costs[i];
+      }
+      k.slack = c.slack;
+      k.mmse = c.mmse ? 1 : 0;
+      k.costed = c.costed ? 1 : 0;
+      d.constants = upload(&k, 1);
+      ProxFactors* f = allocate<ProxFactors>(1);
+      factors.push_back(f);
+      d.factors = f;
+      d.zeta = allocate<float>(c.coefficient_count());
+      coefficients.push_back(allocate<double>(c.coefficient_count()));
+      components.push_back(d);
+    }
+    state[0] = fields(with_tgv);
+    state[1] = fields(with_tgv);
+    tilde = fields(with_tgv);
+    xt = allocate<float>(n);
+    v = allocate<float>(n);
+    if (with_tgv) div2 = allocate<float>(2 * n);
+    canvas = allocate<double>(static_cast<std::size_t>(g.channels) * g.rows * g.columns);
+    std::size_t most = 3u * norms_grid_blocks(g);
+    for (const ComponentDevice& d : components) {
+      most = std::max<std::size_t>(most, conjugate_grid_blocks(g, d));
+      most = std::max<std::size_t>(most, start_grid_blocks(d));
+      const int count = std::max(primal_grid_blocks(g, d), start_grid_blocks(d));
+      value_counts.push_back(count);
+      value_written.push_back(0);
+    }
+    partial_count = most;
+    partials = allocate<double>(most);
+    std::size_t values = 0;
+    for (int count : value_counts) values += count;
+    value_partials = allocate<double>(values);
+    host_partials.resize(std::max(most, values));
+  }
+
+  double* value_slot(std::size_t c) {
+    std::size_t offset = 0;
+    for (std::size_t k = 0; k < c; ++k) offset += value_counts[k];
+    return value_partials + offset;
+  }
+
+  // The binary32 factors of each component's proximal map at the plan's tau.
+  void set_factors(const Plan& p) {
+    for (std::size_t c = 0; c < frame.components.size(); ++c) {
+      const Component& comp = frame.components[c];
+      ProxFactors f{};
+      const double step = p.tau / static_cast<double>(comp.cells());
+      for (int k = 0; k < 64; ++k) {
+        f.step[k] = static_cast<float>(comp.steps[k]);
+        const double t = step * comp.weights[k];
+        const double r = 1.0 / (1.0 + t);
+        const double tf = step * comp.flat_weights[k];
+        const double rf = 1.0 / (1.0 + tf);
+        f.t[k] = static_cast<float>(t);
+        f.r[k] = static_cast<float>(r);
+        f.t_flat[k] = static_cast<float>(tf);
+        f.r_flat[k] = static_cast<float>(rf);
+        f.h[k] = static_cast<float>(step * comp.costs[k] * r);
+        f.h_flat[k] = static_cast<float>(step * comp.costs[k] * rf);
+        f.shrink[k] = static_cast<float>(comp.shrink[k]);
+      }
+      f.slack = static_cast<float>(comp.slack);
+      f.mmse = comp.mmse ? 1 : 0;
+      f.costed = comp.costed ? 1 : 0;
+      if (error == cudaSuccess) error = cudaMemcpyAsync(factors[c], &f, sizeof(f), cudaMemcpyHostToDevice, stream);
+      // The pageable source must outlive the copy.
+      if (error == cudaSuccess) error = cudaStreamSynchronize(stream);
+    }
+  }
+
+  // The sum of n doubles of the device in index order.
+  double sum_of(const double* device, std::size_t n, std::size_t offset = 0) {
+    if (error != cudaSuccess || n == 0) return 0.0;
+    error = cudaMemcpyAsync(host_partials.data(), device + offset, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    if (error == cudaSuccess) error = cudaStreamSynchronize(stream);
+    double total = 0.0;
+    for (std::size_t k = 0; k < n; ++k) total += host_partials[k];
+    return total;
+  }
+
+  double max_of(const double* device, std::size_t n, std::size_t offset) {
+    if (error != cudaSuccess || n == 0) return 0.0;
+    error = cudaMemcpyAsync(host_partials.data(), device + offset, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    if (error == cudaSuccess) error = cudaStreamSynchronize(stream);
+    double most = 0.0;
+    for (std::size_t k = 0; k < n; ++k) most = std::fmax(most, host_partials[k]);
+    return most;
+  }
+
+  double data_value() {
+    double total = 0.0;
+    for (std::size_t c = 0; c < components.size(); ++c) total += sum_of(value_slot(c), value_written[c]);
+    return total;
+  }
+
+  // The start (cpp/src/primal_dual.hpp:401-432): x from the clipped centres (or the given
+  // coefficients), 128 past the blocks; w = grad x; the duals 0 or given, projected. The
+  // start is the first tilde point.
+  void start(const Start* given, bool for_solver) {
+    for (std::size_t c = 0; c < components.size(); ++c) {
+      StartParams sp;
+      sp.component = components[c];
+      sp.coefficients = coefficients[c];
+      sp.partials = value_slot(c);
+      const double* given_coefficients = nullptr;
+      if (given != nullptr && !given->coefficients.empty()) {
+        given_coefficients = upload(given->coefficients[c].data(), given->coefficients[c].size());
+      }
+      sp.given = given_coefficients;
+      if (error == cudaSuccess) error = launch_start_coefficients(sp, stream);
+      value_written[c] = start_grid_blocks(components[c]);
+      CanvasParams cp;
+      cp.g = g;
+      cp.component = components[c];
+      cp.coefficients = coefficients[c];
+      cp.canvas = canvas + static_cast<std::size_t>(c) * g.rows * g.columns;
+      cp.x = for_solver ? state[0].x + c * g.plane : nullptr;
+      cp.beyond = 128.0;
+      cp.mode = 0;
+      if (error == cudaSuccess) error = launch_canvas(cp, stream);
+    }
+    if (!for_solver) return;
+    const std::size_t n = g.plane * g.channels;
+    auto put = [&](float* to, const std::vector<double>& from, std::size_t entries, std::size_t entry) {
+      // channel-major host fields of `entries` planes each -> the pitched plane `entry`.
+      std::vector<float> staged(n, 0.0f);
+      for (int c = 0; c < g.channels; ++c) {
+        for (int i = 0; i < g.rows; ++i) {
+          for (int j = 0; j < g.columns; ++j) {
+            staged[c * g.plane + static_cast<std::size_t>(i) * g.pitch + j] = static_cast<float>(
+                from[((c * entries + entry) * g.rows + i) * static_cast<std::size_t>(g.columns) + j]);
+          }
+        }
+      }
+      if (error == cudaSuccess) error = cudaMemcpyAsync(to, staged.data(), n * sizeof(float), cudaMemcpyHostToDevice, stream);
+      if (error == cudaSuccess) error = cudaStreamSynchronize(stream);
+    };
+    Fields& s = state[0];
+    const bool given_p = given != nullptr && !given->p.empty();
+    const bool given_w = given != nullptr && !given->w.empty();
+    const bool given_r = given != nullptr && !given->r.empty();
+    if (given_p) {
+      put(s.p1, given->p, 2, 0);
+      put(s.p2, given->p, 2, 1);
+    } else {
+      if (error == cudaSuccess) error = cudaMemsetAsync(s.p1, 0, n * sizeof(float), stream);
+      if (error == cudaSuccess) error = cudaMemsetAsync(s.p2, 0, n * sizeof(float), stream);
+    }
+    if (tgv) {
+      if (given_w) {
+        put(s.w1, given->w, 2, 0);
+        put(s.w2, given->w, 2, 1);
+      } else if (error == cudaSuccess) {
+        error = launch_gradient(s.x, s.w1, s.w2, g, stream);
+      }
+      if (given_r) {
+        put(s.r11, given->r, 3, 0);
+        put(s.r22, given->r, 3, 1);
+        put(s.r12, given->r, 3, 2);
+      } else {
+        for (float* f : {s.r11, s.r22, s.r12}) {
+          if (error == cudaSuccess) error = cudaMemsetAsync(f, 0, n * sizeof(float), stream);
+        }
+      }
+    }
+    if ((given_p || given_r) && error == cudaSuccess) {
+      error = launch_project(s, g, tgv, plan.coupled, static_cast<float>(tgv ? plan.alpha1 : plan.alpha),
+                             static_cast<float>(plan.alpha0), stream);
+    }
+    // The start is the first tilde point.
+    auto copy = [&](float* to, const float* from) {
+      if (error == cudaSuccess && to != nullptr) {
+        error = cudaMemcpyAsync(to, from, n * sizeof(float), cudaMemcpyDeviceToDevice, stream);
+      }
+    };
+    copy(xt, s.x);
+    copy(tilde.p1, s.p1);
+    copy(tilde.p2, s.p2);
+    if (tgv) {
+      copy(tilde.w1, s.w1);
+      copy(tilde.w2, s.w2);
+      copy(tilde.r11, s.r11);
+      copy(tilde.r22, s.r22);
+      copy(tilde.r12, s.r12);
+    }
+    current = 0;
+  }
+
+  void primal(bool keep) {
+    const Fields& s = state[current];
+    for (std::size_t c = 0; c < components.size(); ++c) {
+      PrimalParams pp;
+      pp.g = g;
+      pp.component = components[c];
+      const std::size_t base = c * g.plane;
+      pp.x = s.x + base;
+      pp.p1 = s.p1 + base;
+      pp.p2 = s.p2 + base;
+      pp.xt = xt + base;
+      pp.v = v + base;
+      pp.partials = value_slot(c);
+      pp.descent = static_cast<float>(plan.tau * plan.channel_weights[c]);
+      if (error == cudaSuccess) error = launch_primal(pp, keep, stream);
+      if (keep) value_written[c] = primal_grid_blocks(g, components[c]);
+    }
+  }
+
+  void dual(bool keep) {
+    DualParams dp;
+    dp.g = g;
+    dp.xt = xt;
+    dp.in = state[current];
+    dp.out = state[1 - current];
+    dp.tilde = tilde;
+    for (int c = 0; c < g.channels; ++c) {
+      dp.sigma[c] = static_cast<float>(plan.sigma * plan.channel_weights[c]);
+      dp.tau[c] = static_cast<float>(plan.tau * plan.channel_weights[c]);
+    }
+    dp.rho = static_cast<float>(plan.relaxation);
+    dp.rest = static_cast<float>(1.0 - plan.relaxation);
+    dp.radius = static_cast<float>(tgv ? plan.alpha1 : plan.alpha);
+    dp.radius0 = static_cast<float>(plan.alpha0);
+    if (error == cudaSuccess) error = launch_dual(dp, tgv, plan.coupled, keep, stream);
+    current = 1 - current;
+  }
+
+  // G* of channel c at xi = gamma div(scale q) (cpp/src/frames.cpp:428-493).
+  double conjugate(std::size_t c, const float* q1, const float* q2, double scale) {
+    ConjugateParams cp;
+    cp.g = g;
+    cp.component = components[c];
+    cp.q1 = q1;
+    cp.q2 = q2;
+    cp.scale = scale;
+    cp.gamma = plan.channel_weights[c];
+    cp.radius = plan.free_radius;
+    cp.free = frame.components[c].free ? 1 : 0;
+    cp.partials = partials;
+    if (error == cudaSuccess) error = launch_conjugate(cp, stream);
+    return sum_of(partials, conjugate_grid_blocks(g, components[c]));
+  }
+
+  // The record of the tilde point (cpp/src/primal_dual.hpp:446-501).
+  Record record(std::uint64_t iteration) {
+    Record r;
+    r.iteration = iteration;
+    r.scaling = kNaN;
+    r.partial_gap = kNaN;
+    const double data = data_value();
+    NormParams np;
+    np.g = g;
+    np.xt = xt;
+    np.tilde = tilde;
+    np.div2 = div2;
+    for (int c = 0; c < g.channels; ++c) np.weight[c] = plan.channel_weights[c];
+    np.partials = partials;
+    if (error == cudaSuccess) error = launch_norms(np, tgv, plan.coupled, stream);
+    const std::size_t count = norms_grid_blocks(g);
+    const double first = sum_of(partials, count, 0);
+    if (!tgv) {
+      r.primal = plan.alpha * first + data;
+      double conjugates = 0.0;
+      for (std::size_t c = 0; c < components.size(); ++c) {
+        conjugates += conjugate(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0);
+      }
+      r.dual = -conjugates;
+      return r;
+    }
+    const double second = sum_of(partials, count, count);
+    const double most = max_of(partials, count, 2 * count);
+    r.primal = (plan.alpha1 * first + plan.alpha0 * second) + data;
+    const double theta = most > plan.alpha1 ? plan.alpha1 / most : 1.0;
+    r.scaling = theta;
+    double conjugates = 0.0;
+    for (std::size_t c = 0; c < components.size(); ++c) {
+      const std::size_t base = 2 * c * g.plane;
+      conjugates += conjugate(c, div2 + base, div2 + base + g.plane, -theta);
+    }
+    r.dual = -conjugates;
+    if (plan.partial_radius) {
+      double partial = 0.0, residual = 0.0;
+      for (std::size_t c = 0; c < components.size(); ++c) {
+        partial += conjugate(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0);
+        ResidualParams rp;
+        rp.g = g;
+        rp.p1 = tilde.p1 + c * g.plane;
+        rp.p2 = tilde.p2 + c * g.plane;
+        rp.d1 = div2 + 2 * c * g.plane;
+        rp.d2 = div2 + (2 * c + 1) * g.plane;
+        rp.partials = partials;
+        if (error == cudaSuccess) error = launch_residual(rp, stream);
+        residual += plan.channel_weights[c] * sum_of(partials, count);
+      }
+      r.partial_gap = r.primal + partial + *plan.partial_radius * residual;
+    }
+    return r;
+  }
+
+  // The binary64 result from the last kept coefficients (docs/math.md 5: the canvas whose
+  // coefficients are zeta).
+  void result(Outcome& out) {
+    const std::size_t size = static_cast<std::size_t>(g.rows) * g.columns;
+    out.canvas.resize(size * g.channels);
+    out.coefficients.resize(components.size());
+    for (std::size_t c = 0; c < components.size(); ++c) {
+      const std::size_t count = frame.components[c].coefficient_count();
+      Geometry flat{1, static_cast<int>(count), static_cast<int>(count), 1, count};
+      if (error == cudaSuccess && count > 0) error = launch_widen(components[c].zeta, coefficients[c], flat, stream);
+      CanvasParams cp;
+      cp.g = g;
+      cp.component = components[c];
+      cp.coefficients = coefficients[c];
+      cp.canvas = canvas + c * size;
+      cp.v = v + c * g.plane;
+      cp.mode = 1;
+      if (error == cudaSuccess) error = launch_canvas(cp, stream);
+    }
+    fetch(out);
+  }
+
+  void fetch(Outcome& out) {
+    const std::size_t size = static_cast<std::size_t>(g.rows) * g.columns;
+    out.canvas.resize(size * g.channels);
+    out.coefficients.resize(components.size());
+    if (error == cudaSuccess) {
+      error = cudaMemcpyAsync(out.canvas.data(), canvas, out.canvas.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                              stream);
+    }
+    for (std::size_t c = 0; c < components.size(); ++c) {
+      out.coefficients[c].resize(frame.components[c].coefficient_count());
+      if (error == cudaSuccess && !out.coefficients[c].empty()) {
+        error = cudaMemcpyAsync(out.coefficients[c].data(), coefficients[c], out.coefficients[c].size() * sizeof(double),
+                                cudaMemcpyDeviceToHost, stream);
+      }
+    }
+    if (error == cudaSuccess) error = cudaStreamSynchronize(stream);
+  }
+};
+
+Solver::Solver(const Frame& frame, cudaStream_t stream) : impl_(std::make_unique<Impl>(frame, stream)) {
+  geometry_.rows = static_cast<int>(frame.rows);
+  geometry_.columns = static_cast<int>(frame.columns);
+  geometry_.pitch = static_cast<int>((frame.columns + 31) / 32 * 32);
+  geometry_.channels = static_cast<int>(frame.channels());
+  geometry_.plane = static_cast<std::size_t>(geometry_.rows) * geometry_.pitch;
+  impl_->g = geometry_;
+}
+
+Solver::~Solver() = default;
+
+int Solver::launches_per_iteration() const { return 1 + static_cast<int>(impl_->components.size()); }
+
+bool Solver::solve(Method method, const Plan* plan, const Start* start, const Observer& observer, Outcome& out,
+                   Failure& failure) {
+  Impl& m = *impl_;
+  const bool solver = method == Method::tv || method == Method::tgv;
+  if (!solver) {
+    // The decoder of the centres (docs/math.md 2.3).
+    m.setup(false);
+    m.start(nullptr, false);
+    m.fetch(out);
+    bytes_ = m.bytes;
+    out.solved = false;
+    out.stop = 0;
+    return m.check(failure, "the decoder of the centres");
+  }
+  m.plan = *plan;
+  m.setup(plan->tgv);
+  m.set_factors(*plan);
+  m.start(start, true);
+  bytes_ = m.bytes;
+  if (!m.check(failure, "the start")) return false;
+  out.tau = plan->tau;
+  out.sigma = plan->sigma;
+  const double samples = static_cast<double>(m.g.channels) * m.g.rows * m.g.columns;
+  const std::uint64_t most = plan->iterations;
+  const std::uint64_t every = plan->record_every;
+  using Clock = std::chrono::steady_clock;
+  const auto began = Clock::now();
+  double recording = 0.0;
+  std::int32_t stop = 0;
+  auto take = [&](std::uint64_t iteration) -> bool {
+    const auto at = Clock::now();
+    if (m.error == cudaSuccess) m.error = cudaStreamSynchronize(m.stream);
+    Record r = m.record(iteration);
+    const auto done = Clock::now();
+    recording += std::chrono::duration<double>(done - at).count();
+    r.seconds = std::chrono::duration<double>(at - began).count();
+    if (m.error != cudaSuccess) return true;
+    const double gap = r.primal - r.dual;
+    bool met = false;
+    if (plan->tolerance > 0.0 && gap / samples <= plan->tolerance) met = true;
+    if (plan->relative_tolerance > 0.0 && gap <= plan->relative_tolerance * r.primal) met = true;
+    if (plan->partial_tolerance > 0.0 && !std::isnan(r.partial_gap) &&
+        r.partial_gap / samples <= plan->partial_tolerance) {
+      met = true;
+    }
+    out.records.push_back(r);
+    if (met) {
+      stop = 1;
+      return true;
+    }
+    if (observer && out.records.size() > 1) {
+      const Geometry whole = m.g;
+      if (m.error == cudaSuccess) m.error = launch_widen(m.xt, m.canvas, whole, m.stream);
+      std::vector<double> host(static_cast<std::size_t>(whole.channels) * whole.rows * whole.columns);
+      if (m.error == cudaSuccess) {
+        m.error = cudaMemcpyAsync(host.data(), m.canvas, host.size() * sizeof(double), cudaMemcpyDeviceToHost, m.stream);
+      }
+      if (m.error == cudaSuccess) m.error = cudaStreamSynchronize(m.stream);
+      if (m.error == cudaSuccess && observer(r, gap / samples, host.data())) {
+        stop = 3;
+        return true;
+      }
+    }
+    return false;
+  };
+  auto recorded = [&](std::uint64_t n) { return (every > 0 && n % every == 0) || n == most; };
+  bool stopped = false;
+  if (every > 0 || most == 0) stopped = take(0);
+  std::uint64_t iteration = 0;
+  if (!stopped && most > 0) m.primal(recorded(1));
+  while (!stopped && iteration < most && m.error == cudaSuccess) {
+    const std::uint64_t next = iteration + 1;
+    m.dual(recorded(next));
+    iteration = next;
+    if (recorded(iteration)) stopped = take(iteration);
+    if (!stopped && iteration < most) m.primal(recorded(iteration + 1));
+  }
+  (void)recording;
+  if (!m.check(failure, "the iterations")) return false;
+  out.iterations = iteration;
+  out.stop = stopped ? stop : 2;
+  if (out.stop == 0) out.stop = 2;
+  out.solved = true;
+  if (iteration == 0) {
+    // No iteration: the start itself, in binary64.
+    m.fetch(out);
+  } else {
+    m.result(out);
+  }
+  return m.check(failure, "the result");
+}
+
+bool Solver::prepare(const Plan& plan, Failure& failure) {
+  Impl& m = *impl_;
+  m.plan = plan;
+  m.setup(plan.tgv);
+  m.set_factors(plan);
+  m.start(nullptr, true);
+  bytes_ = m.bytes;
+  m.planned = true;
+  if (!m.check(failure, "the start")) return false;
+  m.primal(true);
+  return m.check(failure, "the first primal step");
+}
+
+bool Solver::iterate(std::uint64_t iterations, Failure& failure) {
+  Impl& m = *impl_;
+  for (std::uint64_t n = 0; n < iterations && m.error == cudaSuccess; ++n) {
+    const bool last = n + 1 == iterations;
+    m.dual(false);
+    m.primal(last);
+  }
+  return m.check(failure, "the iterations");
+}
+
+bool Solver::breakdown(std::uint64_t iterations, double& dual_ms, double& primal_ms, Failure& failure) {
+  Impl& m = *impl_;
+  std::vector<cudaEvent_t> events(3 * iterations);
+  for (cudaEvent_t& e : events) cudaEventCreate(&e);
+  for (std::uint64_t n = 0; n < iterations && m.error == cudaSuccess; ++n) {
+    cudaEventRecord(events[3 * n], m.stream);
+    m.dual(false);
+    cudaEventRecord(events[3 * n + 1], m.stream);
+    m.primal(n + 1 == iterations);
+    cudaEventRecord(events[3 * n + 2], m.stream);
+  }
+  if (m.error == cudaSuccess) m.error = cudaStreamSynchronize(m.stream);
+  double dual = 0.0, primal = 0.0;
+  for (std::uint64_t n = 0; n < iterations && m.error == cudaSuccess; ++n) {
+    float a = 0.0f, b = 0.0f;
+    cudaEventElapsedTime(&a, events[3 * n], events[3 * n + 1]);
+    cudaEventElapsedTime(&b, events[3 * n + 1], events[3 * n + 2]);
+    dual += a;
+    primal += b;
+  }
+  for (cudaEvent_t& e : events) cudaEventDestroy(e);
+  dual_ms = iterations > 0 ? dual / static_cast<double>(iterations) : 0.0;
+  primal_ms = iterations > 0 ? primal / static_cast<double>(iterations) : 0.0;
+  return m.check(failure, "the timed iterations");
+}
+
+bool Solver::finish(Outcome& out, Failure& failure) {
+  Impl& m = *impl_;
+  m.result(out);
+  return m.check(failure, "the result");
+}
+
+}  // namespace urb

@@ -1,0 +1,92 @@
+// The driver of the device solve: the reference's method loop (cpp/src/primal_dual.hpp:957-1013,
+// rust/unround/src/pdhg.rs:641-686) over the kernels of kernels.hpp. Each iteration is two
+// launches on the call's own stream: the dual step of iteration n with the relaxation, then
+// the primal step and proximal map of iteration n+1 (the canvas x~ is the one field carried
+// between them). Records take the tilde point in binary64 sums; the result is computed in
+// binary64 from the last coefficients.
+#pragma once
+
+#include <cstdint>
+#include <functional>
+#include <memory>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "kernels.hpp"
+#include "model.hpp"
+
+namespace urb {
+
+// A record (cpp/include/unround/results.hpp:17-24): the iteration, the solver's seconds,
+// the primal and dual values, TGV's scaling and partial gap (NaN where not taken).
+struct Record {
+  std::uint64_t iteration = 0;
+  double seconds = 0.0;
+  double primal = 0.0;
+  double dual = 0.0;
+  double scaling = 0.0;
+  double partial_gap = 0.0;
+};
+
+// A start (cpp/include/unround/pdhg.hpp:124-133): every component's coefficients, clipped to
+// their intervals, and each channel's duals, projected onto their balls, and TGV's w
+// (channel-major, canvas rows x columns each); an empty part takes the default.
+struct Start {
+  std::vector<std::vector<double>> coefficients;
+  std::vector<double> p;  // C x 2 x rows x columns
+  std::vector<double> w;  // C x 2 x rows x columns
+  std::vector<double> r;  // C x 3 x rows x columns
+};
+
+// What a solve made (rust/unround/src/decode.rs:70-110): the canvas C x rows x columns and
+// each component's coefficients in binary64, the records, the iterations, and why it stopped
+// (0 no solver, 1 converged, 2 iterations, 3 observer).
+struct Outcome {
+  std::vector<double> canvas;
+  std::vector<std::vector<double>> coefficients;
+  std::vector<Record> records;
+  std::uint64_t iterations = 0;
+  std::int32_t stop = 0;
+  bool solved = false;
+  double tau = 0.0;
+  double sigma = 0.0;
+};
+
+// Called with each record after the first, the gap per sample and the record's canvas
+// (C x rows x columns binary64, valid for the call); true stops the solver.
+using Observer = std::function<bool(const Record&, double gap, const double* canvas)>;
+
+class Solver {
+ public:
+  Solver(const Frame& frame, cudaStream_t stream);
+  ~Solver();
+  Solver(const Solver&) = delete;
+  Solver& operator=(const Solver&) = delete;
+
+  // The MMSE decoder (no plan) or TV/TGV by the primal-dual method, into `out`.
+  bool solve(Method method, const Plan* plan, const Start* start, const Observer& observer, Outcome& out,
+             Failure& failure);
+
+  // For measurement: `iterations` iterations of the method from the current state, no
+  // records, launched on the stream and not waited for (the caller times them).
+  bool prepare(const Plan& plan, Failure& failure);
+  bool iterate(std::uint64_t iterations, Failure& failure);
+  // The same with CUDA events around each kernel group: the average device milliseconds of
+  // an iteration's dual step and of its primal steps.
+  bool breakdown(std::uint64_t iterations, double& dual_ms, double& primal_ms, Failure& failure);
+  // The binary64 canvas of the last tilde point, after prepare/iterate.
+  bool finish(Outcome& out, Failure& failure);
+
+  [[nodiscard]] std::size_t device_bytes() const { return bytes_; }
+  [[nodiscard]] const Geometry& geometry() const { return geometry_; }
+  [[nodiscard]] int launches_per_iteration() const;
+
+ private:
+  struct Impl;
+  std::unique_ptr<Impl> impl_;
+  Geometry geometry_;
+  std::size_t bytes_ = 0;
+};
+
+}  // namespace urb

@@ -1,0 +1,638 @@
+"""The reconstruction on a B200, through the C interface of libunround_capi.so.
+
+The drop-in for the reference package's unround.native (python/src/unround/native.py of
+JPEG-Unround): the same functions, data classes and errors, over the same C interface
+(include/unround.h, ABI version 5), so a caller switches by importing this package. ctypes
+releases the GIL while the library computes; every call has its own CUDA stream, so threads
+reconstruct at once. The settings go over as the command line's options, each number as the
+shortest decimal that reads back as the same double (repr); the results come back as NumPy
+arrays, copied, and the library's memory is freed before a function returns.
+
+solve() is the path: levels and tables in, the TV/TGV primal-dual solve on the GPU, the
+binary64 result out. decode() and project(), which need libjpeg-turbo to read a file, raise
+UnroundError with the library's UNSUPPORTED status. solve_from() and measure() are this
+build's extensions (include/unround_b200.h).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import enum
+import functools
+from collections.abc import Callable
+from dataclasses import dataclass
+from typing import Final
+
+import numpy as np
+import numpy.typing as npt
+
+from unround import _loading, jpegio
+from unround.settings import TGV, TV, DataTerm, PdhgOptions, Settings, SubgradientOptions
+
+__all__ = [
+    "ABI_VERSION",
+    "Decoded",
+    "History",
+    "LibraryNotFoundError",
+    "Problem",
+    "Record",
+    "Solution",
+    "Status",
+    "Stop",
+    "Timing",
+    "UnroundError",
+    "UnroundWarning",
+    "decode",
+    "held_options",
+    "library_path",
+    "measure",
+    "options",
+    "project",
+    "solve",
+    "solve_from",
+    "to_rgb",
+    "to_ycbcr",
+    "version",
+]
+
+type Array = npt.NDArray[np.float64]
+type Observer = Callable[["Record"], bool | None]
+
+ABI_VERSION: Final = 5
+_MESSAGE: Final = 4096
+
+
+class _Record(ctypes.Structure):
+    _fields_ = (
+        ("iteration", ctypes.c_uint64),
+        ("gap", ctypes.c_double),
+        ("primal", ctypes.c_double),
+        ("dual", ctypes.c_double),
+        ("channels", ctypes.c_uint64),
+        ("height", ctypes.c_uint64),
+        ("width", ctypes.c_uint64),
+        ("canvas", ctypes.POINTER(ctypes.c_double)),
+    )
+
+
+class _Component(ctypes.Structure):
+    _fields_ = (
+        ("levels", ctypes.POINTER(ctypes.c_int16)),
+        ("rows", ctypes.c_uint32),
+        ("columns", ctypes.c_uint32),
+        ("h_samp_factor", ctypes.c_int32),
+        ("v_samp_factor", ctypes.c_int32),
+        ("quant_table", ctypes.c_uint16 * 64),
+    )
+
+
+class _Input(ctypes.Structure):
+    _fields_ = (
+        ("height", ctypes.c_uint32),
+        ("width", ctypes.c_uint32),
+        ("color_space", ctypes.c_int32),
+        ("count", ctypes.c_uint32),
+        ("components", ctypes.POINTER(_Component)),
+    )
+
+
+class _Start(ctypes.Structure):
+    _fields_ = (
+        ("coefficients", ctypes.POINTER(ctypes.c_double)),
+        ("p", ctypes.POINTER(ctypes.c_double)),
+        ("w", ctypes.POINTER(ctypes.c_double)),
+        ("r", ctypes.POINTER(ctypes.c_double)),
+    )
+
+
+class _Timing(ctypes.Structure):
+    _fields_ = (
+        ("milliseconds", ctypes.c_double),
+        ("dual_milliseconds", ctypes.c_double),
+        ("primal_milliseconds", ctypes.c_double),
+        ("iterations", ctypes.c_uint64),
+        ("launches_per_iteration", ctypes.c_uint64),
+        ("samples", ctypes.c_uint64),
+        ("pixels", ctypes.c_uint64),
+        ("device_bytes", ctypes.c_uint64),
+    )
+
+
+_SIZES: Final = ((_Record, 64), (_Component, 152), (_Input, 24))
+_OBSERVER: Final = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(_Record))
+
+
+class Status(enum.IntEnum):
+    """unround_status."""
+
+    OK = 0
+    ARGUMENT = 1
+    READ = 2
+    UNSUPPORTED = 3
+    OPTIONS = 4
+    IO = 5
+    INTERNAL = 6
+
+
+class Stop(enum.IntEnum):
+    """Why a solver stopped."""
+
+    CONVERGED = 1
+    ITERATIONS = 2
+    OBSERVER = 3
+    STATIONARY = 4
+
+
+class UnroundError(Exception):
+    """Arrays or a file that were not reconstructed: the interface's status and message."""
+
+    def __init__(self, status: Status, message: str) -> None:
+        super().__init__(f"{message} ({status.name.lower()})")
+        self.status = status
+        self.message = message
+
+    def __reduce__(self) -> tuple[type[UnroundError], tuple[Status, str]]:
+        return (type(self), (self.status, self.message))
+
+
+class LibraryNotFoundError(RuntimeError):
+    """The library is not where this module looks for it, or not of its ABI version."""
+
+
+class UnroundWarning(UserWarning):
+    """What a writer left out of a file."""
+
+
+def _bind(library: ctypes.CDLL) -> None:
+    size, handle, u64, i32 = ctypes.c_size_t, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32
+    doubles, u64p, i32p = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(u64), ctypes.POINTER(i32)
+    text = (ctypes.c_char_p, size)
+    made = (_OBSERVER, handle, ctypes.POINTER(handle), *text)
+    table = {
+        "unround_abi_version": (i32,),
+        "unround_version": (ctypes.c_char_p,),
+        "unround_settings_new": (handle, size, ctypes.POINTER(ctypes.c_char_p), *text),
+        "unround_settings_free": (None, handle),
+        "unround_settings_options": (size, handle, ctypes.c_char_p, size),
+        "unround_decode": (i32, ctypes.c_char_p, size, handle, *made),
+        "unround_solve": (i32, ctypes.POINTER(_Input), handle, *made),
+        "unround_project": (i32, ctypes.c_char_p, size, handle, doubles, u64, u64, u64, *made[2:]),
+        "unround_result_free": (None, handle),
+        "unround_result_picture": (doubles, handle, u64p, u64p, u64p),
+        "unround_result_planes": (doubles, handle, u64p),
+        "unround_result_color_space": (i32, handle),
+        "unround_result_canvas": (doubles, handle, u64p, u64p, u64p),
+        "unround_result_components": (u64, handle),
+        "unround_result_coefficients": (doubles, handle, u64, u64p),
+        "unround_result_problem": (doubles, handle, u64, i32, u64p),
+        "unround_result_component": (i32, handle, u64, u64p, u64p, u64p, u64p),
+        "unround_result_solver": (i32, handle, u64p, i32p),
+        "unround_result_record_iterations": (u64p, handle, u64p),
+        "unround_result_record_values": (doubles, handle, i32, u64p),
+        "unround_to_rgb": (i32, doubles, u64, u64, doubles),
+        "unround_to_ycbcr": (i32, doubles, u64, u64, doubles),
+        "unround_b200_solve_from": (i32, ctypes.POINTER(_Input), handle, ctypes.POINTER(_Start), *made),
+        "unround_b200_measure": (i32, ctypes.POINTER(_Input), handle, u64, u64, ctypes.POINTER(_Timing),
+                                 ctypes.POINTER(handle), *text),
+    }
+    for name, (result, *arguments) in table.items():
+        function = getattr(library, name)
+        function.restype = result
+        function.argtypes = arguments
+
+
+def library_path() -> str:
+    """The path of the library this module loads."""
+    path = _loading.configured("UNROUND_LIBRARY") or _loading.bundled(_loading.RUST)
+    if path is None or not path.is_file():
+        where = f"UNROUND_LIBRARY names {path}, where there is no file" if path else "the package holds no library"
+        raise LibraryNotFoundError(f"{where}: build it with python jpeg-unround_b200/build.py")
+    return str(path)
+
+
+@functools.cache
+def _library() -> ctypes.CDLL:
+    for structure, size in _SIZES:
+        if ctypes.sizeof(structure) != size:
+            raise RuntimeError(f"{structure.__name__} is {ctypes.sizeof(structure)} bytes, not {size}")
+    path = library_path()
+    library = ctypes.CDLL(path)
+    _bind(library)
+    found = int(library.unround_abi_version())
+    if found != ABI_VERSION:
+        raise LibraryNotFoundError(f"{path} is of ABI version {found}, and this module of version {ABI_VERSION}")
+    return library
+
+
+def version() -> str:
+    """The version of JPEG-Unround and the implementation, as the library says them."""
+    return _library().unround_version().decode()
+
+
+def _number(value: float) -> str:
+    return repr(float(value))
+
+
+def _data_options(data: DataTerm | tuple[DataTerm, ...]) -> list[str]:
+    terms = (data,) if isinstance(data, DataTerm) else tuple(data)
+    fields: tuple[tuple[str, Callable[[DataTerm], str]], ...] = (
+        ("--mu", lambda t: "rule" if t.mu is None else _number(t.mu)),
+        ("--mu-scale", lambda t: _number(t.mu_scale)),
+        ("--mu-power", lambda t: _number(t.mu_power)),
+        ("--mu-chroma", lambda t: _number(t.mu_chroma)),
+        ("--weight-power", lambda t: _number(t.power)),
+        ("--dc-weight", lambda t: _number(t.dc_weight)),
+        ("--centres", lambda t: t.centres),
+        ("--slack", lambda t: _number(t.slack)),
+        ("--slack-cost", lambda t: _number(t.slack_cost)),
+        ("--flat-weight", lambda t: _number(t.flat_weight)),
+        ("--flat-levels", lambda t: str(t.flat_levels)),
+        ("--flat-dc", lambda t: "any" if t.flat_dc is None else str(t.flat_dc)),
+    )
+    out: list[str] = []
+    for name, of in fields:
+        values = [of(term) for term in terms]
+        out += [name, values[0] if len(set(values)) == 1 else ",".join(values)]
+    return out
+
+
+def _pdhg_options(o: PdhgOptions) -> list[str]:
+    out = ["--relative-tolerance", _number(o.relative_tolerance), "--partial-tolerance", _number(o.partial_tolerance),
+           "--step-product", _number(o.step_product), "--record-every", str(o.record_every),
+           "--free-radius", _number(o.free_radius), "--threads", str(o.threads)]
+    if o.iterations is not None:
+        out += ["--iterations", str(o.iterations)]
+    for name, value in (("--tolerance", o.tolerance), ("--step-ratio", o.step_ratio), ("--relaxation", o.relaxation),
+                        ("--norm-squared", o.norm_squared), ("--partial-radius", o.partial_radius)):
+        if value is not None:
+            out += [name, _number(value)]
+    if not o.scale_with_weight:
+        out.append("--no-weight-scaling")
+    return out
+
+
+def _subgradient_options(o: SubgradientOptions) -> list[str]:
+    out = ["--subgradient-iterations", str(o.iterations), "--subgradient-record-every", str(o.record_every),
+           "--subgradient-step", _number(o.step), "--subgradient-decay", _number(o.decay)]
+    if not o.momentum:
+        out.append("--no-momentum")
+    return out
+
+
+def options(settings: Settings | None = None, *, max_pixels: int = 0, max_scans: int = 0,
+            warnings_are_errors: bool = False) -> list[str]:
+    """The command line's options that are the settings (docs/cli.md). The channel weights and
+    their coupling are those of the method's model: TGV's for TGV, TV's otherwise."""
+    settings = Settings() if settings is None else settings
+    weights: TV | TGV = settings.tgv if settings.method == "tgv" else settings.tv
+    out = ["--method", settings.method, "--alpha", _number(settings.tv.alpha),
+           "--alpha1", _number(settings.tgv.alpha1), "--alpha0", _number(settings.tgv.alpha0)]
+    if weights.channel_weights is not None:
+        out += ["--channel-weights", ",".join(_number(w) for w in weights.channel_weights)]
+    out += ["--channels", "coupled" if weights.coupled else "apart"]
+    out += _data_options(settings.data) + _pdhg_options(settings.pdhg) + _subgradient_options(settings.subgradient)
+    if max_pixels < 0 or max_scans < 0:
+        raise ValueError(f"the limits of reading are at least 0, not {max_pixels} pixels and {max_scans} scans")
+    if max_pixels:
+        out += ["--max-pixels", str(max_pixels)]
+    if max_scans:
+        out += ["--max-scans", str(max_scans)]
+    if warnings_are_errors:
+        out.append("--warnings-are-errors")
+    return out
+
+
+class _Settings:
+    """Settings of the interface made from options, freed with the object."""
+
+    def __init__(self, given: list[str]) -> None:
+        self._library = _library()
+        encoded = [option.encode("utf-8") for option in given]
+        array = (ctypes.c_char_p * max(len(encoded), 1))(*encoded)
+        message = ctypes.create_string_buffer(_MESSAGE)
+        self.handle: int | None = self._library.unround_settings_new(len(encoded), array, message, _MESSAGE)
+        if not self.handle:
+            raise UnroundError(Status.OPTIONS, message.value.decode("utf-8", "replace"))
+
+    def __del__(self) -> None:
+        handle = getattr(self, "handle", None)
+        if handle:
+            self._library.unround_settings_free(handle)
+            self.handle = None
+
+
+def _settings_of(settings: Settings | list[str] | None) -> _Settings:
+    return _Settings(list(settings) if isinstance(settings, list) else options(settings))
+
+
+def held_options(settings: Settings | list[str] | None = None, **limits: int | bool) -> list[str]:
+    """The settings as the library holds them: every value as --name=value or --flag."""
+    library = _library()
+    handle = _Settings(list(settings) if isinstance(settings, list) else options(settings, **limits))  # type: ignore[arg-type]
+    length = int(library.unround_settings_options(handle.handle, None, 0))
+    buffer = ctypes.create_string_buffer(length + 1)
+    library.unround_settings_options(handle.handle, buffer, length + 1)
+    return buffer.value.decode("ascii").split(" ")
+
+
+@dataclass(frozen=True, slots=True, eq=False)
+class Record:
+    """A record as an observer sees it: gap per sample, primal and dual values, canvas (C, H, W)."""
+
+    iteration: int
+    gap: float
+    primal: float
+    dual: float
+    canvas: Array
+
+
+@dataclass(frozen=True, slots=True, eq=False)
+class Problem:
+    """A component's model: the ratio of canvas samples per component sample, the intervals and
+    centres (rows, columns, 8, 8), the steps and weights (8, 8)."""
+
+    ratio: tuple[int, int]
+    lower: Array
+    upper: Array
+    centres: Array
+    steps: Array
+    weights: Array
+
+
+@dataclass(frozen=True, slots=True, eq=False)
+class History:
+    """The records: iterations, seconds, primal and dual values, TGV's scaling and partial gap."""
+
+    iterations: npt.NDArray[np.int64]
+    seconds: Array
+    primal: Array
+    dual: Array
+    scaling: Array
+    partial_gap: Array
+
+    @property
+    def gap(self) -> Array:
+        return np.asarray(self.primal - self.dual, dtype=np.float64)
+
+
+@dataclass(frozen=True, slots=True, eq=False)
+class Solution:
+    """What the solver did: its iterations, why it stopped, and its records."""
+
+    iterations: int
+    stop: Stop
+    history: History
+
+    @property
+    def converged(self) -> bool:
+        return self.stop is Stop.CONVERGED
+
+
+@dataclass(frozen=True, slots=True, eq=False)
+class Decoded:
+    """A reconstruction: the picture (H, W) or (H, W, C) in binary64, the planes (C, H, W), the
+    canvas (C, canvas rows, canvas columns), each component's coefficients and model, and the
+    solver's result (None for the decoder of the centres)."""
+
+    picture: Array
+    planes: Array
+    canvas: Array
+    color_space: jpegio.ColorSpace
+    coefficients: tuple[Array, ...]
+    problems: tuple[Problem, ...]
+    result: Solution | None
+    icc_profile: bytes | None
+    exif_orientation: int
+    input_format: str = "jpeg"
+    bits: int = 8
+    alpha_result: Solution | None = None
+    excess: tuple[Array, ...] | None = None
+
+
+def _copy(pointer: object, shape: tuple[int, ...], dtype: type = np.float64) -> npt.NDArray:
+    count = int(np.prod(shape, dtype=np.int64))
+    if count == 0:
+        return np.zeros(shape, dtype=dtype)
+    if not pointer:
+        raise RuntimeError("the library gave no values where it has some")
+    return np.array(np.ctypeslib.as_array(pointer, shape=(count,)), dtype=dtype, copy=True).reshape(shape)
+
+
+def _decoded(library: ctypes.CDLL, result: ctypes.c_void_p, problems: bool = True) -> Decoded:
+    u = [ctypes.c_uint64() for _ in range(4)]
+    pointer = library.unround_result_picture(result, *(ctypes.byref(x) for x in u[:3]))
+    rows, columns, depth = (int(x.value) for x in u[:3])
+    picture = _copy(pointer, (rows, columns) if depth == 1 else (rows, columns, depth))
+    pointer = library.unround_result_canvas(result, *(ctypes.byref(x) for x in u[:3]))
+    channels, height, width = (int(x.value) for x in u[:3])
+    canvas = _copy(pointer, (channels, height, width))
+    count = ctypes.c_uint64()
+    planes = _copy(library.unround_result_planes(result, ctypes.byref(count)), (channels, rows, columns))
+    coefficients, models = [], []
+    for index in range(int(library.unround_result_components(result))):
+        library.unround_result_component(result, index, *(ctypes.byref(x) for x in u))
+        block_rows, block_columns, down, across = (int(x.value) for x in u)
+        shape = (block_rows, block_columns, 8, 8)
+        coefficients.append(_copy(library.unround_result_coefficients(result, index, ctypes.byref(count)), shape))
+        if problems:
+            arrays = [_copy(library.unround_result_problem(result, index, which, ctypes.byref(count)),
+                            shape if which < 3 else (8, 8)) for which in range(5)]
+            models.append(Problem((down, across), *arrays))
+    iterations, stop = ctypes.c_uint64(), ctypes.c_int32()
+    solution = None
+    if library.unround_result_solver(result, ctypes.byref(iterations), ctypes.byref(stop)):
+        n = ctypes.c_uint64()
+        at = library.unround_result_record_iterations(result, ctypes.byref(n))
+        steps = _copy(at, (int(n.value),), np.int64)
+        values = [_copy(library.unround_result_record_values(result, which, ctypes.byref(n)), (int(n.value),))
+                  for which in range(5)]
+        solution = Solution(int(iterations.value), Stop(int(stop.value)), History(steps, *values))
+    return Decoded(
+        picture=picture, planes=planes, canvas=canvas,
+        color_space=jpegio.ColorSpace(int(library.unround_result_color_space(result))),
+        coefficients=tuple(coefficients), problems=tuple(models), result=solution,
+        icc_profile=None, exif_orientation=0,
+    )
+
+
+class _Watcher:
+    """The observer as the interface calls it; an exception is kept and raised after the call."""
+
+    def __init__(self, observer: Observer | None) -> None:
+        self._observer = observer
+        self.error: BaseException | None = None
+        self.callback = _OBSERVER() if observer is None else _OBSERVER(self._call)
+
+    def _call(self, _user: int | None, pointer: ctypes._Pointer[_Record]) -> int:
+        if self._observer is None or self.error is not None:
+            return 1
+        try:
+            r = pointer.contents
+            seen = Record(int(r.iteration), float(r.gap), float(r.primal), float(r.dual),
+                          _copy(r.canvas, (int(r.channels), int(r.height), int(r.width))))
+            return 1 if self._observer(seen) else 0
+        except BaseException as error:  # noqa: BLE001 -- raised again once the library returns
+            self.error = error
+            return 1
+
+
+def _raise(status: int, message: ctypes.Array[ctypes.c_char]) -> None:
+    if status != Status.OK:
+        known = status in Status.__members__.values()
+        raise UnroundError(Status(status) if known else Status.INTERNAL, message.value.decode("utf-8", "replace"))
+
+
+def _input_of(image: jpegio.Image) -> tuple[_Input, list[object]]:
+    count = len(image.components)
+    kept: list[object] = []
+    raw = (_Component * max(count, 1))()
+    for index, component in enumerate(image.components):
+        levels = np.ascontiguousarray(component.coefficients, dtype=np.int16)
+        if levels.ndim != 4 or levels.shape[2:] != (8, 8):
+            raise ValueError(f"the levels of component {index} are (rows, columns, 8, 8), not {levels.shape}")
+        kept.append(levels)
+        raw[index].levels = levels.ctypes.data_as(ctypes.POINTER(ctypes.c_int16))
+        raw[index].rows, raw[index].columns = int(levels.shape[0]), int(levels.shape[1])
+        raw[index].h_samp_factor = int(component.h_samp_factor)
+        raw[index].v_samp_factor = int(component.v_samp_factor)
+        table = np.asarray(component.quant_table, dtype=np.uint16).reshape(64)
+        raw[index].quant_table = (ctypes.c_uint16 * 64)(*(int(step) for step in table))
+    kept.append(raw)
+    return _Input(int(image.height), int(image.width), int(image.color_space), count, raw), kept
+
+
+def solve(image: jpegio.Image, settings: Settings | list[str] | None = None, *,
+          observer: Observer | None = None) -> Decoded:
+    """Reconstructs an image's components (levels, tables, sampling factors) on the GPU, as the
+    reference's unround.native.solve does (python/src/unround/native.py:758-788). settings may
+    also be the command line's options as a list of strings."""
+    return solve_from(image, settings, observer=observer)
+
+
+def solve_from(image: jpegio.Image, settings: Settings | list[str] | None = None, *,
+               start: dict[str, npt.ArrayLike] | None = None, observer: Observer | None = None) -> Decoded:
+    """solve() from a given start (include/unround_b200.h): 'coefficients' (every component's
+    blocks one after another), 'p' (C, 2, H, W), 'w' (C, 2, H, W), 'r' (C, 3, H, W)."""
+    library = _library()
+    handle = _settings_of(settings)
+    given, kept = _input_of(image)
+    watcher = _Watcher(observer)
+    result = ctypes.c_void_p()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    if start is None:
+        status = library.unround_solve(ctypes.byref(given), handle.handle, watcher.callback, None,
+                                       ctypes.byref(result), message, _MESSAGE)
+    else:
+        raw = _Start()
+        for name in ("coefficients", "p", "w", "r"):
+            if start.get(name) is not None:
+                values = np.ascontiguousarray(start[name], dtype=np.float64).reshape(-1)
+                kept.append(values)
+                setattr(raw, name, values.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        status = library.unround_b200_solve_from(ctypes.byref(given), handle.handle, ctypes.byref(raw),
+                                                 watcher.callback, None, ctypes.byref(result), message, _MESSAGE)
+    try:
+        if watcher.error is not None:
+            raise watcher.error
+        _raise(status, message)
+        return _decoded(library, result)
+    finally:
+        library.unround_result_free(result)
+        del kept
+
+
+@dataclass(frozen=True, slots=True)
+class Timing:
+    """measure(): the device milliseconds of the timed iterations (CUDA events), each kernel
+    group's average per iteration (dual step; primal steps of every component), the iterations,
+    the kernels launched per iteration, the canvas's samples and pixels, the device bytes held."""
+
+    milliseconds: float
+    dual_milliseconds: float
+    primal_milliseconds: float
+    iterations: int
+    launches_per_iteration: int
+    samples: int
+    pixels: int
+    device_bytes: int
+
+
+def measure(image: jpegio.Image, settings: Settings | list[str] | None = None, *, warmup: int = 3,
+            iterations: int = 10, result: bool = False) -> tuple[Timing, Decoded | None]:
+    """Times the iteration loop alone on the GPU (include/unround_b200.h, unround_b200_measure)."""
+    library = _library()
+    handle = _settings_of(settings)
+    given, kept = _input_of(image)
+    timing = _Timing()
+    made = ctypes.c_void_p()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_b200_measure(ctypes.byref(given), handle.handle, warmup, iterations,
+                                          ctypes.byref(timing), ctypes.byref(made) if result else None,
+                                          message, _MESSAGE)
+    try:
+        _raise(status, message)
+        decoded = _decoded(library, made, problems=False) if result else None
+        return Timing(timing.milliseconds, timing.dual_milliseconds, timing.primal_milliseconds, int(timing.iterations), int(timing.launches_per_iteration),
+                      int(timing.samples), int(timing.pixels), int(timing.device_bytes)), decoded
+    finally:
+        if result:
+            library.unround_result_free(made)
+        del kept
+
+
+def decode(source: object, settings: Settings | None = None, **_: object) -> Decoded:
+    """Reading a JPEG file needs libjpeg-turbo: the library refuses with UNSUPPORTED."""
+    library = _library()
+    handle = _settings_of(settings)
+    data = source if isinstance(source, (bytes, bytearray)) else b""
+    result = ctypes.c_void_p()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_decode(bytes(data), len(data), handle.handle, _OBSERVER(), None, ctypes.byref(result),
+                                    message, _MESSAGE)
+    _raise(status, message)
+    try:
+        return _decoded(library, result)
+    finally:
+        library.unround_result_free(result)
+
+
+def project(picture: npt.ArrayLike, source: object, settings: Settings | None = None, **_: object) -> Decoded:
+    """Projecting onto a JPEG file's intervals needs libjpeg-turbo: the library refuses."""
+    library = _library()
+    handle = _settings_of(settings)
+    samples = np.ascontiguousarray(picture, dtype=np.float64)
+    result = ctypes.c_void_p()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    data = source if isinstance(source, (bytes, bytearray)) else b""
+    status = library.unround_project(bytes(data), len(data), handle.handle,
+                                     samples.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), samples.shape[0],
+                                     samples.shape[1] if samples.ndim > 1 else 1,
+                                     samples.shape[2] if samples.ndim > 2 else 1, ctypes.byref(result), message,
+                                     _MESSAGE)
+    _raise(status, message)
+    try:
+        return _decoded(library, result)
+    finally:
+        library.unround_result_free(result)
+
+
+def to_rgb(planes: npt.ArrayLike) -> Array:
+    """JFIF's RGB (H, W, 3) of Y, Cb and Cr planes (3, H, W) (docs/math.md 8)."""
+    values = np.ascontiguousarray(planes, dtype=np.float64)
+    if values.ndim != 3 or values.shape[0] != 3:
+        raise ValueError(f"the planes are (3, height, width), not {values.shape}")
+    out = np.empty((values.shape[1], values.shape[2], 3))
+    p = ctypes.POINTER(ctypes.c_double)
+    _library().unround_to_rgb(values.ctypes.data_as(p), values.shape[1], values.shape[2], out.ctypes.data_as(p))
+    return out
+
+
+def to_ycbcr(picture: npt.ArrayLike) -> Array:
+    """JFIF's Y, Cb and Cr planes (3, H, W) of an RGB picture (H, W, 3)."""
+    values = np.ascontiguousarray(picture, dtype=np.float64)
+    if values.ndim != 3 or values.shape[2] != 3:
+        raise ValueError(f"the picture is (height, width, 3), not {values.shape}")
+    out = np.empty((3, values.shape[0], values.shape[1]))
+    p = ctypes.POINTER(ctypes.c_double)
+    _library().unround_to_ycbcr(values.ctypes.data_as(p), values.shape[0], values.shape[1], out.ctypes.data_as(p))
+    return out
