@@ -70,11 +70,25 @@ std::int32_t guarded(char* message, std::size_t size, Body&& body) {
 
 bool have_device(urb::Failure& failure) {
   int count = 0;
-  const cudaError_t error = cudaGetDeviceCount(&count);
+  cudaError_t error = cudaGetDeviceCount(&count);
   if (error != cudaSuccess || count == 0) {
     failure = {urb::kInternal, std::string("no CUDA device for the solver: ") +
                                    (error != cudaSuccess ? cudaGetErrorString(error) : "none found")};
     return false;
+  }
+  // The solves' buffers come from the device's stream-ordered pool; keep what a solve frees
+  // for the next one instead of returning it to the driver at every synchronization.
+  int device = 0;
+  error = cudaGetDevice(&device);
+  static std::once_flag pooled[64];
+  if (error == cudaSuccess && device >= 0 && device < 64) {
+    std::call_once(pooled[device], [device] {
+      cudaMemPool_t pool = nullptr;
+      if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        std::uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+    });
   }
   return true;
 }

@@ -229,11 +229,25 @@ struct Coefficient {
   float low, high, centre, own_low, own_high;
 };
 
+//
+// DC is taken centred on the middle of its interval, c_DC = q Q + 1024: the block's samples
+// less c_DC / 8 have the DC coefficient e - c_DC, whose interval is [-(1/2 + s) Q, (1/2 + s) Q]
+// and whose centre is 0. The same map in exact arithmetic; in binary32 it keeps DC's values
+// small, where the absolute ones (up to ~2000) would lose ~1e-4 a transform, and lose it alike
+// every iteration in the slow modes of weakly pinned (flat) blocks.
 __device__ __forceinline__ Coefficient coefficient_of(int q, int k, const ProxFactors& F) {
   const float level = static_cast<float>(q);
   const float step = F.step[k];
-  const float shift = k == 0 ? 1024.0f : 0.0f;
   Coefficient c;
+  if (k == 0) {
+    c.low = (-0.5f - F.slack) * step;
+    c.high = (0.5f + F.slack) * step;
+    c.centre = 0.0f;
+    c.own_low = -0.5f * step;
+    c.own_high = 0.5f * step;
+    return c;
+  }
+  const float shift = 0.0f;
   c.low = ((level - 0.5f) - F.slack) * step + shift;
   c.high = ((level + 0.5f) + F.slack) * step + shift;
   if (F.mmse && k != 0) {
@@ -341,14 +355,18 @@ __global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
   float zeta[8];
   int levels[8];
   bool flat = false;
-  if constexpr (CR == 1 && CC == 1) {
-    // The means are v itself.
-  }
+  const std::size_t block =
+      static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
+  // The middle of the block's DC interval over 8, q Q / 8 + 128, exact in binary32: the
+  // block is transformed centred on it (coefficient_of).
+  const float dc_level = in_blocks ? static_cast<float>(P.component.levels[block * 64]) : 0.0f;
+  const float middle = (dc_level * F.step[0] + 1024.0f) * 0.125f;
+  // The means of the cells (v itself where a cell is one sample), centred.
   float mean[8];
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     if constexpr (CR == 1 && CC == 1) {
-      mean[r] = v[r][0];
+      mean[r] = v[r][0] - middle;
     } else {
       float sum = 0.0f;
 #pragma unroll
@@ -358,7 +376,7 @@ __global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
         for (int a = 1; a < CR; ++a) column += v[CR * r + a][c];
         sum = c == 0 ? column : sum + column;
       }
-      mean[r] = sum / static_cast<float>(CR * CC);
+      mean[r] = sum / static_cast<float>(CR * CC) - middle;
     }
   }
   // Column DCT, transpose, row DCT: the lane holds coefficients (v = m, u = 0..7).
@@ -372,10 +390,9 @@ __global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
 #pragma unroll
   for (int u = 0; u < 8; ++u) row[u] = t[m * 9 + u];
   forward8(row, coef);
-  // The clip of the proximal map.
+  // The clip of the proximal map. Kept coefficients are stored as the map gives them: DC
+  // centred (less q Q + 1024), the others as they are.
   {
-    const std::size_t block = static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns +
-                              (in_blocks ? vbx : 0);
     const int4 packed = in_blocks ? __ldg(reinterpret_cast<const int4*>(P.component.levels + block * 64 + m * 8))
                                   : make_int4(0, 0, 0, 0);
     const int words[4] = {packed.x, packed.y, packed.z, packed.w};
@@ -415,7 +432,7 @@ __global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     if constexpr (CR == 1 && CC == 1) {
-      out[r][0] = in_blocks ? back[r] : v[r][0];
+      out[r][0] = in_blocks ? back[r] + middle : v[r][0];
     } else {
       const float change = back[r] - mean[r];
 #pragma unroll
@@ -440,7 +457,13 @@ __global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
     double sum = 0.0;
     if (in_blocks) {
 #pragma unroll
-      for (int u = 0; u < 8; ++u) sum += value_term(zeta[u], levels[u], m * 8 + u, flat, *P.component.constants);
+      for (int u = 0; u < 8; ++u) {
+        const int k = m * 8 + u;
+        const double absolute = k == 0 ? static_cast<double>(zeta[u]) + (static_cast<double>(levels[0]) *
+                                                                          P.component.constants->step[0] + 1024.0)
+                                       : static_cast<double>(zeta[u]);
+        sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
+      }
     }
     cta_sum(sum, P.partials);
   }
@@ -480,6 +503,23 @@ __global__ void __launch_bounds__(256) start_kernel(const StartParams P) {
     }
   }
   cta_sum(sum, P.partials);
+}
+
+// The kept binary32 coefficients made binary64 and absolute: DC, kept centred, plus q Q + 1024
+// (exact in binary64), every coefficient clipped to its binary64 interval.
+__global__ void __launch_bounds__(256) restore_kernel(const ComponentDevice C, double* out) {
+  const std::size_t at = static_cast<std::size_t>(blockIdx.x) * 256 + threadIdx.x;
+  const std::size_t count = static_cast<std::size_t>(C.block_rows) * C.block_columns * 64;
+  if (at >= count) return;
+  const int k = static_cast<int>(at & 63);
+  const Constants64& K = *C.constants;
+  const double level = static_cast<double>(C.levels[at]);
+  const double shift = k == 0 ? 1024.0 : 0.0;
+  double value = static_cast<double>(C.zeta[at]);
+  if (k == 0) value += level * K.step[0] + 1024.0;
+  const double low = ((level - 0.5) - K.slack) * K.step[k] + shift;
+  const double high = ((level + 0.5) + K.slack) * K.step[k] + shift;
+  out[at] = clamp_to(value, low, high);
 }
 
 template <int CR, int CC>
@@ -944,6 +984,13 @@ cudaError_t launch_start_coefficients(const StartParams& p, cudaStream_t stream)
   const int blocks = start_grid_blocks(p.component);
   if (blocks == 0) return cudaSuccess;
   start_kernel<<<blocks, 256, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_restore(const ComponentDevice& c, double* out, cudaStream_t stream) {
+  const std::size_t count = static_cast<std::size_t>(c.block_rows) * c.block_columns * 64;
+  if (count == 0) return cudaSuccess;
+  restore_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, stream>>>(c, out);
   return cudaGetLastError();
 }
 

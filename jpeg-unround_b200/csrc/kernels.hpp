@@ -174,6 +174,8 @@ cudaError_t launch_dual(const DualParams& p, bool tgv, bool coupled, bool keep, 
 cudaError_t launch_primal(const PrimalParams& p, bool keep, cudaStream_t stream);
 cudaError_t launch_start_coefficients(const StartParams& p, cudaStream_t stream);
 cudaError_t launch_canvas(const CanvasParams& p, cudaStream_t stream);
+// The kept coefficients (binary32, DC centred) as binary64 absolute coefficients.
+cudaError_t launch_restore(const ComponentDevice& c, double* out, cudaStream_t stream);
 cudaError_t launch_gradient(const float* x, float* w1, float* w2, const Geometry& g, cudaStream_t stream);
 cudaError_t launch_project(Fields f, const Geometry& g, bool tgv, bool coupled, float radius, float radius0,
                            cudaStream_t stream);

@@ -39,8 +39,8 @@ double power_of(double step, double power) {
 
 // ((q + half) + widen) Q + shift, each operation rounded apart.
 double interval_end(double level, double half, double widen, double step, double shift) {
-  volatile double widened = (level + half) + widen;
-  volatile double scaled = widened * step;
+  const double widened = (level + half) + widen;
+  const double scaled = widened * step;
   return scaled + shift;
 }
 
@@ -71,7 +71,7 @@ double Component::centre(std::int16_t q, int k) const {
   const double level = static_cast<double>(q);
   if (k == 0 || !mmse) return level * steps[k] + (k == 0 ? kLevelShiftDc : 0.0);
   // sign(q) (|q| - delta / Q) Q, 0 for q = 0 (cpp/include/unround/laplace.hpp:51-56).
-  volatile double size = (std::fabs(level) - shrink[k]) * steps[k];
+  const double size = (std::fabs(level) - shrink[k]) * steps[k];
   const double signed_size = level < 0.0 ? -size : size;
   return level == 0.0 ? 0.0 : signed_size;
 }

@@ -421,9 +421,7 @@ struct Solver::Impl {
     out.canvas.resize(size * g.channels);
     out.coefficients.resize(components.size());
     for (std::size_t c = 0; c < components.size(); ++c) {
-      const std::size_t count = frame.components[c].coefficient_count();
-      Geometry flat{1, static_cast<int>(count), static_cast<int>(count), 1, count};
-      if (error == cudaSuccess && count > 0) error = launch_widen(components[c].zeta, coefficients[c], flat, stream);
+      if (error == cudaSuccess) error = launch_restore(components[c], coefficients[c], stream);
       CanvasParams cp;
       cp.g = g;
       cp.component = components[c];
