@@ -76,141 +76,204 @@ __device__ __forceinline__ void cta_sum(double value, double* out) {
 }
 
 // ---------------------------------------------------------------------------------------
-// The dual step (one thread per pixel, every channel of it).
-
-struct Wt {
-  float w1, w2;  // w of s_{n-1}
-  float t1, t2;  // w~
-};
-
-// w~ = w + tau g (p + div2 r) at (i, j) of one channel (cpp/src/primal_dual.hpp:547-557):
-// div2 r = (dx r11 + dy r12, dx r12 + dy r22), forward differences, 0 at the ends.
-__device__ __forceinline__ Wt w_tilde(const Fields& in, std::size_t base, std::size_t at, int i, int j, int rows,
-                                      int columns, int pitch, float tau) {
-  const float r11 = ld(in.r11 + base, at), r12 = ld(in.r12 + base, at), r22 = ld(in.r22 + base, at);
-  float d1 = 0.0f, d2 = 0.0f;
-  if (j + 1 < columns) {
-    d1 = ld(in.r11 + base, at + 1) - r11;
-    d2 = ld(in.r12 + base, at + 1) - r12;
-  }
-  if (i + 1 < rows) {
-    d1 = d1 + (ld(in.r12 + base, at + pitch) - r12);
-    d2 = d2 + (ld(in.r22 + base, at + pitch) - r22);
-  }
-  Wt w;
-  w.w1 = ld(in.w1 + base, at);
-  w.w2 = ld(in.w2 + base, at);
-  w.t1 = w.w1 + tau * (ld(in.p1 + base, at) + d1);
-  w.t2 = w.w2 + tau * (ld(in.p2 + base, at) + d2);
-  return w;
-}
+// The dual step as a sweep: a warp owns 32 columns and walks down a segment of kSegment rows,
+// so that every field of every channel is read once. Row i needs x- of row i + 1 (read one row
+// ahead) and w- of row i - 1 (kept from the row before); the neighbours across come from the
+// lanes beside (shuffles), and the warp's two edge lanes read the one column beyond it (lane 0
+// computes w- of column j - 1, lane 31 reads x- and r of column j + 1). Each value is computed
+// from the same operands by the same operations as in dual_kernel.
+constexpr int kSegment = 64;
 
 template <bool TGV, int C, bool COUPLED, bool KEEP>
-__global__ void __launch_bounds__(256) dual_kernel(const DualParams P) {
-  const int j = blockIdx.x * 32 + threadIdx.x;
-  const int i = blockIdx.y * 8 + threadIdx.y;
+__global__ void __launch_bounds__(256) dual_stream_kernel(const DualParams P) {
+  constexpr unsigned kAll = 0xffffffffu;
+  const int lane = threadIdx.x;
+  const int j = blockIdx.x * 32 + lane;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
-  if (i >= rows || j >= columns) return;
-  const std::size_t at = static_cast<std::size_t>(i) * pitch + j;
-  const bool has_right = j + 1 < columns, has_down = i + 1 < rows;
-  const bool has_left = j > 0, has_up = i > 0;
+  const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kSegment;
+  if (i0 >= rows) return;  // the whole warp
+  const int i1 = min(i0 + kSegment, rows);
+  const bool valid = j < columns;
+  const int jc = valid ? j : columns - 1;
+  const bool has_left = j > 0, has_right = j + 1 < columns;
+  const bool edge_left = lane == 0 && has_left;
+  const bool edge_right = lane == 31 && has_right;
   const float rho = P.rho, rest = P.rest;
+  const std::size_t plane = P.g.plane;
+  auto at = [pitch](int i, int jj) { return static_cast<std::size_t>(i) * pitch + jj; };
 
-  float step_p1[C], step_p2[C], old_p1[C], old_p2[C];
-  float step_r11[C], step_r22[C], step_r12[C], old_r11[C], old_r22[C], old_r12[C];
-  float square_p = 0.0f, square_r = 0.0f;
+  float xt_c[C], x_c[C], xb_c[C], r11_c[C], r12_c[C], r22_c[C], wb1_p[C], wb2_p[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) {
-    const std::size_t base = c * P.g.plane;
-    const float* xt = P.xt + base;
-    const float* x = P.in.x + base;
-    const float xt0 = ld(xt, at), x0 = ld(x, at);
-    const float bar = 2.0f * xt0 - x0;
-    const float gx = has_right ? (2.0f * ld(xt, at + 1) - ld(x, at + 1)) - bar : 0.0f;
-    const float gy = has_down ? (2.0f * ld(xt, at + pitch) - ld(x, at + pitch)) - bar : 0.0f;
-    P.out.x[base + at] = rho * xt0 + rest * x0;
-    const float p1 = ld(P.in.p1 + base, at), p2 = ld(P.in.p2 + base, at);
-    old_p1[c] = p1;
-    old_p2[c] = p2;
-    const float sigma = P.sigma[c];
-    if constexpr (!TGV) {
-      step_p1[c] = p1 + sigma * gx;
-      step_p2[c] = p2 + sigma * gy;
-    } else {
-      const float tau = P.tau[c];
-      const Wt w0 = w_tilde(P.in, base, at, i, j, rows, columns, pitch, tau);
-      const float wb1 = 2.0f * w0.t1 - w0.w1, wb2 = 2.0f * w0.t2 - w0.w2;
-      float wl1 = 0.0f, wl2 = 0.0f, wu1 = 0.0f, wu2 = 0.0f;
-      if (has_left) {
-        const Wt w = w_tilde(P.in, base, at - 1, i, j - 1, rows, columns, pitch, tau);
-        wl1 = 2.0f * w.t1 - w.w1;
-        wl2 = 2.0f * w.t2 - w.w2;
-      }
-      if (has_up) {
-        const Wt w = w_tilde(P.in, base, at - pitch, i - 1, j, rows, columns, pitch, tau);
-        wu1 = 2.0f * w.t1 - w.w1;
-        wu2 = 2.0f * w.t2 - w.w2;
-      }
-      P.out.w1[base + at] = rho * w0.t1 + rest * w0.w1;
-      P.out.w2[base + at] = rho * w0.t2 + rest * w0.w2;
-      if constexpr (KEEP) {
-        P.tilde.w1[base + at] = w0.t1;
-        P.tilde.w2[base + at] = w0.t2;
-      }
-      step_p1[c] = p1 + sigma * (gx - wb1);
-      step_p2[c] = p2 + sigma * (gy - wb2);
-      // E w- = (dx' w1, dy' w2, (dy' w1 + dx' w2) / 2), backward differences.
-      const float own1x = has_right ? wb1 : 0.0f, own2x = has_right ? wb2 : 0.0f;
-      const float own1y = has_down ? wb1 : 0.0f, own2y = has_down ? wb2 : 0.0f;
-      const float exx = own1x - wl1;
-      const float eyy = own2y - wu2;
-      const float exy = 0.5f * ((own1y - wu1) + (own2x - wl2));
-      const float r11 = ld(P.in.r11 + base, at), r22 = ld(P.in.r22 + base, at), r12 = ld(P.in.r12 + base, at);
-      old_r11[c] = r11;
-      old_r22[c] = r22;
-      old_r12[c] = r12;
-      step_r11[c] = r11 + sigma * exx;
-      step_r22[c] = r22 + sigma * eyy;
-      step_r12[c] = r12 + sigma * exy;
-    }
-    if constexpr (COUPLED) {
-      square_p += step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c];
-      if constexpr (TGV) {
-        square_r += step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]);
-      }
-    }
-  }
-  float scale_p = 1.0f, scale_r = 1.0f;
-  if constexpr (COUPLED) {
-    scale_p = ball_scale(square_p, P.radius);
-    if constexpr (TGV) scale_r = ball_scale(square_r, P.radius0);
-  }
-#pragma unroll
-  for (int c = 0; c < C; ++c) {
-    const std::size_t base = c * P.g.plane;
-    float sp = scale_p;
-    if constexpr (!COUPLED) sp = ball_scale(step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c], P.radius);
-    const float q1 = step_p1[c] * sp, q2 = step_p2[c] * sp;
-    P.out.p1[base + at] = rho * q1 + rest * old_p1[c];
-    P.out.p2[base + at] = rho * q2 + rest * old_p2[c];
-    if constexpr (KEEP) {
-      P.tilde.p1[base + at] = q1;
-      P.tilde.p2[base + at] = q2;
-    }
+    const std::size_t base = c * plane;
+    xt_c[c] = ld(P.xt + base, at(i0, jc));
+    x_c[c] = ld(P.in.x + base, at(i0, jc));
+    xb_c[c] = 2.0f * xt_c[c] - x_c[c];
+    r11_c[c] = r12_c[c] = r22_c[c] = wb1_p[c] = wb2_p[c] = 0.0f;
     if constexpr (TGV) {
-      float sr = scale_r;
-      if constexpr (!COUPLED) {
-        sr = ball_scale(step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]),
-                        P.radius0);
+      r11_c[c] = ld(P.in.r11 + base, at(i0, jc));
+      r12_c[c] = ld(P.in.r12 + base, at(i0, jc));
+      r22_c[c] = ld(P.in.r22 + base, at(i0, jc));
+      if (i0 > 0) {
+        // w- of the row above the segment, own column.
+        const int u = i0 - 1;
+        const float a11 = ld(P.in.r11 + base, at(u, jc)), a12 = ld(P.in.r12 + base, at(u, jc));
+        const float a22 = ld(P.in.r22 + base, at(u, jc));
+        float right11 = __shfl_down_sync(kAll, a11, 1), right12 = __shfl_down_sync(kAll, a12, 1);
+        if (edge_right) {
+          right11 = ld(P.in.r11 + base, at(u, j + 1));
+          right12 = ld(P.in.r12 + base, at(u, j + 1));
+        }
+        float d1 = has_right ? right11 - a11 : 0.0f;
+        float d2 = has_right ? right12 - a12 : 0.0f;
+        d1 = d1 + (r12_c[c] - a12);
+        d2 = d2 + (r22_c[c] - a22);
+        const float w1 = ld(P.in.w1 + base, at(u, jc)), w2 = ld(P.in.w2 + base, at(u, jc));
+        const float tau = P.tau[c];
+        const float t1 = w1 + tau * (ld(P.in.p1 + base, at(u, jc)) + d1);
+        const float t2 = w2 + tau * (ld(P.in.p2 + base, at(u, jc)) + d2);
+        wb1_p[c] = 2.0f * t1 - w1;
+        wb2_p[c] = 2.0f * t2 - w2;
       }
-      const float t11 = step_r11[c] * sr, t22 = step_r22[c] * sr, t12 = step_r12[c] * sr;
-      P.out.r11[base + at] = rho * t11 + rest * old_r11[c];
-      P.out.r22[base + at] = rho * t22 + rest * old_r22[c];
-      P.out.r12[base + at] = rho * t12 + rest * old_r12[c];
+    }
+  }
+
+  for (int i = i0; i < i1; ++i) {
+    const bool has_down = i + 1 < rows, has_up = i > 0;
+    const std::size_t here = at(i, jc);
+    float step_p1[C], step_p2[C], old_p1[C], old_p2[C];
+    float step_r11[C], step_r22[C], step_r12[C], old_r11[C], old_r22[C], old_r12[C];
+    float square_p = 0.0f, square_r = 0.0f;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const std::size_t base = c * plane;
+      // Row i + 1, read ahead.
+      float xt_n = 0.0f, x_n = 0.0f, r11_n = 0.0f, r12_n = 0.0f, r22_n = 0.0f;
+      if (has_down) {
+        xt_n = ld(P.xt + base, here + pitch);
+        x_n = ld(P.in.x + base, here + pitch);
+        if constexpr (TGV) {
+          r11_n = ld(P.in.r11 + base, here + pitch);
+          r12_n = ld(P.in.r12 + base, here + pitch);
+          r22_n = ld(P.in.r22 + base, here + pitch);
+        }
+      }
+      const float xb_n = 2.0f * xt_n - x_n;
+      float xb_right = __shfl_down_sync(kAll, xb_c[c], 1);
+      if (edge_right) xb_right = 2.0f * ld(P.xt + base, at(i, j + 1)) - ld(P.in.x + base, at(i, j + 1));
+      const float gx = has_right ? xb_right - xb_c[c] : 0.0f;
+      const float gy = has_down ? xb_n - xb_c[c] : 0.0f;
+      if (valid) P.out.x[base + here] = rho * xt_c[c] + rest * x_c[c];
+      const float p1 = ld(P.in.p1 + base, here), p2 = ld(P.in.p2 + base, here);
+      old_p1[c] = p1;
+      old_p2[c] = p2;
+      const float sigma = P.sigma[c];
+      if constexpr (!TGV) {
+        step_p1[c] = p1 + sigma * gx;
+        step_p2[c] = p2 + sigma * gy;
+      } else {
+        const float tau = P.tau[c];
+        float right11 = __shfl_down_sync(kAll, r11_c[c], 1), right12 = __shfl_down_sync(kAll, r12_c[c], 1);
+        if (edge_right) {
+          right11 = ld(P.in.r11 + base, at(i, j + 1));
+          right12 = ld(P.in.r12 + base, at(i, j + 1));
+        }
+        float d1 = has_right ? right11 - r11_c[c] : 0.0f;
+        float d2 = has_right ? right12 - r12_c[c] : 0.0f;
+        d1 = d1 + (has_down ? r12_n - r12_c[c] : 0.0f);
+        d2 = d2 + (has_down ? r22_n - r22_c[c] : 0.0f);
+        const float w1 = ld(P.in.w1 + base, here), w2 = ld(P.in.w2 + base, here);
+        const float t1 = w1 + tau * (p1 + d1), t2 = w2 + tau * (p2 + d2);
+        const float wb1 = 2.0f * t1 - w1, wb2 = 2.0f * t2 - w2;
+        if (valid) {
+          P.out.w1[base + here] = rho * t1 + rest * w1;
+          P.out.w2[base + here] = rho * t2 + rest * w2;
+          if constexpr (KEEP) {
+            P.tilde.w1[base + here] = t1;
+            P.tilde.w2[base + here] = t2;
+          }
+        }
+        // w- of column j - 1.
+        float wl1 = __shfl_up_sync(kAll, wb1, 1), wl2 = __shfl_up_sync(kAll, wb2, 1);
+        if (edge_left) {
+          const std::size_t left = at(i, j - 1);
+          const float l11 = ld(P.in.r11 + base, left), l12 = ld(P.in.r12 + base, left);
+          const float l22 = ld(P.in.r22 + base, left);
+          float e1 = r11_c[c] - l11, e2 = r12_c[c] - l12;
+          e1 = e1 + (has_down ? ld(P.in.r12 + base, left + pitch) - l12 : 0.0f);
+          e2 = e2 + (has_down ? ld(P.in.r22 + base, left + pitch) - l22 : 0.0f);
+          const float lw1 = ld(P.in.w1 + base, left), lw2 = ld(P.in.w2 + base, left);
+          const float lt1 = lw1 + tau * (ld(P.in.p1 + base, left) + e1);
+          const float lt2 = lw2 + tau * (ld(P.in.p2 + base, left) + e2);
+          wl1 = 2.0f * lt1 - lw1;
+          wl2 = 2.0f * lt2 - lw2;
+        }
+        if (!has_left) wl1 = wl2 = 0.0f;
+        const float wu1 = has_up ? wb1_p[c] : 0.0f, wu2 = has_up ? wb2_p[c] : 0.0f;
+        step_p1[c] = p1 + sigma * (gx - wb1);
+        step_p2[c] = p2 + sigma * (gy - wb2);
+        const float own1x = has_right ? wb1 : 0.0f, own2x = has_right ? wb2 : 0.0f;
+        const float own1y = has_down ? wb1 : 0.0f, own2y = has_down ? wb2 : 0.0f;
+        const float exx = own1x - wl1;
+        const float eyy = own2y - wu2;
+        const float exy = 0.5f * ((own1y - wu1) + (own2x - wl2));
+        old_r11[c] = r11_c[c];
+        old_r22[c] = r22_c[c];
+        old_r12[c] = r12_c[c];
+        step_r11[c] = r11_c[c] + sigma * exx;
+        step_r22[c] = r22_c[c] + sigma * eyy;
+        step_r12[c] = r12_c[c] + sigma * exy;
+        wb1_p[c] = wb1;
+        wb2_p[c] = wb2;
+      }
+      if constexpr (COUPLED) {
+        square_p += step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c];
+        if constexpr (TGV) {
+          square_r += step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]);
+        }
+      }
+      xt_c[c] = xt_n;
+      x_c[c] = x_n;
+      xb_c[c] = xb_n;
+      if constexpr (TGV) {
+        r11_c[c] = r11_n;
+        r12_c[c] = r12_n;
+        r22_c[c] = r22_n;
+      }
+    }
+    float scale_p = 1.0f, scale_r = 1.0f;
+    if constexpr (COUPLED) {
+      scale_p = ball_scale(square_p, P.radius);
+      if constexpr (TGV) scale_r = ball_scale(square_r, P.radius0);
+    }
+    if (!valid) continue;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const std::size_t base = c * plane;
+      float sp = scale_p;
+      if constexpr (!COUPLED) sp = ball_scale(step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c], P.radius);
+      const float q1 = step_p1[c] * sp, q2 = step_p2[c] * sp;
+      P.out.p1[base + here] = rho * q1 + rest * old_p1[c];
+      P.out.p2[base + here] = rho * q2 + rest * old_p2[c];
       if constexpr (KEEP) {
-        P.tilde.r11[base + at] = t11;
-        P.tilde.r22[base + at] = t22;
-        P.tilde.r12[base + at] = t12;
+        P.tilde.p1[base + here] = q1;
+        P.tilde.p2[base + here] = q2;
+      }
+      if constexpr (TGV) {
+        float sr = scale_r;
+        if constexpr (!COUPLED) {
+          sr = ball_scale(
+              step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]), P.radius0);
+        }
+        const float t11 = step_r11[c] * sr, t22 = step_r22[c] * sr, t12 = step_r12[c] * sr;
+        P.out.r11[base + here] = rho * t11 + rest * old_r11[c];
+        P.out.r22[base + here] = rho * t22 + rest * old_r22[c];
+        P.out.r12[base + here] = rho * t12 + rest * old_r12[c];
+        if constexpr (KEEP) {
+          P.tilde.r11[base + here] = t11;
+          P.tilde.r22[base + here] = t22;
+          P.tilde.r12[base + here] = t12;
+        }
       }
     }
   }
@@ -296,8 +359,19 @@ __device__ __forceinline__ double value_term(double zeta, int q, int k, bool fla
   return term;
 }
 
+// A lane per canvas column: a component block covers 8 CC columns, so a warp takes 32 / (8 CC)
+// blocks side by side (one for CC = 3, its last 8 lanes idle), and walks down kPrimalRows block
+// rows. The CC lanes of a cell's columns sum their columns and exchange the sums (in the
+// reference's order: down each column, then across), so every lane of the cell holds the
+// cell means of its mean column; the transposes go through shared memory.
+constexpr int kPrimalRows = 4;
+
 template <int CR, int CC, bool KEEP>
-__global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
+__global__ void __launch_bounds__(256, 2) primal_kernel(const PrimalParams P) {
+  constexpr unsigned kAll = 0xffffffffu;
+  constexpr int L = 8 * CC;                  // lanes of a block
+  constexpr int B = L <= 32 ? 32 / L : 1;    // blocks of a warp
+  constexpr int BH = 8 * CR;                 // canvas rows of a block
   __shared__ ProxFactors F;
   __shared__ float tile[kWarps][4][72];
   {
@@ -307,92 +381,76 @@ __global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
     for (int k = tid; k < static_cast<int>(sizeof(ProxFactors) / 4); k += 256) to[k] = from[k];
   }
   __syncthreads();
-  constexpr int BH = 8 * CR, BW = 8 * CC;
-  const int lane = threadIdx.x, b = lane >> 3, m = lane & 7;
+  const int lane = threadIdx.x;
+  const int blk = lane / L, in_block = lane % L, m = in_block / CC, cell = in_block % CC;
+  const bool used = blk < B;
+  const int leader = lane - cell;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
-  const int vbx = blockIdx.x * 4 + b;
-  const int vby = blockIdx.y * kWarps + threadIdx.y;
-  const bool active = vbx * BW < columns && vby * BH < rows;
-  const int j0 = vbx * BW + m * CC;
-  const int i0 = vby * BH;
-  const bool in_blocks = active && vby < P.component.block_rows && vbx < P.component.block_columns;
+  const int vbx = blockIdx.x * B + blk;
+  const int j = vbx * L + in_block;
+  const bool column_in = used && j < columns;
+  const int jc = column_in ? j : 0;
+  const int first = (blockIdx.y * kWarps + threadIdx.y) * kPrimalRows;
+  const int vbr = rows / BH;
   const float descent = P.descent;
-
-  // v = x + tau g div p over the lane's CR x CC cells of each mean row.
-  float v[BH][CC];
-  float p2_above[CC];
+  float* t = tile[threadIdx.y][used ? blk : 0];
+  float p2_above = (column_in && first > 0 && first < vbr) ? ld(P.p2, static_cast<std::size_t>(first * BH - 1) * pitch + jc) : 0.0f;
+  double sum = 0.0;
+  for (int vby = first; vby < min(first + kPrimalRows, vbr); ++vby) {
+    const int i0 = vby * BH;
+    const bool in_blocks = column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
+    // v = x + tau g div p down the lane's column.
+    float v[BH];
 #pragma unroll
-  for (int c = 0; c < CC; ++c) {
-    const int j = j0 + c;
-    p2_above[c] = (active && i0 > 0) ? ld(P.p2, static_cast<std::size_t>(i0 - 1) * pitch + j) : 0.0f;
-  }
-#pragma unroll
-  for (int r = 0; r < BH; ++r) {
-    const int i = i0 + r;
-    const std::size_t row = static_cast<std::size_t>(i) * pitch;
-    float p1[CC], p2[CC], x[CC];
-#pragma unroll
-    for (int c = 0; c < CC; ++c) {
-      p1[c] = active ? ld(P.p1, row + j0 + c) : 0.0f;
-      p2[c] = active ? ld(P.p2, row + j0 + c) : 0.0f;
-      x[c] = active ? ld(P.x, row + j0 + c) : 0.0f;
-    }
-    float left = __shfl_up_sync(0xffffffffu, p1[CC - 1], 1);
-    if (lane == 0) left = (active && j0 > 0) ? ld(P.p1, row + j0 - 1) : 0.0f;
-#pragma unroll
-    for (int c = 0; c < CC; ++c) {
-      const int j = j0 + c;
-      const float before = c == 0 ? left : p1[c - 1];
+    for (int r = 0; r < BH; ++r) {
+      const int i = i0 + r;
+      const std::size_t at = static_cast<std::size_t>(i) * pitch + jc;
+      const float p1 = column_in ? ld(P.p1, at) : 0.0f;
+      const float p2 = column_in ? ld(P.p2, at) : 0.0f;
+      const float x = column_in ? ld(P.x, at) : 0.0f;
+      float before = __shfl_up_sync(kAll, p1, 1);
+      if (lane == 0) before = (column_in && j > 0) ? ld(P.p1, at - 1) : 0.0f;
       // div p = dy' p2 + dx' p1, backward differences.
-      const float dy = (i + 1 < rows ? p2[c] : 0.0f) - (i > 0 ? p2_above[c] : 0.0f);
-      const float dx = (j + 1 < columns ? p1[c] : 0.0f) - (j > 0 ? before : 0.0f);
-      v[r][c] = x[c] + descent * (dy + dx);
-      p2_above[c] = p2[c];
+      const float dy = (i + 1 < rows ? p2 : 0.0f) - (i > 0 ? p2_above : 0.0f);
+      const float dx = (j + 1 < columns ? p1 : 0.0f) - (j > 0 ? before : 0.0f);
+      v[r] = x + descent * (dy + dx);
+      p2_above = p2;
     }
-  }
-
-  float out[BH][CC];
-  float zeta[8];
-  int levels[8];
-  bool flat = false;
-  const std::size_t block =
-      static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
-  // The middle of the block's DC interval over 8, q Q / 8 + 128, exact in binary32: the
-  // block is transformed centred on it (coefficient_of).
-  const float dc_level = in_blocks ? static_cast<float>(P.component.levels[block * 64]) : 0.0f;
-  const float middle = (dc_level * F.step[0] + 1024.0f) * 0.125f;
-  // The means of the cells (v itself where a cell is one sample), centred.
-  float mean[8];
+    const std::size_t block =
+        static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
+    // The middle of the block's DC interval over 8 (exact): the block is taken centred on it.
+    const float dc_level = in_blocks ? static_cast<float>(P.component.levels[block * 64]) : 0.0f;
+    const float middle = (dc_level * F.step[0] + 1024.0f) * 0.125f;
+    float mean[8];
 #pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    if constexpr (CR == 1 && CC == 1) {
-      mean[r] = v[r][0] - middle;
-    } else {
-      float sum = 0.0f;
+    for (int r = 0; r < 8; ++r) {
+      if constexpr (CR == 1 && CC == 1) {
+        mean[r] = v[r] - middle;
+      } else {
+        float column = v[CR * r];
 #pragma unroll
-      for (int c = 0; c < CC; ++c) {
-        float column = v[CR * r][c];
+        for (int a = 1; a < CR; ++a) column += v[CR * r + a];
+        float total = 0.0f;
 #pragma unroll
-        for (int a = 1; a < CR; ++a) column += v[CR * r + a][c];
-        sum = c == 0 ? column : sum + column;
+        for (int c = 0; c < CC; ++c) {
+          const float part = __shfl_sync(kAll, column, leader + c);
+          total = c == 0 ? part : total + part;
+        }
+        mean[r] = total / static_cast<float>(CR * CC) - middle;
       }
-      mean[r] = sum / static_cast<float>(CR * CC) - middle;
     }
-  }
-  // Column DCT, transpose, row DCT: the lane holds coefficients (v = m, u = 0..7).
-  float col[8], coef[8];
-  forward8(mean, col);
-  float* t = tile[threadIdx.y][b];
+    float col[8], row[8], coef[8], zeta[8];
+    forward8(mean, col);
+    __syncwarp();
+    if (cell == 0 && used) {
 #pragma unroll
-  for (int k = 0; k < 8; ++k) t[k * 9 + m] = col[k];
-  __syncwarp();
-  float row[8];
+      for (int k = 0; k < 8; ++k) t[k * 9 + m] = col[k];
+    }
+    __syncwarp();
 #pragma unroll
-  for (int u = 0; u < 8; ++u) row[u] = t[m * 9 + u];
-  forward8(row, coef);
-  // The clip of the proximal map. Kept coefficients are stored as the map gives them: DC
-  // centred (less q Q + 1024), the others as they are.
-  {
+    for (int u = 0; u < 8; ++u) row[u] = t[m * 9 + u];
+    forward8(row, coef);
+    int levels[8];
     const int4 packed = in_blocks ? __ldg(reinterpret_cast<const int4*>(P.component.levels + block * 64 + m * 8))
                                   : make_int4(0, 0, 0, 0);
     const int words[4] = {packed.x, packed.y, packed.z, packed.w};
@@ -401,7 +459,7 @@ __global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
       const unsigned word = static_cast<unsigned>(words[u >> 1]);
       levels[u] = static_cast<int>(static_cast<std::int16_t>((u & 1) ? (word >> 16) : (word & 0xffffu)));
     }
-    flat = in_blocks && P.component.flat[block] != 0;
+    const bool flat = in_blocks && P.component.flat[block] != 0;
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int k = m * 8 + u;
@@ -412,61 +470,52 @@ __global__ void __launch_bounds__(256) primal_kernel(const PrimalParams P) {
       zeta[u] = prox_of(coef[u], tk, rk, hk, c, F.costed != 0);
     }
     if constexpr (KEEP) {
-      if (in_blocks) {
+      // Kept coefficients as the map gives them: DC centred (less q Q + 1024).
+      if (in_blocks && cell == 0) {
         float4* to = reinterpret_cast<float4*>(P.component.zeta + block * 64 + m * 8);
         to[0] = make_float4(zeta[0], zeta[1], zeta[2], zeta[3]);
         to[1] = make_float4(zeta[4], zeta[5], zeta[6], zeta[7]);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int k = m * 8 + u;
+          const double absolute = k == 0 ? static_cast<double>(zeta[u]) +
+                                               (static_cast<double>(levels[0]) * P.component.constants->step[0] + 1024.0)
+                                         : static_cast<double>(zeta[u]);
+          sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
+        }
+      }
+    }
+    inverse8(zeta, row);
+    __syncwarp();
+    if (cell == 0 && used) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) t[m * 9 + c] = row[c];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 8; ++k) col[k] = t[k * 9 + m];
+    float back[8];
+    inverse8(col, back);
+    if (column_in) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+#pragma unroll
+        for (int a = 0; a < CR; ++a) {
+          const int rr = CR * r + a;
+          float out;
+          if constexpr (CR == 1 && CC == 1) {
+            out = in_blocks ? back[r] + middle : v[rr];
+          } else {
+            out = in_blocks ? v[rr] + (back[r] - mean[r]) : v[rr];
+          }
+          const std::size_t at = static_cast<std::size_t>(i0 + rr) * pitch + jc;
+          P.xt[at] = out;
+          if constexpr (KEEP) P.v[at] = v[rr];
+        }
       }
     }
   }
-  // Inverse row DCT, transpose back, inverse column DCT.
-  inverse8(zeta, row);
-  __syncwarp();
-#pragma unroll
-  for (int c = 0; c < 8; ++c) t[m * 9 + c] = row[c];
-  __syncwarp();
-#pragma unroll
-  for (int k = 0; k < 8; ++k) col[k] = t[k * 9 + m];
-  float back[8];
-  inverse8(col, back);
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    if constexpr (CR == 1 && CC == 1) {
-      out[r][0] = in_blocks ? back[r] + middle : v[r][0];
-    } else {
-      const float change = back[r] - mean[r];
-#pragma unroll
-      for (int a = 0; a < CR; ++a) {
-#pragma unroll
-        for (int c = 0; c < CC; ++c) out[CR * r + a][c] = in_blocks ? v[CR * r + a][c] + change : v[CR * r + a][c];
-      }
-    }
-  }
-  if (active) {
-#pragma unroll
-    for (int r = 0; r < BH; ++r) {
-      const std::size_t at = static_cast<std::size_t>(i0 + r) * pitch + j0;
-#pragma unroll
-      for (int c = 0; c < CC; ++c) {
-        P.xt[at + c] = out[r][c];
-        if constexpr (KEEP) P.v[at + c] = v[r][c];
-      }
-    }
-  }
-  if constexpr (KEEP) {
-    double sum = 0.0;
-    if (in_blocks) {
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int k = m * 8 + u;
-        const double absolute = k == 0 ? static_cast<double>(zeta[u]) + (static_cast<double>(levels[0]) *
-                                                                          P.component.constants->step[0] + 1024.0)
-                                       : static_cast<double>(zeta[u]);
-        sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
-      }
-    }
-    cta_sum(sum, P.partials);
-  }
+  if constexpr (KEEP) cta_sum(sum, P.partials);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -891,10 +940,20 @@ cudaError_t by_cells(int cr, int cc, A&&... args) {
   return cudaErrorInvalidValue;
 }
 
+// The primal kernel's grid: 32 / (8 CC) blocks across a warp, kPrimalRows block rows down it,
+// 8 warps down a CTA.
+dim3 primal_grid(const Geometry& g, int cr, int cc) {
+  const int per_warp = 8 * cc <= 32 ? 32 / (8 * cc) : 1;
+  const int vbc = (g.columns + 8 * cc - 1) / (8 * cc);
+  const int vbr = (g.rows + 8 * cr - 1) / (8 * cr);
+  const int segments = (vbr + kPrimalRows - 1) / kPrimalRows;
+  return dim3((vbc + per_warp - 1) / per_warp, (segments + kWarps - 1) / kWarps, 1);
+}
+
 template <int CR, int CC>
 struct PrimalLaunch {
   static cudaError_t run(const PrimalParams& p, bool keep, cudaStream_t s) {
-    const dim3 grid = block_grid(p.g, p.component);
+    const dim3 grid = primal_grid(p.g, CR, CC);
     if (keep) {
       primal_kernel<CR, CC, true><<<grid, dim3(32, kWarps), 0, s>>>(p);
     } else {
@@ -920,12 +979,18 @@ struct ConjugateLaunch {
   }
 };
 
+// The sweep's grid: a warp per 32 columns and kSegment rows, 8 warps (segments) to a CTA.
+dim3 sweep_grid(const Geometry& g) {
+  const int segments = (g.rows + kSegment - 1) / kSegment;
+  return dim3((g.columns + 31) / 32, (segments + 7) / 8, 1);
+}
+
 template <bool TGV, int C, bool COUPLED>
 cudaError_t dual_keep(const DualParams& p, bool keep, cudaStream_t s) {
   if (keep) {
-    dual_kernel<TGV, C, COUPLED, true><<<pixel_grid(p.g), dim3(32, 8), 0, s>>>(p);
+    dual_stream_kernel<TGV, C, COUPLED, true><<<sweep_grid(p.g), dim3(32, 8), 0, s>>>(p);
   } else {
-    dual_kernel<TGV, C, COUPLED, false><<<pixel_grid(p.g), dim3(32, 8), 0, s>>>(p);
+    dual_stream_kernel<TGV, C, COUPLED, false><<<sweep_grid(p.g), dim3(32, 8), 0, s>>>(p);
   }
   return cudaGetLastError();
 }
@@ -966,7 +1031,7 @@ int dual_grid_blocks(const Geometry& g) {
 }
 int norms_grid_blocks(const Geometry& g) { return dual_grid_blocks(g); }
 int primal_grid_blocks(const Geometry& g, const ComponentDevice& c) {
-  const dim3 d = block_grid(g, c);
+  const dim3 d = primal_grid(g, c.cell_rows, c.cell_columns);
   return static_cast<int>(d.x * d.y);
 }
 int conjugate_grid_blocks(const Geometry& g, const ComponentDevice& c) { return primal_grid_blocks(g, c); }

@@ -8,6 +8,7 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace urb {
@@ -91,6 +92,7 @@ struct DualParams {
   float rest = -0.9f;
   float radius = 1.0f;   // alpha of TV, alpha1 of TGV
   float radius0 = 2.0f;  // alpha0
+  int* error = nullptr;  // set to 1 where a bounded wait of the sweep ran out
 };
 
 // The primal step of iteration n+1 for one channel: v = x + tau gamma div p and its proximal
@@ -182,6 +184,14 @@ cudaError_t launch_project(Fields f, const Geometry& g, bool tgv, bool coupled, 
 cudaError_t launch_norms(const NormParams& p, bool tgv, bool coupled, cudaStream_t stream);
 cudaError_t launch_conjugate(const ConjugateParams& p, cudaStream_t stream);
 cudaError_t launch_residual(const ResidualParams& p, cudaStream_t stream);
+// The dual step as a TMA-fed sweep (sweep.cu): `state` maps the input state's planes (fields x,
+// p1, p2 and for TGV w1, w2, r11, r22, r12, each channel after channel, one allocation), `tilde`
+// the planes of x~.
+std::size_t dual_tma_shared_bytes(bool tgv, int channels);
+bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count);
+cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,
+                            bool coupled, bool keep, cudaStream_t stream);
+
 cudaError_t launch_widen(const float* from, double* to, const Geometry& g, cudaStream_t stream);
 cudaError_t launch_narrow(const double* from, float* to, const Geometry& g, cudaStream_t stream);
 

@@ -43,6 +43,11 @@ struct Solver::Impl {
   std::vector<int> value_written;
   bool tgv = false;
   int current = 0;  // which state holds s_n
+  // The sweep's tensor maps (of each state, and of x~), and its error word.
+  CUtensorMap state_maps[2];
+  CUtensorMap tilde_map;
+  bool swept = false;
+  int* error_word = nullptr;
   Plan plan;
   bool planned = false;
   std::vector<double> host_partials;
@@ -73,24 +78,39 @@ struct Solver::Impl {
     return p;
   }
 
+  // A state's fields in one allocation, each field's channels one after another, in the order
+  // x, p1, p2, w1, w2, r11, r22, r12: the planes of the sweep's TMA box (sweep.cu).
   Fields fields(bool with_tgv) {
     const std::size_t n = g.plane * g.channels;
+    const int count = with_tgv ? 8 : 3;
+    float* block = allocate<float>(n * count);
     Fields f;
-    f.x = allocate<float>(n);
-    f.p1 = allocate<float>(n);
-    f.p2 = allocate<float>(n);
+    if (block == nullptr) return f;
+    f.x = block;
+    f.p1 = block + n;
+    f.p2 = block + 2 * n;
     if (with_tgv) {
-      f.w1 = allocate<float>(n);
-      f.w2 = allocate<float>(n);
-      f.r11 = allocate<float>(n);
-      f.r22 = allocate<float>(n);
-      f.r12 = allocate<float>(n);
+      f.w1 = block + 3 * n;
+      f.w2 = block + 4 * n;
+      f.r11 = block + 5 * n;
+      f.r22 = block + 6 * n;
+      f.r12 = block + 7 * n;
     }
     return f;
   }
 
   bool check(Failure& failure, const char* where) {
     if (error == cudaSuccess) error = cudaGetLastError();
+    if (error == cudaSuccess && error_word != nullptr) {
+      int word = 0;
+      error = cudaMemcpyAsync(&word, error_word, sizeof(int), cudaMemcpyDeviceToHost, stream);
+      if (error == cudaSuccess) error = cudaStreamSynchronize(stream);
+      if (error == cudaSuccess && word != 0) {
+        failure.status = kInternal;
+        failure.message = std::string("the device failed in ") + where + ": a bounded wait of the sweep ran out";
+        return false;
+      }
+    }
     if (error == cudaSuccess) return true;
     failure.status = kInternal;
     failure.message = std::string("the device failed in ") + where + ": " + describe(error);
@@ -132,6 +152,13 @@ struct Solver::Impl {
     state[1] = fields(with_tgv);
     tilde = fields(with_tgv);
     xt = allocate<float>(n);
+    error_word = allocate<int>(1);
+    if (error == cudaSuccess) error = cudaMemsetAsync(error_word, 0, sizeof(int), stream);
+    const int planes = (with_tgv ? 8 : 3) * g.channels;
+    if (error == cudaSuccess) {
+      swept = make_sweep_map(state_maps[0], state[0].x, g, planes) &&
+              make_sweep_map(state_maps[1], state[1].x, g, planes) && make_sweep_map(tilde_map, xt, g, g.channels);
+    }
     v = allocate<float>(n);
     if (with_tgv) div2 = allocate<float>(2 * n);
     canvas = allocate<double>(static_cast<std::size_t>(g.channels) * g.rows * g.columns);
@@ -338,7 +365,11 @@ struct Solver::Impl {
     dp.rest = static_cast<float>(1.0 - plan.relaxation);
     dp.radius = static_cast<float>(tgv ? plan.alpha1 : plan.alpha);
     dp.radius0 = static_cast<float>(plan.alpha0);
-    if (error == cudaSuccess) error = launch_dual(dp, tgv, plan.coupled, keep, stream);
+    dp.error = error_word;
+    if (error == cudaSuccess) {
+      error = swept ? launch_dual_tma(state_maps[current], tilde_map, dp, tgv, plan.coupled, keep, stream)
+                    : launch_dual(dp, tgv, plan.coupled, keep, stream);
+    }
     current = 1 - current;
   }
 

@@ -1,0 +1,394 @@
+// The dual step of an iteration as a TMA-fed sweep (sm_100a).
+//
+// A CTA owns a strip of 32 canvas columns and walks down kStrip rows of it in chunks of 8 rows,
+// one row per warp, a lane per column. Each chunk of every field of every channel -- the state
+// s_{n-1} (x, p, and for TGV w and r) and the carried canvas x~ -- comes into shared memory by two
+// cp.async.bulk.tensor loads of a 3D box (40 columns, the strip and 4 on each side, 8 rows, every
+// plane) into a ring of three slots, so that the loads of chunks k + 2 and k + 3 run while chunk
+// k is computed; each value of HBM is read once (the 8 columns beside the strip come from L2).
+// Neighbours across and down are read from shared memory; w- of the row above a chunk is kept
+// from the chunk before. The arithmetic of each value is the dual step of docs/math.md 5,
+// operation for operation as cpp/src/primal_dual.hpp:572-735 orders it (see kernels.cu).
+//
+// The waits on the ring's mbarriers are bounded: a wait that runs out sets the error word,
+// and the CTA leaves without computing further (the host reports an internal error).
+#include <atomic>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "kernels.hpp"
+
+namespace urb {
+
+namespace {
+
+constexpr int kChunk = 8;    // rows of a chunk, one per warp
+constexpr int kHalo = 4;     // columns loaded left of the strip (16-byte aligned start)
+constexpr int kSpan = 40;    // columns loaded: 4 + 32 + 4
+constexpr int kSlots = 3;    // the ring
+constexpr int kStrip = 256;  // rows a CTA sweeps
+constexpr long long kWaitLimit = 1LL << 22;
+
+__device__ __forceinline__ unsigned smem_address(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void barrier_init(std::uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_address(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void barrier_expect(std::uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_address(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool barrier_try(std::uint64_t* bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_address(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Waits for a phase of a barrier, at most kWaitLimit tries; false where it ran out.
+__device__ __forceinline__ bool barrier_wait(std::uint64_t* bar, unsigned parity) {
+  for (long long k = 0; k < kWaitLimit; ++k) {
+    if (barrier_try(bar, parity)) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void load_box(float* to, const CUtensorMap* map, std::uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_address(to)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_address(bar))
+      : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ T ball(T square, T radius) {
+  const T norm = sqrt(square);
+  return norm > radius ? radius / norm : T(1);
+}
+
+template <bool TGV, int C, bool COUPLED, bool KEEP>
+__global__ void __launch_bounds__(256) dual_tma_kernel(const __grid_constant__ CUtensorMap state_map,
+                                                        const __grid_constant__ CUtensorMap tilde_map,
+                                                        const DualParams P) {
+  constexpr int F = TGV ? 8 : 3;  // state planes per channel: x, p1, p2 (+ w1, w2, r11, r22, r12)
+  constexpr int PLANE = kChunk * kSpan;
+  constexpr int SLOT = (F + 1) * C * PLANE;  // floats: the state planes, then x~'s
+  extern __shared__ __align__(128) float ring[];
+  __shared__ __align__(8) std::uint64_t bars[kSlots];
+  __shared__ float carry[2][C][2][32];  // w- of the row above a chunk, own columns
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+  const std::size_t plane = P.g.plane;
+  const int x0 = blockIdx.x * 32;
+  const int i0 = blockIdx.y * kStrip;
+  const int i1 = min(i0 + kStrip, rows);
+  const int chunks = (i1 - i0 + kChunk - 1) / kChunk;
+  const int j = x0 + lane;
+  const bool valid = j < columns;
+  const int jc = valid ? j : columns - 1;
+  const bool has_left = j > 0, has_right = j + 1 < columns;
+  const int own = kHalo + lane;
+  const float rho = P.rho, rest = P.rest;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kSlots; ++s) barrier_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int k) {
+    if (threadIdx.x == 0 && k <= chunks) {
+      const int slot = k % kSlots;
+      float* to = ring + slot * SLOT;
+      barrier_expect(&bars[slot], SLOT * 4);
+      load_box(to, &state_map, &bars[slot], x0 - kHalo, i0 + k * kChunk, 0);
+      load_box(to + F * C * PLANE, &tilde_map, &bars[slot], x0 - kHalo, i0 + k * kChunk, 0);
+    }
+  };
+  issue(0);
+  issue(1);
+  issue(2);
+
+  // w- of the row above the strip (own columns), from global memory.
+  if (TGV && warp == 0) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      float wb1 = 0.0f, wb2 = 0.0f;
+      if (i0 > 0) {
+        const std::size_t base = c * plane;
+        const int u = i0 - 1;
+        const std::size_t a = static_cast<std::size_t>(u) * pitch + jc;
+        const float a11 = __ldg(P.in.r11 + base + a), a12 = __ldg(P.in.r12 + base + a);
+        const float a22 = __ldg(P.in.r22 + base + a);
+        float d1 = has_right ? __ldg(P.in.r11 + base + a + 1) - a11 : 0.0f;
+        float d2 = has_right ? __ldg(P.in.r12 + base + a + 1) - a12 : 0.0f;
+        d1 = d1 + (__ldg(P.in.r12 + base + a + pitch) - a12);
+        d2 = d2 + (__ldg(P.in.r22 + base + a + pitch) - a22);
+        const float w1 = __ldg(P.in.w1 + base + a), w2 = __ldg(P.in.w2 + base + a);
+        const float t1 = w1 + P.tau[c] * (__ldg(P.in.p1 + base + a) + d1);
+        const float t2 = w2 + P.tau[c] * (__ldg(P.in.p2 + base + a) + d2);
+        wb1 = 2.0f * t1 - w1;
+        wb2 = 2.0f * t2 - w2;
+      }
+      carry[0][c][0][lane] = wb1;
+      carry[0][c][1][lane] = wb2;
+    }
+  }
+  __syncthreads();
+
+  bool failed = false;
+  int stopped = chunks;
+  for (int k = 0; k < chunks; ++k) {
+    const bool ready = barrier_wait(&bars[k % kSlots], (k / kSlots) & 1) &&
+                       barrier_wait(&bars[(k + 1) % kSlots], ((k + 1) / kSlots) & 1);
+    if (__syncthreads_or(!ready)) {
+      failed = true;
+      stopped = k;
+      break;
+    }
+    const float* slot = ring + (k % kSlots) * SLOT;
+    const float* next = ring + ((k + 1) % kSlots) * SLOT;
+    const int i = i0 + k * kChunk + warp;
+    // A field's value in shared memory: plane (field, channel), row r of the chunk (8: the next
+    // chunk's first row), column col of the 40.
+    auto S = [&](int field, int c, int r, int col) -> float {
+      const float* s = r < kChunk ? slot : next;
+      return s[((field * C + c) * kChunk + (r < kChunk ? r : 0)) * kSpan + col];
+    };
+    auto XT = [&](int c, int r, int col) -> float {
+      const float* s = r < kChunk ? slot : next;
+      return s[((F * C + c) * kChunk + (r < kChunk ? r : 0)) * kSpan + col];
+    };
+    if (i < i1) {
+      const bool has_down = i + 1 < rows, has_up = i > 0;
+      const std::size_t here = static_cast<std::size_t>(i) * pitch + jc;
+      float step_p1[C], step_p2[C], old_p1[C], old_p2[C];
+      float step_r11[C], step_r22[C], step_r12[C], old_r11[C], old_r22[C], old_r12[C];
+      float square_p = 0.0f, square_r = 0.0f;
+      const int r = warp;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const std::size_t base = c * plane;
+        const float xt0 = XT(c, r, own), x0v = S(0, c, r, own);
+        const float bar = 2.0f * xt0 - x0v;
+        const float gx = has_right ? (2.0f * XT(c, r, own + 1) - S(0, c, r, own + 1)) - bar : 0.0f;
+        const float gy = has_down ? (2.0f * XT(c, r + 1, own) - S(0, c, r + 1, own)) - bar : 0.0f;
+        if (valid) P.out.x[base + here] = rho * xt0 + rest * x0v;
+        const float p1 = S(1, c, r, own), p2 = S(2, c, r, own);
+        old_p1[c] = p1;
+        old_p2[c] = p2;
+        const float sigma = P.sigma[c];
+        if constexpr (!TGV) {
+          step_p1[c] = p1 + sigma * gx;
+          step_p2[c] = p2 + sigma * gy;
+        } else {
+          const float tau = P.tau[c];
+          // w~ at (i, col): w + tau g (p + div2 r), div2 r by forward differences.
+          auto w_tilde = [&](int rr, int col, int ii, int jj, float& t1, float& t2, float& w1, float& w2) {
+            const float r11 = S(5, c, rr, col), r22 = S(6, c, rr, col), r12 = S(7, c, rr, col);
+            float d1 = jj + 1 < columns ? S(5, c, rr, col + 1) - r11 : 0.0f;
+            float d2 = jj + 1 < columns ? S(7, c, rr, col + 1) - r12 : 0.0f;
+            d1 = d1 + (ii + 1 < rows ? S(7, c, rr + 1, col) - r12 : 0.0f);
+            d2 = d2 + (ii + 1 < rows ? S(6, c, rr + 1, col) - r22 : 0.0f);
+            w1 = S(3, c, rr, col);
+            w2 = S(4, c, rr, col);
+            t1 = w1 + tau * (S(1, c, rr, col) + d1);
+            t2 = w2 + tau * (S(2, c, rr, col) + d2);
+          };
+          float t1, t2, w1, w2;
+          w_tilde(r, own, i, j, t1, t2, w1, w2);
+          const float wb1 = 2.0f * t1 - w1, wb2 = 2.0f * t2 - w2;
+          if (valid) {
+            P.out.w1[base + here] = rho * t1 + rest * w1;
+            P.out.w2[base + here] = rho * t2 + rest * w2;
+            if constexpr (KEEP) {
+              P.tilde.w1[base + here] = t1;
+              P.tilde.w2[base + here] = t2;
+            }
+          }
+          float wl1 = 0.0f, wl2 = 0.0f;
+          if (has_left) {
+            float lt1, lt2, lw1, lw2;
+            w_tilde(r, own - 1, i, j - 1, lt1, lt2, lw1, lw2);
+            wl1 = 2.0f * lt1 - lw1;
+            wl2 = 2.0f * lt2 - lw2;
+          }
+          float wu1 = 0.0f, wu2 = 0.0f;
+          if (has_up) {
+            if (r > 0) {
+              float ut1, ut2, uw1, uw2;
+              w_tilde(r - 1, own, i - 1, j, ut1, ut2, uw1, uw2);
+              wu1 = 2.0f * ut1 - uw1;
+              wu2 = 2.0f * ut2 - uw2;
+            } else {
+              wu1 = carry[k & 1][c][0][lane];
+              wu2 = carry[k & 1][c][1][lane];
+            }
+          }
+          if (r == kChunk - 1) {
+            carry[(k + 1) & 1][c][0][lane] = wb1;
+            carry[(k + 1) & 1][c][1][lane] = wb2;
+          }
+          step_p1[c] = p1 + sigma * (gx - wb1);
+          step_p2[c] = p2 + sigma * (gy - wb2);
+          const float own1x = has_right ? wb1 : 0.0f, own2x = has_right ? wb2 : 0.0f;
+          const float own1y = has_down ? wb1 : 0.0f, own2y = has_down ? wb2 : 0.0f;
+          const float exx = own1x - wl1;
+          const float eyy = own2y - wu2;
+          const float exy = 0.5f * ((own1y - wu1) + (own2x - wl2));
+          const float r11 = S(5, c, r, own), r22 = S(6, c, r, own), r12 = S(7, c, r, own);
+          old_r11[c] = r11;
+          old_r22[c] = r22;
+          old_r12[c] = r12;
+          step_r11[c] = r11 + sigma * exx;
+          step_r22[c] = r22 + sigma * eyy;
+          step_r12[c] = r12 + sigma * exy;
+        }
+        if constexpr (COUPLED) {
+          square_p += step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c];
+          if constexpr (TGV) {
+            square_r += step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]);
+          }
+        }
+      }
+      float scale_p = 1.0f, scale_r = 1.0f;
+      if constexpr (COUPLED) {
+        scale_p = ball(square_p, P.radius);
+        if constexpr (TGV) scale_r = ball(square_r, P.radius0);
+      }
+      if (valid) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const std::size_t base = c * plane;
+          float sp = scale_p;
+          if constexpr (!COUPLED) sp = ball(step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c], P.radius);
+          const float q1 = step_p1[c] * sp, q2 = step_p2[c] * sp;
+          P.out.p1[base + here] = rho * q1 + rest * old_p1[c];
+          P.out.p2[base + here] = rho * q2 + rest * old_p2[c];
+          if constexpr (KEEP) {
+            P.tilde.p1[base + here] = q1;
+            P.tilde.p2[base + here] = q2;
+          }
+          if constexpr (TGV) {
+            float sr = scale_r;
+            if constexpr (!COUPLED) {
+              sr = ball(step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]),
+                        P.radius0);
+            }
+            const float t11 = step_r11[c] * sr, t22 = step_r22[c] * sr, t12 = step_r12[c] * sr;
+            P.out.r11[base + here] = rho * t11 + rest * old_r11[c];
+            P.out.r22[base + here] = rho * t22 + rest * old_r22[c];
+            P.out.r12[base + here] = rho * t12 + rest * old_r12[c];
+            if constexpr (KEEP) {
+              P.tilde.r11[base + here] = t11;
+              P.tilde.r22[base + here] = t22;
+              P.tilde.r12[base + here] = t12;
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();  // every warp is done with slot k
+    issue(k + kSlots);
+  }
+  if (failed && threadIdx.x == 0 && P.error != nullptr) atomicExch(P.error, 1);
+  // No load may still write into shared memory when the CTA leaves: wait (bounded) for every
+  // chunk issued and not consumed.
+  if (failed) {
+    for (int k = stopped; k <= min(stopped + kSlots - 1, chunks); ++k) barrier_wait(&bars[k % kSlots], (k / kSlots) & 1);
+  }
+}
+
+}  // namespace
+
+std::size_t dual_tma_shared_bytes(bool tgv, int channels) {
+  const int fields = tgv ? 8 : 3;
+  return static_cast<std::size_t>(kSlots) * (fields + 1) * channels * kChunk * kSpan * sizeof(float);
+}
+
+namespace {
+
+template <bool TGV, int C, bool COUPLED, bool KEEP>
+cudaError_t launch_one(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, cudaStream_t s) {
+  auto kernel = dual_tma_kernel<TGV, C, COUPLED, KEEP>;
+  const std::size_t bytes = dual_tma_shared_bytes(TGV, C);
+  // The shared-memory size above 48 KB is set once per device.
+  static std::atomic<unsigned long long> configured{0};
+  int device = 0;
+  cudaGetDevice(&device);
+  const unsigned long long bit = 1ull << (device & 63);
+  if ((configured.load() & bit) == 0) {
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(bytes));
+    if (e != cudaSuccess) return e;
+    configured.fetch_or(bit);
+  }
+  const dim3 grid((p.g.columns + 31) / 32, (p.g.rows + kStrip - 1) / kStrip, 1);
+  kernel<<<grid, 256, bytes, s>>>(state, tilde, p);
+  return cudaGetLastError();
+}
+
+template <bool TGV, int C, bool COUPLED>
+cudaError_t launch_keep(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool keep,
+                        cudaStream_t s) {
+  return keep ? launch_one<TGV, C, COUPLED, true>(state, tilde, p, s)
+              : launch_one<TGV, C, COUPLED, false>(state, tilde, p, s);
+}
+
+template <bool TGV>
+cudaError_t launch_channels(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool coupled,
+                            bool keep, cudaStream_t s) {
+  switch (p.g.channels) {
+    case 1: return launch_keep<TGV, 1, false>(state, tilde, p, keep, s);
+    case 2: return coupled ? launch_keep<TGV, 2, true>(state, tilde, p, keep, s)
+                           : launch_keep<TGV, 2, false>(state, tilde, p, keep, s);
+    case 3: return coupled ? launch_keep<TGV, 3, true>(state, tilde, p, keep, s)
+                           : launch_keep<TGV, 3, false>(state, tilde, p, keep, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 function = [] {
+    void* found = nullptr;
+    cudaDriverEntryPointQueryResult status;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &found, cudaEnableDefault, &status) != cudaSuccess ||
+        status != cudaDriverEntryPointSuccess) {
+      return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(found);
+  }();
+  return function;
+}
+
+}  // namespace
+
+bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count) {
+  PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
+  if (encode == nullptr) return false;
+  const cuuint64_t dims[3] = {static_cast<cuuint64_t>(g.columns), static_cast<cuuint64_t>(g.rows),
+                              static_cast<cuuint64_t>(count)};
+  const cuuint64_t strides[2] = {static_cast<cuuint64_t>(g.pitch) * sizeof(float), g.plane * sizeof(float)};
+  const cuuint32_t box[3] = {kSpan, kChunk, static_cast<cuuint32_t>(count)};
+  const cuuint32_t steps[3] = {1, 1, 1};
+  const CUresult result = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(planes), dims, strides,
+                                 box, steps, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return result == CUDA_SUCCESS;
+}
+
+cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,
+                            bool coupled, bool keep, cudaStream_t stream) {
+  return tgv ? launch_channels<true>(state, tilde, p, coupled, keep, stream)
+             : launch_channels<false>(state, tilde, p, coupled, keep, stream);
+}
+
+}  // namespace urb
