@@ -15,10 +15,12 @@
 // column/row and the neighbour before the first.
 #include "kernels.hpp"
 
+#include <atomic>
 #include <cfloat>
 #include <cstdint>
 
 #include "dct.cuh"
+#include "tma.cuh"
 
 namespace urb {
 
@@ -516,6 +518,207 @@ __global__ void __launch_bounds__(256, 2) primal_kernel(const PrimalParams P) {
     }
   }
   if constexpr (KEEP) cta_sum(sum, P.partials);
+}
+
+// The primal step fed by TMA: a CTA owns a strip of 32 canvas columns and walks down it by
+// stages of 64 canvas rows (8 / CR block rows, a warp each) and the row above them, every
+// stage one 3D box of the channel's x, p1 and p2 planes (40 columns: the strip and 4 on each
+// side) into a ring of two slots, the next stage's load running while a stage is computed.
+// The computation of a block row is primal_kernel's, from shared memory.
+constexpr int kStageRows = 64;
+constexpr int kPrimalStages = 4;  // stages of a CTA's strip
+
+template <int CR>
+constexpr int primal_warps() {
+  return kStageRows / (8 * CR);
+}
+
+template <int CR, int CC, bool KEEP>
+__global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(const __grid_constant__ CUtensorMap map,
+                                                                             const PrimalParams P) {
+  constexpr unsigned kAll = 0xffffffffu;
+  constexpr int NB = primal_warps<CR>();
+  constexpr int L = 8 * CC, B = 32 / L, BH = 8 * CR;
+  constexpr int SR = kStageRows + 1, SPAN = 40, HALO = 4;
+  constexpr int PLANE = SR * SPAN, SLOT = 3 * PLANE;
+  // Slots 128-byte aligned, as a bulk-tensor copy's shared-memory destination is.
+  constexpr int STRIDE = (SLOT + 31) / 32 * 32;
+  extern __shared__ __align__(128) float ring[];
+  __shared__ __align__(8) std::uint64_t bars[2];
+  __shared__ ProxFactors F;
+  __shared__ float tile[NB][4][72];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  {
+    const float* from = reinterpret_cast<const float*>(P.component.factors);
+    float* to = reinterpret_cast<float*>(&F);
+    for (int k = tid; k < static_cast<int>(sizeof(ProxFactors) / 4); k += 32 * NB) to[k] = from[k];
+  }
+  if (tid == 0) {
+    barrier_init(&bars[0], 1);
+    barrier_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+  const int vbr = rows / BH;
+  const int x0 = blockIdx.x * 32;
+  const int first = blockIdx.y * kPrimalStages * NB;  // the CTA's first block row
+  const int stages = min(kPrimalStages, (vbr - first + NB - 1) / NB);
+  auto issue = [&](int s) {
+    if (tid == 0 && s < stages) {
+      barrier_expect(&bars[s & 1], SLOT * 4);
+      load_box(ring + (s & 1) * STRIDE, &map, &bars[s & 1], x0 - HALO, (first + s * NB) * BH - 1, 0);
+    }
+  };
+  issue(0);
+  issue(1);
+  const int blk = lane / L, in_block = lane % L, m = in_block / CC, cell = in_block % CC;
+  const int leader = lane - cell;
+  const int vbx = blockIdx.x * B + blk;
+  const int j = vbx * L + in_block;
+  const bool column_in = j < columns;
+  const int col = HALO + lane;
+  const float descent = P.descent;
+  float* t = tile[warp][blk];
+  double sum = 0.0;
+  bool failed = false;
+  int stopped = stages;
+  for (int s = 0; s < stages; ++s) {
+    const bool ready = barrier_wait(&bars[s & 1], (s >> 1) & 1);
+    if (__syncthreads_or(!ready)) {
+      failed = true;
+      stopped = s;
+      break;
+    }
+    const float* slot = ring + (s & 1) * STRIDE;
+    const int vby = first + s * NB + warp;
+    if (vby < vbr) {
+      const int i0 = vby * BH;
+      const int base_row = 1 + warp * BH;  // shared-memory row of canvas row i0
+      const bool in_blocks = column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
+      float v[BH];
+#pragma unroll
+      for (int r = 0; r < BH; ++r) {
+        const int i = i0 + r, sr = base_row + r;
+        const float x = slot[0 * PLANE + sr * SPAN + col];
+        const float p1 = slot[1 * PLANE + sr * SPAN + col];
+        const float p2 = slot[2 * PLANE + sr * SPAN + col];
+        const float before = slot[1 * PLANE + sr * SPAN + col - 1];
+        const float above = slot[2 * PLANE + (sr - 1) * SPAN + col];
+        const float dy = (i + 1 < rows ? p2 : 0.0f) - (i > 0 ? above : 0.0f);
+        const float dx = (j + 1 < columns ? p1 : 0.0f) - (j > 0 ? before : 0.0f);
+        v[r] = x + descent * (dy + dx);
+      }
+      const std::size_t block =
+          static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
+      const float dc_level = in_blocks ? static_cast<float>(P.component.levels[block * 64]) : 0.0f;
+      const float middle = (dc_level * F.step[0] + 1024.0f) * 0.125f;
+      float mean[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        if constexpr (CR == 1 && CC == 1) {
+          mean[r] = v[r] - middle;
+        } else {
+          float column = v[CR * r];
+#pragma unroll
+          for (int a = 1; a < CR; ++a) column += v[CR * r + a];
+          float total = 0.0f;
+#pragma unroll
+          for (int c = 0; c < CC; ++c) {
+            const float part = __shfl_sync(kAll, column, leader + c);
+            total = c == 0 ? part : total + part;
+          }
+          mean[r] = total / static_cast<float>(CR * CC) - middle;
+        }
+      }
+      float colv[8], row[8], coef[8], zeta[8];
+      forward8(mean, colv);
+      __syncwarp();
+      if (cell == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t[k * 9 + m] = colv[k];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < 8; ++u) row[u] = t[m * 9 + u];
+      forward8(row, coef);
+      int levels[8];
+      const int4 packed = in_blocks ? __ldg(reinterpret_cast<const int4*>(P.component.levels + block * 64 + m * 8))
+                                    : make_int4(0, 0, 0, 0);
+      const int words[4] = {packed.x, packed.y, packed.z, packed.w};
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const unsigned word = static_cast<unsigned>(words[u >> 1]);
+        levels[u] = static_cast<int>(static_cast<std::int16_t>((u & 1) ? (word >> 16) : (word & 0xffffu)));
+      }
+      const bool flat = in_blocks && P.component.flat[block] != 0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = m * 8 + u;
+        const Coefficient c = coefficient_of(levels[u], k, F);
+        const float tk = flat ? F.t_flat[k] : F.t[k];
+        const float rk = flat ? F.r_flat[k] : F.r[k];
+        const float hk = flat ? F.h_flat[k] : F.h[k];
+        zeta[u] = prox_of(coef[u], tk, rk, hk, c, F.costed != 0);
+      }
+      if constexpr (KEEP) {
+        if (in_blocks && cell == 0) {
+          float4* to = reinterpret_cast<float4*>(P.component.zeta + block * 64 + m * 8);
+          to[0] = make_float4(zeta[0], zeta[1], zeta[2], zeta[3]);
+          to[1] = make_float4(zeta[4], zeta[5], zeta[6], zeta[7]);
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int k = m * 8 + u;
+            const double absolute =
+                k == 0 ? static_cast<double>(zeta[u]) +
+                             (static_cast<double>(levels[0]) * P.component.constants->step[0] + 1024.0)
+                       : static_cast<double>(zeta[u]);
+            sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
+          }
+        }
+      }
+      inverse8(zeta, row);
+      __syncwarp();
+      if (cell == 0) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) t[m * 9 + c] = row[c];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < 8; ++k) colv[k] = t[k * 9 + m];
+      float back[8];
+      inverse8(colv, back);
+      if (column_in) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+#pragma unroll
+          for (int a = 0; a < CR; ++a) {
+            const int rr = CR * r + a;
+            float out;
+            if constexpr (CR == 1 && CC == 1) {
+              out = in_blocks ? back[r] + middle : v[rr];
+            } else {
+              out = in_blocks ? v[rr] + (back[r] - mean[r]) : v[rr];
+            }
+            const std::size_t at = static_cast<std::size_t>(i0 + rr) * pitch + j;
+            P.xt[at] = out;
+            if constexpr (KEEP) P.v[at] = v[rr];
+          }
+        }
+      }
+    }
+    __syncthreads();  // every warp is done with the slot
+    issue(s + 2);
+  }
+  if (failed) {
+    if (tid == 0 && P.error != nullptr) atomicExch(P.error, 1);
+  }
+  if constexpr (KEEP) cta_sum(sum, P.partials);
+  if (failed) {
+    // No load may still write into shared memory when the CTA leaves: the stage that was not
+    // ready and the one after it.
+    for (int s = stopped; s < min(stopped + 2, stages); ++s) barrier_wait(&bars[s & 1], (s >> 1) & 1);
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1039,6 +1242,58 @@ int start_grid_blocks(const ComponentDevice& c) { return (c.block_rows * c.block
 
 cudaError_t launch_dual(const DualParams& p, bool tgv, bool coupled, bool keep, cudaStream_t stream) {
   return tgv ? dual_channels<true>(p, coupled, keep, stream) : dual_channels<false>(p, coupled, keep, stream);
+}
+
+namespace {
+
+dim3 primal_tma_grid(const Geometry& g, int cr) {
+  const int nb = kStageRows / (8 * cr);
+  const int vbr = g.rows / (8 * cr);
+  return dim3((g.columns + 31) / 32, (vbr + kPrimalStages * nb - 1) / (kPrimalStages * nb), 1);
+}
+
+template <int CR, int CC, bool KEEP>
+cudaError_t primal_tma_one(const CUtensorMap& map, const PrimalParams& p, cudaStream_t s) {
+  auto kernel = primal_tma_kernel<CR, CC, KEEP>;
+  constexpr std::size_t bytes = 2 * ((3 * (kStageRows + 1) * 40 + 31) / 32 * 32) * sizeof(float);
+  static std::atomic<unsigned long long> configured{0};
+  int device = 0;
+  cudaGetDevice(&device);
+  const unsigned long long bit = 1ull << (device & 63);
+  if ((configured.load() & bit) == 0) {
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (e != cudaSuccess) return e;
+    configured.fetch_or(bit);
+  }
+  kernel<<<primal_tma_grid(p.g, CR), 32 * primal_warps<CR>(), bytes, s>>>(map, p);
+  return cudaGetLastError();
+}
+
+template <int CR, int CC>
+cudaError_t primal_tma_keep(const CUtensorMap& map, const PrimalParams& p, bool keep, cudaStream_t s) {
+  return keep ? primal_tma_one<CR, CC, true>(map, p, s) : primal_tma_one<CR, CC, false>(map, p, s);
+}
+
+}  // namespace
+
+bool primal_tma_takes(const ComponentDevice& c) {
+  auto fits = [](int n) { return n == 1 || n == 2 || n == 4; };
+  return fits(c.cell_rows) && fits(c.cell_columns);
+}
+
+int primal_tma_grid_blocks(const Geometry& g, const ComponentDevice& c) {
+  const dim3 d = primal_tma_grid(g, c.cell_rows);
+  return static_cast<int>(d.x * d.y);
+}
+
+cudaError_t launch_primal_tma(const CUtensorMap& map, const PrimalParams& p, bool keep, cudaStream_t stream) {
+  const int cr = p.component.cell_rows, cc = p.component.cell_columns;
+#define URB_TMA_CELL(R, C) \
+  if (cr == R && cc == C) return primal_tma_keep<R, C>(map, p, keep, stream);
+  URB_TMA_CELL(1, 1) URB_TMA_CELL(1, 2) URB_TMA_CELL(2, 1) URB_TMA_CELL(2, 2) URB_TMA_CELL(1, 4) URB_TMA_CELL(4, 1)
+  URB_TMA_CELL(2, 4) URB_TMA_CELL(4, 2) URB_TMA_CELL(4, 4)
+#undef URB_TMA_CELL
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_primal(const PrimalParams& p, bool keep, cudaStream_t stream) {

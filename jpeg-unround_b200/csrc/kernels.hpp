@@ -108,6 +108,7 @@ struct PrimalParams {
   float* v = nullptr;
   double* partials = nullptr;
   float descent = 0.0f;  // tau gamma_c
+  int* error = nullptr;  // set to 1 where a bounded wait of the TMA path ran out
 };
 
 // The records (docs/math.md 6): sums over the canvas in binary64 from the binary32 tilde
@@ -189,6 +190,12 @@ cudaError_t launch_residual(const ResidualParams& p, cudaStream_t stream);
 // the planes of x~.
 std::size_t dual_tma_shared_bytes(bool tgv, int channels);
 bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count);
+// The primal step fed by TMA: `map` boxes the channel's x, p1 and p2 planes (make_primal_map,
+// planes `stride` floats apart). Cells of 1, 2 or 4 samples each way; others take launch_primal.
+bool make_primal_map(CUtensorMap& map, const float* x, const Geometry& g, std::size_t stride);
+bool primal_tma_takes(const ComponentDevice& c);
+int primal_tma_grid_blocks(const Geometry& g, const ComponentDevice& c);
+cudaError_t launch_primal_tma(const CUtensorMap& map, const PrimalParams& p, bool keep, cudaStream_t stream);
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,
                             bool coupled, bool keep, cudaStream_t stream);
 

@@ -47,6 +47,8 @@ struct Solver::Impl {
   CUtensorMap state_maps[2];
   CUtensorMap tilde_map;
   bool swept = false;
+  CUtensorMap primal_maps[2][kMaxChannels];
+  bool primal_swept[kMaxChannels] = {};
   int* error_word = nullptr;
   Plan plan;
   bool planned = false;
@@ -158,6 +160,14 @@ struct Solver::Impl {
     if (error == cudaSuccess) {
       swept = make_sweep_map(state_maps[0], state[0].x, g, planes) &&
               make_sweep_map(state_maps[1], state[1].x, g, planes) && make_sweep_map(tilde_map, xt, g, g.channels);
+      // The primal step's maps: a channel's x, p1 and p2 planes, `channels` planes apart.
+      for (std::size_t c = 0; c < components.size(); ++c) {
+        bool made = primal_tma_takes(components[c]);
+        for (int s = 0; s < 2 && made; ++s) {
+          made = make_primal_map(primal_maps[s][c], state[s].x + c * g.plane, g, g.plane * g.channels);
+        }
+        primal_swept[c] = made;
+      }
     }
     v = allocate<float>(n);
     if (with_tgv) div2 = allocate<float>(2 * n);
@@ -166,7 +176,7 @@ struct Solver::Impl {
     for (const ComponentDevice& d : components) {
       most = std::max<std::size_t>(most, conjugate_grid_blocks(g, d));
       most = std::max<std::size_t>(most, start_grid_blocks(d));
-      const int count = std::max(primal_grid_blocks(g, d), start_grid_blocks(d));
+      const int count = std::max({primal_grid_blocks(g, d), primal_tma_grid_blocks(g, d), start_grid_blocks(d)});
       value_counts.push_back(count);
       value_written.push_back(0);
     }
@@ -345,8 +355,14 @@ struct Solver::Impl {
       pp.v = v + base;
       pp.partials = value_slot(c);
       pp.descent = static_cast<float>(plan.tau * plan.channel_weights[c]);
-      if (error == cudaSuccess) error = launch_primal(pp, keep, stream);
-      if (keep) value_written[c] = primal_grid_blocks(g, components[c]);
+      pp.error = error_word;
+      if (primal_swept[c]) {
+        if (error == cudaSuccess) error = launch_primal_tma(primal_maps[current][c], pp, keep, stream);
+        if (keep) value_written[c] = primal_tma_grid_blocks(g, components[c]);
+      } else {
+        if (error == cudaSuccess) error = launch_primal(pp, keep, stream);
+        if (keep) value_written[c] = primal_grid_blocks(g, components[c]);
+      }
     }
   }
 

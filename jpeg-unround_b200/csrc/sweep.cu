@@ -18,6 +18,7 @@
 #include <cudaTypedefs.h>
 
 #include "kernels.hpp"
+#include "tma.cuh"
 
 namespace urb {
 
@@ -28,46 +29,6 @@ constexpr int kHalo = 4;     // columns loaded left of the strip (16-byte aligne
 constexpr int kSpan = 40;    // columns loaded: 4 + 32 + 4
 constexpr int kSlots = 3;    // the ring
 constexpr int kStrip = 256;  // rows a CTA sweeps
-constexpr long long kWaitLimit = 1LL << 22;
-
-__device__ __forceinline__ unsigned smem_address(const void* p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void barrier_init(std::uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_address(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void barrier_expect(std::uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_address(bar)), "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ bool barrier_try(std::uint64_t* bar, unsigned parity) {
-  unsigned done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done)
-      : "r"(smem_address(bar)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
-// Waits for a phase of a barrier, at most kWaitLimit tries; false where it ran out.
-__device__ __forceinline__ bool barrier_wait(std::uint64_t* bar, unsigned parity) {
-  for (long long k = 0; k < kWaitLimit; ++k) {
-    if (barrier_try(bar, parity)) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void load_box(float* to, const CUtensorMap* map, std::uint64_t* bar, int x, int y, int z) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-      "[%5];" ::"r"(smem_address(to)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_address(bar))
-      : "memory");
-}
 
 template <typename T>
 __device__ __forceinline__ T ball(T square, T radius) {
@@ -371,18 +332,33 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
 
 }  // namespace
 
-bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count) {
+namespace {
+
+// A 3D tiled map of `count` float planes `stride` floats apart, each the canvas's rows x columns
+// (rows `pitch` apart), boxes of 40 columns x `box_rows` rows x every plane.
+bool make_map(CUtensorMap& map, const float* planes, const Geometry& g, int count, std::size_t stride,
+              unsigned box_rows) {
   PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
   if (encode == nullptr) return false;
   const cuuint64_t dims[3] = {static_cast<cuuint64_t>(g.columns), static_cast<cuuint64_t>(g.rows),
                               static_cast<cuuint64_t>(count)};
-  const cuuint64_t strides[2] = {static_cast<cuuint64_t>(g.pitch) * sizeof(float), g.plane * sizeof(float)};
-  const cuuint32_t box[3] = {kSpan, kChunk, static_cast<cuuint32_t>(count)};
+  const cuuint64_t strides[2] = {static_cast<cuuint64_t>(g.pitch) * sizeof(float), stride * sizeof(float)};
+  const cuuint32_t box[3] = {kSpan, box_rows, static_cast<cuuint32_t>(count)};
   const cuuint32_t steps[3] = {1, 1, 1};
   const CUresult result = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(planes), dims, strides,
                                  box, steps, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return result == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count) {
+  return make_map(map, planes, g, count, g.plane, kChunk);
+}
+
+bool make_primal_map(CUtensorMap& map, const float* x, const Geometry& g, std::size_t stride) {
+  return make_map(map, x, g, 3, stride, 65);
 }
 
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,
