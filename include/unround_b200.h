@@ -54,6 +54,17 @@ unround_status unround_b200_measure(const unround_input* input, const unround_se
                                     uint64_t iterations, unround_b200_timing* timing, unround_result** result,
                                     char* message, size_t message_size);
 
+/* What the host model makes of an input and settings, without a GPU (the reference computes the
+ * same in Problem::make, cpp/src/model.cpp:134-256, and plan, cpp/src/pdhg.cpp:147-233): of
+ * component `component`, `which` 0 the lower ends of the intervals, 1 the upper ends, 2 the
+ * centres (one per coefficient); 3 the steps, 4 the weights, 5 the weights of flat blocks (64);
+ * 6 whether each block is flat (1 or 0, one per block); 7 the plan: tau, sigma, the most
+ * iterations and the tolerance (4). Writes at most `capacity` doubles into `out` and the count
+ * into *count (out may be null to ask for the count). */
+unround_status unround_b200_model(const unround_input* input, const unround_settings* settings, uint64_t component,
+                                  int32_t which, double* out, uint64_t capacity, uint64_t* count, char* message,
+                                  size_t message_size);
+
 #ifdef __cplusplus
 }
 #endif

@@ -401,6 +401,55 @@ unround_status unround_b200_measure(const unround_input* input, const unround_se
   });
 }
 
+unround_status unround_b200_model(const unround_input* input, const unround_settings* settings, uint64_t component,
+                                  int32_t which, double* out, uint64_t capacity, uint64_t* count, char* message,
+                                  size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (input == nullptr || settings == nullptr) {
+      failure = {urb::kArgument, "the input and the settings are not null pointers"};
+      return false;
+    }
+    std::vector<urb::ComponentInput> inputs;
+    if (!inputs_of(input, inputs, failure)) return false;
+    const urb::Settings& s = settings->settings;
+    auto frame = urb::make_frame(input->height, input->width, input->color_space, inputs, s, failure);
+    if (!frame) return false;
+    if (component >= frame->channels() || which < 0 || which > 7) {
+      failure = {urb::kArgument, "no such component or value of the model"};
+      return false;
+    }
+    const urb::Component& c = frame->components[component];
+    std::vector<double> values;
+    if (which <= 2) {
+      values.resize(c.coefficient_count());
+      for (std::size_t at = 0; at < values.size(); ++at) {
+        const int k = static_cast<int>(at % 64);
+        values[at] = which == 0 ? c.lower(c.levels[at], k) : which == 1 ? c.upper(c.levels[at], k)
+                                                                          : c.centre(c.levels[at], k);
+      }
+    } else if (which == 3) {
+      values.assign(c.steps.begin(), c.steps.end());
+    } else if (which == 4) {
+      values.assign(c.weights.begin(), c.weights.end());
+    } else if (which == 5) {
+      values.assign(c.flat_weights.begin(), c.flat_weights.end());
+    } else if (which == 6) {
+      values.assign(c.flat.begin(), c.flat.end());
+    } else {
+      if (s.method != urb::Method::tv && s.method != urb::Method::tgv) {
+        failure = {urb::kOptions, "a plan is of the primal-dual methods, tv or tgv"};
+        return false;
+      }
+      auto plan = urb::make_plan(s, frame->channels(), failure);
+      if (!plan) return false;
+      values = {plan->tau, plan->sigma, static_cast<double>(plan->iterations), plan->tolerance};
+    }
+    if (count != nullptr) *count = values.size();
+    if (out != nullptr) std::copy_n(values.begin(), std::min<std::size_t>(values.size(), capacity), out);
+    return true;
+  });
+}
+
 unround_status unround_project(const uint8_t*, size_t, const unround_settings*, const double*, uint64_t, uint64_t,
                                uint64_t, unround_result**, char* message, size_t message_size) {
   say(message, message_size, "projecting onto a JPEG file's intervals needs libjpeg-turbo, which this build does "

@@ -46,6 +46,7 @@ __all__ = [
     "held_options",
     "library_path",
     "measure",
+    "model",
     "options",
     "project",
     "solve",
@@ -194,6 +195,7 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_b200_solve_from": (i32, ctypes.POINTER(_Input), handle, ctypes.POINTER(_Start), *made),
         "unround_b200_measure": (i32, ctypes.POINTER(_Input), handle, u64, u64, ctypes.POINTER(_Timing),
                                  ctypes.POINTER(handle), *text),
+        "unround_b200_model": (i32, ctypes.POINTER(_Input), handle, u64, i32, doubles, u64, u64p, *text),
     }
     for name, (result, *arguments) in table.items():
         function = getattr(library, name)
@@ -578,6 +580,28 @@ def measure(image: jpegio.Image, settings: Settings | list[str] | None = None, *
         if result:
             library.unround_result_free(made)
         del kept
+
+
+def model(image: jpegio.Image, settings: Settings | list[str] | None = None, component: int = 0,
+          which: int = 0) -> npt.NDArray[np.float64]:
+    """What the host model makes of the input, without a GPU (include/unround_b200.h,
+    unround_b200_model): which 0/1/2 the intervals' ends and centres, 3/4/5 steps, weights and
+    flat blocks' weights, 6 the flat blocks, 7 the plan (tau, sigma, iterations, tolerance)."""
+    library = _library()
+    handle = _settings_of(settings)
+    given, kept = _input_of(image)
+    count = ctypes.c_uint64()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_b200_model(ctypes.byref(given), handle.handle, component, which, None, 0,
+                                        ctypes.byref(count), message, _MESSAGE)
+    _raise(status, message)
+    out = np.empty(int(count.value))
+    status = library.unround_b200_model(ctypes.byref(given), handle.handle, component, which,
+                                        out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size,
+                                        ctypes.byref(count), message, _MESSAGE)
+    _raise(status, message)
+    del kept
+    return out
 
 
 def decode(source: object, settings: Settings | None = None, **_: object) -> Decoded:

@@ -1,0 +1,108 @@
+"""The C interface without a GPU: the library loads, is of ABI version 5, exports every function
+include/*.h declares with the reference's structure layouts, parses the command line's options
+as the reference does (names, ranges, refusals all at once, values held), and refuses to solve
+loudly where there is no CUDA device (there is no CPU fallback)."""
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from unround import native, synthetic
+
+INCLUDE = Path(__file__).resolve().parents[1] / "include"
+
+
+def _declared() -> list[str]:
+    names = []
+    for header in INCLUDE.rglob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
+        names += re.findall(r"\b(unround_\w+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_exports_every_declared_function():
+    library = ctypes.CDLL(native.library_path())
+    names = _declared()
+    assert "unround_solve" in names and "unround_settings_new" in names
+    missing = [name for name in names if not hasattr(library, name)]
+    assert missing == []
+
+
+def test_version_and_layouts():
+    assert native._library().unround_abi_version() == 5
+    assert "unround" in native.version()
+    assert ctypes.sizeof(native._Record) == 64
+    assert ctypes.sizeof(native._Component) == 152
+    assert native._Component.quant_table.offset == 24
+    assert ctypes.sizeof(native._Input) == 24
+    assert native._Input.components.offset == 16
+
+
+def test_default_settings_held():
+    held = native.held_options()
+    assert "--method=tgv" in held and "--alpha1=1" in held and "--alpha0=2" in held
+    assert "--mu=rule" in held and "--mu-scale=9" in held and "--flat-weight=0.1" in held
+    assert "--record-every=10" in held and "--relaxation=1.9" in held and "--step-product=0.99" in held
+
+
+def test_options_round_trip():
+    given = ["--method", "tv", "--alpha", "0.5", "--mu", "0.01,0.02,0.03", "--centres=mmse", "--flat-dc", "any",
+             "--iterations", "40", "--tolerance", "0", "--no-weight-scaling", "--channels", "apart"]
+    held = native.held_options(given)
+    again = native.held_options(held)
+    assert held == again
+    assert "--mu=0.01,0.02,0.03" in held and "--flat-dc=any" in held and "--no-weight-scaling" in held
+
+
+@pytest.mark.parametrize(
+    "options, fragment",
+    [
+        (["--mu", "-1"], "--mu is at least 0"),
+        (["--method", "nope"], "--method is one of"),
+        (["--relaxation", "2"], "--relaxation is between 0 and 2"),
+        (["--alpha", "1", "--alpha", "2"], "--alpha is given twice"),
+        (["--bogus"], "--bogus is not an option"),
+        (["--method", "tv", "--partial-radius", "3"], "TGV's alone"),
+        (["--partial-tolerance", "1"], "needs --partial-radius"),
+        (["--mu", "1,2", "--slack", "1,2,3"], "one value for every component or one for each"),
+        (["--iterations"], "needs a value"),
+    ],
+)
+def test_refusals(options, fragment):
+    with pytest.raises(native.UnroundError) as raised:
+        native.held_options(options)
+    assert raised.value.status == native.Status.OPTIONS
+    assert fragment in raised.value.message
+
+
+def test_every_refusal_at_once():
+    with pytest.raises(native.UnroundError) as raised:
+        native.held_options(["--mu", "-1", "--relaxation", "3"])
+    assert "--mu" in raised.value.message and "--relaxation" in raised.value.message
+
+
+def test_unsupported_file_paths():
+    with pytest.raises(native.UnroundError) as raised:
+        native.decode(b"\xff\xd8\xff")
+    assert raised.value.status == native.Status.UNSUPPORTED
+
+
+def test_colour_conversions_invert():
+    rng = np.random.default_rng(0)
+    rgb = rng.uniform(0, 255, size=(5, 7, 3))
+    back = native.to_rgb(native.to_ycbcr(rgb))
+    np.testing.assert_allclose(back, rgb, atol=1e-10)
+
+
+def test_solve_fails_loudly_without_a_device():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    image = synthetic.grey(16, 16, seed=0).image
+    with pytest.raises(native.UnroundError) as raised:
+        native.solve(image, ["--method", "tv", "--iterations", "2"])
+    assert raised.value.status == native.Status.INTERNAL
+    assert "CUDA" in raised.value.message
