@@ -65,6 +65,30 @@ unround_status unround_b200_model(const unround_input* input, const unround_sett
                                   int32_t which, double* out, uint64_t capacity, uint64_t* count, char* message,
                                   size_t message_size);
 
+/* The decoder of the centres (what unround_solve computes with --method=mmse, which the settings
+ * must say) into the caller's device buffers, allocating no device memory. It has no counterpart
+ * in the reference's interface. It is for callers that run inside a device-memory budget they do
+ * not own (a framework's allocator that holds the GPU's memory, a loop whose memory is planned
+ * once), where a cudaMalloc may fail or a cudaFree stall the device.
+ *
+ * `canvas` (channels x canvas rows x canvas columns, binary64, the input's colour space) and
+ * `coefficients` (every component's blocks one after another, binary64) are device pointers on
+ * the current device holding `canvas_capacity` and `coefficient_capacity` doubles; both null asks
+ * only for `sizes`, without a device. `sizes` (4, may be null) gets the channels, the canvas rows,
+ * the canvas columns and the coefficient count. The work runs on `stream` (a cudaStream_t; null
+ * is the legacy default stream) and is complete on return.
+ *
+ * Its device scratch is one fixed array of 64 MiB on each device, reserved when this library's
+ * device code is loaded there: an input whose levels, flat flags and constants need more (about
+ * 33 million coefficients) is refused with UNROUND_ERROR_ARGUMENT and left to unround_solve. The
+ * first call on a device looks up the array's address there (cudaGetSymbolAddress), once. Calls
+ * share the array: calls that run at the same time on one device race on it, and the caller
+ * serializes them. */
+unround_status unround_b200_decode_centres_noalloc(const unround_input* input, const unround_settings* settings,
+                                                   double* canvas, uint64_t canvas_capacity, double* coefficients,
+                                                   uint64_t coefficient_capacity, uint64_t* sizes, void* stream,
+                                                   char* message, size_t message_size);
+
 #ifdef __cplusplus
 }
 #endif
