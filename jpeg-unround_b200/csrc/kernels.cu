@@ -20,6 +20,7 @@
 #include <cstdint>
 
 #include "dct.cuh"
+#include "prox.cuh"
 #include "tma.cuh"
 
 namespace urb {
@@ -35,11 +36,6 @@ template <typename T>
 __device__ __forceinline__ T ball_scale(T square, T radius) {
   const T norm = sqrt(square);
   return norm > radius ? radius / norm : T(1);
-}
-
-template <typename T>
-__device__ __forceinline__ T clamp_to(T value, T low, T high) {
-  return fmin(fmax(value, low), high);
 }
 
 // The sum (or the largest) over the CTA of one double per thread, in a fixed order: warp
@@ -287,55 +283,7 @@ __global__ void __launch_bounds__(256) dual_stream_kernel(const DualParams P) {
 // v for the CR x CC samples of each of its cells, the column DCT in registers, and a
 // transpose through shared memory gives each lane one row of coefficients (v = lane, u = 0..7)
 // for the row DCT, the clip, and the inverse row DCT; a second transpose returns the columns.
-
-// The interval and the centre of a coefficient in binary32, from its level
-// (cpp/src/model.cpp:41-46, 237-247; laplace.hpp:51-56).
-struct Coefficient {
-  float low, high, centre, own_low, own_high;
-};
-
-//
-// DC is taken centred on the middle of its interval, c_DC = q Q + 1024: the block's samples
-// less c_DC / 8 have the DC coefficient e - c_DC, whose interval is [-(1/2 + s) Q, (1/2 + s) Q]
-// and whose centre is 0. The same map in exact arithmetic; in binary32 it keeps DC's values
-// small, where the absolute ones (up to ~2000) would lose ~1e-4 a transform, and lose it alike
-// every iteration in the slow modes of weakly pinned (flat) blocks.
-__device__ __forceinline__ Coefficient coefficient_of(int q, int k, const ProxFactors& F) {
-  const float level = static_cast<float>(q);
-  const float step = F.step[k];
-  Coefficient c;
-  if (k == 0) {
-    c.low = (-0.5f - F.slack) * step;
-    c.high = (0.5f + F.slack) * step;
-    c.centre = 0.0f;
-    c.own_low = -0.5f * step;
-    c.own_high = 0.5f * step;
-    return c;
-  }
-  const float shift = 0.0f;
-  c.low = ((level - 0.5f) - F.slack) * step + shift;
-  c.high = ((level + 0.5f) + F.slack) * step + shift;
-  if (F.mmse && k != 0) {
-    const float size = (fabsf(level) - F.shrink[k]) * step;
-    c.centre = q == 0 ? 0.0f : (q < 0 ? -size : size);
-  } else {
-    c.centre = level * step + shift;
-  }
-  c.own_low = (level - 0.5f) * step + shift;
-  c.own_high = (level + 0.5f) * step + shift;
-  return c;
-}
-
-// prox of a coefficient (cpp/src/model.cpp:57-72): z = (e + t c) r clipped, and with a
-// slack's cost moved back by h beyond the file's own interval, not past its end.
-__device__ __forceinline__ float prox_of(float e, float t, float r, float h, const Coefficient& c, bool costed) {
-  const float z = (e + t * c.centre) * r;
-  if (!costed) return clamp_to(z, c.low, c.high);
-  const float above = fmaxf(c.own_high, z - h);
-  const float below = fminf(c.own_low, z + h);
-  const float inside = z < c.own_low ? below : z;
-  return clamp_to(z > c.own_high ? above : inside, c.low, c.high);
-}
+// The interval, the centre and the proximal map of a coefficient are prox.cuh's.
 
 // G's terms at a coefficient in binary64 (cpp/src/model.cpp:384-392): m/2 (c - centre)^2, and
 // the cost of lying beyond the file's own interval.

@@ -198,6 +198,29 @@ int primal_tma_grid_blocks(const Geometry& g, const ComponentDevice& c);
 cudaError_t launch_primal_tma(const CUtensorMap& map, const PrimalParams& p, bool keep, cudaStream_t stream);
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,
                             bool coupled, bool keep, cudaStream_t stream);
+// A 3D tiled map of `count` float planes `stride` floats apart, boxes of 40 columns x
+// `box_rows` rows x every plane (sweep.cu).
+bool make_box_map(CUtensorMap& map, const float* planes, const Geometry& g, int count, std::size_t stride,
+                  unsigned box_rows);
+
+// The whole iteration as one sweep (iteration.cu): the dual step D_n with the relaxation, from
+// x~_n and s_{n-1} (dual.in, dual.xt) to s_n (dual.out), and the primal step P_{n+1} on s_n,
+// x~_{n+1} into `next`; no kept values (records take the split kernels).
+struct IterationParams {
+  DualParams dual;
+  ComponentDevice component[kMaxChannels];
+  float* next = nullptr;
+  int strip_rows = 256;  // rows a CTA sweeps, a multiple of 16 (set by the launcher)
+};
+
+// Whether the fused sweep takes this canvas: 1 or 3 channels, channel 0 of 1 x 1 cells, the
+// others of CR x CC, CR and CC 1 or 2.
+bool iteration_takes(const Geometry& g, const ComponentDevice* components, int count);
+std::size_t iteration_shared_bytes(bool tgv, int channels);
+// The sweep's maps: boxes of 9 rows (a chunk and the row below it).
+bool make_iteration_map(CUtensorMap& map, const float* planes, const Geometry& g, int count);
+cudaError_t launch_iteration(const CUtensorMap& state, const CUtensorMap& tilde, const IterationParams& p, bool tgv,
+                             bool coupled, int cell_rows, int cell_columns, cudaStream_t stream);
 
 cudaError_t launch_widen(const float* from, double* to, const Geometry& g, cudaStream_t stream);
 cudaError_t launch_narrow(const double* from, float* to, const Geometry& g, cudaStream_t stream);

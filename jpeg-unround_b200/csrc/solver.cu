@@ -3,6 +3,7 @@
 
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -15,6 +16,14 @@ constexpr double kNaN = std::numeric_limits<double>::quiet_NaN();
 
 std::string describe(cudaError_t error) {
   return std::string(cudaGetErrorName(error)) + ": " + cudaGetErrorString(error);
+}
+
+// UNROUND_B200_KERNELS=fused runs the iterations that keep nothing as one sweep each
+// (iteration.cu: the dual step and the next primal step, one pass over HBM); otherwise every
+// iteration is the dual sweep and the primal kernels apart, which measure faster on B200.
+bool fused_kernels() {
+  const char* value = std::getenv("UNROUND_B200_KERNELS");
+  return value != nullptr && std::strcmp(value, "fused") == 0;
 }
 
 }  // namespace
@@ -43,10 +52,18 @@ struct Solver::Impl {
   std::vector<int> value_written;
   bool tgv = false;
   int current = 0;  // which state holds s_n
-  // The sweep's tensor maps (of each state, and of x~), and its error word.
+  // The sweep's tensor maps (of each state, and of each x~ buffer), and its error word.
   CUtensorMap state_maps[2];
-  CUtensorMap tilde_map;
+  CUtensorMap tilde_maps[2];
   bool swept = false;
+  // x~ in two buffers when the whole iteration is one sweep (it reads x~_n and writes
+  // x~_{n+1}); `xt` is the current one, xts[xt_id]. The fused sweep's maps, of 9-row boxes.
+  float* xts[2] = {nullptr, nullptr};
+  int xt_id = 0;
+  bool fusable = false;
+  int cell_rows = 1, cell_columns = 1;
+  CUtensorMap iteration_state_maps[2];
+  CUtensorMap iteration_tilde_maps[2];
   CUtensorMap primal_maps[2][kMaxChannels];
   bool primal_swept[kMaxChannels] = {};
   int* error_word = nullptr;
@@ -120,7 +137,7 @@ struct Solver::Impl {
   }
 
   // Device copies of the model: levels, flat blocks, binary64 constants.
-  void setup(bool with_tgv) {
+  void setup(bool with_tgv, bool solving = true) {
     tgv = with_tgv;
     const std::size_t n = g.plane * g.channels;
     for (const Component& c : frame.components) {
@@ -154,12 +171,27 @@ struct Solver::Impl {
     state[1] = fields(with_tgv);
     tilde = fields(with_tgv);
     xt = allocate<float>(n);
+    xts[0] = xt;
+    xt_id = 0;
+    fusable = solving && fused_kernels() &&
+              iteration_takes(g, components.data(), static_cast<int>(components.size()));
+    if (fusable) {
+      xts[1] = allocate<float>(n);
+      cell_rows = components.size() > 1 ? components[1].cell_rows : 1;
+      cell_columns = components.size() > 1 ? components[1].cell_columns : 1;
+    }
     error_word = allocate<int>(1);
     if (error == cudaSuccess) error = cudaMemsetAsync(error_word, 0, sizeof(int), stream);
     const int planes = (with_tgv ? 8 : 3) * g.channels;
     if (error == cudaSuccess) {
       swept = make_sweep_map(state_maps[0], state[0].x, g, planes) &&
-              make_sweep_map(state_maps[1], state[1].x, g, planes) && make_sweep_map(tilde_map, xt, g, g.channels);
+              make_sweep_map(state_maps[1], state[1].x, g, planes) &&
+              make_sweep_map(tilde_maps[0], xts[0], g, g.channels) &&
+              (!fusable || make_sweep_map(tilde_maps[1], xts[1], g, g.channels));
+      fusable = fusable && swept && make_iteration_map(iteration_state_maps[0], state[0].x, g, planes) &&
+                make_iteration_map(iteration_state_maps[1], state[1].x, g, planes) &&
+                make_iteration_map(iteration_tilde_maps[0], xts[0], g, g.channels) &&
+                make_iteration_map(iteration_tilde_maps[1], xts[1], g, g.channels);
       // The primal step's maps: a channel's x, p1 and p2 planes, `channels` planes apart.
       for (std::size_t c = 0; c < components.size(); ++c) {
         bool made = primal_tma_takes(components[c]);
@@ -366,7 +398,7 @@ struct Solver::Impl {
     }
   }
 
-  void dual(bool keep) {
+  DualParams dual_params() const {
     DualParams dp;
     dp.g = g;
     dp.xt = xt;
@@ -382,11 +414,32 @@ struct Solver::Impl {
     dp.radius = static_cast<float>(tgv ? plan.alpha1 : plan.alpha);
     dp.radius0 = static_cast<float>(plan.alpha0);
     dp.error = error_word;
+    return dp;
+  }
+
+  void dual(bool keep) {
+    const DualParams dp = dual_params();
     if (error == cudaSuccess) {
-      error = swept ? launch_dual_tma(state_maps[current], tilde_map, dp, tgv, plan.coupled, keep, stream)
+      error = swept ? launch_dual_tma(state_maps[current], tilde_maps[xt_id], dp, tgv, plan.coupled, keep, stream)
                     : launch_dual(dp, tgv, plan.coupled, keep, stream);
     }
     current = 1 - current;
+  }
+
+  // The dual step of iteration n and the primal step of iteration n + 1 as one sweep
+  // (iteration.cu), keeping nothing: from x~_n and s_{n-1} to s_n and x~_{n+1}.
+  void fused() {
+    IterationParams ip;
+    ip.dual = dual_params();
+    for (std::size_t c = 0; c < components.size(); ++c) ip.component[c] = components[c];
+    ip.next = xts[1 - xt_id];
+    if (error == cudaSuccess) {
+      error = launch_iteration(iteration_state_maps[current], iteration_tilde_maps[xt_id], ip, tgv, plan.coupled,
+                               cell_rows, cell_columns, stream);
+    }
+    current = 1 - current;
+    xt_id = 1 - xt_id;
+    xt = xts[xt_id];
   }
 
   // G* of channel c at xi = gamma div(scale q) (cpp/src/frames.cpp:428-493).
@@ -511,7 +564,9 @@ Solver::Solver(const Frame& frame, cudaStream_t stream) : impl_(std::make_unique
 
 Solver::~Solver() = default;
 
-int Solver::launches_per_iteration() const { return 1 + static_cast<int>(impl_->components.size()); }
+int Solver::launches_per_iteration() const {
+  return impl_->fusable ? 1 : 1 + static_cast<int>(impl_->components.size());
+}
 
 bool Solver::solve(Method method, const Plan* plan, const Start* start, const Observer& observer, Outcome& out,
                    Failure& failure) {
@@ -519,7 +574,7 @@ bool Solver::solve(Method method, const Plan* plan, const Start* start, const Ob
   const bool solver = method == Method::tv || method == Method::tgv;
   if (!solver) {
     // The decoder of the centres (docs/math.md 2.3).
-    m.setup(false);
+    m.setup(false, false);
     m.start(nullptr, false);
     m.fetch(out);
     bytes_ = m.bytes;
@@ -585,6 +640,13 @@ bool Solver::solve(Method method, const Plan* plan, const Start* start, const Ob
   if (!stopped && most > 0) m.primal(recorded(1));
   while (!stopped && iteration < most && m.error == cudaSuccess) {
     const std::uint64_t next = iteration + 1;
+    // One sweep for D_next and P_{next+1} when neither keeps anything: no record after the
+    // dual step, none of the next iterate, and a next iteration to make.
+    if (m.fusable && next < most && !recorded(next) && !recorded(next + 1)) {
+      m.fused();
+      iteration = next;
+      continue;
+    }
     m.dual(recorded(next));
     iteration = next;
     if (recorded(iteration)) stopped = take(iteration);
@@ -622,8 +684,12 @@ bool Solver::iterate(std::uint64_t iterations, Failure& failure) {
   Impl& m = *impl_;
   for (std::uint64_t n = 0; n < iterations && m.error == cudaSuccess; ++n) {
     const bool last = n + 1 == iterations;
-    m.dual(false);
-    m.primal(last);
+    if (m.fusable && !last) {
+      m.fused();
+    } else {
+      m.dual(false);
+      m.primal(last);
+    }
   }
   return m.check(failure, "the iterations");
 }
@@ -632,7 +698,17 @@ bool Solver::breakdown(std::uint64_t iterations, double& dual_ms, double& primal
   Impl& m = *impl_;
   std::vector<cudaEvent_t> events(3 * iterations);
   for (cudaEvent_t& e : events) cudaEventCreate(&e);
+  // With the fused sweep, every iteration but the last is one launch, timed as the dual
+  // group; the last (split, keeping its iterate) is not timed.
+  const std::uint64_t timed = m.fusable && iterations > 1 ? iterations - 1 : iterations;
   for (std::uint64_t n = 0; n < iterations && m.error == cudaSuccess; ++n) {
+    if (m.fusable && n < timed) {
+      cudaEventRecord(events[3 * n], m.stream);
+      m.fused();
+      cudaEventRecord(events[3 * n + 1], m.stream);
+      cudaEventRecord(events[3 * n + 2], m.stream);
+      continue;
+    }
     cudaEventRecord(events[3 * n], m.stream);
     m.dual(false);
     cudaEventRecord(events[3 * n + 1], m.stream);
@@ -641,7 +717,7 @@ bool Solver::breakdown(std::uint64_t iterations, double& dual_ms, double& primal
   }
   if (m.error == cudaSuccess) m.error = cudaStreamSynchronize(m.stream);
   double dual = 0.0, primal = 0.0;
-  for (std::uint64_t n = 0; n < iterations && m.error == cudaSuccess; ++n) {
+  for (std::uint64_t n = 0; n < timed && m.error == cudaSuccess; ++n) {
     float a = 0.0f, b = 0.0f;
     cudaEventElapsedTime(&a, events[3 * n], events[3 * n + 1]);
     cudaEventElapsedTime(&b, events[3 * n + 1], events[3 * n + 2]);
@@ -649,8 +725,8 @@ bool Solver::breakdown(std::uint64_t iterations, double& dual_ms, double& primal
     primal += b;
   }
   for (cudaEvent_t& e : events) cudaEventDestroy(e);
-  dual_ms = iterations > 0 ? dual / static_cast<double>(iterations) : 0.0;
-  primal_ms = iterations > 0 ? primal / static_cast<double>(iterations) : 0.0;
+  dual_ms = timed > 0 ? dual / static_cast<double>(timed) : 0.0;
+  primal_ms = timed > 0 ? primal / static_cast<double>(timed) : 0.0;
   return m.check(failure, "the timed iterations");
 }
 

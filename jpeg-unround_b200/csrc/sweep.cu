@@ -332,12 +332,10 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
 
 }  // namespace
 
-namespace {
-
 // A 3D tiled map of `count` float planes `stride` floats apart, each the canvas's rows x columns
 // (rows `pitch` apart), boxes of 40 columns x `box_rows` rows x every plane.
-bool make_map(CUtensorMap& map, const float* planes, const Geometry& g, int count, std::size_t stride,
-              unsigned box_rows) {
+bool make_box_map(CUtensorMap& map, const float* planes, const Geometry& g, int count, std::size_t stride,
+                  unsigned box_rows) {
   PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
   if (encode == nullptr) return false;
   const cuuint64_t dims[3] = {static_cast<cuuint64_t>(g.columns), static_cast<cuuint64_t>(g.rows),
@@ -351,14 +349,12 @@ bool make_map(CUtensorMap& map, const float* planes, const Geometry& g, int coun
   return result == CUDA_SUCCESS;
 }
 
-}  // namespace
-
 bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count) {
-  return make_map(map, planes, g, count, g.plane, kChunk);
+  return make_box_map(map, planes, g, count, g.plane, kChunk);
 }
 
 bool make_primal_map(CUtensorMap& map, const float* x, const Geometry& g, std::size_t stride) {
-  return make_map(map, x, g, 3, stride, 65);
+  return make_box_map(map, x, g, 3, stride, 65);
 }
 
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,

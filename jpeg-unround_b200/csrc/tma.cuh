@@ -50,4 +50,14 @@ __device__ __forceinline__ void load_box(float* to, const CUtensorMap* map, std:
       : "memory");
 }
 
+// A contiguous bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from
+// global into shared memory, completing on `bar`.
+__device__ __forceinline__ void load_bulk(void* to, const void* from, unsigned bytes, std::uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_address(to)),
+      "l"(from), "r"(bytes), "r"(smem_address(bar))
+      : "memory");
+}
+
 }  // namespace urb
