@@ -681,19 +681,8 @@ cudaError_t launch_one(const CUtensorMap& state, const CUtensorMap& tilde, const
     slots = std::max(1, per_sm * sms);
     resident[device & 63].store(slots);
   }
-  // The strip height that finishes soonest: the CTAs in waves of `slots`, each wave as long as
-  // a strip and the pipeline's start (about two chunks).
   const int strips = (p.dual.g.columns + 31) / 32;
-  int best = 256;
-  long long best_cost = -1;
-  for (int height = 64; height <= 512; height += 16) {
-    const long long ctas = static_cast<long long>(strips) * ((p.dual.g.rows + height - 1) / height);
-    const long long cost = (ctas + slots - 1) / slots * (height + 2 * kRows);
-    if (best_cost < 0 || cost < best_cost) {
-      best_cost = cost;
-      best = height;
-    }
-  }
+  const int best = strip_rows_for(p.dual.g, slots);
   IterationParams q = p;
   q.strip_rows = best;
   const dim3 grid(strips, (p.dual.g.rows + best - 1) / best, 1);

@@ -15,6 +15,7 @@
 // column/row and the neighbour before the first.
 #include "kernels.hpp"
 
+#include <algorithm>
 #include <atomic>
 #include <cfloat>
 #include <cstdint>
@@ -468,13 +469,16 @@ __global__ void __launch_bounds__(256, 2) primal_kernel(const PrimalParams P) {
   if constexpr (KEEP) cta_sum(sum, P.partials);
 }
 
-// The primal step fed by TMA: a CTA owns a strip of 32 canvas columns and walks down it by
-// stages of 64 canvas rows (8 / CR block rows, a warp each) and the row above them, every
-// stage one 3D box of the channel's x, p1 and p2 planes (40 columns: the strip and 4 on each
-// side) into a ring of two slots, the next stage's load running while a stage is computed.
-// The computation of a block row is primal_kernel's, from shared memory.
+// The primal step fed by TMA, persistent: the work is a list of items, each a stage of 64
+// canvas rows (8 / CR block rows, a warp each) of a strip of 32 canvas columns of one of the
+// launch's components (1 or 2 of the same cells, e.g. Cb and Cr); the CTAs the device holds at
+// once take items t = blockIdx.x + n gridDim.x, neighbouring CTAs neighbouring strips, so that
+// the columns two boxes share come from L2. Every item is one 3D box of the channel's x, p1 and
+// p2 planes (40 columns: the strip and 4 on each side; the stage's rows and the row above) and
+// the levels of its blocks, into a ring of two slots: the next item's loads run while an item
+// is computed, across strips and components. The computation of a block row is primal_kernel's,
+// from shared memory.
 constexpr int kStageRows = 64;
-constexpr int kPrimalStages = 4;  // stages of a CTA's strip
 
 template <int CR>
 constexpr int primal_warps() {
@@ -482,8 +486,9 @@ constexpr int primal_warps() {
 }
 
 template <int CR, int CC, bool KEEP>
-__global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(const __grid_constant__ CUtensorMap map,
-                                                                             const PrimalParams P) {
+__global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(const __grid_constant__ CUtensorMap map0,
+                                                                             const __grid_constant__ CUtensorMap map1,
+                                                                             const __grid_constant__ PrimalBatch Q) {
   constexpr unsigned kAll = 0xffffffffu;
   constexpr int NB = primal_warps<CR>();
   constexpr int L = 8 * CC, B = 32 / L, BH = 8 * CR;
@@ -493,13 +498,15 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
   constexpr int STRIDE = (SLOT + 31) / 32 * 32;
   extern __shared__ __align__(128) float ring[];
   __shared__ __align__(8) std::uint64_t bars[2];
-  __shared__ ProxFactors F;
+  __shared__ ProxFactors factors[2];
+  __shared__ PrimalParams parts[2];  // the components' parameters, read per item
   __shared__ float tile[NB][4][72];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  {
-    const float* from = reinterpret_cast<const float*>(P.component.factors);
-    float* to = reinterpret_cast<float*>(&F);
+  for (int z = 0; z < Q.count; ++z) {
+    const float* from = reinterpret_cast<const float*>(Q.part[z].component.factors);
+    float* to = reinterpret_cast<float*>(&factors[z]);
     for (int k = tid; k < static_cast<int>(sizeof(ProxFactors) / 4); k += 32 * NB) to[k] = from[k];
+    if (tid == 0) parts[z] = Q.part[z];
   }
   if (tid == 0) {
     barrier_init(&bars[0], 1);
@@ -507,31 +514,75 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
-  const int vbr = rows / BH;
-  const int x0 = blockIdx.x * 32;
-  const int first = blockIdx.y * kPrimalStages * NB;  // the CTA's first block row
-  const int stages = min(kPrimalStages, (vbr - first + NB - 1) / NB);
-  auto issue = [&](int s) {
-    if (tid == 0 && s < stages) {
-      barrier_expect(&bars[s & 1], SLOT * 4);
-      load_box(ring + (s & 1) * STRIDE, &map, &bars[s & 1], x0 - HALO, (first + s * NB) * BH - 1, 0);
+  const int per_component = Q.strips * Q.stages;
+  const int items = (Q.items - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
+                    static_cast<int>(gridDim.x);  // this CTA's
+  // The CTA's n-th item: its component, strip and stage.
+  auto item_of = [&](int n, int& z, int& strip, int& stage) {
+    const int t = static_cast<int>(blockIdx.x) + n * static_cast<int>(gridDim.x);
+    z = t / per_component;
+    const int rest = t - z * per_component;
+    stage = rest / Q.strips;
+    strip = rest - stage * Q.strips;
+  };
+  // The levels of an item's blocks (NB block rows of B blocks), after the two slots, copied
+  // with the item's box.
+  std::int16_t* const levels_ring = reinterpret_cast<std::int16_t*>(ring + 2 * STRIDE);
+  constexpr int kStageLevels = NB * B * 64;
+  auto issue = [&](int n) {
+    if (tid == 0 && n < items) {
+      int z, strip, stage;
+      item_of(n, z, strip, stage);
+      const PrimalParams& P = parts[z];
+      const int vbr = P.g.rows / BH;
+      const int first = stage * NB;
+      const int vbx0 = strip * B;
+      const int count = min(B, P.component.block_columns - vbx0);
+      int rows_copied = 0;
+      for (int w = 0; w < NB; ++w) {
+        const int vby = first + w;
+        if (vby < vbr && vby < P.component.block_rows && count > 0) ++rows_copied;
+      }
+      barrier_expect(&bars[n & 1], SLOT * 4 + rows_copied * count * 128);
+      load_box(ring + (n & 1) * STRIDE, z == 0 ? &map0 : &map1, &bars[n & 1], strip * 32 - HALO, first * BH - 1, 0);
+      for (int w = 0; w < NB; ++w) {
+        const int vby = first + w;
+        if (vby < vbr && vby < P.component.block_rows && count > 0) {
+          load_bulk(levels_ring + (n & 1) * kStageLevels + w * B * 64,
+                    P.component.levels + (static_cast<std::size_t>(vby) * P.component.block_columns + vbx0) * 64,
+                    count * 128, &bars[n & 1]);
+        }
+      }
     }
   };
   issue(0);
   issue(1);
   const int blk = lane / L, in_block = lane % L, m = in_block / CC, cell = in_block % CC;
   const int leader = lane - cell;
-  const int vbx = blockIdx.x * B + blk;
-  const int j = vbx * L + in_block;
-  const bool column_in = j < columns;
   const int col = HALO + lane;
-  const float descent = P.descent;
   float* t = tile[warp][blk];
-  double sum = 0.0;
+  double sum0 = 0.0, sum1 = 0.0;  // the data term's terms of each component
   bool failed = false;
-  int stopped = stages;
-  for (int s = 0; s < stages; ++s) {
+  int stopped = items;
+  for (int s = 0; s < items; ++s) {
+    int z, strip, stage;
+    item_of(s, z, strip, stage);
+    const PrimalParams& P = parts[z];
+    const ProxFactors& F = factors[z];
+    double sum = 0.0;
+    const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+    const int vbr = rows / BH;
+    const int vbx = strip * B + blk;
+    const int j = vbx * L + in_block;
+    const bool column_in = j < columns;
+    const float descent = P.descent;
+    const int vby = stage * NB + warp;
+    const bool in_blocks =
+        vby < vbr && column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
+    const std::size_t block =
+        static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
+    // Read before the wait, used after the transforms.
+    const bool flat = in_blocks && P.component.flat[block] != 0;
     const bool ready = barrier_wait(&bars[s & 1], (s >> 1) & 1);
     if (__syncthreads_or(!ready)) {
       failed = true;
@@ -539,11 +590,10 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
       break;
     }
     const float* slot = ring + (s & 1) * STRIDE;
-    const int vby = first + s * NB + warp;
+    const std::int16_t* stage_levels = levels_ring + (s & 1) * kStageLevels + (warp * B + blk) * 64;
     if (vby < vbr) {
       const int i0 = vby * BH;
       const int base_row = 1 + warp * BH;  // shared-memory row of canvas row i0
-      const bool in_blocks = column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
       float v[BH];
 #pragma unroll
       for (int r = 0; r < BH; ++r) {
@@ -557,9 +607,7 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
         const float dx = (j + 1 < columns ? p1 : 0.0f) - (j > 0 ? before : 0.0f);
         v[r] = x + descent * (dy + dx);
       }
-      const std::size_t block =
-          static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
-      const float dc_level = in_blocks ? static_cast<float>(P.component.levels[block * 64]) : 0.0f;
+      const float dc_level = in_blocks ? static_cast<float>(stage_levels[0]) : 0.0f;
       const float middle = (dc_level * F.step[0] + 1024.0f) * 0.125f;
       float mean[8];
 #pragma unroll
@@ -591,15 +639,14 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
       for (int u = 0; u < 8; ++u) row[u] = t[m * 9 + u];
       forward8(row, coef);
       int levels[8];
-      const int4 packed = in_blocks ? __ldg(reinterpret_cast<const int4*>(P.component.levels + block * 64 + m * 8))
-                                    : make_int4(0, 0, 0, 0);
+      const int4 packed =
+          in_blocks ? *reinterpret_cast<const int4*>(stage_levels + m * 8) : make_int4(0, 0, 0, 0);
       const int words[4] = {packed.x, packed.y, packed.z, packed.w};
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const unsigned word = static_cast<unsigned>(words[u >> 1]);
         levels[u] = static_cast<int>(static_cast<std::int16_t>((u & 1) ? (word >> 16) : (word & 0xffffu)));
       }
-      const bool flat = in_blocks && P.component.flat[block] != 0;
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const int k = m * 8 + u;
@@ -655,17 +702,25 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
         }
       }
     }
+    if (z == 0) {
+      sum0 += sum;
+    } else {
+      sum1 += sum;
+    }
     __syncthreads();  // every warp is done with the slot
     issue(s + 2);
   }
   if (failed) {
-    if (tid == 0 && P.error != nullptr) atomicExch(P.error, 1);
+    if (tid == 0 && parts[0].error != nullptr) atomicExch(parts[0].error, 1);
   }
-  if constexpr (KEEP) cta_sum(sum, P.partials);
+  if constexpr (KEEP) {
+    cta_sum(sum0, parts[0].partials);
+    if (Q.count > 1) cta_sum(sum1, parts[1].partials);
+  }
   if (failed) {
-    // No load may still write into shared memory when the CTA leaves: the stage that was not
+    // No load may still write into shared memory when the CTA leaves: the item that was not
     // ready and the one after it.
-    for (int s = stopped; s < min(stopped + 2, stages); ++s) barrier_wait(&bars[s & 1], (s >> 1) & 1);
+    for (int s = stopped; s < min(stopped + 2, items); ++s) barrier_wait(&bars[s & 1], (s >> 1) & 1);
   }
 }
 
@@ -1194,32 +1249,51 @@ cudaError_t launch_dual(const DualParams& p, bool tgv, bool coupled, bool keep, 
 
 namespace {
 
-dim3 primal_tma_grid(const Geometry& g, int cr) {
+// A component's items: strips of 32 columns times stages of 64 rows.
+int primal_tma_items_of(const Geometry& g, int cr) {
   const int nb = kStageRows / (8 * cr);
   const int vbr = g.rows / (8 * cr);
-  return dim3((g.columns + 31) / 32, (vbr + kPrimalStages * nb - 1) / (kPrimalStages * nb), 1);
+  return (g.columns + 31) / 32 * ((vbr + nb - 1) / nb);
 }
 
 template <int CR, int CC, bool KEEP>
-cudaError_t primal_tma_one(const CUtensorMap& map, const PrimalParams& p, cudaStream_t s) {
+cudaError_t primal_tma_one(const CUtensorMap* maps, const PrimalParams* parts, int count, cudaStream_t s,
+                           int* grid) {
   auto kernel = primal_tma_kernel<CR, CC, KEEP>;
-  constexpr std::size_t bytes = 2 * ((3 * (kStageRows + 1) * 40 + 31) / 32 * 32) * sizeof(float);
-  static std::atomic<unsigned long long> configured{0};
+  constexpr int threads = 32 * primal_warps<CR>();
+  // Two slots of the x, p1, p2 box, then two items' levels.
+  constexpr std::size_t bytes = 2 * ((3 * (kStageRows + 1) * 40 + 31) / 32 * 32) * sizeof(float) +
+                                2 * (kStageRows / (8 * CR)) * (32 / (8 * CC)) * 64 * sizeof(std::int16_t);
+  // Once per device: the shared-memory size above 48 KB, and how many CTAs the device holds.
+  static std::atomic<int> resident[64] = {};
   int device = 0;
   cudaGetDevice(&device);
-  const unsigned long long bit = 1ull << (device & 63);
-  if ((configured.load() & bit) == 0) {
-    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  int slots = resident[device & 63].load();
+  if (slots == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    int per_sm = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, bytes);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    configured.fetch_or(bit);
+    slots = std::max(1, per_sm * sms);
+    resident[device & 63].store(slots);
   }
-  kernel<<<primal_tma_grid(p.g, CR), 32 * primal_warps<CR>(), bytes, s>>>(map, p);
+  PrimalBatch batch;
+  batch.count = count;
+  for (int z = 0; z < count; ++z) batch.part[z] = parts[z];
+  batch.strips = (parts[0].g.columns + 31) / 32;
+  batch.stages = primal_tma_items_of(parts[0].g, CR) / batch.strips;
+  batch.items = count * batch.strips * batch.stages;
+  *grid = std::min(batch.items, slots);
+  kernel<<<*grid, threads, bytes, s>>>(maps[0], maps[count > 1 ? 1 : 0], batch);
   return cudaGetLastError();
 }
 
 template <int CR, int CC>
-cudaError_t primal_tma_keep(const CUtensorMap& map, const PrimalParams& p, bool keep, cudaStream_t s) {
-  return keep ? primal_tma_one<CR, CC, true>(map, p, s) : primal_tma_one<CR, CC, false>(map, p, s);
+cudaError_t primal_tma_keep(const CUtensorMap* maps, const PrimalParams* parts, int count, bool keep, cudaStream_t s,
+                            int* grid) {
+  return keep ? primal_tma_one<CR, CC, true>(maps, parts, count, s, grid)
+              : primal_tma_one<CR, CC, false>(maps, parts, count, s, grid);
 }
 
 }  // namespace
@@ -1230,14 +1304,16 @@ bool primal_tma_takes(const ComponentDevice& c) {
 }
 
 int primal_tma_grid_blocks(const Geometry& g, const ComponentDevice& c) {
-  const dim3 d = primal_tma_grid(g, c.cell_rows);
-  return static_cast<int>(d.x * d.y);
+  // At most one CTA an item of either component of a launch.
+  return 2 * primal_tma_items_of(g, c.cell_rows);
 }
 
-cudaError_t launch_primal_tma(const CUtensorMap& map, const PrimalParams& p, bool keep, cudaStream_t stream) {
-  const int cr = p.component.cell_rows, cc = p.component.cell_columns;
+cudaError_t launch_primal_tma(const CUtensorMap* maps, const PrimalParams* parts, int count, bool keep,
+                              cudaStream_t stream, int* grid) {
+  if (count < 1 || count > 2) return cudaErrorInvalidValue;
+  const int cr = parts[0].component.cell_rows, cc = parts[0].component.cell_columns;
 #define URB_TMA_CELL(R, C) \
-  if (cr == R && cc == C) return primal_tma_keep<R, C>(map, p, keep, stream);
+  if (cr == R && cc == C) return primal_tma_keep<R, C>(maps, parts, count, keep, stream, grid);
   URB_TMA_CELL(1, 1) URB_TMA_CELL(1, 2) URB_TMA_CELL(2, 1) URB_TMA_CELL(2, 2) URB_TMA_CELL(1, 4) URB_TMA_CELL(4, 1)
   URB_TMA_CELL(2, 4) URB_TMA_CELL(4, 2) URB_TMA_CELL(4, 4)
 #undef URB_TMA_CELL

@@ -93,6 +93,7 @@ struct DualParams {
   float radius = 1.0f;   // alpha of TV, alpha1 of TGV
   float radius0 = 2.0f;  // alpha0
   int* error = nullptr;  // set to 1 where a bounded wait of the sweep ran out
+  int strip_rows = 256;  // rows a CTA of the sweep walks, a multiple of 8 (set by its launcher)
 };
 
 // The primal step of iteration n+1 for one channel: v = x + tau gamma div p and its proximal
@@ -190,12 +191,27 @@ cudaError_t launch_residual(const ResidualParams& p, cudaStream_t stream);
 // the planes of x~.
 std::size_t dual_tma_shared_bytes(bool tgv, int channels);
 bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count);
-// The primal step fed by TMA: `map` boxes the channel's x, p1 and p2 planes (make_primal_map,
-// planes `stride` floats apart). Cells of 1, 2 or 4 samples each way; others take launch_primal.
+// The primal step fed by TMA, persistent CTAs over (component, strip, stage) items: `maps[z]`
+// boxes component z's x, p1 and p2 planes (make_primal_map, planes `stride` floats apart); one
+// launch takes 1 or 2 components of the same cells and geometry (e.g. Cb and Cr) and writes each
+// CTA's sum of each component's data term into that component's partials. Cells of 1, 2 or 4
+// samples each way; others take launch_primal. *grid: the CTAs launched.
+struct PrimalBatch {
+  PrimalParams part[2];
+  int count = 1;
+  int strips = 0;
+  int stages = 0;
+  int items = 0;
+};
 bool make_primal_map(CUtensorMap& map, const float* x, const Geometry& g, std::size_t stride);
 bool primal_tma_takes(const ComponentDevice& c);
+// An upper bound of the CTAs of a launch (the partials a component needs).
 int primal_tma_grid_blocks(const Geometry& g, const ComponentDevice& c);
-cudaError_t launch_primal_tma(const CUtensorMap& map, const PrimalParams& p, bool keep, cudaStream_t stream);
+cudaError_t launch_primal_tma(const CUtensorMap* maps, const PrimalParams* parts, int count, bool keep,
+                              cudaStream_t stream, int* grid);
+// The rows a CTA of a strip sweep walks (a multiple of 16) so that the sweep's CTAs, `slots`
+// of them resident at once, finish soonest (sweep.cu).
+int strip_rows_for(const Geometry& g, int slots);
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,
                             bool coupled, bool keep, cudaStream_t stream);
 // A 3D tiled map of `count` float planes `stride` floats apart, boxes of 40 columns x

@@ -220,11 +220,13 @@ struct Solver::Impl {
     host_partials.resize(std::max(most, values));
   }
 
-  double* value_slot(std::size_t c) {
+  std::size_t value_offset(std::size_t c) const {
     std::size_t offset = 0;
     for (std::size_t k = 0; k < c; ++k) offset += value_counts[k];
-    return value_partials + offset;
+    return offset;
   }
+
+  double* value_slot(std::size_t c) { return value_partials + value_offset(c); }
 
   // The binary32 factors of each component's proximal map at the plan's tau.
   void set_factors(const Plan& p) {
@@ -373,28 +375,47 @@ struct Solver::Impl {
     current = 0;
   }
 
-  void primal(bool keep) {
+  PrimalParams primal_params(std::size_t c) const {
     const Fields& s = state[current];
-    for (std::size_t c = 0; c < components.size(); ++c) {
-      PrimalParams pp;
-      pp.g = g;
-      pp.component = components[c];
-      const std::size_t base = c * g.plane;
-      pp.x = s.x + base;
-      pp.p1 = s.p1 + base;
-      pp.p2 = s.p2 + base;
-      pp.xt = xt + base;
-      pp.v = v + base;
-      pp.partials = value_slot(c);
-      pp.descent = static_cast<float>(plan.tau * plan.channel_weights[c]);
-      pp.error = error_word;
-      if (primal_swept[c]) {
-        if (error == cudaSuccess) error = launch_primal_tma(primal_maps[current][c], pp, keep, stream);
-        if (keep) value_written[c] = primal_tma_grid_blocks(g, components[c]);
-      } else {
+    PrimalParams pp;
+    pp.g = g;
+    pp.component = components[c];
+    const std::size_t base = c * g.plane;
+    pp.x = s.x + base;
+    pp.p1 = s.p1 + base;
+    pp.p2 = s.p2 + base;
+    pp.xt = xt + base;
+    pp.v = v + base;
+    pp.partials = value_partials + value_offset(c);
+    pp.descent = static_cast<float>(plan.tau * plan.channel_weights[c]);
+    pp.error = error_word;
+    return pp;
+  }
+
+  // The primal step of every component; the TMA path takes two components of the same cells
+  // (Cb and Cr) in one launch.
+  void primal(bool keep) {
+    for (std::size_t c = 0; c < components.size();) {
+      if (!primal_swept[c]) {
+        const PrimalParams pp = primal_params(c);
         if (error == cudaSuccess) error = launch_primal(pp, keep, stream);
         if (keep) value_written[c] = primal_grid_blocks(g, components[c]);
+        ++c;
+        continue;
       }
+      const bool pair = c + 1 < components.size() && primal_swept[c + 1] &&
+                        components[c + 1].cell_rows == components[c].cell_rows &&
+                        components[c + 1].cell_columns == components[c].cell_columns;
+      const int count = pair ? 2 : 1;
+      const PrimalParams parts[2] = {primal_params(c), primal_params(pair ? c + 1 : c)};
+      const CUtensorMap maps[2] = {primal_maps[current][c], primal_maps[current][pair ? c + 1 : c]};
+      int grid = 0;
+      if (error == cudaSuccess) error = launch_primal_tma(maps, parts, count, keep, stream, &grid);
+      if (keep) {
+        value_written[c] = grid;
+        if (pair) value_written[c + 1] = grid;
+      }
+      c += count;
     }
   }
 

@@ -1,17 +1,25 @@
 // The dual step of an iteration as a TMA-fed sweep (sm_100a).
 //
-// A CTA owns a strip of 32 canvas columns and walks down kStrip rows of it in chunks of 8 rows,
-// one row per warp, a lane per column. Each chunk of every field of every channel -- the state
-// s_{n-1} (x, p, and for TGV w and r) and the carried canvas x~ -- comes into shared memory by two
-// cp.async.bulk.tensor loads of a 3D box (40 columns, the strip and 4 on each side, 8 rows, every
-// plane) into a ring of three slots, so that the loads of chunks k + 2 and k + 3 run while chunk
-// k is computed; each value of HBM is read once (the 8 columns beside the strip come from L2).
-// Neighbours across and down are read from shared memory; w- of the row above a chunk is kept
-// from the chunk before. The arithmetic of each value is the dual step of docs/math.md 5,
-// operation for operation as cpp/src/primal_dual.hpp:572-735 orders it (see kernels.cu).
+// A CTA owns a strip of 32 canvas columns and walks down strip_rows rows of it in chunks of 8
+// rows, one row per warp, a lane per column. Each chunk of every field of every channel -- the
+// state s_{n-1} (x, p, and for TGV w and r) and the carried canvas x~ -- comes into shared memory
+// by two cp.async.bulk.tensor loads of a 3D box (40 columns, the strip and 4 on each side, 8 rows,
+// every plane) into a ring of three slots, so that the loads of chunks k + 2 and k + 3 run while
+// chunk k is computed; each value of HBM is read once (the 8 columns beside the strip come from
+// L2). The strip height is chosen per launch so that the CTAs fill the device's SMs in whole
+// waves as nearly as possible.
+//
+// w~ = w + tau (p + div2 r) is evaluated once per pixel: a chunk's row warps make x_n, w~, w-
+// and p_n at their pixels and leave w- in shared memory; after a barrier each pixel's r step
+// takes w- of its left neighbour by a shuffle (of the strip's first column, from a ninth, side
+// warp that makes w- at column x0 - 1) and of its upper neighbour from shared memory (of the
+// chunk's first row, kept from the chunk before). The arithmetic of each value is the dual step
+// of docs/math.md 5, operation for operation as cpp/src/primal_dual.hpp:572-735 orders it (see
+// kernels.cu).
 //
 // The waits on the ring's mbarriers are bounded: a wait that runs out sets the error word,
 // and the CTA leaves without computing further (the host reports an internal error).
+#include <algorithm>
 #include <atomic>
 
 #include <cuda.h>
@@ -28,7 +36,9 @@ constexpr int kChunk = 8;    // rows of a chunk, one per warp
 constexpr int kHalo = 4;     // columns loaded left of the strip (16-byte aligned start)
 constexpr int kSpan = 40;    // columns loaded: 4 + 32 + 4
 constexpr int kSlots = 3;    // the ring
-constexpr int kStrip = 256;  // rows a CTA sweeps
+constexpr int kStrip = 256;  // rows a CTA sweeps unless the launcher finds better
+constexpr int kThreads = 32 * (kChunk + 1);  // the row warps and the side warp
+constexpr unsigned kAll = 0xffffffffu;
 
 template <typename T>
 __device__ __forceinline__ T ball(T square, T radius) {
@@ -37,21 +47,24 @@ __device__ __forceinline__ T ball(T square, T radius) {
 }
 
 template <bool TGV, int C, bool COUPLED, bool KEEP>
-__global__ void __launch_bounds__(256) dual_tma_kernel(const __grid_constant__ CUtensorMap state_map,
-                                                        const __grid_constant__ CUtensorMap tilde_map,
-                                                        const DualParams P) {
+__global__ void __launch_bounds__(kThreads, 2) dual_tma_kernel(const __grid_constant__ CUtensorMap state_map,
+                                                                const __grid_constant__ CUtensorMap tilde_map,
+                                                                const DualParams P) {
   constexpr int F = TGV ? 8 : 3;  // state planes per channel: x, p1, p2 (+ w1, w2, r11, r22, r12)
   constexpr int PLANE = kChunk * kSpan;
   constexpr int SLOT = (F + 1) * C * PLANE;  // floats: the state planes, then x~'s
+  constexpr int W = TGV ? C : 1;
   extern __shared__ __align__(128) float ring[];
   __shared__ __align__(8) std::uint64_t bars[kSlots];
-  __shared__ float carry[2][C][2][32];  // w- of the row above a chunk, own columns
+  __shared__ float carry[2][W][2][32];      // w- of the row above a chunk, own columns
+  __shared__ float wbar[W][2][kChunk][32];  // w- of each row of the chunk
+  __shared__ float wleft[W][2][kChunk];     // w- at column x0 - 1
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
   const std::size_t plane = P.g.plane;
   const int x0 = blockIdx.x * 32;
-  const int i0 = blockIdx.y * kStrip;
-  const int i1 = min(i0 + kStrip, rows);
+  const int i0 = blockIdx.y * P.strip_rows;
+  const int i1 = min(i0 + P.strip_rows, rows);
   const int chunks = (i1 - i0 + kChunk - 1) / kChunk;
   const int j = x0 + lane;
   const bool valid = j < columns;
@@ -117,7 +130,6 @@ __global__ void __launch_bounds__(256) dual_tma_kernel(const __grid_constant__ C
     }
     const float* slot = ring + (k % kSlots) * SLOT;
     const float* next = ring + ((k + 1) % kSlots) * SLOT;
-    const int i = i0 + k * kChunk + warp;
     // A field's value in shared memory: plane (field, channel), row r of the chunk (8: the next
     // chunk's first row), column col of the 40.
     auto S = [&](int field, int c, int r, int col) -> float {
@@ -128,13 +140,30 @@ __global__ void __launch_bounds__(256) dual_tma_kernel(const __grid_constant__ C
       const float* s = r < kChunk ? slot : next;
       return s[((F * C + c) * kChunk + (r < kChunk ? r : 0)) * kSpan + col];
     };
-    if (i < i1) {
-      const bool has_down = i + 1 < rows, has_up = i > 0;
-      const std::size_t here = static_cast<std::size_t>(i) * pitch + jc;
+    // w~ at (row rr of the chunk, column col of the box): w + tau g (p + div2 r), div2 r by
+    // forward differences; (ii, jj) the pixel on the canvas.
+    auto w_tilde = [&](int c, int rr, int col, int ii, int jj, float& t1, float& t2, float& w1, float& w2) {
+      const float tau = P.tau[c];
+      const float r11 = S(5, c, rr, col), r22 = S(6, c, rr, col), r12 = S(7, c, rr, col);
+      float d1 = jj + 1 < columns ? S(5, c, rr, col + 1) - r11 : 0.0f;
+      float d2 = jj + 1 < columns ? S(7, c, rr, col + 1) - r12 : 0.0f;
+      d1 = d1 + (ii + 1 < rows ? S(7, c, rr + 1, col) - r12 : 0.0f);
+      d2 = d2 + (ii + 1 < rows ? S(6, c, rr + 1, col) - r22 : 0.0f);
+      w1 = S(3, c, rr, col);
+      w2 = S(4, c, rr, col);
+      t1 = w1 + tau * (S(1, c, rr, col) + d1);
+      t2 = w2 + tau * (S(2, c, rr, col) + d2);
+    };
+    const int r = warp;
+    const int i = i0 + k * kChunk + r;
+    const bool row = warp < kChunk && i < i1;
+    const std::size_t here = static_cast<std::size_t>(row ? i : 0) * pitch + jc;
+    float wb1[C], wb2[C];
+    // ---- The row warps: x, w and p at the pixel; w- left in shared memory.
+    if (row) {
+      const bool has_down = i + 1 < rows;
       float step_p1[C], step_p2[C], old_p1[C], old_p2[C];
-      float step_r11[C], step_r22[C], step_r12[C], old_r11[C], old_r22[C], old_r12[C];
-      float square_p = 0.0f, square_r = 0.0f;
-      const int r = warp;
+      float square_p = 0.0f;
 #pragma unroll
       for (int c = 0; c < C; ++c) {
         const std::size_t base = c * plane;
@@ -148,25 +177,14 @@ __global__ void __launch_bounds__(256) dual_tma_kernel(const __grid_constant__ C
         old_p2[c] = p2;
         const float sigma = P.sigma[c];
         if constexpr (!TGV) {
+          wb1[c] = wb2[c] = 0.0f;
           step_p1[c] = p1 + sigma * gx;
           step_p2[c] = p2 + sigma * gy;
         } else {
-          const float tau = P.tau[c];
-          // w~ at (i, col): w + tau g (p + div2 r), div2 r by forward differences.
-          auto w_tilde = [&](int rr, int col, int ii, int jj, float& t1, float& t2, float& w1, float& w2) {
-            const float r11 = S(5, c, rr, col), r22 = S(6, c, rr, col), r12 = S(7, c, rr, col);
-            float d1 = jj + 1 < columns ? S(5, c, rr, col + 1) - r11 : 0.0f;
-            float d2 = jj + 1 < columns ? S(7, c, rr, col + 1) - r12 : 0.0f;
-            d1 = d1 + (ii + 1 < rows ? S(7, c, rr + 1, col) - r12 : 0.0f);
-            d2 = d2 + (ii + 1 < rows ? S(6, c, rr + 1, col) - r22 : 0.0f);
-            w1 = S(3, c, rr, col);
-            w2 = S(4, c, rr, col);
-            t1 = w1 + tau * (S(1, c, rr, col) + d1);
-            t2 = w2 + tau * (S(2, c, rr, col) + d2);
-          };
           float t1, t2, w1, w2;
-          w_tilde(r, own, i, j, t1, t2, w1, w2);
-          const float wb1 = 2.0f * t1 - w1, wb2 = 2.0f * t2 - w2;
+          w_tilde(c, r, own, i, j, t1, t2, w1, w2);
+          wb1[c] = 2.0f * t1 - w1;
+          wb2[c] = 2.0f * t2 - w2;
           if (valid) {
             P.out.w1[base + here] = rho * t1 + rest * w1;
             P.out.w2[base + here] = rho * t2 + rest * w2;
@@ -175,56 +193,19 @@ __global__ void __launch_bounds__(256) dual_tma_kernel(const __grid_constant__ C
               P.tilde.w2[base + here] = t2;
             }
           }
-          float wl1 = 0.0f, wl2 = 0.0f;
-          if (has_left) {
-            float lt1, lt2, lw1, lw2;
-            w_tilde(r, own - 1, i, j - 1, lt1, lt2, lw1, lw2);
-            wl1 = 2.0f * lt1 - lw1;
-            wl2 = 2.0f * lt2 - lw2;
-          }
-          float wu1 = 0.0f, wu2 = 0.0f;
-          if (has_up) {
-            if (r > 0) {
-              float ut1, ut2, uw1, uw2;
-              w_tilde(r - 1, own, i - 1, j, ut1, ut2, uw1, uw2);
-              wu1 = 2.0f * ut1 - uw1;
-              wu2 = 2.0f * ut2 - uw2;
-            } else {
-              wu1 = carry[k & 1][c][0][lane];
-              wu2 = carry[k & 1][c][1][lane];
-            }
-          }
+          wbar[c][0][r][lane] = wb1[c];
+          wbar[c][1][r][lane] = wb2[c];
           if (r == kChunk - 1) {
-            carry[(k + 1) & 1][c][0][lane] = wb1;
-            carry[(k + 1) & 1][c][1][lane] = wb2;
+            carry[(k + 1) & 1][c][0][lane] = wb1[c];
+            carry[(k + 1) & 1][c][1][lane] = wb2[c];
           }
-          step_p1[c] = p1 + sigma * (gx - wb1);
-          step_p2[c] = p2 + sigma * (gy - wb2);
-          const float own1x = has_right ? wb1 : 0.0f, own2x = has_right ? wb2 : 0.0f;
-          const float own1y = has_down ? wb1 : 0.0f, own2y = has_down ? wb2 : 0.0f;
-          const float exx = own1x - wl1;
-          const float eyy = own2y - wu2;
-          const float exy = 0.5f * ((own1y - wu1) + (own2x - wl2));
-          const float r11 = S(5, c, r, own), r22 = S(6, c, r, own), r12 = S(7, c, r, own);
-          old_r11[c] = r11;
-          old_r22[c] = r22;
-          old_r12[c] = r12;
-          step_r11[c] = r11 + sigma * exx;
-          step_r22[c] = r22 + sigma * eyy;
-          step_r12[c] = r12 + sigma * exy;
+          step_p1[c] = p1 + sigma * (gx - wb1[c]);
+          step_p2[c] = p2 + sigma * (gy - wb2[c]);
         }
-        if constexpr (COUPLED) {
-          square_p += step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c];
-          if constexpr (TGV) {
-            square_r += step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]);
-          }
-        }
+        if constexpr (COUPLED) square_p += step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c];
       }
-      float scale_p = 1.0f, scale_r = 1.0f;
-      if constexpr (COUPLED) {
-        scale_p = ball(square_p, P.radius);
-        if constexpr (TGV) scale_r = ball(square_r, P.radius0);
-      }
+      float scale_p = 1.0f;
+      if constexpr (COUPLED) scale_p = ball(square_p, P.radius);
       if (valid) {
 #pragma unroll
         for (int c = 0; c < C; ++c) {
@@ -238,7 +219,60 @@ __global__ void __launch_bounds__(256) dual_tma_kernel(const __grid_constant__ C
             P.tilde.p1[base + here] = q1;
             P.tilde.p2[base + here] = q2;
           }
-          if constexpr (TGV) {
+        }
+      }
+    } else if (TGV && warp == kChunk && lane < kChunk && x0 > 0 && i0 + k * kChunk + lane < i1) {
+      // ---- The side warp: w- at column x0 - 1 of the chunk's rows (a lane each).
+      const int rr = lane, ii = i0 + k * kChunk + rr;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        float t1, t2, w1, w2;
+        w_tilde(c, rr, kHalo - 1, ii, x0 - 1, t1, t2, w1, w2);
+        wleft[c][0][rr] = 2.0f * t1 - w1;
+        wleft[c][1][rr] = 2.0f * t2 - w2;
+      }
+    }
+    if constexpr (TGV) {
+      __syncthreads();
+      // ---- The r step from w- of the pixel and of its left and upper neighbours.
+      if (row) {
+        const bool has_down = i + 1 < rows, has_up = i > 0;
+        float step_r11[C], step_r22[C], step_r12[C], old_r11[C], old_r22[C], old_r12[C];
+        float square_r = 0.0f;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          float wl1 = __shfl_up_sync(kAll, wb1[c], 1), wl2 = __shfl_up_sync(kAll, wb2[c], 1);
+          if (lane == 0) {
+            wl1 = wleft[c][0][r];
+            wl2 = wleft[c][1][r];
+          }
+          if (!has_left) wl1 = wl2 = 0.0f;
+          float wu1 = r > 0 ? wbar[c][0][r - 1][lane] : carry[k & 1][c][0][lane];
+          float wu2 = r > 0 ? wbar[c][1][r - 1][lane] : carry[k & 1][c][1][lane];
+          if (!has_up) wu1 = wu2 = 0.0f;
+          const float own1x = has_right ? wb1[c] : 0.0f, own2x = has_right ? wb2[c] : 0.0f;
+          const float own1y = has_down ? wb1[c] : 0.0f, own2y = has_down ? wb2[c] : 0.0f;
+          const float exx = own1x - wl1;
+          const float eyy = own2y - wu2;
+          const float exy = 0.5f * ((own1y - wu1) + (own2x - wl2));
+          const float r11 = S(5, c, r, own), r22 = S(6, c, r, own), r12 = S(7, c, r, own);
+          old_r11[c] = r11;
+          old_r22[c] = r22;
+          old_r12[c] = r12;
+          const float sigma = P.sigma[c];
+          step_r11[c] = r11 + sigma * exx;
+          step_r22[c] = r22 + sigma * eyy;
+          step_r12[c] = r12 + sigma * exy;
+          if constexpr (COUPLED) {
+            square_r += step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]);
+          }
+        }
+        float scale_r = 1.0f;
+        if constexpr (COUPLED) scale_r = ball(square_r, P.radius0);
+        if (valid) {
+#pragma unroll
+          for (int c = 0; c < C; ++c) {
+            const std::size_t base = c * plane;
             float sr = scale_r;
             if constexpr (!COUPLED) {
               sr = ball(step_r11[c] * step_r11[c] + step_r22[c] * step_r22[c] + 2.0f * (step_r12[c] * step_r12[c]),
@@ -275,25 +309,48 @@ std::size_t dual_tma_shared_bytes(bool tgv, int channels) {
   return static_cast<std::size_t>(kSlots) * (fields + 1) * channels * kChunk * kSpan * sizeof(float);
 }
 
+// The strip height that finishes a sweep soonest: its CTAs in waves of `slots`, each wave as long
+// as a strip and the pipeline's start (about two chunks).
+int strip_rows_for(const Geometry& g, int slots) {
+  const int strips = (g.columns + 31) / 32;
+  int best = kStrip;
+  long long best_cost = -1;
+  for (int height = 64; height <= 512; height += 16) {
+    const long long ctas = static_cast<long long>(strips) * ((g.rows + height - 1) / height);
+    const long long cost = (ctas + slots - 1) / slots * (height + 2 * kChunk);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = height;
+    }
+  }
+  return best;
+}
+
 namespace {
 
 template <bool TGV, int C, bool COUPLED, bool KEEP>
 cudaError_t launch_one(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, cudaStream_t s) {
   auto kernel = dual_tma_kernel<TGV, C, COUPLED, KEEP>;
   const std::size_t bytes = dual_tma_shared_bytes(TGV, C);
-  // The shared-memory size above 48 KB is set once per device.
-  static std::atomic<unsigned long long> configured{0};
+  // Once per device: the shared-memory size above 48 KB, and how many CTAs the device holds at
+  // once (its SMs times the CTAs an SM holds).
+  static std::atomic<int> resident[64] = {};
   int device = 0;
   cudaGetDevice(&device);
-  const unsigned long long bit = 1ull << (device & 63);
-  if ((configured.load() & bit) == 0) {
-    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(bytes));
+  int slots = resident[device & 63].load();
+  if (slots == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    int per_sm = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, bytes);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    configured.fetch_or(bit);
+    slots = std::max(1, per_sm * sms);
+    resident[device & 63].store(slots);
   }
-  const dim3 grid((p.g.columns + 31) / 32, (p.g.rows + kStrip - 1) / kStrip, 1);
-  kernel<<<grid, 256, bytes, s>>>(state, tilde, p);
+  DualParams q = p;
+  q.strip_rows = strip_rows_for(p.g, slots);
+  const dim3 grid((p.g.columns + 31) / 32, (p.g.rows + q.strip_rows - 1) / q.strip_rows, 1);
+  kernel<<<grid, kThreads, bytes, s>>>(state, tilde, q);
   return cudaGetLastError();
 }
 
