@@ -54,6 +54,27 @@ unround_status unround_b200_measure(const unround_input* input, const unround_se
                                     uint64_t iterations, unround_b200_timing* timing, unround_result** result,
                                     char* message, size_t message_size);
 
+/* Many pictures solved together (no counterpart in the reference, whose callers solve one
+ * picture a call): `count` inputs, each with its settings (tv or tgv, the same number of
+ * iterations, --record-every 0), into `count` results, each freed by unround_result_free and
+ * each the result unround_solve gives that picture alone to binary32 rounding. The iterations but the
+ * last run for all pictures at once -- one launch per kernel class an iteration (the dual sweep
+ * of each method and channel count, the primal step of each cell layout) over tables of tiles
+ * of all pictures, captured in one CUDA graph launched once. `timing` (may be null) gets that
+ * part's device milliseconds (CUDA events), its iterations and launches per iteration, and the
+ * samples and pixels of all pictures. On failure no result is made. */
+typedef struct unround_b200_batch_timing {
+  double milliseconds;
+  uint64_t iterations;
+  uint64_t launches_per_iteration;
+  uint64_t samples;
+  uint64_t pixels;
+} unround_b200_batch_timing;
+
+unround_status unround_b200_solve_batch(uint64_t count, const unround_input* inputs,
+                                        const unround_settings* const* settings, unround_result** results,
+                                        unround_b200_batch_timing* timing, char* message, size_t message_size);
+
 /* What the host model makes of an input and settings, without a GPU (the reference computes the
  * same in Problem::make, cpp/src/model.cpp:134-256, and plan, cpp/src/pdhg.cpp:147-233): of
  * component `component`, `which` 0 the lower ends of the intervals, 1 the upper ends, 2 the

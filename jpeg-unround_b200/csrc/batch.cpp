@@ -1,0 +1,213 @@
+// The batched solve (batch.hpp).
+#include "batch.hpp"
+
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+
+#include "kernels.hpp"
+
+namespace urb {
+
+namespace {
+
+constexpr int kTileRows = 128;  // rows of a tile of the batched dual sweep (a multiple of 8)
+
+std::string describe(cudaError_t error) {
+  return std::string(cudaGetErrorName(error)) + ": " + cudaGetErrorString(error);
+}
+
+// Device memory owned for the call, freed on the stream at the end.
+struct Owned {
+  cudaStream_t stream;
+  std::vector<void*> blocks;
+  explicit Owned(cudaStream_t s) : stream(s) {}
+  ~Owned() {
+    for (void* p : blocks) cudaFreeAsync(p, stream);
+    cudaStreamSynchronize(stream);
+  }
+  template <typename T>
+  cudaError_t upload(const std::vector<T>& host, T** device) {
+    *device = nullptr;
+    if (host.empty()) return cudaSuccess;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, host.size() * sizeof(T), stream);
+    if (e != cudaSuccess) return e;
+    blocks.push_back(p);
+    *device = static_cast<T*>(p);
+    return cudaMemcpyAsync(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, stream);
+  }
+};
+
+struct DualClass {
+  bool tgv = false;
+  int channels = 1;
+  bool coupled = false;
+  std::vector<DualTile> tiles;
+  DualTile* device = nullptr;
+};
+
+struct PrimalClass {
+  int cell_rows = 1;
+  int cell_columns = 1;
+  std::vector<PrimalItem> items;
+  PrimalItem* device = nullptr;
+};
+
+}  // namespace
+
+bool check_batch(const std::vector<BatchEntry>& entries, Failure& failure) {
+  if (entries.empty()) {
+    failure = {kArgument, "a batch has at least one picture"};
+    return false;
+  }
+  const std::uint64_t most = entries[0].plan.iterations;
+  for (const BatchEntry& e : entries) {
+    if (e.plan.iterations != most) {
+      failure = {kArgument, "the pictures of a batch take the same number of iterations"};
+      return false;
+    }
+    if (e.plan.record_every != 0) {
+      failure = {kArgument, "a batch records each picture at its last iteration only: give --record-every 0"};
+      return false;
+    }
+  }
+  return true;
+}
+
+bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, std::vector<Outcome>& outcomes,
+                 BatchTiming& timing, Failure& failure) {
+  if (!check_batch(entries, failure)) return false;
+  const std::uint64_t most = entries[0].plan.iterations;
+  // Each picture's solver, started.
+  std::vector<std::unique_ptr<Solver>> solvers;
+  for (const BatchEntry& e : entries) {
+    solvers.push_back(std::make_unique<Solver>(*e.frame, stream));
+    if (!solvers.back()->begin_batch(e.plan, failure)) return false;
+  }
+  // The tables: each picture's entry, each component's, and per class the tiles and items.
+  std::vector<DualBatchImage> images(entries.size());
+  std::vector<PrimalBatchComponent> components;
+  std::map<std::tuple<bool, int, bool>, DualClass> duals;
+  std::map<std::pair<int, int>, PrimalClass> primals;
+  timing = BatchTiming{};
+  for (std::size_t n = 0; n < entries.size(); ++n) {
+    std::vector<PrimalBatchComponent> own;
+    if (!solvers[n]->batch_entries(images[n], own)) {
+      failure = {kUnsupported, "picture " + std::to_string(n) +
+                                   " has cells the batched primal step does not take (1, 2 or 4 samples each way)"};
+      return false;
+    }
+    const Geometry& g = solvers[n]->geometry();
+    const Plan& plan = entries[n].plan;
+    timing.samples += static_cast<std::uint64_t>(g.channels) * g.rows * g.columns;
+    timing.pixels += static_cast<std::uint64_t>(entries[n].frame->height) * entries[n].frame->width;
+    DualClass& dual = duals[{plan.tgv, g.channels, plan.coupled && g.channels > 1}];
+    dual.tgv = plan.tgv;
+    dual.channels = g.channels;
+    dual.coupled = plan.coupled && g.channels > 1;
+    for (int x0 = 0; x0 < g.columns; x0 += 32) {
+      for (int i0 = 0; i0 < g.rows; i0 += kTileRows) {
+        dual.tiles.push_back({static_cast<int>(n), x0, i0, std::min(i0 + kTileRows, g.rows)});
+      }
+    }
+    for (std::size_t c = 0; c < own.size(); ++c) {
+      const ComponentDevice& comp = own[c].params[0].component;
+      PrimalClass& primal = primals[{comp.cell_rows, comp.cell_columns}];
+      primal.cell_rows = comp.cell_rows;
+      primal.cell_columns = comp.cell_columns;
+      const int z = static_cast<int>(components.size());
+      const int strips = (g.columns + 31) / 32, stages = primal_batch_stages(g, comp.cell_rows);
+      for (int stage = 0; stage < stages; ++stage) {
+        for (int strip = 0; strip < strips; ++strip) primal.items.push_back({z, strip, stage, 0});
+      }
+      components.push_back(own[c]);
+    }
+  }
+  Owned owned(stream);
+  DualBatchImage* images_device = nullptr;
+  PrimalBatchComponent* components_device = nullptr;
+  cudaError_t error = owned.upload(images, &images_device);
+  if (error == cudaSuccess) error = owned.upload(components, &components_device);
+  for (auto& [key, dual] : duals) {
+    if (error == cudaSuccess) error = owned.upload(dual.tiles, &dual.device);
+  }
+  for (auto& [key, primal] : primals) {
+    if (error == cudaSuccess) error = owned.upload(primal.items, &primal.device);
+  }
+  // Iteration k (1-based): the primal steps read the state of parity (k - 1) % 2, the dual
+  // steps read it and write the other.
+  auto iteration = [&](std::uint64_t k, cudaStream_t on) {
+    const int parity = static_cast<int>((k - 1) % 2);
+    for (auto& [key, primal] : primals) {
+      if (error == cudaSuccess) {
+        error = launch_primal_batch(primal.device, static_cast<int>(primal.items.size()), components_device, parity,
+                                    primal.cell_rows, primal.cell_columns, on);
+      }
+    }
+    for (auto& [key, dual] : duals) {
+      if (error == cudaSuccess) {
+        error = launch_dual_batch(dual.device, static_cast<int>(dual.tiles.size()), images_device, parity, dual.tgv,
+                                  dual.channels, dual.coupled, on);
+      }
+    }
+  };
+  // The batch makes iterations 1 .. most - 1; each picture's last (which keeps its values for
+  // the record and the result) runs on its own.
+  const std::uint64_t batched = most > 0 ? most - 1 : 0;
+  timing.iterations = batched;
+  timing.launches_per_iteration = primals.size() + duals.size();
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t began = nullptr, ended = nullptr;
+  if (error == cudaSuccess) error = cudaEventCreate(&began);
+  if (error == cudaSuccess) error = cudaEventCreate(&ended);
+  if (batched > 1 && error == cudaSuccess) {
+    // Set up every launcher (shared memory, occupancy) before the capture: a launch of no work.
+    for (auto& [key, primal] : primals) {
+      if (error == cudaSuccess) {
+        error = launch_primal_batch(primal.device, 0, components_device, 0, primal.cell_rows, primal.cell_columns,
+                                    stream);
+      }
+    }
+    for (auto& [key, dual] : duals) {
+      if (error == cudaSuccess) {
+        error = launch_dual_batch(dual.device, 0, images_device, 0, dual.tgv, dual.channels, dual.coupled, stream);
+      }
+    }
+    if (error == cudaSuccess) error = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+    if (error == cudaSuccess) {
+      for (std::uint64_t k = 2; k <= batched; ++k) iteration(k, stream);
+      const cudaError_t ended_capture = cudaStreamEndCapture(stream, &graph);
+      if (error == cudaSuccess) error = ended_capture;
+    }
+    if (error == cudaSuccess) error = cudaGraphInstantiate(&exec, graph, 0);
+  }
+  if (error == cudaSuccess) error = cudaEventRecord(began, stream);
+  if (batched > 0) iteration(1, stream);
+  if (exec != nullptr && error == cudaSuccess) error = cudaGraphLaunch(exec, stream);
+  if (error == cudaSuccess) error = cudaEventRecord(ended, stream);
+  if (error == cudaSuccess) error = cudaEventSynchronize(ended);
+  float milliseconds = 0.0f;
+  if (error == cudaSuccess) error = cudaEventElapsedTime(&milliseconds, began, ended);
+  timing.milliseconds = milliseconds;
+  if (exec != nullptr) cudaGraphExecDestroy(exec);
+  if (graph != nullptr) cudaGraphDestroy(graph);
+  if (began != nullptr) cudaEventDestroy(began);
+  if (ended != nullptr) cudaEventDestroy(ended);
+  if (error != cudaSuccess) {
+    failure = {kInternal, "the device failed in the batched iterations: " + describe(error)};
+    return false;
+  }
+  outcomes.assign(entries.size(), Outcome{});
+  for (std::size_t n = 0; n < entries.size(); ++n) {
+    if (!solvers[n]->finish_batch(batched, outcomes[n], failure)) {
+      failure.message = "picture " + std::to_string(n) + ": " + failure.message;
+      return false;
+    }
+  }
+  return true;
+}
+
+}  // namespace urb

@@ -12,6 +12,7 @@
 
 #include <cuda_runtime.h>
 
+#include "batch.hpp"
 #include "model.hpp"
 #include "settings.hpp"
 #include "solver.hpp"
@@ -397,6 +398,65 @@ unround_status unround_b200_measure(const unround_input* input, const unround_se
       }
     }
     if (result != nullptr) *result = result_of(std::move(*frame), std::move(outcome));
+    return true;
+  });
+}
+
+unround_status unround_b200_solve_batch(uint64_t count, const unround_input* inputs,
+                                        const unround_settings* const* settings, unround_result** results,
+                                        unround_b200_batch_timing* timing, char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (count == 0 || inputs == nullptr || settings == nullptr || results == nullptr) {
+      failure = {urb::kArgument, "a batch has pictures, settings and result slots (not null pointers)"};
+      return false;
+    }
+    for (uint64_t n = 0; n < count; ++n) results[n] = nullptr;
+    std::vector<urb::Frame> frames;
+    frames.reserve(count);
+    std::vector<urb::BatchEntry> entries;
+    for (uint64_t n = 0; n < count; ++n) {
+      if (settings[n] == nullptr) {
+        failure = {urb::kArgument, "picture " + std::to_string(n) + " has no settings"};
+        return false;
+      }
+      const urb::Settings& s = settings[n]->settings;
+      if (s.method != urb::Method::tv && s.method != urb::Method::tgv) {
+        failure = {urb::kOptions, "picture " + std::to_string(n) + ": a batch solves by tv or tgv"};
+        return false;
+      }
+      std::vector<urb::ComponentInput> components;
+      if (!inputs_of(&inputs[n], components, failure)) return false;
+      auto frame = urb::make_frame(inputs[n].height, inputs[n].width, inputs[n].color_space, components, s, failure);
+      if (!frame) {
+        failure.message = "picture " + std::to_string(n) + ": " + failure.message;
+        return false;
+      }
+      frames.push_back(std::move(*frame));
+      auto plan = urb::make_plan(s, frames.back().channels(), failure);
+      if (!plan) {
+        failure.message = "picture " + std::to_string(n) + ": " + failure.message;
+        return false;
+      }
+      entries.push_back({&frames.back(), *plan});
+    }
+    if (!urb::check_batch(entries, failure)) return false;
+    if (!have_device(failure)) return false;
+    Stream stream;
+    if (stream.error != cudaSuccess) {
+      failure = {urb::kInternal, std::string("a CUDA stream: ") + cudaGetErrorString(stream.error)};
+      return false;
+    }
+    std::vector<urb::Outcome> outcomes;
+    urb::BatchTiming measured;
+    if (!urb::solve_batch(entries, stream.stream, outcomes, measured, failure)) return false;
+    if (timing != nullptr) {
+      timing->milliseconds = measured.milliseconds;
+      timing->iterations = measured.iterations;
+      timing->launches_per_iteration = measured.launches_per_iteration;
+      timing->samples = measured.samples;
+      timing->pixels = measured.pixels;
+    }
+    for (uint64_t n = 0; n < count; ++n) results[n] = result_of(std::move(frames[n]), std::move(outcomes[n]));
     return true;
   });
 }

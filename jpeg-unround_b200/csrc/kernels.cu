@@ -485,11 +485,138 @@ constexpr int primal_warps() {
   return kStageRows / (8 * CR);
 }
 
+// One warp's block row of a stage, from shared memory: `slot` the stage's box (x, p1, p2: the
+// row above and 64 rows of 40 columns each), `stage_levels` the levels of the lane's block.
+// v = x + tau gamma div p, the cell means less the middle of the DC interval, the DCT, the
+// clip, the inverse DCT, x~ written (and with KEEP zeta and v, and the data term's terms added
+// to `sum`). `t` is the warp's transpose tile.
+template <int CR, int CC, bool KEEP>
+__device__ __forceinline__ void primal_block_row(const float* slot, const std::int16_t* stage_levels,
+                                                 const PrimalParams& P, const ProxFactors& F, float* t, int warp,
+                                                 int lane, int vby, int j, bool column_in, bool in_blocks, bool flat,
+                                                 std::size_t block, double& sum) {
+  constexpr unsigned kAll = 0xffffffffu;
+  constexpr int L = 8 * CC, BH = 8 * CR;
+  constexpr int SPAN = 40, HALO = 4, PLANE = (kStageRows + 1) * SPAN;
+  const int in_block = lane % L, m = in_block / CC, cell = in_block % CC;
+  const int leader = lane - cell;
+  const int col = HALO + lane;
+  const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+  const float descent = P.descent;
+  const int i0 = vby * BH;
+  const int base_row = 1 + warp * BH;  // shared-memory row of canvas row i0
+  float v[BH];
+#pragma unroll
+  for (int r = 0; r < BH; ++r) {
+    const int i = i0 + r, sr = base_row + r;
+    const float x = slot[0 * PLANE + sr * SPAN + col];
+    const float p1 = slot[1 * PLANE + sr * SPAN + col];
+    const float p2 = slot[2 * PLANE + sr * SPAN + col];
+    const float before = slot[1 * PLANE + sr * SPAN + col - 1];
+    const float above = slot[2 * PLANE + (sr - 1) * SPAN + col];
+    const float dy = (i + 1 < rows ? p2 : 0.0f) - (i > 0 ? above : 0.0f);
+    const float dx = (j + 1 < columns ? p1 : 0.0f) - (j > 0 ? before : 0.0f);
+    v[r] = x + descent * (dy + dx);
+  }
+  const float dc_level = in_blocks ? static_cast<float>(stage_levels[0]) : 0.0f;
+  const float middle = (dc_level * F.step[0] + 1024.0f) * 0.125f;
+  float mean[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    if constexpr (CR == 1 && CC == 1) {
+      mean[r] = v[r] - middle;
+    } else {
+      float column = v[CR * r];
+#pragma unroll
+      for (int a = 1; a < CR; ++a) column += v[CR * r + a];
+      float total = 0.0f;
+#pragma unroll
+      for (int c = 0; c < CC; ++c) {
+        const float part = __shfl_sync(kAll, column, leader + c);
+        total = c == 0 ? part : total + part;
+      }
+      mean[r] = total / static_cast<float>(CR * CC) - middle;
+    }
+  }
+  float colv[8], row[8], coef[8], zeta[8];
+  forward8(mean, colv);
+  __syncwarp();
+  if (cell == 0) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t[k * 9 + m] = colv[k];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int u = 0; u < 8; ++u) row[u] = t[m * 9 + u];
+  forward8(row, coef);
+  int levels[8];
+  const int4 packed = in_blocks ? *reinterpret_cast<const int4*>(stage_levels + m * 8) : make_int4(0, 0, 0, 0);
+  const int words[4] = {packed.x, packed.y, packed.z, packed.w};
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const unsigned word = static_cast<unsigned>(words[u >> 1]);
+    levels[u] = static_cast<int>(static_cast<std::int16_t>((u & 1) ? (word >> 16) : (word & 0xffffu)));
+  }
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int k = m * 8 + u;
+    const Coefficient c = coefficient_of(levels[u], k, F);
+    const float tk = flat ? F.t_flat[k] : F.t[k];
+    const float rk = flat ? F.r_flat[k] : F.r[k];
+    const float hk = flat ? F.h_flat[k] : F.h[k];
+    zeta[u] = prox_of(coef[u], tk, rk, hk, c, F.costed != 0);
+  }
+  if constexpr (KEEP) {
+    if (in_blocks && cell == 0) {
+      float4* to = reinterpret_cast<float4*>(P.component.zeta + block * 64 + m * 8);
+      to[0] = make_float4(zeta[0], zeta[1], zeta[2], zeta[3]);
+      to[1] = make_float4(zeta[4], zeta[5], zeta[6], zeta[7]);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = m * 8 + u;
+        const double absolute =
+            k == 0 ? static_cast<double>(zeta[u]) +
+                         (static_cast<double>(levels[0]) * P.component.constants->step[0] + 1024.0)
+                   : static_cast<double>(zeta[u]);
+        sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
+      }
+    }
+  }
+  inverse8(zeta, row);
+  __syncwarp();
+  if (cell == 0) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) t[m * 9 + c] = row[c];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 8; ++k) colv[k] = t[k * 9 + m];
+  float back[8];
+  inverse8(colv, back);
+  if (column_in) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+#pragma unroll
+      for (int a = 0; a < CR; ++a) {
+        const int rr = CR * r + a;
+        float out;
+        if constexpr (CR == 1 && CC == 1) {
+          out = in_blocks ? back[r] + middle : v[rr];
+        } else {
+          out = in_blocks ? v[rr] + (back[r] - mean[r]) : v[rr];
+        }
+        const std::size_t at = static_cast<std::size_t>(i0 + rr) * pitch + j;
+        P.xt[at] = out;
+        if constexpr (KEEP) P.v[at] = v[rr];
+      }
+    }
+  }
+}
+
 template <int CR, int CC, bool KEEP>
 __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(const __grid_constant__ CUtensorMap map0,
                                                                              const __grid_constant__ CUtensorMap map1,
                                                                              const __grid_constant__ PrimalBatch Q) {
-  constexpr unsigned kAll = 0xffffffffu;
   constexpr int NB = primal_warps<CR>();
   constexpr int L = 8 * CC, B = 32 / L, BH = 8 * CR;
   constexpr int SR = kStageRows + 1, SPAN = 40, HALO = 4;
@@ -557,9 +684,7 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
   };
   issue(0);
   issue(1);
-  const int blk = lane / L, in_block = lane % L, m = in_block / CC, cell = in_block % CC;
-  const int leader = lane - cell;
-  const int col = HALO + lane;
+  const int blk = lane / L, in_block = lane % L;
   float* t = tile[warp][blk];
   double sum0 = 0.0, sum1 = 0.0;  // the data term's terms of each component
   bool failed = false;
@@ -570,12 +695,10 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
     const PrimalParams& P = parts[z];
     const ProxFactors& F = factors[z];
     double sum = 0.0;
-    const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
-    const int vbr = rows / BH;
+    const int vbr = P.g.rows / BH;
     const int vbx = strip * B + blk;
     const int j = vbx * L + in_block;
-    const bool column_in = j < columns;
-    const float descent = P.descent;
+    const bool column_in = j < P.g.columns;
     const int vby = stage * NB + warp;
     const bool in_blocks =
         vby < vbr && column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
@@ -592,115 +715,8 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
     const float* slot = ring + (s & 1) * STRIDE;
     const std::int16_t* stage_levels = levels_ring + (s & 1) * kStageLevels + (warp * B + blk) * 64;
     if (vby < vbr) {
-      const int i0 = vby * BH;
-      const int base_row = 1 + warp * BH;  // shared-memory row of canvas row i0
-      float v[BH];
-#pragma unroll
-      for (int r = 0; r < BH; ++r) {
-        const int i = i0 + r, sr = base_row + r;
-        const float x = slot[0 * PLANE + sr * SPAN + col];
-        const float p1 = slot[1 * PLANE + sr * SPAN + col];
-        const float p2 = slot[2 * PLANE + sr * SPAN + col];
-        const float before = slot[1 * PLANE + sr * SPAN + col - 1];
-        const float above = slot[2 * PLANE + (sr - 1) * SPAN + col];
-        const float dy = (i + 1 < rows ? p2 : 0.0f) - (i > 0 ? above : 0.0f);
-        const float dx = (j + 1 < columns ? p1 : 0.0f) - (j > 0 ? before : 0.0f);
-        v[r] = x + descent * (dy + dx);
-      }
-      const float dc_level = in_blocks ? static_cast<float>(stage_levels[0]) : 0.0f;
-      const float middle = (dc_level * F.step[0] + 1024.0f) * 0.125f;
-      float mean[8];
-#pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        if constexpr (CR == 1 && CC == 1) {
-          mean[r] = v[r] - middle;
-        } else {
-          float column = v[CR * r];
-#pragma unroll
-          for (int a = 1; a < CR; ++a) column += v[CR * r + a];
-          float total = 0.0f;
-#pragma unroll
-          for (int c = 0; c < CC; ++c) {
-            const float part = __shfl_sync(kAll, column, leader + c);
-            total = c == 0 ? part : total + part;
-          }
-          mean[r] = total / static_cast<float>(CR * CC) - middle;
-        }
-      }
-      float colv[8], row[8], coef[8], zeta[8];
-      forward8(mean, colv);
-      __syncwarp();
-      if (cell == 0) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) t[k * 9 + m] = colv[k];
-      }
-      __syncwarp();
-#pragma unroll
-      for (int u = 0; u < 8; ++u) row[u] = t[m * 9 + u];
-      forward8(row, coef);
-      int levels[8];
-      const int4 packed =
-          in_blocks ? *reinterpret_cast<const int4*>(stage_levels + m * 8) : make_int4(0, 0, 0, 0);
-      const int words[4] = {packed.x, packed.y, packed.z, packed.w};
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const unsigned word = static_cast<unsigned>(words[u >> 1]);
-        levels[u] = static_cast<int>(static_cast<std::int16_t>((u & 1) ? (word >> 16) : (word & 0xffffu)));
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int k = m * 8 + u;
-        const Coefficient c = coefficient_of(levels[u], k, F);
-        const float tk = flat ? F.t_flat[k] : F.t[k];
-        const float rk = flat ? F.r_flat[k] : F.r[k];
-        const float hk = flat ? F.h_flat[k] : F.h[k];
-        zeta[u] = prox_of(coef[u], tk, rk, hk, c, F.costed != 0);
-      }
-      if constexpr (KEEP) {
-        if (in_blocks && cell == 0) {
-          float4* to = reinterpret_cast<float4*>(P.component.zeta + block * 64 + m * 8);
-          to[0] = make_float4(zeta[0], zeta[1], zeta[2], zeta[3]);
-          to[1] = make_float4(zeta[4], zeta[5], zeta[6], zeta[7]);
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const int k = m * 8 + u;
-            const double absolute =
-                k == 0 ? static_cast<double>(zeta[u]) +
-                             (static_cast<double>(levels[0]) * P.component.constants->step[0] + 1024.0)
-                       : static_cast<double>(zeta[u]);
-            sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
-          }
-        }
-      }
-      inverse8(zeta, row);
-      __syncwarp();
-      if (cell == 0) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) t[m * 9 + c] = row[c];
-      }
-      __syncwarp();
-#pragma unroll
-      for (int k = 0; k < 8; ++k) colv[k] = t[k * 9 + m];
-      float back[8];
-      inverse8(colv, back);
-      if (column_in) {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-#pragma unroll
-          for (int a = 0; a < CR; ++a) {
-            const int rr = CR * r + a;
-            float out;
-            if constexpr (CR == 1 && CC == 1) {
-              out = in_blocks ? back[r] + middle : v[rr];
-            } else {
-              out = in_blocks ? v[rr] + (back[r] - mean[r]) : v[rr];
-            }
-            const std::size_t at = static_cast<std::size_t>(i0 + rr) * pitch + j;
-            P.xt[at] = out;
-            if constexpr (KEEP) P.v[at] = v[rr];
-          }
-        }
-      }
+      primal_block_row<CR, CC, KEEP>(slot, stage_levels, P, F, t, warp, lane, vby, j, column_in, in_blocks, flat,
+                                     block, sum);
     }
     if (z == 0) {
       sum0 += sum;
@@ -720,6 +736,108 @@ __global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(con
   if (failed) {
     // No load may still write into shared memory when the CTA leaves: the item that was not
     // ready and the one after it.
+    for (int s = stopped; s < min(stopped + 2, items); ++s) barrier_wait(&bars[s & 1], (s >> 1) & 1);
+  }
+}
+
+// The primal step of a batch (many components of one cell layout, of many images, of different
+// sizes): a table of items (component, strip, stage); each CTA takes a contiguous range of it
+// through the same two-slot ring as primal_tma_kernel. Each item's parameters and box map are
+// the component's entry of `components` in global memory (the map read through the tensor-map
+// proxy after an acquire fence); its factors are read from global memory. Nothing is kept (the
+// batch's last primal step, which keeps, runs per image).
+template <int CR, int CC>
+__global__ void __launch_bounds__(32 * primal_warps<CR>())
+    primal_batch_kernel(const PrimalItem* __restrict__ list, int count, const PrimalBatchComponent* components,
+                        int parity) {
+  constexpr int NB = primal_warps<CR>();
+  constexpr int L = 8 * CC, B = 32 / L, BH = 8 * CR;
+  constexpr int SR = kStageRows + 1, SPAN = 40, HALO = 4;
+  constexpr int PLANE = SR * SPAN, SLOT = 3 * PLANE;
+  constexpr int STRIDE = (SLOT + 31) / 32 * 32;
+  extern __shared__ __align__(128) float ring[];
+  __shared__ __align__(8) std::uint64_t bars[2];
+  __shared__ PrimalParams parts[2];  // of the items in the two slots
+  __shared__ float tile[NB][4][72];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int first = static_cast<int>(static_cast<long long>(blockIdx.x) * count / gridDim.x);
+  const int items = static_cast<int>(static_cast<long long>(blockIdx.x + 1) * count / gridDim.x) - first;
+  if (tid == 0) {
+    barrier_init(&bars[0], 1);
+    barrier_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  std::int16_t* const levels_ring = reinterpret_cast<std::int16_t*>(ring + 2 * STRIDE);
+  constexpr int kStageLevels = NB * B * 64;
+  auto issue = [&](int n) {
+    if (tid == 0 && n < items) {
+      const PrimalItem item = list[first + n];
+      const PrimalBatchComponent& entry = components[item.component];
+      const PrimalParams& P = entry.params[parity];
+      parts[n & 1] = P;
+      const CUtensorMap* map = &entry.map[parity];
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+      const int vbr = P.g.rows / BH;
+      const int stage_first = item.stage * NB;
+      const int vbx0 = item.strip * B;
+      const int blocks = min(B, P.component.block_columns - vbx0);
+      int rows_copied = 0;
+      for (int w = 0; w < NB; ++w) {
+        const int vby = stage_first + w;
+        if (vby < vbr && vby < P.component.block_rows && blocks > 0) ++rows_copied;
+      }
+      barrier_expect(&bars[n & 1], SLOT * 4 + rows_copied * blocks * 128);
+      load_box(ring + (n & 1) * STRIDE, map, &bars[n & 1], item.strip * 32 - HALO, stage_first * BH - 1, 0);
+      for (int w = 0; w < NB; ++w) {
+        const int vby = stage_first + w;
+        if (vby < vbr && vby < P.component.block_rows && blocks > 0) {
+          load_bulk(levels_ring + (n & 1) * kStageLevels + w * B * 64,
+                    P.component.levels + (static_cast<std::size_t>(vby) * P.component.block_columns + vbx0) * 64,
+                    blocks * 128, &bars[n & 1]);
+        }
+      }
+    }
+  };
+  issue(0);
+  issue(1);
+  __syncthreads();  // the first two items' parameters
+  const int blk = lane / L, in_block = lane % L;
+  float* t = tile[warp][blk];
+  double sum = 0.0;  // unused: nothing is kept
+  bool failed = false;
+  int stopped = items;
+  for (int s = 0; s < items; ++s) {
+    const PrimalItem item = list[first + s];
+    const PrimalParams& P = parts[s & 1];
+    const ProxFactors& F = *P.component.factors;
+    const int vbr = P.g.rows / BH;
+    const int vbx = item.strip * B + blk;
+    const int j = vbx * L + in_block;
+    const bool column_in = j < P.g.columns;
+    const int vby = item.stage * NB + warp;
+    const bool in_blocks =
+        vby < vbr && column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
+    const std::size_t block =
+        static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
+    const bool flat = in_blocks && P.component.flat[block] != 0;
+    const bool ready = barrier_wait(&bars[s & 1], (s >> 1) & 1);
+    if (__syncthreads_or(!ready)) {
+      failed = true;
+      stopped = s;
+      break;
+    }
+    const float* slot = ring + (s & 1) * STRIDE;
+    const std::int16_t* stage_levels = levels_ring + (s & 1) * kStageLevels + (warp * B + blk) * 64;
+    if (vby < vbr) {
+      primal_block_row<CR, CC, false>(slot, stage_levels, P, F, t, warp, lane, vby, j, column_in, in_blocks, flat,
+                                      block, sum);
+    }
+    __syncthreads();  // every warp is done with the slot and its parameters
+    issue(s + 2);
+  }
+  if (failed && tid == 0 && parts[stopped & 1].error != nullptr) atomicExch(parts[stopped & 1].error, 1);
+  if (failed) {
     for (int s = stopped; s < min(stopped + 2, items); ++s) barrier_wait(&bars[s & 1], (s >> 1) & 1);
   }
 }
@@ -1296,7 +1414,48 @@ cudaError_t primal_tma_keep(const CUtensorMap* maps, const PrimalParams* parts, 
               : primal_tma_one<CR, CC, false>(maps, parts, count, s, grid);
 }
 
+template <int CR, int CC>
+cudaError_t primal_batch_one(const PrimalItem* list, int count, const PrimalBatchComponent* components, int parity,
+                             cudaStream_t s) {
+  auto kernel = primal_batch_kernel<CR, CC>;
+  constexpr int threads = 32 * primal_warps<CR>();
+  constexpr std::size_t bytes = 2 * ((3 * (kStageRows + 1) * 40 + 31) / 32 * 32) * sizeof(float) +
+                                2 * (kStageRows / (8 * CR)) * (32 / (8 * CC)) * 64 * sizeof(std::int16_t);
+  static std::atomic<int> resident[64] = {};
+  int device = 0;
+  cudaGetDevice(&device);
+  int slots = resident[device & 63].load();
+  if (slots == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    int per_sm = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, bytes);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    slots = std::max(1, per_sm * sms);
+    resident[device & 63].store(slots);
+  }
+  if (count <= 0) return cudaSuccess;
+  kernel<<<std::min(count, slots), threads, bytes, s>>>(list, count, components, parity);
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t launch_primal_batch(const PrimalItem* list, int count, const PrimalBatchComponent* components, int parity,
+                                int cell_rows, int cell_columns, cudaStream_t stream) {
+#define URB_BATCH_CELL(R, C) \
+  if (cell_rows == R && cell_columns == C) return primal_batch_one<R, C>(list, count, components, parity, stream);
+  URB_BATCH_CELL(1, 1) URB_BATCH_CELL(1, 2) URB_BATCH_CELL(2, 1) URB_BATCH_CELL(2, 2) URB_BATCH_CELL(1, 4)
+  URB_BATCH_CELL(4, 1) URB_BATCH_CELL(2, 4) URB_BATCH_CELL(4, 2) URB_BATCH_CELL(4, 4)
+#undef URB_BATCH_CELL
+  return cudaErrorInvalidValue;
+}
+
+int primal_batch_stages(const Geometry& g, int cell_rows) {
+  const int nb = kStageRows / (8 * cell_rows);
+  const int vbr = g.rows / (8 * cell_rows);
+  return (vbr + nb - 1) / nb;
+}
 
 bool primal_tma_takes(const ComponentDevice& c) {
   auto fits = [](int n) { return n == 1 || n == 2 || n == 4; };

@@ -212,6 +212,43 @@ cudaError_t launch_primal_tma(const CUtensorMap* maps, const PrimalParams* parts
 // The rows a CTA of a strip sweep walks (a multiple of 16) so that the sweep's CTAs, `slots`
 // of them resident at once, finish soonest (sweep.cu).
 int strip_rows_for(const Geometry& g, int slots);
+
+// The batched solve (batch.cu): one launch steps many images' states. A component's or an
+// image's entry holds its tensor maps and parameters for each state parity (the state the step
+// reads: 0 or 1), in device memory; the maps are read through the tensor-map proxy.
+struct alignas(64) PrimalBatchComponent {
+  CUtensorMap map[2];      // the component's x, p1, p2 planes of each state (make_primal_map)
+  PrimalParams params[2];  // its primal step reading each state
+};
+// An item of a batched primal step: a stage of 64 canvas rows of a strip of 32 columns.
+struct PrimalItem {
+  int component = 0;
+  int strip = 0;
+  int stage = 0;
+  int pad = 0;
+};
+// The stages of a strip of a component of cells `cell_rows` high.
+int primal_batch_stages(const Geometry& g, int cell_rows);
+// The primal step (no values kept) of every item of `list`, of components of the same cells.
+cudaError_t launch_primal_batch(const PrimalItem* list, int count, const PrimalBatchComponent* components, int parity,
+                                int cell_rows, int cell_columns, cudaStream_t stream);
+
+struct alignas(64) DualBatchImage {
+  CUtensorMap state[2];   // the sweep's maps of each state (make_sweep_map)
+  CUtensorMap tilde;      // of x~
+  DualParams params[2];   // the dual step from each state
+};
+// A tile of a batched dual step: columns x0 .. x0 + 31, rows i0 .. i1 - 1 of an image.
+struct DualTile {
+  int image = 0;
+  int x0 = 0;
+  int i0 = 0;
+  int i1 = 0;
+};
+// The dual step (no values kept) of every tile of `tiles`, of images of the same method and
+// channels.
+cudaError_t launch_dual_batch(const DualTile* tiles, int count, const DualBatchImage* images, int parity, bool tgv,
+                              int channels, bool coupled, cudaStream_t stream);
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,
                             bool coupled, bool keep, cudaStream_t stream);
 // A 3D tiled map of `count` float planes `stride` floats apart, boxes of 40 columns x

@@ -609,6 +609,14 @@ bool Solver::solve(Method method, const Plan* plan, const Start* start, const Ob
   m.start(start, true);
   bytes_ = m.bytes;
   if (!m.check(failure, "the start")) return false;
+  return run(0, observer, out, failure);
+}
+
+// The method's loop from `first` iterations made (their primal and dual steps done, the state
+// of iteration `first` the current one) to the end: records, stops and the result.
+bool Solver::run(std::uint64_t first, const Observer& observer, Outcome& out, Failure& failure) {
+  Impl& m = *impl_;
+  const Plan* plan = &m.plan;
   out.tau = plan->tau;
   out.sigma = plan->sigma;
   const double samples = static_cast<double>(m.g.channels) * m.g.rows * m.g.columns;
@@ -656,9 +664,9 @@ bool Solver::solve(Method method, const Plan* plan, const Start* start, const Ob
   };
   auto recorded = [&](std::uint64_t n) { return (every > 0 && n % every == 0) || n == most; };
   bool stopped = false;
-  if (every > 0 || most == 0) stopped = take(0);
-  std::uint64_t iteration = 0;
-  if (!stopped && most > 0) m.primal(recorded(1));
+  if (first == 0 && (every > 0 || most == 0)) stopped = take(0);
+  std::uint64_t iteration = first;
+  if (!stopped && first < most) m.primal(recorded(first + 1));
   while (!stopped && iteration < most && m.error == cudaSuccess) {
     const std::uint64_t next = iteration + 1;
     // One sweep for D_next and P_{next+1} when neither keeps anything: no record after the
@@ -686,6 +694,51 @@ bool Solver::solve(Method method, const Plan* plan, const Start* start, const Ob
     m.result(out);
   }
   return m.check(failure, "the result");
+}
+
+bool Solver::begin_batch(const Plan& plan, Failure& failure) {
+  Impl& m = *impl_;
+  m.plan = plan;
+  m.setup(plan.tgv, false);
+  m.set_factors(plan);
+  m.start(nullptr, true);
+  bytes_ = m.bytes;
+  return m.check(failure, "the start");
+}
+
+bool Solver::batch_entries(DualBatchImage& image, std::vector<PrimalBatchComponent>& components) {
+  Impl& m = *impl_;
+  if (!m.swept) return false;
+  const int saved = m.current;
+  for (int s = 0; s < 2; ++s) {
+    m.current = s;
+    image.state[s] = m.state_maps[s];
+    image.params[s] = m.dual_params();
+  }
+  image.tilde = m.tilde_maps[m.xt_id];
+  components.clear();
+  for (std::size_t c = 0; c < m.components.size(); ++c) {
+    if (!m.primal_swept[c]) {
+      m.current = saved;
+      return false;
+    }
+    PrimalBatchComponent entry;
+    for (int s = 0; s < 2; ++s) {
+      m.current = s;
+      entry.map[s] = m.primal_maps[s][c];
+      entry.params[s] = m.primal_params(c);
+    }
+    components.push_back(entry);
+  }
+  m.current = saved;
+  return true;
+}
+
+bool Solver::finish_batch(std::uint64_t done, Outcome& out, Failure& failure) {
+  Impl& m = *impl_;
+  m.current = static_cast<int>(done % 2);
+  if (!m.check(failure, "the batched iterations")) return false;
+  return run(done, Observer{}, out, failure);
 }
 
 bool Solver::prepare(const Plan& plan, Failure& failure) {

@@ -78,11 +78,21 @@ class Solver {
   // The binary64 canvas of the last tilde point, after prepare/iterate.
   bool finish(Outcome& out, Failure& failure);
 
+  // For a batched loop (batch.cpp runs the iterations of many solvers in one graph): the start
+  // and no iteration; the entries of this solver's state that the batched kernels read (false
+  // where a kernel of this state has no batched form); and, after `done` iterations made by the
+  // batch (the state of iteration `done` current), the rest as solve() makes it: the remaining
+  // iterations, the records and the result. The batch's plans record at the last iteration only.
+  bool begin_batch(const Plan& plan, Failure& failure);
+  bool batch_entries(DualBatchImage& image, std::vector<PrimalBatchComponent>& components);
+  bool finish_batch(std::uint64_t done, Outcome& out, Failure& failure);
+
   [[nodiscard]] std::size_t device_bytes() const { return bytes_; }
   [[nodiscard]] const Geometry& geometry() const { return geometry_; }
   [[nodiscard]] int launches_per_iteration() const;
 
  private:
+  bool run(std::uint64_t first, const Observer& observer, Outcome& out, Failure& failure);
   struct Impl;
   std::unique_ptr<Impl> impl_;
   Geometry geometry_;

@@ -46,10 +46,11 @@ __device__ __forceinline__ T ball(T square, T radius) {
   return norm > radius ? radius / norm : T(1);
 }
 
+// One CTA's strip: columns x0 .. x0 + 31, rows i0 .. i1 - 1 (a whole number of chunks, or the
+// canvas's last rows), of the image whose maps and parameters these are.
 template <bool TGV, int C, bool COUPLED, bool KEEP>
-__global__ void __launch_bounds__(kThreads, 2) dual_tma_kernel(const __grid_constant__ CUtensorMap state_map,
-                                                                const __grid_constant__ CUtensorMap tilde_map,
-                                                                const DualParams P) {
+__device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const CUtensorMap* tilde_map,
+                                           const DualParams& P, int x0, int i0, int i1) {
   constexpr int F = TGV ? 8 : 3;  // state planes per channel: x, p1, p2 (+ w1, w2, r11, r22, r12)
   constexpr int PLANE = kChunk * kSpan;
   constexpr int SLOT = (F + 1) * C * PLANE;  // floats: the state planes, then x~'s
@@ -62,9 +63,6 @@ __global__ void __launch_bounds__(kThreads, 2) dual_tma_kernel(const __grid_cons
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
   const std::size_t plane = P.g.plane;
-  const int x0 = blockIdx.x * 32;
-  const int i0 = blockIdx.y * P.strip_rows;
-  const int i1 = min(i0 + P.strip_rows, rows);
   const int chunks = (i1 - i0 + kChunk - 1) / kChunk;
   const int j = x0 + lane;
   const bool valid = j < columns;
@@ -83,8 +81,8 @@ __global__ void __launch_bounds__(kThreads, 2) dual_tma_kernel(const __grid_cons
       const int slot = k % kSlots;
       float* to = ring + slot * SLOT;
       barrier_expect(&bars[slot], SLOT * 4);
-      load_box(to, &state_map, &bars[slot], x0 - kHalo, i0 + k * kChunk, 0);
-      load_box(to + F * C * PLANE, &tilde_map, &bars[slot], x0 - kHalo, i0 + k * kChunk, 0);
+      load_box(to, state_map, &bars[slot], x0 - kHalo, i0 + k * kChunk, 0);
+      load_box(to + F * C * PLANE, tilde_map, &bars[slot], x0 - kHalo, i0 + k * kChunk, 0);
     }
   };
   issue(0);
@@ -302,6 +300,32 @@ __global__ void __launch_bounds__(kThreads, 2) dual_tma_kernel(const __grid_cons
   }
 }
 
+template <bool TGV, int C, bool COUPLED, bool KEEP>
+__global__ void __launch_bounds__(kThreads, 2) dual_tma_kernel(const __grid_constant__ CUtensorMap state_map,
+                                                                const __grid_constant__ CUtensorMap tilde_map,
+                                                                const DualParams P) {
+  const int i0 = blockIdx.y * P.strip_rows;
+  dual_strip<TGV, C, COUPLED, KEEP>(&state_map, &tilde_map, P, blockIdx.x * 32, i0, min(i0 + P.strip_rows, P.g.rows));
+}
+
+// The dual step of a batch: a CTA a tile of the table, of the image whose entry (maps and
+// parameters, in global memory) the tile names; the maps are read through the tensor-map proxy
+// after an acquire fence.
+template <bool TGV, int C, bool COUPLED>
+__global__ void __launch_bounds__(kThreads, 2) dual_batch_kernel(const DualTile* __restrict__ tiles,
+                                                                  const DualBatchImage* images, int parity) {
+  __shared__ DualParams P;
+  const DualTile tile = tiles[blockIdx.x];
+  const DualBatchImage& image = images[tile.image];
+  if (threadIdx.x == 0) {
+    P = image.params[parity];
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&image.state[parity]) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&image.tilde) : "memory");
+  }
+  __syncthreads();
+  dual_strip<TGV, C, COUPLED, false>(&image.state[parity], &image.tilde, P, tile.x0, tile.i0, tile.i1);
+}
+
 }  // namespace
 
 std::size_t dual_tma_shared_bytes(bool tgv, int channels) {
@@ -418,6 +442,49 @@ cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, 
                             bool coupled, bool keep, cudaStream_t stream) {
   return tgv ? launch_channels<true>(state, tilde, p, coupled, keep, stream)
              : launch_channels<false>(state, tilde, p, coupled, keep, stream);
+}
+
+namespace {
+
+template <bool TGV, int C, bool COUPLED>
+cudaError_t dual_batch_one(const DualTile* tiles, int count, const DualBatchImage* images, int parity, cudaStream_t s) {
+  auto kernel = dual_batch_kernel<TGV, C, COUPLED>;
+  const std::size_t bytes = dual_tma_shared_bytes(TGV, C);
+  // The shared-memory size above 48 KB is set once per device.
+  static std::atomic<unsigned long long> configured{0};
+  int device = 0;
+  cudaGetDevice(&device);
+  const unsigned long long bit = 1ull << (device & 63);
+  if ((configured.load() & bit) == 0) {
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(bytes));
+    if (e != cudaSuccess) return e;
+    configured.fetch_or(bit);
+  }
+  if (count <= 0) return cudaSuccess;
+  kernel<<<count, kThreads, bytes, s>>>(tiles, images, parity);
+  return cudaGetLastError();
+}
+
+template <bool TGV>
+cudaError_t dual_batch_channels(const DualTile* tiles, int count, const DualBatchImage* images, int parity,
+                                int channels, bool coupled, cudaStream_t s) {
+  switch (channels) {
+    case 1: return dual_batch_one<TGV, 1, false>(tiles, count, images, parity, s);
+    case 2: return coupled ? dual_batch_one<TGV, 2, true>(tiles, count, images, parity, s)
+                           : dual_batch_one<TGV, 2, false>(tiles, count, images, parity, s);
+    case 3: return coupled ? dual_batch_one<TGV, 3, true>(tiles, count, images, parity, s)
+                           : dual_batch_one<TGV, 3, false>(tiles, count, images, parity, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_dual_batch(const DualTile* tiles, int count, const DualBatchImage* images, int parity, bool tgv,
+                              int channels, bool coupled, cudaStream_t stream) {
+  return tgv ? dual_batch_channels<true>(tiles, count, images, parity, channels, coupled, stream)
+             : dual_batch_channels<false>(tiles, count, images, parity, channels, coupled, stream);
 }
 
 }  // namespace urb

@@ -31,6 +31,7 @@ from unround.settings import TGV, TV, DataTerm, PdhgOptions, Settings, Subgradie
 
 __all__ = [
     "ABI_VERSION",
+    "BatchTiming",
     "Decoded",
     "History",
     "LibraryNotFoundError",
@@ -50,6 +51,7 @@ __all__ = [
     "options",
     "project",
     "solve",
+    "solve_batch",
     "solve_from",
     "to_rgb",
     "to_ycbcr",
@@ -116,6 +118,16 @@ class _Timing(ctypes.Structure):
         ("samples", ctypes.c_uint64),
         ("pixels", ctypes.c_uint64),
         ("device_bytes", ctypes.c_uint64),
+    )
+
+
+class _BatchTiming(ctypes.Structure):
+    _fields_ = (
+        ("milliseconds", ctypes.c_double),
+        ("iterations", ctypes.c_uint64),
+        ("launches_per_iteration", ctypes.c_uint64),
+        ("samples", ctypes.c_uint64),
+        ("pixels", ctypes.c_uint64),
     )
 
 
@@ -196,6 +208,8 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_b200_measure": (i32, ctypes.POINTER(_Input), handle, u64, u64, ctypes.POINTER(_Timing),
                                  ctypes.POINTER(handle), *text),
         "unround_b200_model": (i32, ctypes.POINTER(_Input), handle, u64, i32, doubles, u64, u64p, *text),
+        "unround_b200_solve_batch": (i32, u64, ctypes.POINTER(_Input), ctypes.POINTER(handle), ctypes.POINTER(handle),
+                                     ctypes.POINTER(_BatchTiming), *text),
     }
     for name, (result, *arguments) in table.items():
         function = getattr(library, name)
@@ -579,6 +593,56 @@ def measure(image: jpegio.Image, settings: Settings | list[str] | None = None, *
     finally:
         if result:
             library.unround_result_free(made)
+        del kept
+
+
+@dataclass(frozen=True, slots=True)
+class BatchTiming:
+    """solve_batch(): the device milliseconds of the batched iterations (CUDA events), their
+    count, the launches an iteration of the whole batch takes, and all pictures' samples and
+    pixels."""
+
+    milliseconds: float
+    iterations: int
+    launches_per_iteration: int
+    samples: int
+    pixels: int
+
+
+def solve_batch(images: list[jpegio.Image], settings: Settings | list[str] | list | None = None
+                ) -> tuple[list[Decoded], BatchTiming]:
+    """Solves many pictures together on the GPU (include/unround_b200.h, unround_b200_solve_batch):
+    each result is the one solve() gives that picture alone. settings: one for all pictures, or
+    a list with one per picture (Settings or option lists); all take tv or tgv, the same number
+    of iterations and --record-every 0."""
+    library = _library()
+    count = len(images)
+    if count == 0:
+        raise ValueError("a batch has at least one picture")
+    per_picture = isinstance(settings, list) and len(settings) == count and not all(
+        isinstance(s, str) for s in settings)
+    handles = [_settings_of(settings[n] if per_picture else settings) for n in range(count)]
+    inputs = (_Input * count)()
+    kept: list[object] = []
+    for n, image in enumerate(images):
+        given, held = _input_of(image)
+        inputs[n] = given
+        kept.append(held)
+    settings_array = (ctypes.c_void_p * count)(*(h.handle for h in handles))
+    results = (ctypes.c_void_p * count)()
+    timing = _BatchTiming()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_b200_solve_batch(count, inputs, settings_array, results, ctypes.byref(timing), message,
+                                              _MESSAGE)
+    try:
+        _raise(status, message)
+        decoded = [_decoded(library, results[n]) for n in range(count)]
+        return decoded, BatchTiming(timing.milliseconds, int(timing.iterations), int(timing.launches_per_iteration),
+                                    int(timing.samples), int(timing.pixels))
+    finally:
+        for n in range(count):
+            if results[n]:
+                library.unround_result_free(results[n])
         del kept
 
 

@@ -150,3 +150,43 @@ def colour(rows: int, columns: int, *, quality: int = 75, seed: int = 0, noise: 
         c = pad(means, -(-means.shape[0] // 8) * 8, -(-means.shape[1] // 8) * 8)
         components.append((quantize(c, chroma_q)[:c_rows, :c_columns], chroma_q, 1, 1))
     return Synthetic(rgb, jpegio.image_of(rows, columns, jpegio.ColorSpace.YCBCR, components))
+
+
+@dataclass(frozen=True)
+class MixEntry:
+    """A picture of a mix and the options it is solved with."""
+
+    image: jpegio.Image
+    options: list[str]
+    colour: bool
+    method: str
+    quality: int
+    alpha: float
+
+
+def mix(count: int = 64, *, seed: int = 3, smallest: int = 256, largest: int = 2048, iterations: int = 300,
+        noise: float = 2.0) -> list[MixEntry]:
+    """A seeded mix of pictures of uneven sizes and settings, as a batch of many users' requests:
+    sides drawn uniformly from the multiples of 16 in [smallest, largest], greyscale or 4:2:0
+    colour with equal odds, quality uniform in 10..90, TV or TGV with equal odds, alpha
+    log-uniform in [0.3, 3] (TGV: alpha1 = alpha, alpha0 = 2 alpha), `iterations` iterations, no
+    tolerance, a record at the last iteration only."""
+    rng = np.random.default_rng(seed)
+    sides = np.arange(smallest, largest + 1, 16)
+    out = []
+    for n in range(count):
+        rows, columns = int(rng.choice(sides)), int(rng.choice(sides))
+        colour_picture = bool(rng.integers(0, 2))
+        quality = int(rng.integers(10, 91))
+        tgv = bool(rng.integers(0, 2))
+        alpha = float(np.exp(rng.uniform(np.log(0.3), np.log(3.0))))
+        picture_seed = int(rng.integers(0, 2**31))
+        made = (colour(rows, columns, quality=quality, seed=picture_seed, noise=noise) if colour_picture
+                else grey(rows, columns, quality=quality, seed=picture_seed, noise=noise))
+        common = ["--iterations", str(iterations), "--tolerance", "0", "--record-every", "0"]
+        if tgv:
+            options = ["--method", "tgv", "--alpha1", repr(alpha), "--alpha0", repr(2 * alpha), *common]
+        else:
+            options = ["--method", "tv", "--alpha", repr(alpha), *common]
+        out.append(MixEntry(made.image, options, colour_picture, "tgv" if tgv else "tv", quality, alpha))
+    return out
