@@ -216,6 +216,58 @@ def _call(image) -> int:
         del kept
 
 
+MIX_ITERATIONS = 300
+
+
+def _mix_arm(args: argparse.Namespace, rank: int, world: int) -> None:
+    """The batched solve of a seeded mix of pictures (sides multiples of 16 in [256, 2048], grey
+    or 4:2:0 colour, quality 10..90, TV or TGV, alpha log-uniform in [0.3, 3], 300 iterations)
+    in one CUDA graph, against the same pictures solved one after another with plain launches.
+    value: all pictures' pixel-iterations over the batched iterations' device time (CUDA events
+    around the graph launch); image_at_a_time: the same over the sum of each picture's
+    iteration loop alone (unround_b200_measure, CUDA events); e2e: through the drop-in batch
+    call with host arrays (levels in, binary64 results out), wall clock. Each rank solves its
+    own mix (weak scaling); rank 0 prints."""
+    from unround import native, synthetic
+
+    mix = synthetic.mix(args.pictures, seed=3 + rank, iterations=MIX_ITERATIONS)
+    images, options = [e.image for e in mix], [e.options for e in mix]
+    pixels = sum(e.image.height * e.image.width for e in mix)
+    for _ in range(max(1, args.warmup)):
+        native.solve_batch(images[:2], options[:2])  # warm the call path and the kernels
+    with Clocks(0) as clocks:
+        began = time.perf_counter()
+        decoded, timing = native.solve_batch(images, options)
+        e2e_seconds = time.perf_counter() - began
+    batched = pixels * timing.iterations / (timing.milliseconds / 1e3) / 1e6
+    alone_ms = 0.0
+    for image, option in zip(images, options):
+        measured, _ = native.measure(image, option, warmup=0, iterations=timing.iterations)
+        alone_ms += measured.milliseconds
+    alone = pixels * timing.iterations / (alone_ms / 1e3) / 1e6
+    d2h = sum(d.canvas.nbytes + sum(c.nbytes for c in d.coefficients) + d.picture.nbytes for d in decoded)
+    h2d = sum(sum(c.coefficients.nbytes for c in e.image.components) for e in mix)
+    if rank != 0:
+        return
+    line = {
+        "metric": f"batched TV/TGV mix Mpx*iter/s on 1 B200 ({args.pictures} pictures, {MIX_ITERATIONS} iterations)",
+        "value": batched, "unit": "Mpx*iter/s", "n_gpus": world, "steps": 1, "warmup": args.warmup,
+        "ms_per_step": timing.milliseconds, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded mix: sides 16k in [256, 2048], grey/4:2:0, Q 10..90, TV/TGV)",
+        "config": {"workload": f"mix-{args.pictures}", "pictures": args.pictures, "pixels": pixels,
+                   "samples": timing.samples, "iterations_timed": timing.iterations,
+                   "tgv": sum(e.method == "tgv" for e in mix), "colour": sum(e.colour for e in mix),
+                   "l2": "state larger than L2, no flush"},
+        "image_at_a_time": {"value": alone, "unit": "Mpx*iter/s", "ms": alone_ms},
+        "speedup_vs_image_at_a_time": batched / alone,
+        "e2e": {"value": pixels * MIX_ITERATIONS / e2e_seconds / 1e6, "unit": "Mpx*iter/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": timing.launches_per_iteration * timing.iterations,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -224,6 +276,9 @@ def main() -> None:
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--height", type=int, default=HEIGHT, help="a smaller picture for profiling")
     parser.add_argument("--width", type=int, default=WIDTH)
+    parser.add_argument("--workload", default="tgv-colour", choices=["tgv-colour", "mix"],
+                        help="mix: the batched solve of 64 uneven pictures against image-at-a-time launches")
+    parser.add_argument("--pictures", type=int, default=64, help="pictures of the mix")
     args = parser.parse_args()
     globals()["HEIGHT"], globals()["WIDTH"] = args.height, args.width
     rank, local_rank, world = _rank()
@@ -232,6 +287,9 @@ def main() -> None:
         os.environ["CUDA_VISIBLE_DEVICES"] = str(local_rank)
     for path in (ROOT / "jpeg-unround_b200", ROOT):
         sys.path.insert(0, str(path))
+    if args.workload == "mix":
+        _mix_arm(args, rank, world)
+        return
     group = None
     if world > 1:
         import datetime
