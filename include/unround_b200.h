@@ -75,6 +75,43 @@ unround_status unround_b200_solve_batch(uint64_t count, const unround_input* inp
                                         const unround_settings* const* settings, unround_result** results,
                                         unround_b200_batch_timing* timing, char* message, size_t message_size);
 
+/* The unrolled TGV solve of greyscale pictures and its adjoint (no counterpart in the
+ * reference, which solves and does not differentiate): `iterations` iterations of the method
+ * from the solver's start, with per-picture alpha0, alpha1, tau and sigma given as device
+ * arrays, to the last primal iterate x~_N; and the gradient of a loss of x~_N with respect to
+ * the four parameters, by the adjoint of every step, the states recomputed between checkpoints
+ * kept every `checkpoint_every` iterations. Every pointer is device memory of the current
+ * device; the caller allocates `checkpoint_floats` floats for the checkpoints and
+ * `workspace_floats` for the workspace; the work runs on `stream` and is not waited for.
+ * The problem's constants (made by the host model, unround_b200_model): */
+typedef struct unround_b200_unrolled {
+  uint64_t images, rows, columns; /* canvases of whole 8x8 blocks */
+  uint64_t iterations;
+  uint64_t checkpoint_every;
+  float relaxation;
+  const float* lower;       /* [images][blocks][64]: each coefficient's interval and centre, the */
+  const float* upper;       /* DC's less the middle of its interval (the block's mean times 8) */
+  const float* centre;
+  const float* middle;      /* [images][blocks]: the middle of the DC interval / 8 */
+  const float* weight;      /* [images][64]: the data term's weights, and those of flat blocks */
+  const float* flat_weight;
+  const uint8_t* flat;      /* [images][blocks] */
+  const float* start;       /* [images][rows][columns]: x0, the start's canvas */
+} unround_b200_unrolled;
+
+uint64_t unround_b200_unrolled_checkpoint_floats(const unround_b200_unrolled* problem);
+uint64_t unround_b200_unrolled_workspace_floats(const unround_b200_unrolled* problem);
+unround_status unround_b200_unrolled_forward(const unround_b200_unrolled* problem, const float* alpha0,
+                                             const float* alpha1, const float* tau, const float* sigma,
+                                             float* checkpoints, float* workspace, float* output, void* stream,
+                                             char* message, size_t message_size);
+/* `output_grad` the loss's gradient with respect to x~_N; `grads` [4][images] binary64: alpha0,
+ * alpha1, tau, sigma. Needs the checkpoints of a forward pass with the same parameters. */
+unround_status unround_b200_unrolled_backward(const unround_b200_unrolled* problem, const float* alpha0,
+                                              const float* alpha1, const float* tau, const float* sigma,
+                                              const float* checkpoints, float* workspace, const float* output_grad,
+                                              double* grads, void* stream, char* message, size_t message_size);
+
 /* What the host model makes of an input and settings, without a GPU (the reference computes the
  * same in Problem::make, cpp/src/model.cpp:134-256, and plan, cpp/src/pdhg.cpp:147-233): of
  * component `component`, `which` 0 the lower ends of the intervals, 1 the upper ends, 2 the
