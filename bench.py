@@ -268,6 +268,88 @@ def _mix_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     print(json.dumps(line))
 
 
+def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
+    """The differentiable unrolled TGV solve of 16 greyscale 512x512 pictures (quality 30),
+    100 iterations, checkpoints every 10: a step is one forward pass with the loss
+    (MSE against the clean pictures) and its backward pass (the adjoint) to the gradients of
+    every picture's alpha0, alpha1, tau and sigma. value: pixel-iterations of the forward and
+    backward pass per second (device time by CUDA events); forward: the same of the forward
+    pass alone; ratio: (forward + backward) / forward."""
+    import numpy as np
+    import torch
+
+    from unround import synthetic
+    from unround.unrolled import UnrolledProblem, unrolled_tgv
+
+    pictures, side, iterations, every = 16, 512, 100, 10
+    made = [synthetic.grey(side, side, quality=30, seed=100 * rank + s, noise=2) for s in range(pictures)]
+    problem = UnrolledProblem([m.image for m in made], ["--method", "tgv", "--alpha1", "1", "--alpha0", "2"],
+                              iterations=iterations, checkpoint_every=every)
+    clean = torch.tensor(np.stack([m.samples for m in made]), dtype=torch.float32, device="cuda")
+    base = [torch.full((pictures,), v, dtype=torch.float32, device="cuda")
+            for v in (2.0, 1.0, problem.tau, problem.sigma)]
+    h2d = sum(m.image.components[0].coefficients.nbytes for m in made)
+
+    def forward_only():
+        with torch.no_grad():
+            out = unrolled_tgv(problem, *base)
+            return torch.mean((out - clean) ** 2)
+
+    def forward_backward():
+        leaves = [b.clone().requires_grad_(True) for b in base]
+        loss = torch.mean((unrolled_tgv(problem, *leaves) - clean) ** 2)
+        loss.backward()
+        return loss, leaves
+
+    for _ in range(max(3, args.warmup)):
+        forward_only()
+        forward_backward()
+    torch.cuda.synchronize()
+    start, mid, end = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    steps = max(1, args.steps)
+    with Clocks(0) as clocks:
+        start.record()
+        for _ in range(steps):
+            forward_only()
+        mid.record()
+        for _ in range(steps):
+            loss, leaves = forward_backward()
+        end.record()
+        torch.cuda.synchronize()
+    forward_ms = start.elapsed_time(mid) / steps
+    both_ms = mid.elapsed_time(end) / steps
+    grads = torch.stack([leaf.grad for leaf in leaves]).cpu()  # the step's result read on the host
+    pixels = pictures * side * side
+    # End to end: levels in from the host (the problem made from the files' levels), gradients out.
+    began = time.perf_counter()
+    problem_e2e = UnrolledProblem([m.image for m in made], ["--method", "tgv", "--alpha1", "1", "--alpha0", "2"],
+                                  iterations=iterations, checkpoint_every=every)
+    leaves = [b.clone().requires_grad_(True) for b in base]
+    torch.mean((unrolled_tgv(problem_e2e, *leaves) - clean) ** 2).backward()
+    e2e_grads = torch.stack([leaf.grad for leaf in leaves]).cpu()
+    e2e_seconds = time.perf_counter() - began
+    if rank != 0:
+        return
+    line = {
+        "metric": "unrolled TGV forward+adjoint Mpx*iter/s on 1 B200 (16 x 512x512, 100 iterations, checkpoints 10)",
+        "value": pixels * iterations / (both_ms / 1e3) / 1e6, "unit": "Mpx*iter/s", "n_gpus": world, "steps": steps,
+        "warmup": max(3, args.warmup), "ms_per_step": both_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded piecewise-smooth + noise sigma 2, quality 30)",
+        "config": {"workload": "unrolled-tgv-16x512", "pictures": pictures, "iterations": iterations,
+                   "checkpoint_every": every, "loss": "MSE against the clean pictures",
+                   "l2": "state 16 x 512^2 x 9 fields = 151 MB, larger than L2"},
+        "forward": {"value": pixels * iterations / (forward_ms / 1e3) / 1e6, "ms": forward_ms},
+        "forward_backward_over_forward": both_ms / forward_ms,
+        "grad_finite": bool(torch.isfinite(grads).all()) and bool(torch.isfinite(e2e_grads).all()),
+        "e2e": {"value": pixels * iterations / e2e_seconds / 1e6, "unit": "Mpx*iter/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": int(e2e_grads.numel() * 4)},
+        "gpu_launches": iterations * 2 + iterations * 5 + iterations * 2,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    del loss
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -276,8 +358,9 @@ def main() -> None:
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--height", type=int, default=HEIGHT, help="a smaller picture for profiling")
     parser.add_argument("--width", type=int, default=WIDTH)
-    parser.add_argument("--workload", default="tgv-colour", choices=["tgv-colour", "mix"],
-                        help="mix: the batched solve of 64 uneven pictures against image-at-a-time launches")
+    parser.add_argument("--workload", default="tgv-colour", choices=["tgv-colour", "mix", "unrolled"],
+                        help="mix: the batched solve of 64 uneven pictures against image-at-a-time launches; "
+                             "unrolled: the differentiable unrolled TGV solve, forward and forward+adjoint")
     parser.add_argument("--pictures", type=int, default=64, help="pictures of the mix")
     args = parser.parse_args()
     globals()["HEIGHT"], globals()["WIDTH"] = args.height, args.width
@@ -289,6 +372,9 @@ def main() -> None:
         sys.path.insert(0, str(path))
     if args.workload == "mix":
         _mix_arm(args, rank, world)
+        return
+    if args.workload == "unrolled":
+        _unrolled_arm(args, rank, world)
         return
     group = None
     if world > 1:
