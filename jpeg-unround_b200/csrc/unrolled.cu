@@ -12,11 +12,12 @@
 // a, b) with t = tau m_k (m_k the data term's weight of frequency k, of a flat block where the
 // block is flat) and e the DCT of the block less the middle of its DC interval.
 //
-// The adjoint runs the iterations backwards: the adjoint of D_k (three per-pixel kernels: the
-// projections' Jacobians at each pixel; the transposes of E and grad, which gather the first
-// kernel's results of the neighbours; the transpose of div2), then of P_k (a block kernel: the
-// DCT of the adjoint, the clip's mask, the inverse DCT; and a per-pixel kernel for div's
-// transpose). The states s_k are kept every `checkpoint` iterations by the forward pass; the
+// The adjoint runs the iterations backwards: the adjoint of D_k (two per-pixel kernels: the
+// projections' Jacobians at each pixel; then the transposes of E, grad and div2, which gather
+// the first kernel's results of the neighbours and recompute w~'s adjoint of the left and upper
+// ones), then of P_k (a block kernel: the DCT of the adjoint, the clip's mask, the inverse DCT,
+// to the adjoint of v, which the next dual step undone reads for div's transpose). The states
+// s_k are kept every `checkpoint` iterations by the forward pass; the
 // backward pass recomputes each segment's states from its checkpoint. The parameters' gradients
 // are sums over pixels and iterations, reduced per CTA and added in binary64.
 #include <algorithm>
@@ -174,9 +175,30 @@ __device__ __forceinline__ float primal_v(const Problem& q, const Planes& s, int
   return s.x[k] + q.tau[z] * (dy + dx);
 }
 
+// The DCT basis C[k][n] at k * 9 + n (rows padded against bank conflicts), for a CTA's
+// transforms: filled once per CTA from the compile-time values.
+struct BasisTable {
+  float v[8 * 9];
+};
+
+__device__ __forceinline__ void fill_basis(BasisTable& table) {
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  if (t < 64) {
+    const int k = t >> 3, n = t & 7;
+    float c = 0.0f;
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+#pragma unroll
+      for (int nn = 0; nn < 8; ++nn) c = (kk == k && nn == n) ? basis_as<float>(kk, nn) : c;
+    }
+    table.v[k * 9 + n] = c;
+  }
+  __syncthreads();
+}
+
 // The 2D transform of a CTA's 4 blocks in shared memory, in place: forward (C V C^T) or inverse
 // (C^T V C); `t` holds the values [8][33], each thread one.
-__device__ __forceinline__ float transform(float value, float (*t)[33], bool forward) {
+__device__ __forceinline__ float transform(float value, float (*t)[33], const BasisTable& basis, bool forward) {
   const int tx = threadIdx.x, ty = threadIdx.y, n0 = tx & ~7, u = tx & 7;
   t[ty][tx] = value;
   __syncthreads();
@@ -184,7 +206,7 @@ __device__ __forceinline__ float transform(float value, float (*t)[33], bool for
   float acc = 0.0f;
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
-    const float c = forward ? basis_as<float>(ty, a) : basis_as<float>(a, ty);
+    const float c = forward ? basis.v[ty * 9 + a] : basis.v[a * 9 + ty];
     acc = fmaf(c, t[a][tx], acc);
   }
   __syncthreads();
@@ -194,7 +216,7 @@ __device__ __forceinline__ float transform(float value, float (*t)[33], bool for
   float out = 0.0f;
 #pragma unroll
   for (int b = 0; b < 8; ++b) {
-    const float c = forward ? basis_as<float>(u, b) : basis_as<float>(b, u);
+    const float c = forward ? basis.v[u * 9 + b] : basis.v[b * 9 + u];
     out = fmaf(c, t[ty][n0 + b], out);
   }
   __syncthreads();
@@ -226,6 +248,8 @@ __device__ __forceinline__ Clip clip_of(const Problem& q, int z, std::size_t blo
 
 __global__ void __launch_bounds__(256) primal_kernel(Problem q, Planes s, float* xt) {
   __shared__ float t[8][33];
+  __shared__ BasisTable basis;
+  fill_basis(basis);
   const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
   const bool in = j < q.columns;
   const int jc = in ? j : q.columns - 1;
@@ -233,10 +257,10 @@ __global__ void __launch_bounds__(256) primal_kernel(Problem q, Planes s, float*
   const std::size_t block = static_cast<std::size_t>(by) * q.blocks_across + bx;
   const float middle = q.middle[static_cast<std::size_t>(z) * q.blocks_down * q.blocks_across + block];
   const float v = primal_v(q, s, z, i, jc);
-  const float e = transform(v - middle, t, true);
+  const float e = transform(v - middle, t, basis, true);
   const int kk = threadIdx.y * 8 + (threadIdx.x & 7);
   const Clip c = clip_of(q, z, block, kk, e);
-  const float back = transform(c.z, t, false);
+  const float back = transform(c.z, t, basis, false);
   if (in) xt[at(q, z, i, j)] = back + middle;
 }
 
@@ -268,13 +292,54 @@ struct Scratch {
   float* s11;
   float* s22;
   float* s12;
-  float* t1;  // the adjoint of w~
-  float* t2;
-  float* v;   // the adjoint of v of the primal step
+  float* v;   // the adjoint of v of a primal step
 };
 
-__global__ void __launch_bounds__(256) dual_adjoint_local(Problem q, Planes s, const float* xt, Planes a, Scratch w,
-                                                          double* grads) {
+// The adjoint of x and p of s_k: that of the dual step after it (`a`) and that of the primal
+// step P_{k+1}, whose v = x + tau div p has the adjoint `vbar` (null where there is none):
+// x^ += v^, p^ += tau div^T v^ = -tau grad v^.
+__device__ __forceinline__ float adjoint_x(const Planes& a, const float* vbar, std::size_t k) {
+  return vbar != nullptr ? a.x[k] + vbar[k] : a.x[k];
+}
+
+__device__ __forceinline__ void adjoint_p(const Problem& q, const Planes& a, const float* vbar, float tau, int i, int j,
+                                          std::size_t k, float& p1, float& p2) {
+  p1 = a.p1[k];
+  p2 = a.p2[k];
+  if (vbar != nullptr) {
+    const float v = vbar[k];
+    if (j + 1 < q.columns) p1 += -tau * (vbar[k + 1] - v);
+    if (i + 1 < q.rows) p2 += -tau * (vbar[k + q.columns] - v);
+  }
+}
+
+// The adjoint of w~ at a pixel from the local kernel's adjoints of q and s: that of w- is
+// -sigma q^ + sigma E^T s^ (E^T gathering s^ of the pixel and of its right and lower ones), and
+// w~ = (w- + w) / 2 gives it twice, beside the relaxation's rho w'^.
+__device__ __forceinline__ void w_tilde_bar(const Problem& q, const Planes& a, const Scratch& w, int z, int i, int j,
+                                            float& t1, float& t2, float& wb1, float& wb2) {
+  const std::size_t k = at(q, z, i, j);
+  const int W = q.columns;
+  const float sigma = q.sigma[z], rho = q.rho;
+  wb1 = -sigma * w.q1[k];
+  wb2 = -sigma * w.q2[k];
+  float e1 = 0.0f, e2 = 0.0f;
+  if (j + 1 < W) {
+    e1 += w.s11[k] - w.s11[k + 1];
+    e2 += 0.5f * (w.s12[k] - w.s12[k + 1]);
+  }
+  if (i + 1 < q.rows) {
+    e2 += w.s22[k] - w.s22[k + W];
+    e1 += 0.5f * (w.s12[k] - w.s12[k + W]);
+  }
+  wb1 += sigma * e1;
+  wb2 += sigma * e2;
+  t1 = rho * a.w1[k] + 2.0f * wb1;
+  t2 = rho * a.w2[k] + 2.0f * wb2;
+}
+
+__global__ void __launch_bounds__(256) dual_adjoint_local(Problem q, Planes s, const float* xt, Planes a,
+                                                          const float* vbar, Scratch w, double* grads) {
   const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
   const bool in = i < q.rows && j < q.columns;
   float g_alpha0 = 0.0f, g_alpha1 = 0.0f, g_sigma = 0.0f;
@@ -283,7 +348,9 @@ __global__ void __launch_bounds__(256) dual_adjoint_local(Problem q, Planes s, c
     const float rho = q.rho;
     const DualPoint d = dual_point(q, s, xt, z, i, j);
     // p~ = proj(q): the adjoint of q from that of p~.
-    const float pb1 = rho * a.p1[k], pb2 = rho * a.p2[k];
+    float ap1, ap2;
+    adjoint_p(q, a, vbar, q.tau[z], i, j, k, ap1, ap2);
+    const float pb1 = rho * ap1, pb2 = rho * ap2;
     float qb1 = pb1, qb2 = pb2;
     const float alpha1 = q.alpha1[z];
     const float nq = sqrtf(d.q1 * d.q1 + d.q2 * d.q2);
@@ -319,8 +386,8 @@ __global__ void __launch_bounds__(256) dual_adjoint_local(Problem q, Planes s, c
   add_sum(g_sigma, grads + 3 * q.images + z);
 }
 
-__global__ void __launch_bounds__(256) dual_adjoint_gather(Problem q, Planes s, Planes a, Scratch w, Planes b,
-                                                           float* xt_bar, double* grads) {
+__global__ void __launch_bounds__(256) dual_adjoint_gather(Problem q, Planes s, Planes a, const float* vbar,
+                                                           Scratch w, Planes b, float* xt_bar, double* grads) {
   const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
   const bool in = i < q.rows && j < q.columns;
   float g_tau = 0.0f;
@@ -329,26 +396,26 @@ __global__ void __launch_bounds__(256) dual_adjoint_gather(Problem q, Planes s, 
     const int W = q.columns, H = q.rows;
     const float rho = q.rho, rest = 1.0f - q.rho, sigma = q.sigma[z], tau = q.tau[z];
     const bool right = j + 1 < W, down = i + 1 < H;
-    // The adjoint of w- : -sigma q^ + sigma E^T s^.
-    float wb1 = -sigma * w.q1[k], wb2 = -sigma * w.q2[k];
-    float e1 = 0.0f, e2 = 0.0f;
-    if (right) {
-      e1 += w.s11[k] - w.s11[k + 1];
-      e2 += 0.5f * (w.s12[k] - w.s12[k + 1]);
-    }
-    if (down) {
-      e2 += w.s22[k] - w.s22[k + W];
-      e1 += 0.5f * (w.s12[k] - w.s12[k + W]);
-    }
-    wb1 += sigma * e1;
-    wb2 += sigma * e2;
-    const float tb1 = rho * a.w1[k] + 2.0f * wb1, tb2 = rho * a.w2[k] + 2.0f * wb2;
+    float tb1, tb2, wb1, wb2;
+    w_tilde_bar(q, a, w, z, i, j, tb1, tb2, wb1, wb2);
+    float ap1, ap2;
+    adjoint_p(q, a, vbar, tau, i, j, k, ap1, ap2);
     b.w1[k] = rest * a.w1[k] - wb1 + tb1;
     b.w2[k] = rest * a.w2[k] - wb2 + tb2;
-    b.p1[k] = rest * a.p1[k] + w.q1[k] + tau * tb1;
-    b.p2[k] = rest * a.p2[k] + w.q2[k] + tau * tb2;
-    w.t1[k] = tb1;
-    w.t2[k] = tb2;
+    b.p1[k] = rest * ap1 + w.q1[k] + tau * tb1;
+    b.p2[k] = rest * ap2 + w.q2[k] + tau * tb2;
+    // r^: the relaxation's, s^, and div2^T of d^ = tau w~^ (w~^ of the pixel and of its left and
+    // upper ones).
+    float l1 = 0.0f, l2 = 0.0f, u1 = 0.0f, u2 = 0.0f, unused1, unused2;
+    if (j > 0) w_tilde_bar(q, a, w, z, i, j - 1, l1, l2, unused1, unused2);
+    if (i > 0) w_tilde_bar(q, a, w, z, i - 1, j, u1, u2, unused1, unused2);
+    const float db1 = tau * tb1, db2 = tau * tb2;
+    const float div11 = tau * l1 - (right ? db1 : 0.0f);
+    const float div12 = tau * u1 - (down ? db1 : 0.0f) + tau * l2 - (right ? db2 : 0.0f);
+    const float div22 = tau * u2 - (down ? db2 : 0.0f);
+    b.r11[k] = rest * a.r11[k] + w.s11[k] + div11;
+    b.r22[k] = rest * a.r22[k] + w.s22[k] + div22;
+    b.r12[k] = rest * a.r12[k] + w.s12[k] + div12;
     // d/dtau of w~ = p + div2 r.
     const float r11 = s.r11[k], r22 = s.r22[k], r12 = s.r12[k];
     float d1 = right ? s.r11[k + 1] - r11 : 0.0f;
@@ -360,35 +427,19 @@ __global__ void __launch_bounds__(256) dual_adjoint_gather(Problem q, Planes s, 
     float div = (right ? w.q1[k] : 0.0f) - (j > 0 ? w.q1[k - 1] : 0.0f) + (down ? w.q2[k] : 0.0f) -
                 (i > 0 ? w.q2[k - W] : 0.0f);
     const float xbb = -sigma * div;
-    xt_bar[k] = rho * a.x[k] + 2.0f * xbb;
-    b.x[k] = rest * a.x[k] - xbb;
+    const float ax = adjoint_x(a, vbar, k);
+    xt_bar[k] = rho * ax + 2.0f * xbb;
+    b.x[k] = rest * ax - xbb;
   }
   add_sum(g_tau, grads + 2 * q.images + z);
-}
-
-__global__ void __launch_bounds__(256) dual_adjoint_r(Problem q, Planes a, Scratch w, Planes b) {
-  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-  if (i >= q.rows || j >= q.columns) return;
-  const std::size_t k = at(q, z, i, j);
-  const int W = q.columns, H = q.rows;
-  const float rest = 1.0f - q.rho, tau = q.tau[z];
-  const bool right = j + 1 < W, down = i + 1 < H;
-  // div2^T of d^ = tau w~^.
-  const float d1 = tau * w.t1[k], d2 = tau * w.t2[k];
-  const float d1_left = j > 0 ? tau * w.t1[k - 1] : 0.0f, d2_left = j > 0 ? tau * w.t2[k - 1] : 0.0f;
-  const float d1_up = i > 0 ? tau * w.t1[k - W] : 0.0f, d2_up = i > 0 ? tau * w.t2[k - W] : 0.0f;
-  const float r11 = d1_left - (right ? d1 : 0.0f);
-  const float r12 = d1_up - (down ? d1 : 0.0f) + d2_left - (right ? d2 : 0.0f);
-  const float r22 = d2_up - (down ? d2 : 0.0f);
-  b.r11[k] = rest * a.r11[k] + w.s11[k] + r11;
-  b.r22[k] = rest * a.r22[k] + w.s22[k] + r22;
-  b.r12[k] = rest * a.r12[k] + w.s12[k] + r12;
 }
 
 // The primal step's adjoint, per block: from the adjoint of x~ (`xt_bar`) the adjoint of v.
 __global__ void __launch_bounds__(256) primal_adjoint_block(Problem q, Planes s, const float* xt_bar, Scratch w,
                                                             double* grads) {
   __shared__ float t[8][33];
+  __shared__ BasisTable basis;
+  fill_basis(basis);
   const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
   const bool in = j < q.columns;
   const int jc = in ? j : q.columns - 1;
@@ -397,15 +448,15 @@ __global__ void __launch_bounds__(256) primal_adjoint_block(Problem q, Planes s,
   const std::size_t k = at(q, z, i, jc);
   const float middle = q.middle[static_cast<std::size_t>(z) * q.blocks_down * q.blocks_across + block];
   const float v = primal_v(q, s, z, i, jc);
-  const float e = transform(v - middle, t, true);
+  const float e = transform(v - middle, t, basis, true);
   const int kk = threadIdx.y * 8 + (threadIdx.x & 7);
   const Clip c = clip_of(q, z, block, kk, e);
-  const float zb = transform(in ? xt_bar[k] : 0.0f, t, true);
+  const float zb = transform(in ? xt_bar[k] : 0.0f, t, basis, true);
   // zeta = (e + t c) r inside the interval, t = tau m, r = 1 / (1 + t): d zeta / d e = r and
   // d zeta / d tau = m (c - e) r^2; outside it zeta is an end of the interval.
   const float eb = c.inside ? c.r * zb : 0.0f;
   float g_tau = c.inside ? zb * c.weight * (c.centre - e) * (c.r * c.r) : 0.0f;
-  const float vb = transform(eb, t, false);
+  const float vb = transform(eb, t, basis, false);
   // d v / d tau = div p.
   const float dy = (i + 1 < q.rows ? s.p2[k] : 0.0f) - (i > 0 ? s.p2[k - q.columns] : 0.0f);
   const float dx = (jc + 1 < q.columns ? s.p1[k] : 0.0f) - (jc > 0 ? s.p1[k - 1] : 0.0f);
@@ -416,17 +467,6 @@ __global__ void __launch_bounds__(256) primal_adjoint_block(Problem q, Planes s,
     g_tau = 0.0f;
   }
   add_sum(g_tau, grads + 2 * q.images + z);
-}
-
-// ... and the adjoint of x and p from that of v: x^ += v^, p^ += tau div^T v^ = -tau grad v^.
-__global__ void __launch_bounds__(256) primal_adjoint_gather(Problem q, Scratch w, Planes b) {
-  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-  if (i >= q.rows || j >= q.columns) return;
-  const std::size_t k = at(q, z, i, j);
-  const float tau = q.tau[z], vb = w.v[k];
-  b.x[k] += vb;
-  if (j + 1 < q.columns) b.p1[k] += -tau * (w.v[k + 1] - vb);
-  if (i + 1 < q.rows) b.p2[k] += -tau * (w.v[k + q.columns] - vb);
 }
 
 // ---- Host side.
@@ -505,7 +545,7 @@ extern "C" uint64_t unround_b200_unrolled_workspace_floats(const unround_b200_un
   if (!urb::check(problem).empty()) return 0;
   const std::uint64_t plane = problem->images * problem->rows * problem->columns;
   // Two states ping-pong, x~, a segment's states and x~s, two adjoints, x~'s adjoint, scratch.
-  return (2 * 8 + 1 + problem->checkpoint_every * 9 + 2 * 8 + 1 + 8) * plane;
+  return (2 * 8 + 1 + problem->checkpoint_every * 9 + 2 * 8 + 1 + 6) * plane;
 }
 
 extern "C" unround_status unround_b200_unrolled_forward(const unround_b200_unrolled* problem, const float* alpha0,
@@ -578,8 +618,9 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
   float* xt_bar = adjoint_base + 16 * plane;
   float* scratch_base = xt_bar + plane;
   const urb::Scratch scratch{scratch_base,             scratch_base + plane,     scratch_base + 2 * plane,
-                             scratch_base + 3 * plane, scratch_base + 4 * plane, scratch_base + 5 * plane,
-                             scratch_base + 6 * plane, scratch_base + 7 * plane};
+                             scratch_base + 3 * plane, scratch_base + 4 * plane, scratch_base + 5 * plane};
+  // The adjoint of v of the primal step after the dual step being undone (none after the last).
+  const float* vbar = nullptr;
   auto state_of = [&](std::uint64_t step) { return urb::planes_of(segment + step * 9 * plane, plane); };
   auto tilde_of = [&](std::uint64_t step) { return segment + step * 9 * plane + 8 * plane; };
   const dim3 grid = urb::pixel_grid(q), block(32, 8);
@@ -604,17 +645,17 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
       const std::uint64_t step = k - 1 - k0;
       const Planes s = state_of(step);
       if (k < n) {
-        // D_k: the adjoint of s_k is adjoint[current]; write that of s_{k-1} into the other,
-        // and that of x~_k into xt_bar.
+        // D_k: the adjoint of s_k is adjoint[current] and P_{k+1}'s (vbar); write that of
+        // s_{k-1} into the other, and that of x~_k into xt_bar.
         const Planes a = adjoint[current], b = adjoint[1 - current];
-        urb::dual_adjoint_local<<<grid, block, 0, on>>>(q, s, tilde_of(step), a, scratch, grads);
-        urb::dual_adjoint_gather<<<grid, block, 0, on>>>(q, s, a, scratch, b, xt_bar, grads);
-        urb::dual_adjoint_r<<<grid, block, 0, on>>>(q, a, scratch, b);
+        urb::dual_adjoint_local<<<grid, block, 0, on>>>(q, s, tilde_of(step), a, vbar, scratch, grads);
+        urb::dual_adjoint_gather<<<grid, block, 0, on>>>(q, s, a, vbar, scratch, b, xt_bar, grads);
         current = 1 - current;
       }
-      // P_k: from the adjoint of x~_k to those of x and p of s_{k-1}.
+      // P_k: from the adjoint of x~_k that of its v, which the next dual step undone (D_{k-1})
+      // adds to the adjoints of x and p of s_{k-1}.
       urb::primal_adjoint_block<<<grid, block, 0, on>>>(q, s, xt_bar, scratch, grads);
-      urb::primal_adjoint_gather<<<grid, block, 0, on>>>(q, scratch, adjoint[current]);
+      vbar = scratch.v;
     }
   }
   const cudaError_t error = cudaGetLastError();
