@@ -400,13 +400,9 @@ def main() -> None:
         group.barrier()
     with Clocks(local_rank if world == 1 else 0) as clocks:
         timing, _ = native.measure(image, OPTIONS, warmup=args.warmup * ITERATIONS, iterations=args.steps * ITERATIONS)
-    seconds = timing.milliseconds / 1e3
-    if group is not None:
-        import torch
+    from unround.sharding import max_over_ranks
 
-        worst = torch.tensor([seconds], dtype=torch.float64)
-        group.all_reduce(worst, op=group.ReduceOp.MAX)
-        seconds = float(worst.item())
+    seconds = max_over_ranks(timing.milliseconds / 1e3)  # the slowest rank's
     pixels = timing.pixels
     value = world * pixels * args.steps * ITERATIONS / seconds / 1e6
     # End to end through the drop-in call, host arrays in and out.
@@ -417,13 +413,7 @@ def main() -> None:
     began = time.perf_counter()
     for _ in range(args.steps):
         d2h = _call(image)
-    e2e_seconds = time.perf_counter() - began
-    if group is not None:
-        import torch
-
-        worst = torch.tensor([e2e_seconds], dtype=torch.float64)
-        group.all_reduce(worst, op=group.ReduceOp.MAX)
-        e2e_seconds = float(worst.item())
+    e2e_seconds = max_over_ranks(time.perf_counter() - began)
     e2e = world * pixels * args.steps * ITERATIONS / e2e_seconds / 1e6
     peak, peak_kind = _peaks()
     samples = timing.samples
