@@ -268,6 +268,64 @@ def _mix_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     print(json.dumps(line))
 
 
+LARGE_OPTIONS = ["--method", "tgv", "--alpha1", "1.5", "--alpha0", "3", "--iterations", "1000", "--tolerance", "0",
+                 "--record-every", "50"]
+
+
+def _large_arm(args: argparse.Namespace, rank: int, world: int) -> None:
+    """BASELINE's large single solve: 8192^2 TGV (alpha0 3, alpha1 1.5), 1000 iterations. value:
+    the iteration loop's device time (CUDA events, no records); e2e: the drop-in solve with the
+    primal-dual gap recorded every 50 iterations, host arrays in and out; and the binary64 check
+    that every coefficient of all 1,048,576 blocks lies in its interval."""
+    import numpy as np
+
+    from unround import native, synthetic
+
+    made = synthetic.large(seed=5 + rank)
+    image = made.image
+    iterations = 1000
+    timed_options = [*LARGE_OPTIONS[:-2], "--record-every", "0"]
+    with Clocks(0) as clocks:
+        timing, _ = native.measure(image, timed_options, warmup=max(3, args.warmup) * 10, iterations=iterations)
+    pixels = timing.pixels
+    value = pixels * iterations / (timing.milliseconds / 1e3) / 1e6
+    began = time.perf_counter()
+    decoded = native.solve(image, LARGE_OPTIONS)
+    e2e_seconds = time.perf_counter() - began
+    lower = native.model(image, LARGE_OPTIONS, 0, 0)
+    upper = native.model(image, LARGE_OPTIONS, 0, 1)
+    zeta = decoded.coefficients[0].reshape(-1)
+    inside = bool(np.all((zeta >= lower) & (zeta <= upper)))
+    history = decoded.result.history
+    peak, peak_kind = _peaks()
+    if rank != 0:
+        return
+    line = {
+        "metric": "TGV PDHG Mpx*iter/s on 1 B200 (8192x8192 grey, custom table, 1000 iterations)",
+        "value": value, "unit": "Mpx*iter/s", "n_gpus": world, "steps": 1, "warmup": max(3, args.warmup) * 10,
+        "ms_per_step": timing.milliseconds, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded piecewise-smooth + noise sigma 2, table steps U{1..64})",
+        "config": {"workload": "tgv-grey-8192-custom", "alpha1": 1.5, "alpha0": 3.0, "iterations": iterations,
+                   "samples": timing.samples, "l2": "state 4.3 GB, larger than L2"},
+        "roofline": {"bound": "hbm", "kernel": "dual_tma_kernel<tgv,1>", "achieved":
+                     DUAL_BYTES * timing.samples / (timing.dual_milliseconds / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "peak_kind": peak_kind,
+                     "frac": DUAL_BYTES * timing.samples / (timing.dual_milliseconds / 1e3) / 1e9 / peak,
+                     "iteration_bytes_per_sample": 66.0,
+                     "iteration_frac": 66.0 * timing.samples / (timing.milliseconds / iterations / 1e3) / 1e9 / peak,
+                     "dual_ms": timing.dual_milliseconds, "primal_ms": timing.primal_milliseconds},
+        "gap_per_sample_every_50": [float(g) / timing.samples for g in history.gap],
+        "record_iterations": [int(n) for n in history.iterations],
+        "all_blocks_inside_intervals_fp64": inside, "blocks": int(zeta.size // 64),
+        "e2e": {"value": pixels * iterations / e2e_seconds / 1e6, "unit": "Mpx*iter/s",
+                "h2d_bytes_per_step": int(image.components[0].coefficients.nbytes),
+                "d2h_bytes_per_step": int(decoded.canvas.nbytes + zeta.nbytes)},
+        "gpu_launches": timing.launches_per_iteration * iterations,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
 def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     """The differentiable unrolled TGV solve of 16 greyscale 512x512 pictures (quality 30),
     100 iterations, checkpoints every 10: a step is one forward pass with the loss
@@ -358,7 +416,7 @@ def main() -> None:
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--height", type=int, default=HEIGHT, help="a smaller picture for profiling")
     parser.add_argument("--width", type=int, default=WIDTH)
-    parser.add_argument("--workload", default="tgv-colour", choices=["tgv-colour", "mix", "unrolled"],
+    parser.add_argument("--workload", default="tgv-colour", choices=["tgv-colour", "mix", "unrolled", "large"],
                         help="mix: the batched solve of 64 uneven pictures against image-at-a-time launches; "
                              "unrolled: the differentiable unrolled TGV solve, forward and forward+adjoint")
     parser.add_argument("--pictures", type=int, default=64, help="pictures of the mix")
@@ -375,6 +433,9 @@ def main() -> None:
         return
     if args.workload == "unrolled":
         _unrolled_arm(args, rank, world)
+        return
+    if args.workload == "large":
+        _large_arm(args, rank, world)
         return
     group = None
     if world > 1:

@@ -152,6 +152,13 @@ def colour(rows: int, columns: int, *, quality: int = 75, seed: int = 0, noise: 
     return Synthetic(rgb, jpegio.image_of(rows, columns, jpegio.ColorSpace.YCBCR, components))
 
 
+def large(side: int = 8192, *, seed: int = 5) -> Synthetic:
+    """A large greyscale picture (the generator plus Gaussian noise sigma 2) quantized with a
+    custom table of steps drawn uniformly from 1..64 (a custom table: no quality factor applies)."""
+    steps = np.random.default_rng(seed).integers(1, 65, size=64)
+    return grey(side, side, seed=seed, noise=2.0, steps=steps)
+
+
 @dataclass(frozen=True)
 class MixEntry:
     """A picture of a mix and the options it is solved with."""
