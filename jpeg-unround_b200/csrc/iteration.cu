@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(32 * kWarps, 2)
 #pragma unroll
       for (int c = 0; c < L::kPlain; ++c) {
         const float dc = plain_in[c] ? static_cast<float>(lv[c][lane >> 3][0]) : 0.0f;
-        middle[c] = (dc * factors[c].step[0] + 1024.0f) * 0.125f;
+        middle[c] = (dc * factors[c].plain[0].x + 1024.0f) * 0.125f;
         tbuf[c][r][lane] = row_transform(v[c] - middle[c], forward_basis);
       }
       if constexpr (L::kChroma) {
@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(32 * kWarps, 2)
             const int s = q * 32 + lane, cc = s / per, mcol = s % per;
             const float dc =
                 chroma_in[q] ? static_cast<float>(lv[L::kPlain + q][chroma_block[q]][0]) : 0.0f;
-            const float chroma_middle = (dc * factors[1 + cc].step[0] + 1024.0f) * 0.125f;
+            const float chroma_middle = (dc * factors[1 + cc].plain[0].x + 1024.0f) * 0.125f;
             float total = 0.0f;
 #pragma unroll
             for (int b = 0; b < CC; ++b) {
@@ -601,9 +601,7 @@ __global__ void __launch_bounds__(32 * kWarps, 2)
         float zeta = 0.0f;
         if (in) {
           const int level = lv[q][blk][kk];
-          const Coefficient coefficient = coefficient_of(level, kk, fc);
-          zeta = prox_of(e, flat ? fc.t_flat[kk] : fc.t[kk], flat ? fc.r_flat[kk] : fc.r[kk],
-                         flat ? fc.h_flat[kk] : fc.h[kk], coefficient, fc.costed != 0);
+          zeta = prox_at(e, level, kk, flat, fc);
         }
         zbuf[q][r][lane] = zeta;
       }
@@ -737,7 +735,7 @@ std::size_t iteration_shared_bytes(bool tgv, int channels) {
 }
 
 bool make_iteration_map(CUtensorMap& map, const float* planes, const Geometry& g, int count) {
-  return make_box_map(map, planes, g, count, g.plane, kBox);
+  return make_box_map(map, planes, g, count, g.plane, kBox, kSpan);
 }
 
 cudaError_t launch_iteration(const CUtensorMap& state, const CUtensorMap& tilde, const IterationParams& p, bool tgv,

@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(256, 2) primal_kernel(const PrimalParams P) {
         static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
     // The middle of the block's DC interval over 8 (exact): the block is taken centred on it.
     const float dc_level = in_blocks ? static_cast<float>(P.component.levels[block * 64]) : 0.0f;
-    const float middle = (dc_level * F.step[0] + 1024.0f) * 0.125f;
+    const float middle = (dc_level * F.plain[0].x + 1024.0f) * 0.125f;
     float mean[8];
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
@@ -412,14 +412,7 @@ __global__ void __launch_bounds__(256, 2) primal_kernel(const PrimalParams P) {
     }
     const bool flat = in_blocks && P.component.flat[block] != 0;
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int k = m * 8 + u;
-      const Coefficient c = coefficient_of(levels[u], k, F);
-      const float tk = flat ? F.t_flat[k] : F.t[k];
-      const float rk = flat ? F.r_flat[k] : F.r[k];
-      const float hk = flat ? F.h_flat[k] : F.h[k];
-      zeta[u] = prox_of(coef[u], tk, rk, hk, c, F.costed != 0);
-    }
+    for (int u = 0; u < 8; ++u) zeta[u] = prox_at(coef[u], levels[u], m * 8 + u, flat, F);
     if constexpr (KEEP) {
       // Kept coefficients as the map gives them: DC centred (less q Q + 1024).
       if (in_blocks && cell == 0) {
@@ -469,24 +462,36 @@ __global__ void __launch_bounds__(256, 2) primal_kernel(const PrimalParams P) {
   if constexpr (KEEP) cta_sum(sum, P.partials);
 }
 
-// The primal step fed by TMA, persistent: the work is a list of items, each a stage of 64
-// canvas rows (8 / CR block rows, a warp each) of a strip of 32 canvas columns of one of the
-// launch's components (1 or 2 of the same cells, e.g. Cb and Cr); the CTAs the device holds at
-// once take items t = blockIdx.x + n gridDim.x, neighbouring CTAs neighbouring strips, so that
-// the columns two boxes share come from L2. Every item is one 3D box of the channel's x, p1 and
-// p2 planes (40 columns: the strip and 4 on each side; the stage's rows and the row above) and
-// the levels of its blocks, into a ring of two slots: the next item's loads run while an item
-// is computed, across strips and components. The computation of a block row is primal_kernel's,
-// from shared memory.
+// The primal step fed by TMA works on items, each a stage of 64 canvas rows (8 / CR block rows,
+// a compute warp each) of a strip of 32 canvas columns of a component. An item is one 3D box of
+// the channel's x, p1 and p2 planes (36 columns: the strip and 4 to its left; the stage's rows
+// and the row above) and the levels of its blocks, loaded into a slot of a ring while the
+// items before it are computed. The computation of a block row is primal_kernel's, from shared
+// memory.
 constexpr int kStageRows = 64;
+constexpr int kPrimalSpan = 36;  // box columns: 4 + 32 (x at 16-byte boundaries; p1 from j - 1)
 
 template <int CR>
 constexpr int primal_warps() {
   return kStageRows / (8 * CR);
 }
 
+// Slots of the ring: the most that leave room for two CTAs of 256 threads on an SM (luma), or
+// for three of 128 (2x2 chroma cells).
+template <int CR>
+constexpr int primal_slots() {
+  return CR == 1 ? 3 : 2;
+}
+
+// The dynamic shared memory of a primal CTA: the slots' boxes (x, p1, p2), then their levels.
+template <int CR, int CC>
+constexpr std::size_t primal_shared_bytes() {
+  return primal_slots<CR>() * (((3 * (kStageRows + 1) * kPrimalSpan + 31) / 32 * 32) * sizeof(float) +
+                               primal_warps<CR>() * (32 / (8 * CC)) * 64 * sizeof(std::int16_t));
+}
+
 // One warp's block row of a stage, from shared memory: `slot` the stage's box (x, p1, p2: the
-// row above and 64 rows of 40 columns each), `stage_levels` the levels of the lane's block.
+// row above and 64 rows of 36 columns each), `stage_levels` the levels of the lane's block.
 // v = x + tau gamma div p, the cell means less the middle of the DC interval, the DCT, the
 // clip, the inverse DCT, x~ written (and with KEEP zeta and v, and the data term's terms added
 // to `sum`). `t` is the warp's transpose tile.
@@ -497,7 +502,7 @@ __device__ __forceinline__ void primal_block_row(const float* slot, const std::i
                                                  std::size_t block, double& sum) {
   constexpr unsigned kAll = 0xffffffffu;
   constexpr int L = 8 * CC, BH = 8 * CR;
-  constexpr int SPAN = 40, HALO = 4, PLANE = (kStageRows + 1) * SPAN;
+  constexpr int SPAN = kPrimalSpan, HALO = 4, PLANE = (kStageRows + 1) * SPAN;
   const int in_block = lane % L, m = in_block / CC, cell = in_block % CC;
   const int leader = lane - cell;
   const int col = HALO + lane;
@@ -519,7 +524,7 @@ __device__ __forceinline__ void primal_block_row(const float* slot, const std::i
     v[r] = x + descent * (dy + dx);
   }
   const float dc_level = in_blocks ? static_cast<float>(stage_levels[0]) : 0.0f;
-  const float middle = (dc_level * F.step[0] + 1024.0f) * 0.125f;
+  const float middle = (dc_level * F.plain[0].x + 1024.0f) * 0.125f;
   float mean[8];
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
@@ -558,14 +563,7 @@ __device__ __forceinline__ void primal_block_row(const float* slot, const std::i
     levels[u] = static_cast<int>(static_cast<std::int16_t>((u & 1) ? (word >> 16) : (word & 0xffffu)));
   }
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    const int k = m * 8 + u;
-    const Coefficient c = coefficient_of(levels[u], k, F);
-    const float tk = flat ? F.t_flat[k] : F.t[k];
-    const float rk = flat ? F.r_flat[k] : F.r[k];
-    const float hk = flat ? F.h_flat[k] : F.h[k];
-    zeta[u] = prox_of(coef[u], tk, rk, hk, c, F.costed != 0);
-  }
+  for (int u = 0; u < 8; ++u) zeta[u] = prox_at(coef[u], levels[u], m * 8 + u, flat, F);
   if constexpr (KEEP) {
     if (in_blocks && cell == 0) {
       float4* to = reinterpret_cast<float4*>(P.component.zeta + block * 64 + m * 8);
@@ -613,232 +611,277 @@ __device__ __forceinline__ void primal_block_row(const float* slot, const std::i
   }
 }
 
+// The CTA's items t = blockIdx.x + n gridDim.x, n = 0, 1, ..., as (component, stage, strip):
+// one division at the start, then additions.
+struct ItemWalk {
+  int z, stage, strip;
+  int strips, stages, step_stages, step_strips;
+  __device__ ItemWalk(int first, int step, int strips_, int stages_) : strips(strips_), stages(stages_) {
+    const int per_component = strips * stages;
+    z = first / per_component;
+    const int rest = first - z * per_component;
+    stage = rest / strips;
+    strip = rest - stage * strips;
+    step_stages = step / strips;
+    step_strips = step - step_stages * strips;
+  }
+  __device__ void next() {
+    strip += step_strips;
+    stage += step_stages;
+    if (strip >= strips) {
+      strip -= strips;
+      ++stage;
+    }
+    while (stage >= stages && stages > 0) {
+      stage -= stages;
+      ++z;
+    }
+  }
+};
+
+// The loads of an item (a stage of a strip) into a slot: the box of x, p1, p2 and the levels
+// of its blocks, block row by block row (a bulk copy each), on the slot's barrier.
+template <int CR, int CC>
+__device__ __forceinline__ void primal_issue(float* box, std::int16_t* levels, const CUtensorMap* map,
+                                             std::uint64_t* bar, const PrimalParams& P, int strip, int stage) {
+  constexpr int NB = primal_warps<CR>();
+  constexpr int B = 32 / (8 * CC), BH = 8 * CR;
+  constexpr int SLOT = 3 * (kStageRows + 1) * kPrimalSpan;
+  const int vbr = P.g.rows / BH;
+  const int first = stage * NB;
+  const int vbx0 = strip * B;
+  const int blocks = min(B, P.component.block_columns - vbx0);
+  int rows_copied = 0;
+  for (int w = 0; w < NB; ++w) {
+    const int vby = first + w;
+    if (vby < vbr && vby < P.component.block_rows && blocks > 0) ++rows_copied;
+  }
+  barrier_expect(bar, SLOT * 4 + rows_copied * blocks * 128);
+  load_box(box, map, bar, strip * 32 - 4, first * BH - 1, 0);
+  for (int w = 0; w < NB; ++w) {
+    const int vby = first + w;
+    if (vby < vbr && vby < P.component.block_rows && blocks > 0) {
+      load_bulk(levels + w * B * 64,
+                P.component.levels + (static_cast<std::size_t>(vby) * P.component.block_columns + vbx0) * 64,
+                blocks * 128, bar);
+    }
+  }
+}
+
+// The primal step fed by TMA, persistent and warp-specialized: NB warps compute (a block row
+// of every item each) and one more issues the loads. The items are a list of (component, strip,
+// stage) -- a stage is 64 canvas rows, 8 / CR block rows, of a strip of 32 canvas columns of
+// one of the launch's components (1 or 2 of the same cells, e.g. Cb and Cr); the CTAs the
+// device holds at once take items t = blockIdx.x + n gridDim.x, neighbouring CTAs
+// neighbouring strips, so that the columns two boxes share come from L2. An item's loads fill
+// a slot of a ring of S: its `full` barrier ends when the bytes are in, its `empty` barrier
+// when every compute warp is done with it, and only then is the slot loaded again, so the
+// compute warps never wait for one another.
 template <int CR, int CC, bool KEEP>
-__global__ void __launch_bounds__(32 * primal_warps<CR>()) primal_tma_kernel(const __grid_constant__ CUtensorMap map0,
-                                                                             const __grid_constant__ CUtensorMap map1,
-                                                                             const __grid_constant__ PrimalBatch Q) {
+__global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
+    primal_tma_kernel(const __grid_constant__ CUtensorMap map0, const __grid_constant__ CUtensorMap map1,
+                      const __grid_constant__ PrimalBatch Q) {
+  constexpr unsigned kAll = 0xffffffffu;
   constexpr int NB = primal_warps<CR>();
   constexpr int L = 8 * CC, B = 32 / L, BH = 8 * CR;
-  constexpr int SR = kStageRows + 1, SPAN = 40, HALO = 4;
-  constexpr int PLANE = SR * SPAN, SLOT = 3 * PLANE;
+  constexpr int SLOT = 3 * (kStageRows + 1) * kPrimalSpan;
   // Slots 128-byte aligned, as a bulk-tensor copy's shared-memory destination is.
   constexpr int STRIDE = (SLOT + 31) / 32 * 32;
+  constexpr int S = primal_slots<CR>();
+  constexpr int kStageLevels = NB * B * 64;
   extern __shared__ __align__(128) float ring[];
-  __shared__ __align__(8) std::uint64_t bars[2];
+  __shared__ __align__(8) std::uint64_t full[S], empty[S];
   __shared__ ProxFactors factors[2];
   __shared__ PrimalParams parts[2];  // the components' parameters, read per item
   __shared__ float tile[NB][4][72];
+  __shared__ int failures;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int z = 0; z < Q.count; ++z) {
     const float* from = reinterpret_cast<const float*>(Q.part[z].component.factors);
     float* to = reinterpret_cast<float*>(&factors[z]);
-    for (int k = tid; k < static_cast<int>(sizeof(ProxFactors) / 4); k += 32 * NB) to[k] = from[k];
+    for (int k = tid; k < static_cast<int>(sizeof(ProxFactors) / 4); k += 32 * (NB + 1)) to[k] = from[k];
     if (tid == 0) parts[z] = Q.part[z];
   }
   if (tid == 0) {
-    barrier_init(&bars[0], 1);
-    barrier_init(&bars[1], 1);
+    for (int s = 0; s < S; ++s) {
+      barrier_init(&full[s], 1);
+      barrier_init(&empty[s], NB);
+    }
+    failures = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const int per_component = Q.strips * Q.stages;
   const int items = (Q.items - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
                     static_cast<int>(gridDim.x);  // this CTA's
-  // The CTA's n-th item: its component, strip and stage.
-  auto item_of = [&](int n, int& z, int& strip, int& stage) {
-    const int t = static_cast<int>(blockIdx.x) + n * static_cast<int>(gridDim.x);
-    z = t / per_component;
-    const int rest = t - z * per_component;
-    stage = rest / Q.strips;
-    strip = rest - stage * Q.strips;
-  };
-  // The levels of an item's blocks (NB block rows of B blocks), after the two slots, copied
-  // with the item's box.
-  std::int16_t* const levels_ring = reinterpret_cast<std::int16_t*>(ring + 2 * STRIDE);
-  constexpr int kStageLevels = NB * B * 64;
-  auto issue = [&](int n) {
-    if (tid == 0 && n < items) {
-      int z, strip, stage;
-      item_of(n, z, strip, stage);
-      const PrimalParams& P = parts[z];
-      const int vbr = P.g.rows / BH;
-      const int first = stage * NB;
-      const int vbx0 = strip * B;
-      const int count = min(B, P.component.block_columns - vbx0);
-      int rows_copied = 0;
-      for (int w = 0; w < NB; ++w) {
-        const int vby = first + w;
-        if (vby < vbr && vby < P.component.block_rows && count > 0) ++rows_copied;
-      }
-      barrier_expect(&bars[n & 1], SLOT * 4 + rows_copied * count * 128);
-      load_box(ring + (n & 1) * STRIDE, z == 0 ? &map0 : &map1, &bars[n & 1], strip * 32 - HALO, first * BH - 1, 0);
-      for (int w = 0; w < NB; ++w) {
-        const int vby = first + w;
-        if (vby < vbr && vby < P.component.block_rows && count > 0) {
-          load_bulk(levels_ring + (n & 1) * kStageLevels + w * B * 64,
-                    P.component.levels + (static_cast<std::size_t>(vby) * P.component.block_columns + vbx0) * 64,
-                    count * 128, &bars[n & 1]);
-        }
-      }
-    }
-  };
-  issue(0);
-  issue(1);
-  const int blk = lane / L, in_block = lane % L;
-  float* t = tile[warp][blk];
+  // The levels of an item's blocks (NB block rows of B blocks), after the slots.
+  std::int16_t* const levels_ring = reinterpret_cast<std::int16_t*>(ring + S * STRIDE);
+  ItemWalk walk(static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x), Q.strips, Q.stages);
   double sum0 = 0.0, sum1 = 0.0;  // the data term's terms of each component
-  bool failed = false;
-  int stopped = items;
-  for (int s = 0; s < items; ++s) {
-    int z, strip, stage;
-    item_of(s, z, strip, stage);
-    const PrimalParams& P = parts[z];
-    const ProxFactors& F = factors[z];
-    double sum = 0.0;
-    const int vbr = P.g.rows / BH;
-    const int vbx = strip * B + blk;
-    const int j = vbx * L + in_block;
-    const bool column_in = j < P.g.columns;
-    const int vby = stage * NB + warp;
-    const bool in_blocks =
-        vby < vbr && column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
-    const std::size_t block =
-        static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
-    // Read before the wait, used after the transforms.
-    const bool flat = in_blocks && P.component.flat[block] != 0;
-    const bool ready = barrier_wait(&bars[s & 1], (s >> 1) & 1);
-    if (__syncthreads_or(!ready)) {
-      failed = true;
-      stopped = s;
-      break;
+  int issued = 0;
+  if (warp == NB) {
+    if (lane == 0) {
+      for (int n = 0; n < items; ++n, walk.next()) {
+        const int slot = n % S;
+        if (n >= S && !barrier_wait(&empty[slot], (n / S - 1) & 1)) {
+          atomicAdd(&failures, 1);
+          break;
+        }
+        primal_issue<CR, CC>(ring + slot * STRIDE, levels_ring + slot * kStageLevels, walk.z == 0 ? &map0 : &map1,
+                             &full[slot], parts[walk.z], walk.strip, walk.stage);
+        issued = n + 1;
+      }
     }
-    const float* slot = ring + (s & 1) * STRIDE;
-    const std::int16_t* stage_levels = levels_ring + (s & 1) * kStageLevels + (warp * B + blk) * 64;
-    if (vby < vbr) {
-      primal_block_row<CR, CC, KEEP>(slot, stage_levels, P, F, t, warp, lane, vby, j, column_in, in_blocks, flat,
-                                     block, sum);
+  } else {
+    const int blk = lane / L, in_block = lane % L;
+    float* t = tile[warp][blk];
+    for (int s = 0; s < items; ++s, walk.next()) {
+      const int z = walk.z;
+      const PrimalParams& P = parts[z];
+      const ProxFactors& F = factors[z];
+      double sum = 0.0;
+      const int vbr = P.g.rows / BH;
+      const int vbx = walk.strip * B + blk;
+      const int j = vbx * L + in_block;
+      const bool column_in = j < P.g.columns;
+      const int vby = walk.stage * NB + warp;
+      const bool in_blocks =
+          vby < vbr && column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
+      const std::size_t block =
+          static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
+      // Read before the wait, used after the transforms.
+      const bool flat = in_blocks && P.component.flat[block] != 0;
+      const bool ready = barrier_wait(&full[s % S], (s / S) & 1);
+      if (__any_sync(kAll, !ready)) {
+        if (lane == 0) atomicAdd(&failures, 1);
+        break;
+      }
+      const float* slot = ring + (s % S) * STRIDE;
+      const std::int16_t* stage_levels = levels_ring + (s % S) * kStageLevels + (warp * B + blk) * 64;
+      if (vby < vbr) {
+        primal_block_row<CR, CC, KEEP>(slot, stage_levels, P, F, t, warp, lane, vby, j, column_in, in_blocks, flat,
+                                       block, sum);
+      }
+      if (z == 0) {
+        sum0 += sum;
+      } else {
+        sum1 += sum;
+      }
+      __syncwarp();
+      if (lane == 0) barrier_arrive(&empty[s % S]);  // the warp is done with the slot
     }
-    if (z == 0) {
-      sum0 += sum;
-    } else {
-      sum1 += sum;
-    }
-    __syncthreads();  // every warp is done with the slot
-    issue(s + 2);
   }
-  if (failed) {
+  __syncthreads();
+  if (failures != 0) {
     if (tid == 0 && parts[0].error != nullptr) atomicExch(parts[0].error, 1);
+    // No load may still write into shared memory when the CTA leaves: the last one issued into
+    // each slot is waited for.
+    if (warp == NB && lane == 0) {
+      for (int n = max(issued - S, 0); n < issued; ++n) barrier_wait(&full[n % S], (n / S) & 1);
+    }
   }
   if constexpr (KEEP) {
     cta_sum(sum0, parts[0].partials);
     if (Q.count > 1) cta_sum(sum1, parts[1].partials);
   }
-  if (failed) {
-    // No load may still write into shared memory when the CTA leaves: the item that was not
-    // ready and the one after it.
-    for (int s = stopped; s < min(stopped + 2, items); ++s) barrier_wait(&bars[s & 1], (s >> 1) & 1);
-  }
 }
 
 // The primal step of a batch (many components of one cell layout, of many images, of different
-// sizes): a table of items (component, strip, stage); each CTA takes a contiguous range of it
-// through the same two-slot ring as primal_tma_kernel. Each item's parameters and box map are
-// the component's entry of `components` in global memory (the map read through the tensor-map
-// proxy after an acquire fence); its factors are read from global memory. Nothing is kept (the
-// batch's last primal step, which keeps, runs per image).
+// sizes): a table of items (component, strip, stage); each CTA takes a contiguous range of it,
+// warp-specialized as primal_tma_kernel is. Each item's parameters and box map are the
+// component's entry of `components` in global memory (the map read through the tensor-map
+// proxy after an acquire fence), its parameters copied into the slot's with its loads; its
+// factors are read from global memory. Nothing is kept (the batch's last primal step, which
+// keeps, runs per image).
 template <int CR, int CC>
-__global__ void __launch_bounds__(32 * primal_warps<CR>())
+__global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
     primal_batch_kernel(const PrimalItem* __restrict__ list, int count, const PrimalBatchComponent* components,
                         int parity) {
+  constexpr unsigned kAll = 0xffffffffu;
   constexpr int NB = primal_warps<CR>();
   constexpr int L = 8 * CC, B = 32 / L, BH = 8 * CR;
-  constexpr int SR = kStageRows + 1, SPAN = 40, HALO = 4;
-  constexpr int PLANE = SR * SPAN, SLOT = 3 * PLANE;
+  constexpr int SLOT = 3 * (kStageRows + 1) * kPrimalSpan;
   constexpr int STRIDE = (SLOT + 31) / 32 * 32;
+  constexpr int S = primal_slots<CR>();
+  constexpr int kStageLevels = NB * B * 64;
   extern __shared__ __align__(128) float ring[];
-  __shared__ __align__(8) std::uint64_t bars[2];
-  __shared__ PrimalParams parts[2];  // of the items in the two slots
+  __shared__ __align__(8) std::uint64_t full[S], empty[S];
+  __shared__ PrimalParams parts[S];  // of the items in the slots
   __shared__ float tile[NB][4][72];
+  __shared__ int failures;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int first = static_cast<int>(static_cast<long long>(blockIdx.x) * count / gridDim.x);
   const int items = static_cast<int>(static_cast<long long>(blockIdx.x + 1) * count / gridDim.x) - first;
   if (tid == 0) {
-    barrier_init(&bars[0], 1);
-    barrier_init(&bars[1], 1);
+    for (int s = 0; s < S; ++s) {
+      barrier_init(&full[s], 1);
+      barrier_init(&empty[s], NB);
+    }
+    failures = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  std::int16_t* const levels_ring = reinterpret_cast<std::int16_t*>(ring + 2 * STRIDE);
-  constexpr int kStageLevels = NB * B * 64;
-  auto issue = [&](int n) {
-    if (tid == 0 && n < items) {
-      const PrimalItem item = list[first + n];
-      const PrimalBatchComponent& entry = components[item.component];
-      const PrimalParams& P = entry.params[parity];
-      parts[n & 1] = P;
-      const CUtensorMap* map = &entry.map[parity];
-      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
-      const int vbr = P.g.rows / BH;
-      const int stage_first = item.stage * NB;
-      const int vbx0 = item.strip * B;
-      const int blocks = min(B, P.component.block_columns - vbx0);
-      int rows_copied = 0;
-      for (int w = 0; w < NB; ++w) {
-        const int vby = stage_first + w;
-        if (vby < vbr && vby < P.component.block_rows && blocks > 0) ++rows_copied;
-      }
-      barrier_expect(&bars[n & 1], SLOT * 4 + rows_copied * blocks * 128);
-      load_box(ring + (n & 1) * STRIDE, map, &bars[n & 1], item.strip * 32 - HALO, stage_first * BH - 1, 0);
-      for (int w = 0; w < NB; ++w) {
-        const int vby = stage_first + w;
-        if (vby < vbr && vby < P.component.block_rows && blocks > 0) {
-          load_bulk(levels_ring + (n & 1) * kStageLevels + w * B * 64,
-                    P.component.levels + (static_cast<std::size_t>(vby) * P.component.block_columns + vbx0) * 64,
-                    blocks * 128, &bars[n & 1]);
+  std::int16_t* const levels_ring = reinterpret_cast<std::int16_t*>(ring + S * STRIDE);
+  int issued = 0;
+  if (warp == NB) {
+    if (lane == 0) {
+      for (int n = 0; n < items; ++n) {
+        const int slot = n % S;
+        if (n >= S && !barrier_wait(&empty[slot], (n / S - 1) & 1)) {
+          atomicAdd(&failures, 1);
+          break;
         }
+        const PrimalItem item = list[first + n];
+        const PrimalBatchComponent& entry = components[item.component];
+        parts[slot] = entry.params[parity];  // seen by the compute warps with the slot's bytes
+        const CUtensorMap* map = &entry.map[parity];
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+        primal_issue<CR, CC>(ring + slot * STRIDE, levels_ring + slot * kStageLevels, map, &full[slot], parts[slot],
+                             item.strip, item.stage);
+        issued = n + 1;
       }
     }
-  };
-  issue(0);
-  issue(1);
-  __syncthreads();  // the first two items' parameters
-  const int blk = lane / L, in_block = lane % L;
-  float* t = tile[warp][blk];
-  double sum = 0.0;  // unused: nothing is kept
-  bool failed = false;
-  int stopped = items;
-  for (int s = 0; s < items; ++s) {
-    const PrimalItem item = list[first + s];
-    const PrimalParams& P = parts[s & 1];
-    const ProxFactors& F = *P.component.factors;
-    const int vbr = P.g.rows / BH;
-    const int vbx = item.strip * B + blk;
-    const int j = vbx * L + in_block;
-    const bool column_in = j < P.g.columns;
-    const int vby = item.stage * NB + warp;
-    const bool in_blocks =
-        vby < vbr && column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
-    const std::size_t block =
-        static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
-    const bool flat = in_blocks && P.component.flat[block] != 0;
-    const bool ready = barrier_wait(&bars[s & 1], (s >> 1) & 1);
-    if (__syncthreads_or(!ready)) {
-      failed = true;
-      stopped = s;
-      break;
+  } else {
+    const int blk = lane / L, in_block = lane % L;
+    float* t = tile[warp][blk];
+    double sum = 0.0;  // unused: nothing is kept
+    for (int s = 0; s < items; ++s) {
+      const PrimalItem item = list[first + s];
+      const bool ready = barrier_wait(&full[s % S], (s / S) & 1);
+      if (__any_sync(kAll, !ready)) {
+        if (lane == 0) atomicAdd(&failures, 1);
+        break;
+      }
+      const PrimalParams& P = parts[s % S];
+      const ProxFactors& F = *P.component.factors;
+      const int vbr = P.g.rows / BH;
+      const int vbx = item.strip * B + blk;
+      const int j = vbx * L + in_block;
+      const bool column_in = j < P.g.columns;
+      const int vby = item.stage * NB + warp;
+      const bool in_blocks =
+          vby < vbr && column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
+      const std::size_t block =
+          static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
+      const bool flat = in_blocks && P.component.flat[block] != 0;
+      const float* slot = ring + (s % S) * STRIDE;
+      const std::int16_t* stage_levels = levels_ring + (s % S) * kStageLevels + (warp * B + blk) * 64;
+      if (vby < vbr) {
+        primal_block_row<CR, CC, false>(slot, stage_levels, P, F, t, warp, lane, vby, j, column_in, in_blocks, flat,
+                                        block, sum);
+      }
+      __syncwarp();
+      if (lane == 0) barrier_arrive(&empty[s % S]);  // the warp is done with the slot and its parameters
     }
-    const float* slot = ring + (s & 1) * STRIDE;
-    const std::int16_t* stage_levels = levels_ring + (s & 1) * kStageLevels + (warp * B + blk) * 64;
-    if (vby < vbr) {
-      primal_block_row<CR, CC, false>(slot, stage_levels, P, F, t, warp, lane, vby, j, column_in, in_blocks, flat,
-                                      block, sum);
-    }
-    __syncthreads();  // every warp is done with the slot and its parameters
-    issue(s + 2);
   }
-  if (failed && tid == 0 && parts[stopped & 1].error != nullptr) atomicExch(parts[stopped & 1].error, 1);
-  if (failed) {
-    for (int s = stopped; s < min(stopped + 2, items); ++s) barrier_wait(&bars[s & 1], (s >> 1) & 1);
+  __syncthreads();
+  if (failures != 0) {
+    if (tid == 0 && items > 0) {
+      int* error = components[list[first].component].params[parity].error;
+      if (error != nullptr) atomicExch(error, 1);
+    }
+    if (warp == NB && lane == 0) {
+      for (int n = max(issued - S, 0); n < issued; ++n) barrier_wait(&full[n % S], (n / S) & 1);
+    }
   }
 }
 
@@ -1378,10 +1421,8 @@ template <int CR, int CC, bool KEEP>
 cudaError_t primal_tma_one(const CUtensorMap* maps, const PrimalParams* parts, int count, cudaStream_t s,
                            int* grid) {
   auto kernel = primal_tma_kernel<CR, CC, KEEP>;
-  constexpr int threads = 32 * primal_warps<CR>();
-  // Two slots of the x, p1, p2 box, then two items' levels.
-  constexpr std::size_t bytes = 2 * ((3 * (kStageRows + 1) * 40 + 31) / 32 * 32) * sizeof(float) +
-                                2 * (kStageRows / (8 * CR)) * (32 / (8 * CC)) * 64 * sizeof(std::int16_t);
+  constexpr int threads = 32 * (primal_warps<CR>() + 1);  // the compute warps and the loader
+  constexpr std::size_t bytes = primal_shared_bytes<CR, CC>();
   // Once per device: the shared-memory size above 48 KB, and how many CTAs the device holds.
   static std::atomic<int> resident[64] = {};
   int device = 0;
@@ -1403,6 +1444,7 @@ cudaError_t primal_tma_one(const CUtensorMap* maps, const PrimalParams* parts, i
   batch.stages = primal_tma_items_of(parts[0].g, CR) / batch.strips;
   batch.items = count * batch.strips * batch.stages;
   *grid = std::min(batch.items, slots);
+  if (*grid <= 0) return cudaSuccess;  // no block row
   kernel<<<*grid, threads, bytes, s>>>(maps[0], maps[count > 1 ? 1 : 0], batch);
   return cudaGetLastError();
 }
@@ -1418,9 +1460,8 @@ template <int CR, int CC>
 cudaError_t primal_batch_one(const PrimalItem* list, int count, const PrimalBatchComponent* components, int parity,
                              cudaStream_t s) {
   auto kernel = primal_batch_kernel<CR, CC>;
-  constexpr int threads = 32 * primal_warps<CR>();
-  constexpr std::size_t bytes = 2 * ((3 * (kStageRows + 1) * 40 + 31) / 32 * 32) * sizeof(float) +
-                                2 * (kStageRows / (8 * CR)) * (32 / (8 * CC)) * 64 * sizeof(std::int16_t);
+  constexpr int threads = 32 * (primal_warps<CR>() + 1);  // the compute warps and the loader
+  constexpr std::size_t bytes = primal_shared_bytes<CR, CC>();
   static std::atomic<int> resident[64] = {};
   int device = 0;
   cudaGetDevice(&device);

@@ -16,15 +16,24 @@ namespace urb {
 constexpr int kMaxChannels = 3;
 
 // The per-frequency factors of a component's proximal map in binary32, for one step tau
-// (docs/math.md 4.1, 4.4; cpp/src/model.cpp:483-497): t = (tau / n_c) m, r = 1 / (1 + t),
-// and with a slack's cost h = (tau / n_c) lambda r, in a block that is not flat and in one
-// that is; the steps Q; delta / Q of the MMSE centres.
+// (docs/math.md 4.1, 4.4; cpp/src/model.cpp:483-497), with t = (tau / n_c) m and
+// r = 1 / (1 + t): z = (e + t c) r = e r + (t r) c, clipped to q Q -+ (1/2 + s) Q. They are
+// packed four to a frequency, {Q, r, t r, (1/2 + s) Q}, so that one 16-byte load gives a
+// coefficient's map: `plain` for a block that is not flat, `flat` for one that is, frequency k
+// at prox_slot(k). With a slack's cost, h = (tau / n_c) lambda r of each; delta / Q of the MMSE
+// centres.
+//
+// prox_slot keeps frequency k = 8 v + u in row v and puts it at column u ^ v of that row: a
+// warp's eight lanes of a block read one frequency of every row (the primal step's lanes hold
+// rows), or every frequency of one row (the fused iteration's hold columns), and either way
+// eight different 16-byte bank groups of shared memory, one wavefront.
+__host__ __device__ constexpr int prox_slot(int k) {
+  return (k & ~7) | ((k ^ (k >> 3)) & 7);
+}
+
 struct ProxFactors {
-  float step[64];
-  float t[64];
-  float r[64];
-  float t_flat[64];
-  float r_flat[64];
+  float4 plain[64];
+  float4 flat[64];
   float h[64];
   float h_flat[64];
   float shrink[64];
@@ -251,10 +260,10 @@ cudaError_t launch_dual_batch(const DualTile* tiles, int count, const DualBatchI
                               int channels, bool coupled, cudaStream_t stream);
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,
                             bool coupled, bool keep, cudaStream_t stream);
-// A 3D tiled map of `count` float planes `stride` floats apart, boxes of 40 columns x
-// `box_rows` rows x every plane (sweep.cu).
+// A 3D tiled map of `count` float planes `stride` floats apart, boxes of `box_columns` columns
+// (a multiple of 4) x `box_rows` rows x every plane (sweep.cu).
 bool make_box_map(CUtensorMap& map, const float* planes, const Geometry& g, int count, std::size_t stride,
-                  unsigned box_rows);
+                  unsigned box_rows, unsigned box_columns);
 
 // The whole iteration as one sweep (iteration.cu): the dual step D_n with the relaxation, from
 // x~_n and s_{n-1} (dual.in, dual.xt) to s_n (dual.out), and the primal step P_{n+1} on s_n,

@@ -235,15 +235,16 @@ struct Solver::Impl {
       ProxFactors f{};
       const double step = p.tau / static_cast<double>(comp.cells());
       for (int k = 0; k < 64; ++k) {
-        f.step[k] = static_cast<float>(comp.steps[k]);
+        const double q = static_cast<double>(comp.steps[k]);
+        const double reach = (0.5 + comp.slack) * q;
         const double t = step * comp.weights[k];
         const double r = 1.0 / (1.0 + t);
         const double tf = step * comp.flat_weights[k];
         const double rf = 1.0 / (1.0 + tf);
-        f.t[k] = static_cast<float>(t);
-        f.r[k] = static_cast<float>(r);
-        f.t_flat[k] = static_cast<float>(tf);
-        f.r_flat[k] = static_cast<float>(rf);
+        f.plain[prox_slot(k)] = make_float4(static_cast<float>(q), static_cast<float>(r),
+                                            static_cast<float>(t * r), static_cast<float>(reach));
+        f.flat[prox_slot(k)] = make_float4(static_cast<float>(q), static_cast<float>(rf),
+                                           static_cast<float>(tf * rf), static_cast<float>(reach));
         f.h[k] = static_cast<float>(step * comp.costs[k] * r);
         f.h_flat[k] = static_cast<float>(step * comp.costs[k] * rf);
         f.shrink[k] = static_cast<float>(comp.shrink[k]);

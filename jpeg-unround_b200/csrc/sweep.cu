@@ -416,13 +416,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
 // A 3D tiled map of `count` float planes `stride` floats apart, each the canvas's rows x columns
 // (rows `pitch` apart), boxes of 40 columns x `box_rows` rows x every plane.
 bool make_box_map(CUtensorMap& map, const float* planes, const Geometry& g, int count, std::size_t stride,
-                  unsigned box_rows) {
+                  unsigned box_rows, unsigned box_columns) {
   PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
   if (encode == nullptr) return false;
   const cuuint64_t dims[3] = {static_cast<cuuint64_t>(g.columns), static_cast<cuuint64_t>(g.rows),
                               static_cast<cuuint64_t>(count)};
   const cuuint64_t strides[2] = {static_cast<cuuint64_t>(g.pitch) * sizeof(float), stride * sizeof(float)};
-  const cuuint32_t box[3] = {kSpan, box_rows, static_cast<cuuint32_t>(count)};
+  const cuuint32_t box[3] = {box_columns, box_rows, static_cast<cuuint32_t>(count)};
   const cuuint32_t steps[3] = {1, 1, 1};
   const CUresult result = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(planes), dims, strides,
                                  box, steps, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -431,11 +431,11 @@ bool make_box_map(CUtensorMap& map, const float* planes, const Geometry& g, int 
 }
 
 bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count) {
-  return make_box_map(map, planes, g, count, g.plane, kChunk);
+  return make_box_map(map, planes, g, count, g.plane, kChunk, kSpan);
 }
 
 bool make_primal_map(CUtensorMap& map, const float* x, const Geometry& g, std::size_t stride) {
-  return make_box_map(map, x, g, 3, stride, 65);
+  return make_box_map(map, x, g, 3, stride, 65, 36);
 }
 
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,

@@ -24,6 +24,11 @@ __device__ __forceinline__ void barrier_expect(std::uint64_t* bar, unsigned byte
                : "memory");
 }
 
+// One arrival (release: the thread's earlier writes are seen by whoever sees the phase end).
+__device__ __forceinline__ void barrier_arrive(std::uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_address(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool barrier_try(std::uint64_t* bar, unsigned parity) {
   unsigned done;
   asm volatile(
