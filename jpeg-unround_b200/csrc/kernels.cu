@@ -517,10 +517,11 @@ __device__ __forceinline__ void primal_block_row(const float* slot, const std::i
     const float x = slot[0 * PLANE + sr * SPAN + col];
     const float p1 = slot[1 * PLANE + sr * SPAN + col];
     const float p2 = slot[2 * PLANE + sr * SPAN + col];
+    // Row -1 and column -1 lie outside the planes: the box holds zeros there.
     const float before = slot[1 * PLANE + sr * SPAN + col - 1];
     const float above = slot[2 * PLANE + (sr - 1) * SPAN + col];
-    const float dy = (i + 1 < rows ? p2 : 0.0f) - (i > 0 ? above : 0.0f);
-    const float dx = (j + 1 < columns ? p1 : 0.0f) - (j > 0 ? before : 0.0f);
+    const float dy = (i + 1 < rows ? p2 : 0.0f) - above;
+    const float dx = (j + 1 < columns ? p1 : 0.0f) - before;
     v[r] = x + descent * (dy + dx);
   }
   const float dc_level = in_blocks ? static_cast<float>(stage_levels[0]) : 0.0f;
@@ -734,6 +735,16 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
   } else {
     const int blk = lane / L, in_block = lane % L;
     float* t = tile[warp][blk];
+    // The flat flag of the lane's block in an item, read an item ahead of its use.
+    auto flag_of = [&](const ItemWalk& w) -> std::uint8_t {
+      const PrimalParams& P = parts[w.z];
+      const int vbx = w.strip * B + blk, vby = w.stage * NB + warp;
+      const bool in = vby < P.g.rows / BH && vbx * L + in_block < P.g.columns && vby < P.component.block_rows &&
+                      vbx < P.component.block_columns;
+      return in ? P.component.flat[static_cast<std::size_t>(vby) * P.component.block_columns + vbx] : 0;
+    };
+    ItemWalk ahead = walk;
+    std::uint8_t flat_next = items > 0 ? flag_of(ahead) : 0;
     for (int s = 0; s < items; ++s, walk.next()) {
       const int z = walk.z;
       const PrimalParams& P = parts[z];
@@ -748,8 +759,9 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
           vby < vbr && column_in && vby < P.component.block_rows && vbx < P.component.block_columns;
       const std::size_t block =
           static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
-      // Read before the wait, used after the transforms.
-      const bool flat = in_blocks && P.component.flat[block] != 0;
+      const bool flat = in_blocks && flat_next != 0;
+      ahead.next();
+      flat_next = s + 1 < items ? flag_of(ahead) : 0;
       const bool ready = barrier_wait(&full[s % S], (s / S) & 1);
       if (__any_sync(kAll, !ready)) {
         if (lane == 0) atomicAdd(&failures, 1);
