@@ -264,6 +264,11 @@ cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, 
 // (a multiple of 4) x `box_rows` rows x every plane (sweep.cu).
 bool make_box_map(CUtensorMap& map, const float* planes, const Geometry& g, int count, std::size_t stride,
                   unsigned box_rows, unsigned box_columns);
+// A 4D tiled map of `fields` planes `plane` floats apart, each `images` pictures of rows x
+// columns (packed), boxes of `box_columns` (a multiple of 4) x `box_rows` of one picture x every
+// field (sweep.cu).
+bool make_fields_map(CUtensorMap& map, const float* base, int columns, int rows, int images, int fields,
+                     std::size_t plane, unsigned box_columns, unsigned box_rows);
 
 // The whole iteration as one sweep (iteration.cu): the dual step D_n with the relaxation, from
 // x~_n and s_{n-1} (dual.in, dual.xt) to s_n (dual.out), and the primal step P_{n+1} on s_n,

@@ -430,6 +430,22 @@ bool make_box_map(CUtensorMap& map, const float* planes, const Geometry& g, int 
   return result == CUDA_SUCCESS;
 }
 
+bool make_fields_map(CUtensorMap& map, const float* base, int columns, int rows, int images, int fields,
+                     std::size_t plane, unsigned box_columns, unsigned box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
+  if (encode == nullptr) return false;
+  const cuuint64_t dims[4] = {static_cast<cuuint64_t>(columns), static_cast<cuuint64_t>(rows),
+                              static_cast<cuuint64_t>(images), static_cast<cuuint64_t>(fields)};
+  const cuuint64_t strides[3] = {static_cast<cuuint64_t>(columns) * sizeof(float),
+                                 static_cast<cuuint64_t>(rows) * columns * sizeof(float), plane * sizeof(float)};
+  const cuuint32_t box[4] = {box_columns, box_rows, 1, static_cast<cuuint32_t>(fields)};
+  const cuuint32_t steps[4] = {1, 1, 1, 1};
+  const CUresult result = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(base), dims, strides,
+                                 box, steps, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return result == CUDA_SUCCESS;
+}
+
 bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count) {
   return make_box_map(map, planes, g, count, g.plane, kChunk, kSpan);
 }

@@ -21,13 +21,16 @@
 // backward pass recomputes each segment's states from its checkpoint. The parameters' gradients
 // are sums over pixels and iterations, reduced per CTA and added in binary64.
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
 #include "dct.cuh"
+#include "kernels.hpp"
 #include "unround.h"
 #include "unround_b200.h"
 
@@ -167,101 +170,120 @@ __global__ void __launch_bounds__(256) start_kernel(Problem q, const float* x0, 
   s.w2[k] = i + 1 < q.rows ? x0[k + q.columns] - x : 0.0f;
 }
 
-// A CTA a row of 4 blocks: thread (tx, ty) the pixel (8 by + ty, 32 bx + tx).
-__device__ __forceinline__ float primal_v(const Problem& q, const Planes& s, int z, int i, int j) {
-  const std::size_t k = at(q, z, i, j);
-  const float dy = (i + 1 < q.rows ? s.p2[k] : 0.0f) - (i > 0 ? s.p2[k - q.columns] : 0.0f);
-  const float dx = (j + 1 < q.columns ? s.p1[k] : 0.0f) - (j > 0 ? s.p1[k - 1] : 0.0f);
-  return s.x[k] + q.tau[z] * (dy + dx);
+// ---- The block kernels: a warp per block row of a strip of 32 columns (4 blocks), a lane per
+// column; a CTA of 8 warps takes 8 block rows of the strip. The 2D transforms run in registers,
+// 8 values a lane, with one transpose through the block's tile of the warp: forward2 takes the
+// lane's column of its block and gives row m = lane % 8 of the coefficients (frequency
+// k = 8 m + u at [u]); inverse2 takes that row and gives the lane's column back.
+__device__ __forceinline__ void forward2(const float (&column)[8], float (&row)[8], float* t, int m) {
+  float f[8], g[8];
+  forward8(column, f);
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 8; ++k) t[k * 9 + m] = f[k];
+  __syncwarp();
+#pragma unroll
+  for (int u = 0; u < 8; ++u) g[u] = t[m * 9 + u];
+  forward8(g, row);
 }
 
-// The DCT basis C[k][n] at k * 9 + n (rows padded against bank conflicts), for a CTA's
-// transforms: filled once per CTA from the compile-time values.
-struct BasisTable {
-  float v[8 * 9];
+__device__ __forceinline__ void inverse2(const float (&row)[8], float (&column)[8], float* t, int m) {
+  float f[8], g[8];
+  inverse8(row, f);
+  __syncwarp();
+#pragma unroll
+  for (int n = 0; n < 8; ++n) t[m * 9 + n] = f[n];
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 8; ++k) g[k] = t[k * 9 + m];
+  inverse8(g, column);
+}
+
+// v = x + tau div p down the lane's column of block row `by` (column jc), and div p itself;
+// div p = dy' p2 + dx' p1 by backward differences, the neighbour to the left from the lane
+// beside.
+__device__ __forceinline__ void column_v(const Problem& q, const Planes& s, int z, int by, int jc, float tau,
+                                         float (&v)[8], float (&div)[8]) {
+  const int lane = threadIdx.x, i0 = by * 8;
+  float above = i0 > 0 ? s.p2[at(q, z, i0 - 1, jc)] : 0.0f;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int i = i0 + r;
+    const std::size_t k = at(q, z, i, jc);
+    const float p1 = s.p1[k], p2 = s.p2[k];
+    float before = __shfl_up_sync(kAll, p1, 1);
+    if (lane == 0) before = jc > 0 ? s.p1[k - 1] : 0.0f;
+    const float dy = (i + 1 < q.rows ? p2 : 0.0f) - (i > 0 ? above : 0.0f);
+    const float dx = (jc + 1 < q.columns ? p1 : 0.0f) - (jc > 0 ? before : 0.0f);
+    div[r] = dy + dx;
+    v[r] = s.x[k] + tau * div[r];
+    above = p2;
+  }
+}
+
+// The clip of row m of a block's coefficients, `e` their values: zeta = clip((e + t c) r, a, b),
+// t = tau m_k (of a flat block where the block is flat), r = 1 / (1 + t); `inside` where the
+// unclipped value lies strictly inside (a, b), and the pieces of d zeta / d tau there.
+struct ClipRow {
+  float zeta[8], r[8], weight[8], centre[8];
+  bool inside[8];
 };
 
-__device__ __forceinline__ void fill_basis(BasisTable& table) {
-  const int t = threadIdx.y * blockDim.x + threadIdx.x;
-  if (t < 64) {
-    const int k = t >> 3, n = t & 7;
-    float c = 0.0f;
+__device__ __forceinline__ void clip_row(const Problem& q, int z, std::size_t block, int m, float tau,
+                                         const float (&e)[8], ClipRow& out) {
+  const std::size_t blocks = static_cast<std::size_t>(q.blocks_down) * q.blocks_across;
+  const bool flat = q.flat[static_cast<std::size_t>(z) * blocks + block] != 0;
+  const float* weights = (flat ? q.flat_weight : q.weight) + z * 64 + m * 8;
+  const std::size_t c = (static_cast<std::size_t>(z) * blocks + block) * 64 + m * 8;
+  float lower[8], upper[8];
 #pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-#pragma unroll
-      for (int nn = 0; nn < 8; ++nn) c = (kk == k && nn == n) ? basis_as<float>(kk, nn) : c;
-    }
-    table.v[k * 9 + n] = c;
+  for (int h = 0; h < 2; ++h) {
+    const float4 wv = *reinterpret_cast<const float4*>(weights + 4 * h);
+    const float4 cv = *reinterpret_cast<const float4*>(q.centre + c + 4 * h);
+    const float4 lv = *reinterpret_cast<const float4*>(q.lower + c + 4 * h);
+    const float4 uv = *reinterpret_cast<const float4*>(q.upper + c + 4 * h);
+    out.weight[4 * h] = wv.x, out.weight[4 * h + 1] = wv.y, out.weight[4 * h + 2] = wv.z, out.weight[4 * h + 3] = wv.w;
+    out.centre[4 * h] = cv.x, out.centre[4 * h + 1] = cv.y, out.centre[4 * h + 2] = cv.z, out.centre[4 * h + 3] = cv.w;
+    lower[4 * h] = lv.x, lower[4 * h + 1] = lv.y, lower[4 * h + 2] = lv.z, lower[4 * h + 3] = lv.w;
+    upper[4 * h] = uv.x, upper[4 * h + 1] = uv.y, upper[4 * h + 2] = uv.z, upper[4 * h + 3] = uv.w;
   }
-  __syncthreads();
-}
-
-// The 2D transform of a CTA's 4 blocks in shared memory, in place: forward (C V C^T) or inverse
-// (C^T V C); `t` holds the values [8][33], each thread one.
-__device__ __forceinline__ float transform(float value, float (*t)[33], const BasisTable& basis, bool forward) {
-  const int tx = threadIdx.x, ty = threadIdx.y, n0 = tx & ~7, u = tx & 7;
-  t[ty][tx] = value;
-  __syncthreads();
-  // Columns: row ty of the result from the 8 rows of the column tx.
-  float acc = 0.0f;
 #pragma unroll
-  for (int a = 0; a < 8; ++a) {
-    const float c = forward ? basis.v[ty * 9 + a] : basis.v[a * 9 + ty];
-    acc = fmaf(c, t[a][tx], acc);
+  for (int u = 0; u < 8; ++u) {
+    const float t = tau * out.weight[u];
+    out.r[u] = 1.0f / (1.0f + t);
+    const float zz = (e[u] + t * out.centre[u]) * out.r[u];
+    out.inside[u] = zz > lower[u] && zz < upper[u];
+    out.zeta[u] = fminf(fmaxf(zz, lower[u]), upper[u]);
   }
-  __syncthreads();
-  t[ty][tx] = acc;
-  __syncthreads();
-  // Rows: element u of the block's row ty from its 8 elements.
-  float out = 0.0f;
-#pragma unroll
-  for (int b = 0; b < 8; ++b) {
-    const float c = forward ? basis.v[u * 9 + b] : basis.v[b * 9 + u];
-    out = fmaf(c, t[ty][n0 + b], out);
-  }
-  __syncthreads();
-  return out;
-}
-
-struct Clip {
-  float z, r, t, weight, centre, e;
-  bool inside;
-};
-
-__device__ __forceinline__ Clip clip_of(const Problem& q, int z, std::size_t block, int kk, float e) {
-  const float tau = q.tau[z];
-  const bool flat = q.flat[static_cast<std::size_t>(z) * q.blocks_down * q.blocks_across + block] != 0;
-  const float m = flat ? q.flat_weight[z * 64 + kk] : q.weight[z * 64 + kk];
-  const std::size_t c = ((static_cast<std::size_t>(z) * q.blocks_down * q.blocks_across) + block) * 64 + kk;
-  Clip out;
-  out.weight = m;
-  out.t = tau * m;
-  out.r = 1.0f / (1.0f + out.t);
-  out.centre = q.centre[c];
-  out.e = e;
-  const float zz = (e + out.t * out.centre) * out.r;
-  const float a = q.lower[c], b = q.upper[c];
-  out.inside = zz > a && zz < b;
-  out.z = fminf(fmaxf(zz, a), b);
-  return out;
 }
 
 __global__ void __launch_bounds__(256) primal_kernel(Problem q, Planes s, float* xt) {
-  __shared__ float t[8][33];
-  __shared__ BasisTable basis;
-  fill_basis(basis);
-  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  __shared__ float tiles[8][4][72];
+  const int lane = threadIdx.x, warp = threadIdx.y, z = blockIdx.z;
+  const int by = blockIdx.y * 8 + warp;
+  if (by >= q.blocks_down) return;  // the whole warp; no CTA barrier follows
+  const int j = blockIdx.x * 32 + lane;
   const bool in = j < q.columns;
-  const int jc = in ? j : q.columns - 1;
-  const int bx = jc / 8, by = blockIdx.y;
-  const std::size_t block = static_cast<std::size_t>(by) * q.blocks_across + bx;
-  const float middle = q.middle[static_cast<std::size_t>(z) * q.blocks_down * q.blocks_across + block];
-  const float v = primal_v(q, s, z, i, jc);
-  const float e = transform(v - middle, t, basis, true);
-  const int kk = threadIdx.y * 8 + (threadIdx.x & 7);
-  const Clip c = clip_of(q, z, block, kk, e);
-  const float back = transform(c.z, t, basis, false);
-  if (in) xt[at(q, z, i, j)] = back + middle;
+  const int jc = in ? j : q.columns - 1, m = lane & 7;
+  const std::size_t blocks = static_cast<std::size_t>(q.blocks_down) * q.blocks_across;
+  const std::size_t block = static_cast<std::size_t>(by) * q.blocks_across + jc / 8;
+  float* t = tiles[warp][lane >> 3];
+  const float tau = q.tau[z];
+  float v[8], div[8];
+  column_v(q, s, z, by, jc, tau, v, div);
+  const float middle = q.middle[static_cast<std::size_t>(z) * blocks + block];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) v[r] -= middle;
+  float e[8];
+  forward2(v, e, t, m);
+  ClipRow c;
+  clip_row(q, z, block, m, tau, e, c);
+  float back[8];
+  inverse2(c.zeta, back, t, m);
+  if (in) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) xt[at(q, z, by * 8 + r, j)] = back[r] + middle;
+  }
 }
 
 __global__ void __launch_bounds__(256) dual_kernel(Problem q, Planes s, const float* xt, Planes out) {
@@ -282,187 +304,308 @@ __global__ void __launch_bounds__(256) dual_kernel(Problem q, Planes s, const fl
   out.r12[k] = rho * (d.s12 * sr) + rest * s.r12[k];
 }
 
-// ---- Adjoint. `a` holds the adjoint of s_k (the dual step's output) on entry; the kernels
-// write the adjoint of s_{k-1} into `b` and the adjoint of x~_k into `xt_bar`. Gradients:
-// [0] alpha0, [1] alpha1, [2] tau, [3] sigma, each [image].
+// ---- Adjoint. `a` holds the adjoint of s_k (the dual step's output) and, as its ninth plane,
+// that of v of the primal step P_{k+1} after it; the kernels write the adjoint of s_{k-1} into
+// `b` and the adjoint of x~_k into `xt_bar`. Gradients: [0] alpha0, [1] alpha1, [2] tau,
+// [3] sigma, each [image].
+//
+// The dual step's adjoint is one kernel over tiles of 16 rows x 32 columns. A tile's CTA loads,
+// by two 4D bulk-tensor copies, the 9 planes of s_{k-1} and x~_k and the 9 of the adjoint with
+// halos (2 rows above and 2 below, 4 columns each side: whole 16-byte words), and then in shared
+// memory: w~ over the tile and a ring of 2 (1), the adjoints of the projections' points q and s
+// over the tile and a ring of 1 (2), the adjoint of w~ over the tile and the ring's left column
+// and upper row (3), and the tile's adjoints (4). A halo's values are recomputed by each tile
+// that needs them; the gradients count the tile's own pixels only.
+constexpr int kAdjointRows = 16;                 // a tile's rows
+constexpr int kAdjointSpan = 40;                 // columns of a box: 4 + 32 + 4
+constexpr int kStateRows = kAdjointRows + 4;     // s_{k-1}, x~_k: rows i0 - 2 .. i0 + 17
+constexpr int kBarRows = kAdjointRows + 3;       // the adjoint: rows i0 - 1 .. i0 + 17
+constexpr int kFields = 9;
+constexpr int kTildeRows = kAdjointRows + 3, kTildeColumns = 36;  // (1): rows i0 - 2 .., columns j0 - 2 ..
+constexpr int kPointRows = kAdjointRows + 2, kPointColumns = 34;  // (2): rows i0 - 1 .., columns j0 - 1 ..
+constexpr int kBackRows = kAdjointRows + 1, kBackColumns = 33;    // (3): rows i0 - 1 .., columns j0 - 1 ..
+constexpr int kStateFloats = kFields * kStateRows * kAdjointSpan;
+constexpr int kBarFloats = kFields * kBarRows * kAdjointSpan;
+constexpr int kTildeFloats = 2 * kTildeRows * kTildeColumns;
+constexpr int kPointFloats = 5 * kPointRows * kTildeColumns;
+static_assert(2 * kBackRows * kTildeColumns <= kTildeFloats, "(3) reuses the space of (1)");
+static_assert(kStateFloats % 32 == 0, "the adjoint's box starts 128-byte aligned");
+constexpr std::size_t kAdjointShared =
+    static_cast<std::size_t>(kStateFloats + kBarFloats + kTildeFloats + kPointFloats) * sizeof(float);
 
-struct Scratch {
-  float* q1;  // the adjoint of the projections' points q and s
-  float* q2;
-  float* s11;
-  float* s22;
-  float* s12;
-  float* v;   // the adjoint of v of a primal step
-};
-
-// The adjoint of x and p of s_k: that of the dual step after it (`a`) and that of the primal
-// step P_{k+1}, whose v = x + tau div p has the adjoint `vbar` (null where there is none):
-// x^ += v^, p^ += tau div^T v^ = -tau grad v^.
-__device__ __forceinline__ float adjoint_x(const Planes& a, const float* vbar, std::size_t k) {
-  return vbar != nullptr ? a.x[k] + vbar[k] : a.x[k];
+__device__ __forceinline__ unsigned shared_address(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ void adjoint_p(const Problem& q, const Planes& a, const float* vbar, float tau, int i, int j,
-                                          std::size_t k, float& p1, float& p2) {
-  p1 = a.p1[k];
-  p2 = a.p2[k];
-  if (vbar != nullptr) {
-    const float v = vbar[k];
-    if (j + 1 < q.columns) p1 += -tau * (vbar[k + 1] - v);
-    if (i + 1 < q.rows) p2 += -tau * (vbar[k + q.columns] - v);
-  }
+__device__ __forceinline__ void load_fields(float* to, const CUtensorMap* map, std::uint64_t* bar, int x, int y,
+                                            int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(shared_address(to)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(0), "r"(shared_address(bar))
+      : "memory");
 }
 
-// The adjoint of w~ at a pixel from the local kernel's adjoints of q and s: that of w- is
-// -sigma q^ + sigma E^T s^ (E^T gathering s^ of the pixel and of its right and lower ones), and
-// w~ = (w- + w) / 2 gives it twice, beside the relaxation's rho w'^.
-__device__ __forceinline__ void w_tilde_bar(const Problem& q, const Planes& a, const Scratch& w, int z, int i, int j,
-                                            float& t1, float& t2, float& wb1, float& wb2) {
-  const std::size_t k = at(q, z, i, j);
-  const int W = q.columns;
-  const float sigma = q.sigma[z], rho = q.rho;
-  wb1 = -sigma * w.q1[k];
-  wb2 = -sigma * w.q2[k];
-  float e1 = 0.0f, e2 = 0.0f;
-  if (j + 1 < W) {
-    e1 += w.s11[k] - w.s11[k + 1];
-    e2 += 0.5f * (w.s12[k] - w.s12[k + 1]);
+__device__ __forceinline__ bool wait_phase(std::uint64_t* bar, unsigned parity) {
+  for (long long n = 0; n < (1LL << 22); ++n) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(shared_address(bar)), "r"(parity)
+        : "memory");
+    if (done != 0) return true;
   }
-  if (i + 1 < q.rows) {
-    e2 += w.s22[k] - w.s22[k + W];
-    e1 += 0.5f * (w.s12[k] - w.s12[k + W]);
-  }
-  wb1 += sigma * e1;
-  wb2 += sigma * e2;
-  t1 = rho * a.w1[k] + 2.0f * wb1;
-  t2 = rho * a.w2[k] + 2.0f * wb2;
+  return false;
 }
 
-__global__ void __launch_bounds__(256) dual_adjoint_local(Problem q, Planes s, const float* xt, Planes a,
-                                                          const float* vbar, Scratch w, double* grads) {
-  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-  const bool in = i < q.rows && j < q.columns;
+__global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant__ CUtensorMap state_map,
+                                                           const __grid_constant__ CUtensorMap bar_map, Problem q,
+                                                           Planes b, float* xt_bar, double* grads) {
+  extern __shared__ __align__(128) float shared[];
+  __shared__ __align__(8) std::uint64_t loaded;
+  float* const S = shared;                       // [field][row][column], row i0 - 2 + r, column j0 - 4 + c
+  float* const A = S + kStateFloats;             // [field][row][column], row i0 - 1 + r, column j0 - 4 + c
+  float* const T = A + kBarFloats;               // (1) w~, then (3) the adjoint of w~
+  float* const L = T + kTildeFloats;             // (2) q^1, q^2, s^11, s^22, s^12
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int z = blockIdx.z, i0 = blockIdx.y * kAdjointRows, j0 = blockIdx.x * 32;
+  const int H = q.rows, W = q.columns;
+  const float rho = q.rho, rest = 1.0f - q.rho, tau = q.tau[z], sigma = q.sigma[z];
+  const float alpha0 = q.alpha0[z], alpha1 = q.alpha1[z];
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(shared_address(&loaded)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(shared_address(&loaded)),
+                 "r"(static_cast<unsigned>((kStateFloats + kBarFloats) * sizeof(float)))
+                 : "memory");
+    load_fields(S, &state_map, &loaded, j0 - 4, i0 - 2, z);
+    load_fields(A, &bar_map, &loaded, j0 - 4, i0 - 1, z);
+  }
+  const bool ready = wait_phase(&loaded, 0);
+  if (__syncthreads_or(!ready)) {
+    // The loads did not land: the gradients say so, and no copy may still be writing into the
+    // CTA's shared memory when it leaves.
+    if (tid == 0) {
+      atomicAdd(grads + 3 * q.images + z, static_cast<double>(__int_as_float(0x7fc00000)));
+      wait_phase(&loaded, 0);
+    }
+    return;
+  }
+  auto s_at = [&](int f, int i, int j) -> float { return S[(f * kStateRows + i - i0 + 2) * kAdjointSpan + j - j0 + 4]; };
+  auto a_at = [&](int f, int i, int j) -> float { return A[(f * kBarRows + i - i0 + 1) * kAdjointSpan + j - j0 + 4]; };
+  auto t_at = [&](int f, int i, int j) -> float& { return T[(f * kTildeRows + i - i0 + 2) * kTildeColumns + j - j0 + 2]; };
+  auto l_at = [&](int f, int i, int j) -> float& { return L[(f * kPointRows + i - i0 + 1) * kTildeColumns + j - j0 + 1]; };
+  auto tb_at = [&](int f, int i, int j) -> float& { return T[(f * kBackRows + i - i0 + 1) * kTildeColumns + j - j0 + 1]; };
+  enum { X = 0, P1, P2, W1, W2, R11, R22, R12, EXTRA };  // EXTRA: x~ in S, v^ in A
+
+  // (1) w~ = w + tau (p + div2 r), div2 r by forward differences.
+  for (int n = tid; n < kTildeRows * kTildeColumns; n += 256) {
+    const int i = i0 - 2 + n / kTildeColumns, j = j0 - 2 + n % kTildeColumns;
+    const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
+    float d1 = j + 1 < W ? s_at(R11, i, j + 1) - r11 : 0.0f;
+    float d2 = j + 1 < W ? s_at(R12, i, j + 1) - r12 : 0.0f;
+    d1 = d1 + (i + 1 < H ? s_at(R12, i + 1, j) - r12 : 0.0f);
+    d2 = d2 + (i + 1 < H ? s_at(R22, i + 1, j) - r22 : 0.0f);
+    t_at(0, i, j) = s_at(W1, i, j) + tau * (s_at(P1, i, j) + d1);
+    t_at(1, i, j) = s_at(W2, i, j) + tau * (s_at(P2, i, j) + d2);
+  }
+  __syncthreads();
+
+  // (2) The points q = p + sigma (grad x- - w-) and s = r + sigma E w-, and the adjoints of q
+  // and s through the projections onto the balls (d/d alpha1, d/d alpha0 and d/d sigma beside).
   float g_alpha0 = 0.0f, g_alpha1 = 0.0f, g_sigma = 0.0f;
-  if (in) {
-    const std::size_t k = at(q, z, i, j);
-    const float rho = q.rho;
-    const DualPoint d = dual_point(q, s, xt, z, i, j);
-    // p~ = proj(q): the adjoint of q from that of p~.
-    float ap1, ap2;
-    adjoint_p(q, a, vbar, q.tau[z], i, j, k, ap1, ap2);
-    const float pb1 = rho * ap1, pb2 = rho * ap2;
-    float qb1 = pb1, qb2 = pb2;
-    const float alpha1 = q.alpha1[z];
-    const float nq = sqrtf(d.q1 * d.q1 + d.q2 * d.q2);
-    if (nq > alpha1) {
-      const float dot = d.q1 * pb1 + d.q2 * pb2;
-      const float f = alpha1 / nq, h = dot / (nq * nq);
-      qb1 = f * (pb1 - d.q1 * h);
-      qb2 = f * (pb2 - d.q2 * h);
-      g_alpha1 = dot / nq;
-    }
-    // r~ = proj_F(s), |s|^2 = s11^2 + s22^2 + 2 s12^2.
-    const float rb11 = rho * a.r11[k], rb22 = rho * a.r22[k], rb12 = rho * a.r12[k];
-    float sb11 = rb11, sb22 = rb22, sb12 = rb12;
-    const float alpha0 = q.alpha0[z];
-    const float ns = sqrtf(d.s11 * d.s11 + d.s22 * d.s22 + 2.0f * (d.s12 * d.s12));
-    if (ns > alpha0) {
-      const float dot = d.s11 * rb11 + d.s22 * rb22 + d.s12 * rb12;
-      const float f = alpha0 / ns, h = dot / (ns * ns);
-      sb11 = f * (rb11 - d.s11 * h);
-      sb22 = f * (rb22 - d.s22 * h);
-      sb12 = f * (rb12 - 2.0f * d.s12 * h);
-      g_alpha0 = dot / ns;
-    }
-    g_sigma = qb1 * (d.g1 - d.b1) + qb2 * (d.g2 - d.b2) + sb11 * d.e11 + sb22 * d.e22 + sb12 * d.e12;
-    w.q1[k] = qb1;
-    w.q2[k] = qb2;
-    w.s11[k] = sb11;
-    w.s22[k] = sb22;
-    w.s12[k] = sb12;
-  }
-  add_sum(g_alpha0, grads + 0 * q.images + z);
-  add_sum(g_alpha1, grads + 1 * q.images + z);
-  add_sum(g_sigma, grads + 3 * q.images + z);
-}
-
-__global__ void __launch_bounds__(256) dual_adjoint_gather(Problem q, Planes s, Planes a, const float* vbar,
-                                                           Scratch w, Planes b, float* xt_bar, double* grads) {
-  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-  const bool in = i < q.rows && j < q.columns;
-  float g_tau = 0.0f;
-  if (in) {
-    const std::size_t k = at(q, z, i, j);
-    const int W = q.columns, H = q.rows;
-    const float rho = q.rho, rest = 1.0f - q.rho, sigma = q.sigma[z], tau = q.tau[z];
+  for (int n = tid; n < kPointRows * kPointColumns; n += 256) {
+    const int i = i0 - 1 + n / kPointColumns, j = j0 - 1 + n % kPointColumns;
     const bool right = j + 1 < W, down = i + 1 < H;
-    float tb1, tb2, wb1, wb2;
-    w_tilde_bar(q, a, w, z, i, j, tb1, tb2, wb1, wb2);
-    float ap1, ap2;
-    adjoint_p(q, a, vbar, tau, i, j, k, ap1, ap2);
-    b.w1[k] = rest * a.w1[k] - wb1 + tb1;
-    b.w2[k] = rest * a.w2[k] - wb2 + tb2;
-    b.p1[k] = rest * ap1 + w.q1[k] + tau * tb1;
-    b.p2[k] = rest * ap2 + w.q2[k] + tau * tb2;
-    // r^: the relaxation's, s^, and div2^T of d^ = tau w~^ (w~^ of the pixel and of its left and
-    // upper ones).
-    float l1 = 0.0f, l2 = 0.0f, u1 = 0.0f, u2 = 0.0f, unused1, unused2;
-    if (j > 0) w_tilde_bar(q, a, w, z, i, j - 1, l1, l2, unused1, unused2);
-    if (i > 0) w_tilde_bar(q, a, w, z, i - 1, j, u1, u2, unused1, unused2);
+    const float bar = 2.0f * s_at(EXTRA, i, j) - s_at(X, i, j);
+    const float g1 = right ? (2.0f * s_at(EXTRA, i, j + 1) - s_at(X, i, j + 1)) - bar : 0.0f;
+    const float g2 = down ? (2.0f * s_at(EXTRA, i + 1, j) - s_at(X, i + 1, j)) - bar : 0.0f;
+    const float b1 = 2.0f * t_at(0, i, j) - s_at(W1, i, j);
+    const float b2 = 2.0f * t_at(1, i, j) - s_at(W2, i, j);
+    const float q1 = s_at(P1, i, j) + sigma * (g1 - b1);
+    const float q2 = s_at(P2, i, j) + sigma * (g2 - b2);
+    float l1 = 0.0f, l2 = 0.0f, u1 = 0.0f, u2 = 0.0f;
+    if (j > 0) {
+      l1 = 2.0f * t_at(0, i, j - 1) - s_at(W1, i, j - 1);
+      l2 = 2.0f * t_at(1, i, j - 1) - s_at(W2, i, j - 1);
+    }
+    if (i > 0) {
+      u1 = 2.0f * t_at(0, i - 1, j) - s_at(W1, i - 1, j);
+      u2 = 2.0f * t_at(1, i - 1, j) - s_at(W2, i - 1, j);
+    }
+    const float own1x = right ? b1 : 0.0f, own2x = right ? b2 : 0.0f;
+    const float own1y = down ? b1 : 0.0f, own2y = down ? b2 : 0.0f;
+    const float e11 = own1x - l1, e22 = own2y - u2, e12 = 0.5f * ((own1y - u1) + (own2x - l2));
+    const float s11 = s_at(R11, i, j) + sigma * e11;
+    const float s22 = s_at(R22, i, j) + sigma * e22;
+    const float s12 = s_at(R12, i, j) + sigma * e12;
+    // The adjoint of p of s_k: that of the relaxation's p and of P_{k+1}'s v = x + tau div p,
+    // p^ += tau div^T v^ = -tau grad v^.
+    const float v = a_at(EXTRA, i, j);
+    float ap1 = a_at(P1, i, j), ap2 = a_at(P2, i, j);
+    if (right) ap1 += -tau * (a_at(EXTRA, i, j + 1) - v);
+    if (down) ap2 += -tau * (a_at(EXTRA, i + 1, j) - v);
+    const float pb1 = rho * ap1, pb2 = rho * ap2;
+    float qb1 = pb1, qb2 = pb2, ga1 = 0.0f;
+    const float nq = sqrtf(q1 * q1 + q2 * q2);
+    if (nq > alpha1) {
+      const float dot = q1 * pb1 + q2 * pb2;
+      const float f = alpha1 / nq, h = dot / (nq * nq);
+      qb1 = f * (pb1 - q1 * h);
+      qb2 = f * (pb2 - q2 * h);
+      ga1 = dot / nq;
+    }
+    const float rb11 = rho * a_at(R11, i, j), rb22 = rho * a_at(R22, i, j), rb12 = rho * a_at(R12, i, j);
+    float sb11 = rb11, sb22 = rb22, sb12 = rb12, ga0 = 0.0f;
+    const float ns = sqrtf(s11 * s11 + s22 * s22 + 2.0f * (s12 * s12));
+    if (ns > alpha0) {
+      const float dot = s11 * rb11 + s22 * rb22 + s12 * rb12;
+      const float f = alpha0 / ns, h = dot / (ns * ns);
+      sb11 = f * (rb11 - s11 * h);
+      sb22 = f * (rb22 - s22 * h);
+      sb12 = f * (rb12 - 2.0f * s12 * h);
+      ga0 = dot / ns;
+    }
+    l_at(0, i, j) = qb1;
+    l_at(1, i, j) = qb2;
+    l_at(2, i, j) = sb11;
+    l_at(3, i, j) = sb22;
+    l_at(4, i, j) = sb12;
+    if (i >= i0 && i < i0 + kAdjointRows && j >= j0 && j < j0 + 32 && i < H && j < W) {
+      g_alpha0 += ga0;
+      g_alpha1 += ga1;
+      g_sigma += qb1 * (g1 - b1) + qb2 * (g2 - b2) + sb11 * e11 + sb22 * e22 + sb12 * e12;
+    }
+  }
+  __syncthreads();
+
+  // (3) The adjoint of w~: that of w- is -sigma q^ + sigma E^T s^ (E^T gathering s^ of the pixel
+  // and of its right and lower ones), and w~ = (w- + w) / 2 gives it twice, beside the
+  // relaxation's rho w'^. Over the tile and the column to its left and the row above it.
+  auto w_minus_bar = [&](int i, int j, float& wb1, float& wb2) {
+    wb1 = -sigma * l_at(0, i, j);
+    wb2 = -sigma * l_at(1, i, j);
+    float e1 = 0.0f, e2 = 0.0f;
+    if (j + 1 < W) {
+      e1 += l_at(2, i, j) - l_at(2, i, j + 1);
+      e2 += 0.5f * (l_at(4, i, j) - l_at(4, i, j + 1));
+    }
+    if (i + 1 < H) {
+      e2 += l_at(3, i, j) - l_at(3, i + 1, j);
+      e1 += 0.5f * (l_at(4, i, j) - l_at(4, i + 1, j));
+    }
+    wb1 += sigma * e1;
+    wb2 += sigma * e2;
+  };
+  for (int n = tid; n < kBackRows * kBackColumns; n += 256) {
+    const int i = i0 - 1 + n / kBackColumns, j = j0 - 1 + n % kBackColumns;
+    float wb1, wb2;
+    w_minus_bar(i, j, wb1, wb2);
+    tb_at(0, i, j) = rho * a_at(W1, i, j) + 2.0f * wb1;
+    tb_at(1, i, j) = rho * a_at(W2, i, j) + 2.0f * wb2;
+  }
+  __syncthreads();
+
+  // (4) The tile's adjoints of s_{k-1} and of x~_k.
+  float g_tau = 0.0f;
+  for (int n = tid; n < kAdjointRows * 32; n += 256) {
+    const int i = i0 + n / 32, j = j0 + n % 32;
+    if (i >= H || j >= W) continue;
+    const std::size_t k = at(q, z, i, j);
+    const bool right = j + 1 < W, down = i + 1 < H;
+    const float tb1 = tb_at(0, i, j), tb2 = tb_at(1, i, j);
+    float wb1, wb2;
+    w_minus_bar(i, j, wb1, wb2);
+    const float v = a_at(EXTRA, i, j);
+    float ap1 = a_at(P1, i, j), ap2 = a_at(P2, i, j);
+    if (right) ap1 += -tau * (a_at(EXTRA, i, j + 1) - v);
+    if (down) ap2 += -tau * (a_at(EXTRA, i + 1, j) - v);
+    b.w1[k] = rest * a_at(W1, i, j) - wb1 + tb1;
+    b.w2[k] = rest * a_at(W2, i, j) - wb2 + tb2;
+    b.p1[k] = rest * ap1 + l_at(0, i, j) + tau * tb1;
+    b.p2[k] = rest * ap2 + l_at(1, i, j) + tau * tb2;
+    // r^: the relaxation's, s^, and div2^T of d^ = tau w~^ (w~^ of the pixel and of its left
+    // and upper ones).
+    const float l1 = j > 0 ? tb_at(0, i, j - 1) : 0.0f, l2 = j > 0 ? tb_at(1, i, j - 1) : 0.0f;
+    const float u1 = i > 0 ? tb_at(0, i - 1, j) : 0.0f, u2 = i > 0 ? tb_at(1, i - 1, j) : 0.0f;
     const float db1 = tau * tb1, db2 = tau * tb2;
     const float div11 = tau * l1 - (right ? db1 : 0.0f);
     const float div12 = tau * u1 - (down ? db1 : 0.0f) + tau * l2 - (right ? db2 : 0.0f);
     const float div22 = tau * u2 - (down ? db2 : 0.0f);
-    b.r11[k] = rest * a.r11[k] + w.s11[k] + div11;
-    b.r22[k] = rest * a.r22[k] + w.s22[k] + div22;
-    b.r12[k] = rest * a.r12[k] + w.s12[k] + div12;
+    b.r11[k] = rest * a_at(R11, i, j) + l_at(2, i, j) + div11;
+    b.r22[k] = rest * a_at(R22, i, j) + l_at(3, i, j) + div22;
+    b.r12[k] = rest * a_at(R12, i, j) + l_at(4, i, j) + div12;
     // d/dtau of w~ = p + div2 r.
-    const float r11 = s.r11[k], r22 = s.r22[k], r12 = s.r12[k];
-    float d1 = right ? s.r11[k + 1] - r11 : 0.0f;
-    float d2 = right ? s.r12[k + 1] - r12 : 0.0f;
-    d1 = d1 + (down ? s.r12[k + W] - r12 : 0.0f);
-    d2 = d2 + (down ? s.r22[k + W] - r22 : 0.0f);
-    g_tau = tb1 * (s.p1[k] + d1) + tb2 * (s.p2[k] + d2);
+    const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
+    float d1 = right ? s_at(R11, i, j + 1) - r11 : 0.0f;
+    float d2 = right ? s_at(R12, i, j + 1) - r12 : 0.0f;
+    d1 = d1 + (down ? s_at(R12, i + 1, j) - r12 : 0.0f);
+    d2 = d2 + (down ? s_at(R22, i + 1, j) - r22 : 0.0f);
+    g_tau += tb1 * (s_at(P1, i, j) + d1) + tb2 * (s_at(P2, i, j) + d2);
     // The adjoint of x- : grad^T (sigma q^) = -div (sigma q^).
-    float div = (right ? w.q1[k] : 0.0f) - (j > 0 ? w.q1[k - 1] : 0.0f) + (down ? w.q2[k] : 0.0f) -
-                (i > 0 ? w.q2[k - W] : 0.0f);
+    const float div = (right ? l_at(0, i, j) : 0.0f) - (j > 0 ? l_at(0, i, j - 1) : 0.0f) +
+                      (down ? l_at(1, i, j) : 0.0f) - (i > 0 ? l_at(1, i - 1, j) : 0.0f);
     const float xbb = -sigma * div;
-    const float ax = adjoint_x(a, vbar, k);
+    const float ax = a_at(X, i, j) + v;
     xt_bar[k] = rho * ax + 2.0f * xbb;
     b.x[k] = rest * ax - xbb;
   }
+  add_sum(g_alpha0, grads + 0 * q.images + z);
+  add_sum(g_alpha1, grads + 1 * q.images + z);
   add_sum(g_tau, grads + 2 * q.images + z);
+  add_sum(g_sigma, grads + 3 * q.images + z);
 }
 
 // The primal step's adjoint, per block: from the adjoint of x~ (`xt_bar`) the adjoint of v.
-__global__ void __launch_bounds__(256) primal_adjoint_block(Problem q, Planes s, const float* xt_bar, Scratch w,
+// x~ = C^T zeta C + middle and e = C (v - middle) C^T, so zeta^ = C x~^ C^T and v^ = C^T e^ C.
+__global__ void __launch_bounds__(256) primal_adjoint_block(Problem q, Planes s, const float* xt_bar, float* vbar,
                                                             double* grads) {
-  __shared__ float t[8][33];
-  __shared__ BasisTable basis;
-  fill_basis(basis);
-  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-  const bool in = j < q.columns;
-  const int jc = in ? j : q.columns - 1;
-  const int bx = jc / 8, by = blockIdx.y;
-  const std::size_t block = static_cast<std::size_t>(by) * q.blocks_across + bx;
-  const std::size_t k = at(q, z, i, jc);
-  const float middle = q.middle[static_cast<std::size_t>(z) * q.blocks_down * q.blocks_across + block];
-  const float v = primal_v(q, s, z, i, jc);
-  const float e = transform(v - middle, t, basis, true);
-  const int kk = threadIdx.y * 8 + (threadIdx.x & 7);
-  const Clip c = clip_of(q, z, block, kk, e);
-  const float zb = transform(in ? xt_bar[k] : 0.0f, t, basis, true);
+  __shared__ float tiles[8][4][72];
+  const int lane = threadIdx.x, warp = threadIdx.y, z = blockIdx.z;
+  const int by_raw = blockIdx.y * 8 + warp;
+  const bool active = by_raw < q.blocks_down;  // every warp joins the CTA's sum
+  const int by = active ? by_raw : 0;
+  const int j = blockIdx.x * 32 + lane;
+  const bool in = active && j < q.columns;
+  const int jc = j < q.columns ? j : q.columns - 1, m = lane & 7;
+  const std::size_t blocks = static_cast<std::size_t>(q.blocks_down) * q.blocks_across;
+  const std::size_t block = static_cast<std::size_t>(by) * q.blocks_across + jc / 8;
+  float* t = tiles[warp][lane >> 3];
+  const float tau = q.tau[z];
+  float v[8], div[8], xb[8];
+  column_v(q, s, z, by, jc, tau, v, div);
+  const float middle = q.middle[static_cast<std::size_t>(z) * blocks + block];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    v[r] -= middle;
+    xb[r] = in ? xt_bar[at(q, z, by * 8 + r, j)] : 0.0f;
+  }
+  float e[8], zb[8];
+  forward2(v, e, t, m);
+  forward2(xb, zb, t, m);
+  ClipRow c;
+  clip_row(q, z, block, m, tau, e, c);
   // zeta = (e + t c) r inside the interval, t = tau m, r = 1 / (1 + t): d zeta / d e = r and
   // d zeta / d tau = m (c - e) r^2; outside it zeta is an end of the interval.
-  const float eb = c.inside ? c.r * zb : 0.0f;
-  float g_tau = c.inside ? zb * c.weight * (c.centre - e) * (c.r * c.r) : 0.0f;
-  const float vb = transform(eb, t, basis, false);
+  float eb[8], g_tau = 0.0f;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    eb[u] = c.inside[u] ? c.r[u] * zb[u] : 0.0f;
+    g_tau += c.inside[u] ? zb[u] * c.weight[u] * (c.centre[u] - e[u]) * (c.r[u] * c.r[u]) : 0.0f;
+  }
+  float vb[8];
+  inverse2(eb, vb, t, m);
   // d v / d tau = div p.
-  const float dy = (i + 1 < q.rows ? s.p2[k] : 0.0f) - (i > 0 ? s.p2[k - q.columns] : 0.0f);
-  const float dx = (jc + 1 < q.columns ? s.p1[k] : 0.0f) - (jc > 0 ? s.p1[k - 1] : 0.0f);
   if (in) {
-    w.v[k] = vb;
-    g_tau += vb * (dy + dx);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      vbar[at(q, z, by * 8 + r, j)] = vb[r];
+      g_tau += vb[r] * div[r];
+    }
   } else {
     g_tau = 0.0f;
   }
@@ -504,6 +647,11 @@ dim3 pixel_grid(const Problem& q) {
   return dim3((q.columns + 31) / 32, (q.rows + 7) / 8, q.images);
 }
 
+// The block kernels' grid: a CTA 8 block rows of a strip of 32 columns.
+dim3 block_grid(const Problem& q) {
+  return dim3((q.columns + 31) / 32, (q.blocks_down + 7) / 8, q.images);
+}
+
 std::string check(const unround_b200_unrolled* u) {
   if (u == nullptr) return "the problem is a null pointer";
   if (u->images == 0 || u->rows == 0 || u->columns == 0) return "the problem has pictures of rows and columns";
@@ -525,6 +673,21 @@ void tell(char* buffer, std::size_t size, const std::string& text) {
   buffer[end] = 0;
 }
 
+// The dual step's adjoint takes more than 48 KB of shared memory: allowed once per device.
+bool prepare_dual_adjoint() {
+  static std::atomic<unsigned long long> configured{0};
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return false;
+  const unsigned long long bit = 1ull << (device & 63);
+  if ((configured.load() & bit) != 0) return true;
+  if (cudaFuncSetAttribute(dual_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(kAdjointShared)) != cudaSuccess) {
+    return false;
+  }
+  configured.fetch_or(bit);
+  return true;
+}
+
 std::uint64_t checkpoints_of(const unround_b200_unrolled& u) {
   // s_0, s_K, s_2K, ... up to s_{N-1}.
   return (u.iterations - 1) / u.checkpoint_every + 1;
@@ -544,8 +707,9 @@ extern "C" uint64_t unround_b200_unrolled_checkpoint_floats(const unround_b200_u
 extern "C" uint64_t unround_b200_unrolled_workspace_floats(const unround_b200_unrolled* problem) {
   if (!urb::check(problem).empty()) return 0;
   const std::uint64_t plane = problem->images * problem->rows * problem->columns;
-  // Two states ping-pong, x~, a segment's states and x~s, two adjoints, x~'s adjoint, scratch.
-  return (2 * 8 + 1 + problem->checkpoint_every * 9 + 2 * 8 + 1 + 6) * plane;
+  // Two states ping-pong, x~, a segment's states and x~s, two adjoints of a state with that of
+  // v after each, x~'s adjoint.
+  return (2 * 8 + 1 + problem->checkpoint_every * 9 + 2 * 9 + 1) * plane;
 }
 
 extern "C" unround_status unround_b200_unrolled_forward(const unround_b200_unrolled* problem, const float* alpha0,
@@ -577,7 +741,7 @@ extern "C" unround_status unround_b200_unrolled_forward(const unround_b200_unrol
       cudaMemcpyAsync(checkpoints + (k - 1) / every * 8 * plane, state[current].x, 8 * plane * sizeof(float),
                       cudaMemcpyDeviceToDevice, on);
     }
-    urb::primal_kernel<<<grid, block, 0, on>>>(q, state[current], k == n ? output : xt);
+    urb::primal_kernel<<<urb::block_grid(q), block, 0, on>>>(q, state[current], k == n ? output : xt);
     if (k < n) {
       urb::dual_kernel<<<grid, block, 0, on>>>(q, state[current], xt, state[1 - current]);
       current = 1 - current;
@@ -610,24 +774,37 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
   const urb::Problem q = urb::problem_of(*problem, alpha0, alpha1, tau, sigma);
   const std::size_t plane = q.plane;
   const std::uint64_t n = problem->iterations, every = problem->checkpoint_every;
-  // The workspace: the segment's states s_{k0} .. s_{k0+K-1} and x~_{k0+1} .. x~_{k0+K} (9 planes
-  // each step), two adjoints of a state, the adjoint of x~, and the scratch.
+  // The workspace: the segment's states s_{k0} .. s_{k0+K-1}, each followed by x~ of the step
+  // after it (9 planes a step), two adjoints of a state, each followed by that of v of the
+  // primal step after it (9 planes each), and the adjoint of x~.
   float* segment = workspace + 17 * plane;
   float* adjoint_base = segment + every * 9 * plane;
-  Planes adjoint[2] = {urb::planes_of(adjoint_base, plane), urb::planes_of(adjoint_base + 8 * plane, plane)};
-  float* xt_bar = adjoint_base + 16 * plane;
-  float* scratch_base = xt_bar + plane;
-  const urb::Scratch scratch{scratch_base,             scratch_base + plane,     scratch_base + 2 * plane,
-                             scratch_base + 3 * plane, scratch_base + 4 * plane, scratch_base + 5 * plane};
-  // The adjoint of v of the primal step after the dual step being undone (none after the last).
-  const float* vbar = nullptr;
+  float* const adjoint[2] = {adjoint_base, adjoint_base + 9 * plane};
+  float* xt_bar = adjoint_base + 18 * plane;
   auto state_of = [&](std::uint64_t step) { return urb::planes_of(segment + step * 9 * plane, plane); };
   auto tilde_of = [&](std::uint64_t step) { return segment + step * 9 * plane + 8 * plane; };
+  // The dual step's adjoint reads 9 planes of each by bulk-tensor copies.
+  std::vector<CUtensorMap> state_maps(every);
+  CUtensorMap bar_maps[2];
+  bool mapped = urb::prepare_dual_adjoint();
+  const int W = static_cast<int>(q.columns), H = static_cast<int>(q.rows), images = static_cast<int>(q.images);
+  for (std::uint64_t step = 0; step < every && mapped; ++step) {
+    mapped = urb::make_fields_map(state_maps[step], segment + step * 9 * plane, W, H, images, 9, plane, 40,
+                                  urb::kStateRows);
+  }
+  for (int c = 0; c < 2 && mapped; ++c) {
+    mapped = urb::make_fields_map(bar_maps[c], adjoint[c], W, H, images, 9, plane, 40, urb::kBarRows);
+  }
+  if (!mapped) {
+    urb::tell(message, message_size, "the device's bulk-tensor copies could not be set up for the adjoint");
+    return UNROUND_ERROR_INTERNAL;
+  }
   const dim3 grid = urb::pixel_grid(q), block(32, 8);
+  const dim3 tiles((q.columns + 31) / 32, (q.rows + urb::kAdjointRows - 1) / urb::kAdjointRows, q.images);
   cudaMemsetAsync(grads, 0, 4 * problem->images * sizeof(double), on);
   // The adjoint of s_N's predecessor starts at zero; that of x~_N is the output's gradient.
   int current = 0;
-  cudaMemsetAsync(adjoint[current].x, 0, 8 * plane * sizeof(float), on);
+  cudaMemsetAsync(adjoint[current], 0, 9 * plane * sizeof(float), on);
   cudaMemcpyAsync(xt_bar, output_grad, plane * sizeof(float), cudaMemcpyDeviceToDevice, on);
   const std::uint64_t segments = urb::checkpoints_of(*problem);
   for (std::uint64_t seg = segments; seg-- > 0;) {
@@ -637,25 +814,23 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
     cudaMemcpyAsync(segment, checkpoints + seg * 8 * plane, 8 * plane * sizeof(float), cudaMemcpyDeviceToDevice, on);
     for (std::uint64_t k = k0 + 1; k <= k1; ++k) {
       const std::uint64_t step = k - 1 - k0;  // s_{k-1} is state_of(step)
-      urb::primal_kernel<<<grid, block, 0, on>>>(q, state_of(step), tilde_of(step));
+      urb::primal_kernel<<<urb::block_grid(q), block, 0, on>>>(q, state_of(step), tilde_of(step));
       if (k < k1) urb::dual_kernel<<<grid, block, 0, on>>>(q, state_of(step), tilde_of(step), state_of(step + 1));
     }
     // Backwards through the segment: at iteration k, D_k (k < N) then P_k.
     for (std::uint64_t k = k1; k > k0; --k) {
       const std::uint64_t step = k - 1 - k0;
-      const Planes s = state_of(step);
       if (k < n) {
-        // D_k: the adjoint of s_k is adjoint[current] and P_{k+1}'s (vbar); write that of
-        // s_{k-1} into the other, and that of x~_k into xt_bar.
-        const Planes a = adjoint[current], b = adjoint[1 - current];
-        urb::dual_adjoint_local<<<grid, block, 0, on>>>(q, s, tilde_of(step), a, vbar, scratch, grads);
-        urb::dual_adjoint_gather<<<grid, block, 0, on>>>(q, s, a, vbar, scratch, b, xt_bar, grads);
+        // D_k: the adjoint of s_k and of P_{k+1}'s v are adjoint[current]; write that of s_{k-1}
+        // into the other, and that of x~_k into xt_bar.
+        urb::dual_adjoint_kernel<<<tiles, block, urb::kAdjointShared, on>>>(
+            state_maps[step], bar_maps[current], q, urb::planes_of(adjoint[1 - current], plane), xt_bar, grads);
         current = 1 - current;
       }
-      // P_k: from the adjoint of x~_k that of its v, which the next dual step undone (D_{k-1})
-      // adds to the adjoints of x and p of s_{k-1}.
-      urb::primal_adjoint_block<<<grid, block, 0, on>>>(q, s, xt_bar, scratch, grads);
-      vbar = scratch.v;
+      // P_k: from the adjoint of x~_k that of its v, beside the adjoint of s_{k-1}, which the
+      // next dual step undone (D_{k-1}) reads.
+      urb::primal_adjoint_block<<<urb::block_grid(q), block, 0, on>>>(q, state_of(step), xt_bar,
+                                                                       adjoint[current] + 8 * plane, grads);
     }
   }
   const cudaError_t error = cudaGetLastError();
