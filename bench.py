@@ -326,13 +326,30 @@ def _large_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     print(json.dumps(line))
 
 
+def _unrolled_forward_launches(iterations: int) -> int:
+    """The start, N primal steps and N - 1 dual steps."""
+    return 2 * iterations
+
+
+def _unrolled_backward_launches(iterations: int, every: int) -> int:
+    """Per segment of checkpoints K apart: the recomputed dual steps and primal steps, then the
+    dual steps' adjoints (N - 1) and the primal steps' adjoints (N)."""
+    launches = 0
+    for k0 in range(0, iterations, every):
+        k1 = min(k0 + every, iterations)
+        launches += (k1 - k0 - 1) + max(k1 - k0 - 2, 0) + (1 if k1 - k0 > 1 and k1 < iterations else 0)
+    return launches + (iterations - 1) + iterations
+
+
 def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     """The differentiable unrolled TGV solve of 16 greyscale 512x512 pictures (quality 30),
     100 iterations, checkpoints every 10: a step is one forward pass with the loss
     (MSE against the clean pictures) and its backward pass (the adjoint) to the gradients of
     every picture's alpha0, alpha1, tau and sigma. value: pixel-iterations of the forward and
     backward pass per second (device time by CUDA events); forward: the same of the forward
-    pass alone; ratio: (forward + backward) / forward."""
+    pass alone; ratio: (forward + backward) / forward. every_iterate_kept: the forward and
+    backward pass with a checkpoint every iteration (no state recomputed; 9 planes an iteration
+    in HBM)."""
     import numpy as np
     import torch
 
@@ -359,11 +376,20 @@ def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
         loss.backward()
         return loss, leaves
 
+    # The same with every iterate kept (a checkpoint every iteration: no recomputation).
+    kept = UnrolledProblem([m.image for m in made], ["--method", "tgv", "--alpha1", "1", "--alpha0", "2"],
+                           iterations=iterations, checkpoint_every=1)
+
+    def forward_backward_kept():
+        leaves = [b.clone().requires_grad_(True) for b in base]
+        torch.mean((unrolled_tgv(kept, *leaves) - clean) ** 2).backward()
+
     for _ in range(max(3, args.warmup)):
         forward_only()
         forward_backward()
+        forward_backward_kept()
     torch.cuda.synchronize()
-    start, mid, end = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    start, mid, end, last = (torch.cuda.Event(enable_timing=True) for _ in range(4))
     steps = max(1, args.steps)
     with Clocks(0) as clocks:
         start.record()
@@ -373,9 +399,13 @@ def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
         for _ in range(steps):
             loss, leaves = forward_backward()
         end.record()
+        for _ in range(steps):
+            forward_backward_kept()
+        last.record()
         torch.cuda.synchronize()
     forward_ms = start.elapsed_time(mid) / steps
     both_ms = mid.elapsed_time(end) / steps
+    kept_ms = end.elapsed_time(last) / steps
     grads = torch.stack([leaf.grad for leaf in leaves]).cpu()  # the step's result read on the host
     pixels = pictures * side * side
     # End to end: levels in from the host (the problem made from the files' levels), gradients out.
@@ -398,10 +428,13 @@ def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
                    "l2": "state 16 x 512^2 x 9 fields = 151 MB, larger than L2"},
         "forward": {"value": pixels * iterations / (forward_ms / 1e3) / 1e6, "ms": forward_ms},
         "forward_backward_over_forward": both_ms / forward_ms,
+        "every_iterate_kept": {"checkpoint_every": 1, "ms": kept_ms, "forward_backward_over_forward": kept_ms / forward_ms,
+                               "checkpoint_bytes": kept.checkpoint_floats * 4},
         "grad_finite": bool(torch.isfinite(grads).all()) and bool(torch.isfinite(e2e_grads).all()),
         "e2e": {"value": pixels * iterations / e2e_seconds / 1e6, "unit": "Mpx*iter/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(e2e_grads.numel() * 4)},
-        "gpu_launches": iterations * 2 + iterations * 5 + iterations * 2,
+        "gpu_launches": steps * (2 * _unrolled_forward_launches(iterations) + _unrolled_backward_launches(iterations, every)
+                                 + _unrolled_forward_launches(iterations) + _unrolled_backward_launches(iterations, 1)),
         "clocks": clocks.summary(),
     }
     print(json.dumps(line))

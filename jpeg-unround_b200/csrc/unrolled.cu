@@ -699,17 +699,21 @@ std::uint64_t checkpoints_of(const unround_b200_unrolled& u) {
 
 using urb::Planes;
 
+// Storage. A checkpoint c holds s_{cK} and x~_{cK+1} (9 planes), both written by the forward pass
+// where they are made (no copies). The forward pass's other states ping-pong through the first
+// 18 planes of the workspace (a state and the x~ after it each). The backward pass recomputes a
+// segment's states s_{k0+1} .. s_{k0+K-1} and their x~ into K - 1 slots of 9 planes, and keeps
+// two adjoints of a state (each followed by that of v of the primal step after it) and the
+// adjoint of x~: 9 (K - 1) + 19 planes, never fewer than the forward pass's 18.
 extern "C" uint64_t unround_b200_unrolled_checkpoint_floats(const unround_b200_unrolled* problem) {
   if (!urb::check(problem).empty()) return 0;
-  return urb::checkpoints_of(*problem) * 8 * problem->images * problem->rows * problem->columns;
+  return urb::checkpoints_of(*problem) * 9 * problem->images * problem->rows * problem->columns;
 }
 
 extern "C" uint64_t unround_b200_unrolled_workspace_floats(const unround_b200_unrolled* problem) {
   if (!urb::check(problem).empty()) return 0;
   const std::uint64_t plane = problem->images * problem->rows * problem->columns;
-  // Two states ping-pong, x~, a segment's states and x~s, two adjoints of a state with that of
-  // v after each, x~'s adjoint.
-  return (2 * 8 + 1 + problem->checkpoint_every * 9 + 2 * 9 + 1) * plane;
+  return (9 * (problem->checkpoint_every - 1) + 19) * plane;
 }
 
 extern "C" unround_status unround_b200_unrolled_forward(const unround_b200_unrolled* problem, const float* alpha0,
@@ -729,22 +733,20 @@ extern "C" unround_status unround_b200_unrolled_forward(const unround_b200_unrol
   const cudaStream_t on = static_cast<cudaStream_t>(stream);
   const urb::Problem q = urb::problem_of(*problem, alpha0, alpha1, tau, sigma);
   const std::size_t plane = q.plane;
-  Planes state[2] = {urb::planes_of(workspace, plane), urb::planes_of(workspace + 8 * plane, plane)};
-  float* xt = workspace + 16 * plane;
-  const dim3 grid = urb::pixel_grid(q), block(32, 8);
-  urb::start_kernel<<<grid, block, 0, on>>>(q, problem->start, state[0]);
   const std::uint64_t n = problem->iterations, every = problem->checkpoint_every;
-  int current = 0;
+  float* const spare[2] = {workspace, workspace + 9 * plane};
+  const dim3 grid = urb::pixel_grid(q), block(32, 8);
+  // s_{k-1} and then x~_k live at `current`: 9 planes.
+  float* current = checkpoints;
+  urb::start_kernel<<<grid, block, 0, on>>>(q, problem->start, urb::planes_of(current, plane));
   for (std::uint64_t k = 1; k <= n; ++k) {
-    // s_{k-1} is state[current]; keep it where k - 1 is a checkpoint.
-    if ((k - 1) % every == 0) {
-      cudaMemcpyAsync(checkpoints + (k - 1) / every * 8 * plane, state[current].x, 8 * plane * sizeof(float),
-                      cudaMemcpyDeviceToDevice, on);
-    }
-    urb::primal_kernel<<<urb::block_grid(q), block, 0, on>>>(q, state[current], k == n ? output : xt);
+    urb::primal_kernel<<<urb::block_grid(q), block, 0, on>>>(q, urb::planes_of(current, plane),
+                                                              k == n ? output : current + 8 * plane);
     if (k < n) {
-      urb::dual_kernel<<<grid, block, 0, on>>>(q, state[current], xt, state[1 - current]);
-      current = 1 - current;
+      float* next = k % every == 0 ? checkpoints + k / every * 9 * plane : (current == spare[0] ? spare[1] : spare[0]);
+      urb::dual_kernel<<<grid, block, 0, on>>>(q, urb::planes_of(current, plane), current + 8 * plane,
+                                               urb::planes_of(next, plane));
+      current = next;
     }
   }
   const cudaError_t error = cudaGetLastError();
@@ -774,22 +776,25 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
   const urb::Problem q = urb::problem_of(*problem, alpha0, alpha1, tau, sigma);
   const std::size_t plane = q.plane;
   const std::uint64_t n = problem->iterations, every = problem->checkpoint_every;
-  // The workspace: the segment's states s_{k0} .. s_{k0+K-1}, each followed by x~ of the step
-  // after it (9 planes a step), two adjoints of a state, each followed by that of v of the
-  // primal step after it (9 planes each), and the adjoint of x~.
-  float* segment = workspace + 17 * plane;
-  float* adjoint_base = segment + every * 9 * plane;
+  const std::uint64_t segments = urb::checkpoints_of(*problem);
+  float* const recomputed = workspace;  // s_{k0+1} .. s_{k0+K-1}, 9 planes each
+  float* const adjoint_base = workspace + (every - 1) * 9 * plane;
   float* const adjoint[2] = {adjoint_base, adjoint_base + 9 * plane};
-  float* xt_bar = adjoint_base + 18 * plane;
-  auto state_of = [&](std::uint64_t step) { return urb::planes_of(segment + step * 9 * plane, plane); };
-  auto tilde_of = [&](std::uint64_t step) { return segment + step * 9 * plane + 8 * plane; };
-  // The dual step's adjoint reads 9 planes of each by bulk-tensor copies.
-  std::vector<CUtensorMap> state_maps(every);
+  float* const xt_bar = adjoint_base + 18 * plane;
+  // s_{k0 + step} and x~ after it: the checkpoint at step 0, the recomputed slots after.
+  auto storage_of = [&](std::uint64_t seg, std::uint64_t step) -> float* {
+    return step == 0 ? const_cast<float*>(checkpoints) + seg * 9 * plane : recomputed + (step - 1) * 9 * plane;
+  };
+  // The dual step's adjoint reads the 9 planes of each by bulk-tensor copies.
+  std::vector<CUtensorMap> checkpoint_maps(segments), recomputed_maps(every > 1 ? every - 1 : 0);
   CUtensorMap bar_maps[2];
   bool mapped = urb::prepare_dual_adjoint();
   const int W = static_cast<int>(q.columns), H = static_cast<int>(q.rows), images = static_cast<int>(q.images);
-  for (std::uint64_t step = 0; step < every && mapped; ++step) {
-    mapped = urb::make_fields_map(state_maps[step], segment + step * 9 * plane, W, H, images, 9, plane, 40,
+  for (std::uint64_t c = 0; c < segments && mapped; ++c) {
+    mapped = urb::make_fields_map(checkpoint_maps[c], storage_of(c, 0), W, H, images, 9, plane, 40, urb::kStateRows);
+  }
+  for (std::uint64_t step = 1; step < every && mapped; ++step) {
+    mapped = urb::make_fields_map(recomputed_maps[step - 1], storage_of(0, step), W, H, images, 9, plane, 40,
                                   urb::kStateRows);
   }
   for (int c = 0; c < 2 && mapped; ++c) {
@@ -806,16 +811,24 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
   int current = 0;
   cudaMemsetAsync(adjoint[current], 0, 9 * plane * sizeof(float), on);
   cudaMemcpyAsync(xt_bar, output_grad, plane * sizeof(float), cudaMemcpyDeviceToDevice, on);
-  const std::uint64_t segments = urb::checkpoints_of(*problem);
   for (std::uint64_t seg = segments; seg-- > 0;) {
-    const std::uint64_t k0 = seg * every;                          // the checkpoint s_{k0}
+    const std::uint64_t k0 = seg * every;                             // the checkpoint s_{k0}
     const std::uint64_t k1 = std::min<std::uint64_t>(k0 + every, n);  // the segment's iterations k0+1 .. k1
-    // Recompute s_{k0} .. s_{k1-1} and x~_{k0+1} .. x~_{k1} (x~_N is not needed: x~_bar starts there).
-    cudaMemcpyAsync(segment, checkpoints + seg * 8 * plane, 8 * plane * sizeof(float), cudaMemcpyDeviceToDevice, on);
-    for (std::uint64_t k = k0 + 1; k <= k1; ++k) {
-      const std::uint64_t step = k - 1 - k0;  // s_{k-1} is state_of(step)
-      urb::primal_kernel<<<urb::block_grid(q), block, 0, on>>>(q, state_of(step), tilde_of(step));
-      if (k < k1) urb::dual_kernel<<<grid, block, 0, on>>>(q, state_of(step), tilde_of(step), state_of(step + 1));
+    // Recompute s_{k0+1} .. s_{k1-1} and x~_{k0+2} .. x~_{k1} (x~_{k0+1} is the checkpoint's;
+    // x~_N is not needed: x~_bar starts there).
+    for (std::uint64_t k = k0 + 1; k < k1; ++k) {
+      const std::uint64_t step = k - 1 - k0;  // s_{k-1} is storage_of(seg, step)
+      float* from = storage_of(seg, step);
+      if (step > 0) {
+        urb::primal_kernel<<<urb::block_grid(q), block, 0, on>>>(q, urb::planes_of(from, plane), from + 8 * plane);
+      }
+      urb::dual_kernel<<<grid, block, 0, on>>>(q, urb::planes_of(from, plane), from + 8 * plane,
+                                               urb::planes_of(storage_of(seg, step + 1), plane));
+    }
+    if (k1 - k0 > 1 && k1 < n) {
+      // x~_{k1} of the segment's last state, for D_{k1}'s adjoint.
+      float* last = storage_of(seg, k1 - 1 - k0);
+      urb::primal_kernel<<<urb::block_grid(q), block, 0, on>>>(q, urb::planes_of(last, plane), last + 8 * plane);
     }
     // Backwards through the segment: at iteration k, D_k (k < N) then P_k.
     for (std::uint64_t k = k1; k > k0; --k) {
@@ -823,14 +836,15 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
       if (k < n) {
         // D_k: the adjoint of s_k and of P_{k+1}'s v are adjoint[current]; write that of s_{k-1}
         // into the other, and that of x~_k into xt_bar.
+        const CUtensorMap& state_map = step == 0 ? checkpoint_maps[seg] : recomputed_maps[step - 1];
         urb::dual_adjoint_kernel<<<tiles, block, urb::kAdjointShared, on>>>(
-            state_maps[step], bar_maps[current], q, urb::planes_of(adjoint[1 - current], plane), xt_bar, grads);
+            state_map, bar_maps[current], q, urb::planes_of(adjoint[1 - current], plane), xt_bar, grads);
         current = 1 - current;
       }
       // P_k: from the adjoint of x~_k that of its v, beside the adjoint of s_{k-1}, which the
       // next dual step undone (D_{k-1}) reads.
-      urb::primal_adjoint_block<<<urb::block_grid(q), block, 0, on>>>(q, state_of(step), xt_bar,
-                                                                       adjoint[current] + 8 * plane, grads);
+      urb::primal_adjoint_block<<<urb::block_grid(q), block, 0, on>>>(
+          q, urb::planes_of(storage_of(seg, step), plane), xt_bar, adjoint[current] + 8 * plane, grads);
     }
   }
   const cudaError_t error = cudaGetLastError();
