@@ -12,14 +12,16 @@
 // a, b) with t = tau m_k (m_k the data term's weight of frequency k, of a flat block where the
 // block is flat) and e the DCT of the block less the middle of its DC interval.
 //
-// The adjoint runs the iterations backwards: the adjoint of D_k (two per-pixel kernels: the
-// projections' Jacobians at each pixel; then the transposes of E, grad and div2, which gather
-// the first kernel's results of the neighbours and recompute w~'s adjoint of the left and upper
-// ones), then of P_k (a block kernel: the DCT of the adjoint, the clip's mask, the inverse DCT,
+// P_k is a block kernel (a warp per block row, the transforms in registers); D_k a tile kernel
+// fed by a bulk-tensor copy of s_{k-1} and x~_k with halos.
+//
+// The adjoint runs the iterations backwards: the adjoint of D_k (one tile kernel: the
+// projections' Jacobians, then the transposes of E, grad and div2 over the tile, from shared
+// memory), then of P_k (a block kernel: the DCT of the adjoint, the clip's mask, the inverse DCT,
 // to the adjoint of v, which the next dual step undone reads for div's transpose). The states
-// s_k are kept every `checkpoint` iterations by the forward pass; the
-// backward pass recomputes each segment's states from its checkpoint. The parameters' gradients
-// are sums over pixels and iterations, reduced per CTA and added in binary64.
+// s_k are kept every `checkpoint_every` iterations by the forward pass; the backward pass
+// recomputes each segment's states from its checkpoint. The parameters' gradients are sums
+// over pixels and iterations, reduced per CTA and added in binary64.
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
@@ -76,65 +78,6 @@ __device__ __forceinline__ std::size_t at(const Problem& q, int z, int i, int j)
 __device__ __forceinline__ float ball(float square, float radius) {
   const float norm = sqrtf(square);
   return norm > radius ? radius / norm : 1.0f;
-}
-
-// w~ at a pixel: w + tau (p + div2 r), div2 r by forward differences.
-__device__ __forceinline__ void w_tilde(const Problem& q, const Planes& s, int z, int i, int j, float tau, float& t1,
-                                        float& t2, float& w1, float& w2) {
-  const std::size_t k = at(q, z, i, j);
-  const float r11 = s.r11[k], r22 = s.r22[k], r12 = s.r12[k];
-  float d1 = j + 1 < q.columns ? s.r11[k + 1] - r11 : 0.0f;
-  float d2 = j + 1 < q.columns ? s.r12[k + 1] - r12 : 0.0f;
-  d1 = d1 + (i + 1 < q.rows ? s.r12[k + q.columns] - r12 : 0.0f);
-  d2 = d2 + (i + 1 < q.rows ? s.r22[k + q.columns] - r22 : 0.0f);
-  w1 = s.w1[k];
-  w2 = s.w2[k];
-  t1 = w1 + tau * (s.p1[k] + d1);
-  t2 = w2 + tau * (s.p2[k] + d2);
-}
-
-__device__ __forceinline__ void w_bar(const Problem& q, const Planes& s, int z, int i, int j, float tau, float& b1,
-                                      float& b2) {
-  float t1, t2, w1, w2;
-  w_tilde(q, s, z, i, j, tau, t1, t2, w1, w2);
-  b1 = 2.0f * t1 - w1;
-  b2 = 2.0f * t2 - w2;
-}
-
-// The dual step's points before the projections at a pixel: q = p + sigma (grad x- - w-) with
-// g = grad x-, and s = r + sigma E w- with E; w- of the pixel and of its left and upper ones.
-struct DualPoint {
-  float g1, g2, b1, b2, q1, q2;
-  float e11, e22, e12, s11, s22, s12;
-  float t1, t2, w1, w2;
-};
-
-__device__ __forceinline__ DualPoint dual_point(const Problem& q, const Planes& s, const float* xt, int z, int i,
-                                                int j) {
-  const float tau = q.tau[z], sigma = q.sigma[z];
-  const std::size_t k = at(q, z, i, j);
-  const bool right = j + 1 < q.columns, down = i + 1 < q.rows;
-  DualPoint d;
-  const float bar = 2.0f * xt[k] - s.x[k];
-  d.g1 = right ? (2.0f * xt[k + 1] - s.x[k + 1]) - bar : 0.0f;
-  d.g2 = down ? (2.0f * xt[k + q.columns] - s.x[k + q.columns]) - bar : 0.0f;
-  w_tilde(q, s, z, i, j, tau, d.t1, d.t2, d.w1, d.w2);
-  d.b1 = 2.0f * d.t1 - d.w1;
-  d.b2 = 2.0f * d.t2 - d.w2;
-  d.q1 = s.p1[k] + sigma * (d.g1 - d.b1);
-  d.q2 = s.p2[k] + sigma * (d.g2 - d.b2);
-  float l1 = 0.0f, l2 = 0.0f, u1 = 0.0f, u2 = 0.0f;
-  if (j > 0) w_bar(q, s, z, i, j - 1, tau, l1, l2);
-  if (i > 0) w_bar(q, s, z, i - 1, j, tau, u1, u2);
-  const float own1x = right ? d.b1 : 0.0f, own2x = right ? d.b2 : 0.0f;
-  const float own1y = down ? d.b1 : 0.0f, own2y = down ? d.b2 : 0.0f;
-  d.e11 = own1x - l1;
-  d.e22 = own2y - u2;
-  d.e12 = 0.5f * ((own1y - u1) + (own2x - l2));
-  d.s11 = s.r11[k] + sigma * d.e11;
-  d.s22 = s.r22[k] + sigma * d.e22;
-  d.s12 = s.r12[k] + sigma * d.e12;
-  return d;
 }
 
 // Sums of a value over a CTA of 256 threads, added to a binary64 total.
@@ -286,24 +229,6 @@ __global__ void __launch_bounds__(256) primal_kernel(Problem q, Planes s, float*
   }
 }
 
-__global__ void __launch_bounds__(256) dual_kernel(Problem q, Planes s, const float* xt, Planes out) {
-  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-  if (i >= q.rows || j >= q.columns) return;
-  const std::size_t k = at(q, z, i, j);
-  const float rho = q.rho, rest = 1.0f - q.rho;
-  const DualPoint d = dual_point(q, s, xt, z, i, j);
-  const float sp = ball(d.q1 * d.q1 + d.q2 * d.q2, q.alpha1[z]);
-  const float sr = ball(d.s11 * d.s11 + d.s22 * d.s22 + 2.0f * (d.s12 * d.s12), q.alpha0[z]);
-  out.x[k] = rho * xt[k] + rest * s.x[k];
-  out.p1[k] = rho * (d.q1 * sp) + rest * s.p1[k];
-  out.p2[k] = rho * (d.q2 * sp) + rest * s.p2[k];
-  out.w1[k] = rho * d.t1 + rest * d.w1;
-  out.w2[k] = rho * d.t2 + rest * d.w2;
-  out.r11[k] = rho * (d.s11 * sr) + rest * s.r11[k];
-  out.r22[k] = rho * (d.s22 * sr) + rest * s.r22[k];
-  out.r12[k] = rho * (d.s12 * sr) + rest * s.r12[k];
-}
-
 // ---- Adjoint. `a` holds the adjoint of s_k (the dual step's output) and, as its ninth plane,
 // that of v of the primal step P_{k+1} after it; the kernels write the adjoint of s_{k-1} into
 // `b` and the adjoint of x~_k into `xt_bar`. Gradients: [0] alpha0, [1] alpha1, [2] tau,
@@ -453,22 +378,22 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
     float qb1 = pb1, qb2 = pb2, ga1 = 0.0f;
     const float nq = sqrtf(q1 * q1 + q2 * q2);
     if (nq > alpha1) {
-      const float dot = q1 * pb1 + q2 * pb2;
-      const float f = alpha1 / nq, h = dot / (nq * nq);
+      const float dot = q1 * pb1 + q2 * pb2, inverse = __frcp_rn(nq);
+      const float f = alpha1 * inverse, h = dot * inverse * inverse;
       qb1 = f * (pb1 - q1 * h);
       qb2 = f * (pb2 - q2 * h);
-      ga1 = dot / nq;
+      ga1 = dot * inverse;
     }
     const float rb11 = rho * a_at(R11, i, j), rb22 = rho * a_at(R22, i, j), rb12 = rho * a_at(R12, i, j);
     float sb11 = rb11, sb22 = rb22, sb12 = rb12, ga0 = 0.0f;
     const float ns = sqrtf(s11 * s11 + s22 * s22 + 2.0f * (s12 * s12));
     if (ns > alpha0) {
-      const float dot = s11 * rb11 + s22 * rb22 + s12 * rb12;
-      const float f = alpha0 / ns, h = dot / (ns * ns);
+      const float dot = s11 * rb11 + s22 * rb22 + s12 * rb12, inverse = __frcp_rn(ns);
+      const float f = alpha0 * inverse, h = dot * inverse * inverse;
       sb11 = f * (rb11 - s11 * h);
       sb22 = f * (rb22 - s22 * h);
       sb12 = f * (rb12 - 2.0f * s12 * h);
-      ga0 = dot / ns;
+      ga0 = dot * inverse;
     }
     l_at(0, i, j) = qb1;
     l_at(1, i, j) = qb2;
@@ -558,6 +483,105 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
   add_sum(g_alpha1, grads + 1 * q.images + z);
   add_sum(g_tau, grads + 2 * q.images + z);
   add_sum(g_sigma, grads + 3 * q.images + z);
+}
+
+// The dual step D_k as tiles of 16 rows x 32 columns: s_{k-1} and x~_k (9 planes) with a halo
+// of a row above and below and 4 columns each side by one 4D bulk-tensor copy, w~ over the tile
+// and the column to its left and the row above it in shared memory, then each pixel's step:
+// x- = 2 x~ - x, w- = 2 w~ - w, the points q and s and their projections, and the relaxation.
+constexpr int kForwardRows = kAdjointRows + 2;  // rows i0 - 1 .. i0 + 16
+constexpr int kForwardFloats = kFields * kForwardRows * kAdjointSpan;
+constexpr int kForwardTildeRows = kAdjointRows + 1, kForwardTildeColumns = 33;
+constexpr int kForwardTildeFloats = 2 * kForwardTildeRows * kTildeColumns;
+constexpr std::size_t kForwardShared = static_cast<std::size_t>(kForwardFloats + kForwardTildeFloats) * sizeof(float);
+
+__global__ void __launch_bounds__(256) dual_tile_kernel(const __grid_constant__ CUtensorMap state_map, Problem q,
+                                                        Planes out) {
+  extern __shared__ __align__(128) float shared[];
+  __shared__ __align__(8) std::uint64_t loaded;
+  float* const S = shared;                    // [field][row][column], row i0 - 1 + r, column j0 - 4 + c
+  float* const T = S + kForwardFloats;        // w~, row i0 - 1 + r, column j0 - 1 + c
+  const int lane = threadIdx.x, warp = threadIdx.y, tid = warp * 32 + lane;
+  const int z = blockIdx.z, i0 = blockIdx.y * kAdjointRows, j0 = blockIdx.x * 32;
+  const int H = q.rows, W = q.columns;
+  const float rho = q.rho, rest = 1.0f - q.rho, tau = q.tau[z], sigma = q.sigma[z];
+  const float alpha0 = q.alpha0[z], alpha1 = q.alpha1[z];
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(shared_address(&loaded)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(shared_address(&loaded)),
+                 "r"(static_cast<unsigned>(kForwardFloats * sizeof(float)))
+                 : "memory");
+    load_fields(S, &state_map, &loaded, j0 - 4, i0 - 1, z);
+  }
+  const bool ready = wait_phase(&loaded, 0);
+  if (__syncthreads_or(!ready)) {
+    // The load did not land: the tile's x is not a number, and no copy may still be writing
+    // into the CTA's shared memory when it leaves.
+    for (int rr = warp; rr < kAdjointRows; rr += 8) {
+      const int i = i0 + rr, j = j0 + lane;
+      if (i < H && j < W) out.x[at(q, z, i, j)] = __int_as_float(0x7fc00000);
+    }
+    if (tid == 0) wait_phase(&loaded, 0);
+    return;
+  }
+  auto s_at = [&](int f, int i, int j) -> float { return S[(f * kForwardRows + i - i0 + 1) * kAdjointSpan + j - j0 + 4]; };
+  auto t_at = [&](int f, int i, int j) -> float& { return T[(f * kForwardTildeRows + i - i0 + 1) * kTildeColumns + j - j0 + 1]; };
+  enum { X = 0, P1, P2, W1, W2, R11, R22, R12, XT };
+  // w~ = w + tau (p + div2 r), div2 r by forward differences.
+  for (int n = tid; n < kForwardTildeRows * kForwardTildeColumns; n += 256) {
+    const int i = i0 - 1 + n / kForwardTildeColumns, j = j0 - 1 + n % kForwardTildeColumns;
+    const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
+    float d1 = j + 1 < W ? s_at(R11, i, j + 1) - r11 : 0.0f;
+    float d2 = j + 1 < W ? s_at(R12, i, j + 1) - r12 : 0.0f;
+    d1 = d1 + (i + 1 < H ? s_at(R12, i + 1, j) - r12 : 0.0f);
+    d2 = d2 + (i + 1 < H ? s_at(R22, i + 1, j) - r22 : 0.0f);
+    t_at(0, i, j) = s_at(W1, i, j) + tau * (s_at(P1, i, j) + d1);
+    t_at(1, i, j) = s_at(W2, i, j) + tau * (s_at(P2, i, j) + d2);
+  }
+  __syncthreads();
+  for (int rr = warp; rr < kAdjointRows; rr += 8) {
+    const int i = i0 + rr, j = j0 + lane;
+    if (i >= H || j >= W) continue;
+    const bool right = j + 1 < W, down = i + 1 < H;
+    const float xt = s_at(XT, i, j), x = s_at(X, i, j);
+    const float bar = 2.0f * xt - x;
+    const float g1 = right ? (2.0f * s_at(XT, i, j + 1) - s_at(X, i, j + 1)) - bar : 0.0f;
+    const float g2 = down ? (2.0f * s_at(XT, i + 1, j) - s_at(X, i + 1, j)) - bar : 0.0f;
+    const float t1 = t_at(0, i, j), t2 = t_at(1, i, j), w1 = s_at(W1, i, j), w2 = s_at(W2, i, j);
+    const float b1 = 2.0f * t1 - w1, b2 = 2.0f * t2 - w2;
+    const float p1 = s_at(P1, i, j), p2 = s_at(P2, i, j);
+    const float q1 = p1 + sigma * (g1 - b1);
+    const float q2 = p2 + sigma * (g2 - b2);
+    float l1 = 0.0f, l2 = 0.0f, u1 = 0.0f, u2 = 0.0f;
+    if (j > 0) {
+      l1 = 2.0f * t_at(0, i, j - 1) - s_at(W1, i, j - 1);
+      l2 = 2.0f * t_at(1, i, j - 1) - s_at(W2, i, j - 1);
+    }
+    if (i > 0) {
+      u1 = 2.0f * t_at(0, i - 1, j) - s_at(W1, i - 1, j);
+      u2 = 2.0f * t_at(1, i - 1, j) - s_at(W2, i - 1, j);
+    }
+    const float own1x = right ? b1 : 0.0f, own2x = right ? b2 : 0.0f;
+    const float own1y = down ? b1 : 0.0f, own2y = down ? b2 : 0.0f;
+    const float e11 = own1x - l1, e22 = own2y - u2, e12 = 0.5f * ((own1y - u1) + (own2x - l2));
+    const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
+    const float s11 = r11 + sigma * e11, s22 = r22 + sigma * e22, s12 = r12 + sigma * e12;
+    const float sp = ball(q1 * q1 + q2 * q2, alpha1);
+    const float sr = ball(s11 * s11 + s22 * s22 + 2.0f * (s12 * s12), alpha0);
+    const std::size_t k = at(q, z, i, j);
+    out.x[k] = rho * xt + rest * x;
+    out.p1[k] = rho * (q1 * sp) + rest * p1;
+    out.p2[k] = rho * (q2 * sp) + rest * p2;
+    out.w1[k] = rho * t1 + rest * w1;
+    out.w2[k] = rho * t2 + rest * w2;
+    out.r11[k] = rho * (s11 * sr) + rest * r11;
+    out.r22[k] = rho * (s22 * sr) + rest * r22;
+    out.r12[k] = rho * (s12 * sr) + rest * r12;
+  }
 }
 
 // The primal step's adjoint, per block: from the adjoint of x~ (`xt_bar`) the adjoint of v.
@@ -652,6 +676,16 @@ dim3 block_grid(const Problem& q) {
   return dim3((q.columns + 31) / 32, (q.blocks_down + 7) / 8, q.images);
 }
 
+// The tiled dual step's and its adjoint's grid: a CTA a tile of kAdjointRows x 32.
+dim3 tile_grid(const Problem& q) {
+  return dim3((q.columns + 31) / 32, (q.rows + kAdjointRows - 1) / kAdjointRows, q.images);
+}
+
+// The map of 9 planes (a state and the x~ after it) for the tiled dual step.
+bool make_forward_map(CUtensorMap& map, const float* base, const Problem& q) {
+  return make_fields_map(map, base, q.columns, q.rows, q.images, 9, q.plane, kAdjointSpan, kForwardRows);
+}
+
 std::string check(const unround_b200_unrolled* u) {
   if (u == nullptr) return "the problem is a null pointer";
   if (u->images == 0 || u->rows == 0 || u->columns == 0) return "the problem has pictures of rows and columns";
@@ -735,18 +769,42 @@ extern "C" unround_status unround_b200_unrolled_forward(const unround_b200_unrol
   const std::size_t plane = q.plane;
   const std::uint64_t n = problem->iterations, every = problem->checkpoint_every;
   float* const spare[2] = {workspace, workspace + 9 * plane};
-  const dim3 grid = urb::pixel_grid(q), block(32, 8);
+  // The dual steps read the 9 planes of s_{k-1} and x~_k by bulk-tensor copies: a map of each
+  // checkpoint and of each spare.
+  const std::uint64_t segments = urb::checkpoints_of(*problem);
+  std::vector<CUtensorMap> checkpoint_maps(segments);
+  CUtensorMap spare_maps[2];
+  bool mapped = true;
+  for (std::uint64_t c = 0; c < segments && mapped; ++c) {
+    mapped = urb::make_forward_map(checkpoint_maps[c], checkpoints + c * 9 * plane, q);
+  }
+  for (int c = 0; c < 2 && mapped; ++c) mapped = urb::make_forward_map(spare_maps[c], spare[c], q);
+  if (!mapped) {
+    urb::tell(message, message_size, "the device's bulk-tensor copies could not be set up for the dual steps");
+    return UNROUND_ERROR_INTERNAL;
+  }
+  const dim3 grid = urb::pixel_grid(q), block(32, 8), tiles = urb::tile_grid(q);
   // s_{k-1} and then x~_k live at `current`: 9 planes.
   float* current = checkpoints;
+  const CUtensorMap* current_map = &checkpoint_maps[0];
   urb::start_kernel<<<grid, block, 0, on>>>(q, problem->start, urb::planes_of(current, plane));
   for (std::uint64_t k = 1; k <= n; ++k) {
     urb::primal_kernel<<<urb::block_grid(q), block, 0, on>>>(q, urb::planes_of(current, plane),
                                                               k == n ? output : current + 8 * plane);
     if (k < n) {
-      float* next = k % every == 0 ? checkpoints + k / every * 9 * plane : (current == spare[0] ? spare[1] : spare[0]);
-      urb::dual_kernel<<<grid, block, 0, on>>>(q, urb::planes_of(current, plane), current + 8 * plane,
-                                               urb::planes_of(next, plane));
+      float* next;
+      const CUtensorMap* next_map;
+      if (k % every == 0) {
+        next = checkpoints + k / every * 9 * plane;
+        next_map = &checkpoint_maps[k / every];
+      } else {
+        const int c = current == spare[0] ? 1 : 0;
+        next = spare[c];
+        next_map = &spare_maps[c];
+      }
+      urb::dual_tile_kernel<<<tiles, block, urb::kForwardShared, on>>>(*current_map, q, urb::planes_of(next, plane));
       current = next;
+      current_map = next_map;
     }
   }
   const cudaError_t error = cudaGetLastError();
@@ -785,17 +843,21 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
   auto storage_of = [&](std::uint64_t seg, std::uint64_t step) -> float* {
     return step == 0 ? const_cast<float*>(checkpoints) + seg * 9 * plane : recomputed + (step - 1) * 9 * plane;
   };
-  // The dual step's adjoint reads the 9 planes of each by bulk-tensor copies.
+  // The dual step and its adjoint read the 9 planes of each by bulk-tensor copies (boxes of
+  // different heights).
   std::vector<CUtensorMap> checkpoint_maps(segments), recomputed_maps(every > 1 ? every - 1 : 0);
+  std::vector<CUtensorMap> checkpoint_forward(segments), recomputed_forward(every > 1 ? every - 1 : 0);
   CUtensorMap bar_maps[2];
   bool mapped = urb::prepare_dual_adjoint();
   const int W = static_cast<int>(q.columns), H = static_cast<int>(q.rows), images = static_cast<int>(q.images);
   for (std::uint64_t c = 0; c < segments && mapped; ++c) {
-    mapped = urb::make_fields_map(checkpoint_maps[c], storage_of(c, 0), W, H, images, 9, plane, 40, urb::kStateRows);
+    mapped = urb::make_fields_map(checkpoint_maps[c], storage_of(c, 0), W, H, images, 9, plane, 40, urb::kStateRows) &&
+             urb::make_forward_map(checkpoint_forward[c], storage_of(c, 0), q);
   }
   for (std::uint64_t step = 1; step < every && mapped; ++step) {
     mapped = urb::make_fields_map(recomputed_maps[step - 1], storage_of(0, step), W, H, images, 9, plane, 40,
-                                  urb::kStateRows);
+                                  urb::kStateRows) &&
+             urb::make_forward_map(recomputed_forward[step - 1], storage_of(0, step), q);
   }
   for (int c = 0; c < 2 && mapped; ++c) {
     mapped = urb::make_fields_map(bar_maps[c], adjoint[c], W, H, images, 9, plane, 40, urb::kBarRows);
@@ -804,8 +866,7 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
     urb::tell(message, message_size, "the device's bulk-tensor copies could not be set up for the adjoint");
     return UNROUND_ERROR_INTERNAL;
   }
-  const dim3 grid = urb::pixel_grid(q), block(32, 8);
-  const dim3 tiles((q.columns + 31) / 32, (q.rows + urb::kAdjointRows - 1) / urb::kAdjointRows, q.images);
+  const dim3 block(32, 8), tiles = urb::tile_grid(q);
   cudaMemsetAsync(grads, 0, 4 * problem->images * sizeof(double), on);
   // The adjoint of s_N's predecessor starts at zero; that of x~_N is the output's gradient.
   int current = 0;
@@ -822,8 +883,9 @@ extern "C" unround_status unround_b200_unrolled_backward(const unround_b200_unro
       if (step > 0) {
         urb::primal_kernel<<<urb::block_grid(q), block, 0, on>>>(q, urb::planes_of(from, plane), from + 8 * plane);
       }
-      urb::dual_kernel<<<grid, block, 0, on>>>(q, urb::planes_of(from, plane), from + 8 * plane,
-                                               urb::planes_of(storage_of(seg, step + 1), plane));
+      const CUtensorMap& from_map = step == 0 ? checkpoint_forward[seg] : recomputed_forward[step - 1];
+      urb::dual_tile_kernel<<<tiles, block, urb::kForwardShared, on>>>(from_map, q,
+                                                                       urb::planes_of(storage_of(seg, step + 1), plane));
     }
     if (k1 - k0 > 1 && k1 < n) {
       // x~_{k1} of the segment's last state, for D_{k1}'s adjoint.
