@@ -251,9 +251,12 @@ constexpr int kPointRows = kAdjointRows + 2, kPointColumns = 34;  // (2): rows i
 constexpr int kBackRows = kAdjointRows + 1, kBackColumns = 33;    // (3): rows i0 - 1 .., columns j0 - 1 ..
 constexpr int kStateFloats = kFields * kStateRows * kAdjointSpan;
 constexpr int kBarFloats = kFields * kBarRows * kAdjointSpan;
-constexpr int kTildeFloats = 2 * kTildeRows * kTildeColumns;
-constexpr int kPointFloats = 5 * kPointRows * kTildeColumns;
-static_assert(2 * kBackRows * kTildeColumns <= kTildeFloats, "(3) reuses the space of (1)");
+// (1), (2) and (3) are kept in rows of kAdjointSpan, as the boxes are, and walked as rows x
+// kAdjointSpan points (the columns past each one's width idle): a warp's 32 points are 32
+// consecutive words of every array it reads or writes, across row ends too.
+constexpr int kTildeFloats = 2 * kTildeRows * kAdjointSpan;
+constexpr int kPointFloats = 5 * kPointRows * kAdjointSpan;
+static_assert(2 * kBackRows * kAdjointSpan <= kTildeFloats, "(3) reuses the space of (1)");
 static_assert(kStateFloats % 32 == 0, "the adjoint's box starts 128-byte aligned");
 constexpr std::size_t kAdjointShared =
     static_cast<std::size_t>(kStateFloats + kBarFloats + kTildeFloats + kPointFloats) * sizeof(float);
@@ -322,14 +325,15 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
   }
   auto s_at = [&](int f, int i, int j) -> float { return S[(f * kStateRows + i - i0 + 2) * kAdjointSpan + j - j0 + 4]; };
   auto a_at = [&](int f, int i, int j) -> float { return A[(f * kBarRows + i - i0 + 1) * kAdjointSpan + j - j0 + 4]; };
-  auto t_at = [&](int f, int i, int j) -> float& { return T[(f * kTildeRows + i - i0 + 2) * kTildeColumns + j - j0 + 2]; };
-  auto l_at = [&](int f, int i, int j) -> float& { return L[(f * kPointRows + i - i0 + 1) * kTildeColumns + j - j0 + 1]; };
-  auto tb_at = [&](int f, int i, int j) -> float& { return T[(f * kBackRows + i - i0 + 1) * kTildeColumns + j - j0 + 1]; };
+  auto t_at = [&](int f, int i, int j) -> float& { return T[(f * kTildeRows + i - i0 + 2) * kAdjointSpan + j - j0 + 2]; };
+  auto l_at = [&](int f, int i, int j) -> float& { return L[(f * kPointRows + i - i0 + 1) * kAdjointSpan + j - j0 + 1]; };
+  auto tb_at = [&](int f, int i, int j) -> float& { return T[(f * kBackRows + i - i0 + 1) * kAdjointSpan + j - j0 + 1]; };
   enum { X = 0, P1, P2, W1, W2, R11, R22, R12, EXTRA };  // EXTRA: x~ in S, v^ in A
 
   // (1) w~ = w + tau (p + div2 r), div2 r by forward differences.
-  for (int n = tid; n < kTildeRows * kTildeColumns; n += 256) {
-    const int i = i0 - 2 + n / kTildeColumns, j = j0 - 2 + n % kTildeColumns;
+  for (int n = tid; n < kTildeRows * kAdjointSpan; n += 256) {
+    if (n % kAdjointSpan >= kTildeColumns) continue;
+    const int i = i0 - 2 + n / kAdjointSpan, j = j0 - 2 + n % kAdjointSpan;
     const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
     float d1 = j + 1 < W ? s_at(R11, i, j + 1) - r11 : 0.0f;
     float d2 = j + 1 < W ? s_at(R12, i, j + 1) - r12 : 0.0f;
@@ -343,8 +347,9 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
   // (2) The points q = p + sigma (grad x- - w-) and s = r + sigma E w-, and the adjoints of q
   // and s through the projections onto the balls (d/d alpha1, d/d alpha0 and d/d sigma beside).
   float g_alpha0 = 0.0f, g_alpha1 = 0.0f, g_sigma = 0.0f;
-  for (int n = tid; n < kPointRows * kPointColumns; n += 256) {
-    const int i = i0 - 1 + n / kPointColumns, j = j0 - 1 + n % kPointColumns;
+  for (int n = tid; n < kPointRows * kAdjointSpan; n += 256) {
+    if (n % kAdjointSpan >= kPointColumns) continue;
+    const int i = i0 - 1 + n / kAdjointSpan, j = j0 - 1 + n % kAdjointSpan;
     const bool right = j + 1 < W, down = i + 1 < H;
     const float bar = 2.0f * s_at(EXTRA, i, j) - s_at(X, i, j);
     const float g1 = right ? (2.0f * s_at(EXTRA, i, j + 1) - s_at(X, i, j + 1)) - bar : 0.0f;
@@ -375,10 +380,12 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
     if (right) ap1 += -tau * (a_at(EXTRA, i, j + 1) - v);
     if (down) ap2 += -tau * (a_at(EXTRA, i + 1, j) - v);
     const float pb1 = rho * ap1, pb2 = rho * ap2;
+    // The projections' branches compare squares: |q| > alpha where |q|^2 > alpha^2, but for
+    // ties within rounding, where the map is continuous; 1 / |q| by the approximate rsqrt.
     float qb1 = pb1, qb2 = pb2, ga1 = 0.0f;
-    const float nq = sqrtf(q1 * q1 + q2 * q2);
-    if (nq > alpha1) {
-      const float dot = q1 * pb1 + q2 * pb2, inverse = __frcp_rn(nq);
+    const float sq = q1 * q1 + q2 * q2;
+    if (sq > alpha1 * alpha1) {
+      const float dot = q1 * pb1 + q2 * pb2, inverse = rsqrtf(sq);
       const float f = alpha1 * inverse, h = dot * inverse * inverse;
       qb1 = f * (pb1 - q1 * h);
       qb2 = f * (pb2 - q2 * h);
@@ -386,9 +393,9 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
     }
     const float rb11 = rho * a_at(R11, i, j), rb22 = rho * a_at(R22, i, j), rb12 = rho * a_at(R12, i, j);
     float sb11 = rb11, sb22 = rb22, sb12 = rb12, ga0 = 0.0f;
-    const float ns = sqrtf(s11 * s11 + s22 * s22 + 2.0f * (s12 * s12));
-    if (ns > alpha0) {
-      const float dot = s11 * rb11 + s22 * rb22 + s12 * rb12, inverse = __frcp_rn(ns);
+    const float ss = s11 * s11 + s22 * s22 + 2.0f * (s12 * s12);
+    if (ss > alpha0 * alpha0) {
+      const float dot = s11 * rb11 + s22 * rb22 + s12 * rb12, inverse = rsqrtf(ss);
       const float f = alpha0 * inverse, h = dot * inverse * inverse;
       sb11 = f * (rb11 - s11 * h);
       sb22 = f * (rb22 - s22 * h);
@@ -426,8 +433,9 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
     wb1 += sigma * e1;
     wb2 += sigma * e2;
   };
-  for (int n = tid; n < kBackRows * kBackColumns; n += 256) {
-    const int i = i0 - 1 + n / kBackColumns, j = j0 - 1 + n % kBackColumns;
+  for (int n = tid; n < kBackRows * kAdjointSpan; n += 256) {
+    if (n % kAdjointSpan >= kBackColumns) continue;
+    const int i = i0 - 1 + n / kAdjointSpan, j = j0 - 1 + n % kAdjointSpan;
     float wb1, wb2;
     w_minus_bar(i, j, wb1, wb2);
     tb_at(0, i, j) = rho * a_at(W1, i, j) + 2.0f * wb1;
@@ -492,7 +500,7 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
 constexpr int kForwardRows = kAdjointRows + 2;  // rows i0 - 1 .. i0 + 16
 constexpr int kForwardFloats = kFields * kForwardRows * kAdjointSpan;
 constexpr int kForwardTildeRows = kAdjointRows + 1, kForwardTildeColumns = 33;
-constexpr int kForwardTildeFloats = 2 * kForwardTildeRows * kTildeColumns;
+constexpr int kForwardTildeFloats = 2 * kForwardTildeRows * kAdjointSpan;  // rows of kAdjointSpan, as the box
 constexpr std::size_t kForwardShared = static_cast<std::size_t>(kForwardFloats + kForwardTildeFloats) * sizeof(float);
 
 __global__ void __launch_bounds__(256) dual_tile_kernel(const __grid_constant__ CUtensorMap state_map, Problem q,
@@ -529,11 +537,12 @@ __global__ void __launch_bounds__(256) dual_tile_kernel(const __grid_constant__ 
     return;
   }
   auto s_at = [&](int f, int i, int j) -> float { return S[(f * kForwardRows + i - i0 + 1) * kAdjointSpan + j - j0 + 4]; };
-  auto t_at = [&](int f, int i, int j) -> float& { return T[(f * kForwardTildeRows + i - i0 + 1) * kTildeColumns + j - j0 + 1]; };
+  auto t_at = [&](int f, int i, int j) -> float& { return T[(f * kForwardTildeRows + i - i0 + 1) * kAdjointSpan + j - j0 + 1]; };
   enum { X = 0, P1, P2, W1, W2, R11, R22, R12, XT };
   // w~ = w + tau (p + div2 r), div2 r by forward differences.
-  for (int n = tid; n < kForwardTildeRows * kForwardTildeColumns; n += 256) {
-    const int i = i0 - 1 + n / kForwardTildeColumns, j = j0 - 1 + n % kForwardTildeColumns;
+  for (int n = tid; n < kForwardTildeRows * kAdjointSpan; n += 256) {
+    if (n % kAdjointSpan >= kForwardTildeColumns) continue;
+    const int i = i0 - 1 + n / kAdjointSpan, j = j0 - 1 + n % kAdjointSpan;
     const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
     float d1 = j + 1 < W ? s_at(R11, i, j + 1) - r11 : 0.0f;
     float d2 = j + 1 < W ? s_at(R12, i, j + 1) - r12 : 0.0f;
