@@ -182,8 +182,9 @@ def _traffic() -> float | None:
 
 def _call(image) -> int:
     """One solve through the C interface, as a C or cgo caller makes it: unround_solve on host
-    arrays (levels in; the binary64 canvas and coefficients out, into the result), then the
-    canvas read on the host. Returns the result's bytes copied from the device."""
+    arrays (levels in; the binary64 canvas, coefficients and RGB picture out, into the result),
+    then the canvas and the picture read on the host. Returns the result's bytes copied from the
+    device (the picture is made on the device and copied like the canvas)."""
     import ctypes
 
     import numpy as np
@@ -205,12 +206,18 @@ def _call(image) -> int:
         canvas = np.ctypeslib.as_array(pointer, shape=(c.value * h.value * w.value,))
         if not np.isfinite(canvas[:: max(1, canvas.size // 4096)]).all():
             raise RuntimeError("the result holds values that are not finite")
+        ph, pw, pc = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        pointer = library.unround_result_picture(result, ctypes.byref(ph), ctypes.byref(pw), ctypes.byref(pc))
+        picture = np.ctypeslib.as_array(pointer, shape=(ph.value * pw.value * pc.value,))
+        if not np.isfinite(picture[:: max(1, picture.size // 4096)]).all():
+            raise RuntimeError("the picture holds values that are not finite")
         coefficients = 0
         for index in range(int(library.unround_result_components(result))):
             count = ctypes.c_uint64()
             library.unround_result_coefficients(result, index, ctypes.byref(count))
             coefficients += count.value
-        return canvas.nbytes + 8 * coefficients
+        # The planes are the canvas here (no cut); a one-channel picture is the planes.
+        return canvas.nbytes + 8 * coefficients + (picture.nbytes if pc.value > 1 else 0)
     finally:
         library.unround_result_free(result)
         del kept

@@ -200,7 +200,8 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
     failure = {kInternal, "the device failed in the batched iterations: " + describe(error)};
     return false;
   }
-  outcomes.assign(entries.size(), Outcome{});
+  outcomes.clear();
+  outcomes.resize(entries.size());
   for (std::size_t n = 0; n < entries.size(); ++n) {
     if (!solvers[n]->finish_batch(batched, outcomes[n], failure)) {
       failure.message = "picture " + std::to_string(n) + ": " + failure.message;

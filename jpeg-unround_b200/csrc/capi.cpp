@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "batch.hpp"
+#include "colour.hpp"
 #include "model.hpp"
 #include "settings.hpp"
 #include "solver.hpp"
@@ -25,10 +26,16 @@ struct unround_settings {
 
 struct unround_result {
   urb::Frame frame;
-  urb::Outcome outcome;
-  std::vector<double> picture;
+  urb::Outcome outcome;  // the canvas, the planes and the picture (made on the device)
   std::uint64_t height = 0, width = 0, channels = 0;
-  std::vector<double> planes;
+  // The planes cut to the picture: the canvas itself where it is no larger; and the picture:
+  // the planes themselves where there is one channel.
+  [[nodiscard]] const double* planes() const {
+    return outcome.planes.empty() ? outcome.canvas.data() : outcome.planes.data();
+  }
+  [[nodiscard]] const double* picture() const {
+    return outcome.picture.empty() ? planes() : outcome.picture.data();
+  }
   std::vector<std::uint64_t> record_iterations;
   std::vector<double> record_values[5];
   // What the model holds, made when first asked for (rust/capi/src/lib.rs:888-930).
@@ -127,18 +134,15 @@ bool inputs_of(const unround_input* input, std::vector<urb::ComponentInput>& out
   return true;
 }
 
-// JFIF's RGB of Y, Cb and Cr (docs/math.md 8; rust/unround/src/colour.rs:45-70): the doubles
-// nearest to 701/500, 443/250, 25251/73375 and 209599/293500.
-constexpr double kCr = 0x1.66e978d4fdf3bp+0;
-constexpr double kCb = 0x1.c5a1cac083127p+0;
-constexpr double kGb = 0x1.6065433a66b17p-2;
-constexpr double kGr = 0x1.6da345743d962p-1;
-// And back: the doubles nearest to 0.299, 0.587, 0.114, 250/443 and 500/701.
-constexpr double kR = 0x1.322d0e5604189p-2;
-constexpr double kG = 0x1.2c8b439581062p-1;
-constexpr double kB = 0x1.d2f1a9fbe76c9p-4;
-constexpr double kToCb = 0x1.20f065b4e0378p-1;
-constexpr double kToCr = 0x1.6d314d0e3e153p-1;
+using urb::kB;
+using urb::kCb;
+using urb::kCr;
+using urb::kG;
+using urb::kGb;
+using urb::kGr;
+using urb::kR;
+using urb::kToCb;
+using urb::kToCr;
 
 void to_rgb(const double* planes, std::size_t size, double* picture) {
   for (std::size_t k = 0; k < size; ++k) {
@@ -166,30 +170,9 @@ unround_result* result_of(urb::Frame&& frame, urb::Outcome&& outcome) {
   made->frame = std::move(frame);
   made->outcome = std::move(outcome);
   const urb::Frame& f = made->frame;
-  const std::size_t h = f.height, w = f.width, count = f.channels();
-  made->height = h;
-  made->width = w;
-  made->planes.resize(count * h * w);
-  for (std::size_t c = 0; c < count; ++c) {
-    for (std::size_t i = 0; i < h; ++i) {
-      const double* from = made->outcome.canvas.data() + (c * f.rows + i) * f.columns;
-      std::copy(from, from + w, made->planes.begin() + static_cast<std::ptrdiff_t>((c * h + i) * w));
-    }
-  }
-  if (f.color_space == 2) {
-    made->channels = 3;
-    made->picture.resize(3 * h * w);
-    to_rgb(made->planes.data(), h * w, made->picture.data());
-  } else if (count == 1) {
-    made->channels = 1;
-    made->picture = made->planes;
-  } else {
-    made->channels = count;
-    made->picture.resize(count * h * w);
-    for (std::size_t k = 0; k < h * w; ++k) {
-      for (std::size_t c = 0; c < count; ++c) made->picture[k * count + c] = made->planes[c * h * w + k];
-    }
-  }
+  made->height = f.height;
+  made->width = f.width;
+  made->channels = f.color_space == 2 ? 3 : f.channels();
   for (const urb::Record& r : made->outcome.records) {
     made->record_iterations.push_back(r.iteration);
     made->record_values[0].push_back(r.seconds);
@@ -529,13 +512,13 @@ const double* unround_result_picture(const unround_result* result, uint64_t* hei
   put(height, result->height);
   put(width, result->width);
   put(channels, result->channels);
-  return result->picture.data();
+  return result->picture();
 }
 
 const double* unround_result_planes(const unround_result* result, uint64_t* count) {
   if (result == nullptr) return nullptr;
-  put(count, result->planes.size());
-  return result->planes.data();
+  put(count, result->frame.channels() * result->height * result->width);
+  return result->planes();
 }
 
 int32_t unround_result_color_space(const unround_result* result) {

@@ -20,6 +20,7 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "colour.hpp"
 #include "dct.cuh"
 #include "prox.cuh"
 #include "tma.cuh"
@@ -897,6 +898,31 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
   }
 }
 
+// The result's picture (capi.cpp's to_rgb, rust/unround/src/decode.rs:306-364): a thread per
+// pixel of the picture; JFIF's RGB by the same binary64 operations in the same order, each
+// rounded on its own (no contraction into fused multiply-adds), so that it equals the host's.
+__global__ void __launch_bounds__(256) picture_kernel(const PictureParams P) {
+  const std::size_t k = static_cast<std::size_t>(blockIdx.x) * 256 + threadIdx.x;
+  const std::size_t pixels = static_cast<std::size_t>(P.height) * P.width;
+  if (k >= pixels) return;
+  const std::size_t i = k / static_cast<std::size_t>(P.width), j = k % static_cast<std::size_t>(P.width);
+  const std::size_t plane = static_cast<std::size_t>(P.rows) * P.columns, at = i * P.columns + j;
+  if (P.picture != nullptr) {
+    if (P.rgb) {
+      const double y = P.canvas[at];
+      const double cb = __dsub_rn(P.canvas[plane + at], 128.0), cr = __dsub_rn(P.canvas[2 * plane + at], 128.0);
+      P.picture[3 * k] = __dadd_rn(y, __dmul_rn(kCr, cr));
+      P.picture[3 * k + 1] = __dsub_rn(__dsub_rn(y, __dmul_rn(kGb, cb)), __dmul_rn(kGr, cr));
+      P.picture[3 * k + 2] = __dadd_rn(y, __dmul_rn(kCb, cb));
+    } else {
+      for (int c = 0; c < P.channels; ++c) P.picture[k * P.channels + c] = P.canvas[c * plane + at];
+    }
+  }
+  if (P.planes != nullptr) {
+    for (int c = 0; c < P.channels; ++c) P.planes[c * pixels + k] = P.canvas[c * plane + at];
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // Binary64: the start's coefficients, and canvases of coefficients.
 
@@ -1552,6 +1578,13 @@ cudaError_t launch_restore(const ComponentDevice& c, double* out, cudaStream_t s
 
 cudaError_t launch_canvas(const CanvasParams& p, cudaStream_t stream) {
   return by_cells<CanvasLaunch>(p.component.cell_rows, p.component.cell_columns, p, stream);
+}
+
+cudaError_t launch_picture(const PictureParams& p, cudaStream_t stream) {
+  const std::size_t pixels = static_cast<std::size_t>(p.height) * p.width;
+  if (pixels == 0 || (p.picture == nullptr && p.planes == nullptr)) return cudaSuccess;
+  picture_kernel<<<static_cast<unsigned>((pixels + 255) / 256), 256, 0, stream>>>(p);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_gradient(const float* x, float* w1, float* w2, const Geometry& g, cudaStream_t stream) {

@@ -187,6 +187,19 @@ cudaError_t launch_dual(const DualParams& p, bool tgv, bool coupled, bool keep, 
 cudaError_t launch_primal(const PrimalParams& p, bool keep, cudaStream_t stream);
 cudaError_t launch_start_coefficients(const StartParams& p, cudaStream_t stream);
 cudaError_t launch_canvas(const CanvasParams& p, cudaStream_t stream);
+// The result's picture from the binary64 canvas (C planes of rows x columns): its height x width
+// pixels with the channels interleaved into `picture` (null: none), for YCbCr (`rgb`) JFIF's
+// RGB; and the planes cut to height x width into `planes` (null: none).
+struct PictureParams {
+  const double* canvas = nullptr;
+  int channels = 1;
+  int rows = 0, columns = 0;
+  int height = 0, width = 0;
+  bool rgb = false;
+  double* picture = nullptr;
+  double* planes = nullptr;
+};
+cudaError_t launch_picture(const PictureParams& p, cudaStream_t stream);
 // The kept coefficients (binary32, DC centred) as binary64 absolute coefficients.
 cudaError_t launch_restore(const ComponentDevice& c, double* out, cudaStream_t stream);
 cudaError_t launch_gradient(const float* x, float* w1, float* w2, const Geometry& g, cudaStream_t stream);

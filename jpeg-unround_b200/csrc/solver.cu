@@ -540,8 +540,6 @@ struct Solver::Impl {
   // coefficients are zeta).
   void result(Outcome& out) {
     const std::size_t size = static_cast<std::size_t>(g.rows) * g.columns;
-    out.canvas.resize(size * g.channels);
-    out.coefficients.resize(components.size());
     for (std::size_t c = 0; c < components.size(); ++c) {
       if (error == cudaSuccess) error = launch_restore(components[c], coefficients[c], stream);
       CanvasParams cp;
@@ -556,20 +554,37 @@ struct Solver::Impl {
     fetch(out);
   }
 
+  // The result into host memory: the binary64 canvas and coefficients, and the picture made
+  // from the canvas on the device (the planes cut to the picture where the canvas is larger,
+  // the channels interleaved, JFIF's RGB of YCbCr), each copied once into pinned memory.
   void fetch(Outcome& out) {
     const std::size_t size = static_cast<std::size_t>(g.rows) * g.columns;
-    out.canvas.resize(size * g.channels);
-    out.coefficients.resize(components.size());
-    if (error == cudaSuccess) {
-      error = cudaMemcpyAsync(out.canvas.data(), canvas, out.canvas.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                              stream);
-    }
-    for (std::size_t c = 0; c < components.size(); ++c) {
-      out.coefficients[c].resize(frame.components[c].coefficient_count());
-      if (error == cudaSuccess && !out.coefficients[c].empty()) {
-        error = cudaMemcpyAsync(out.coefficients[c].data(), coefficients[c], out.coefficients[c].size() * sizeof(double),
-                                cudaMemcpyDeviceToHost, stream);
+    const std::size_t pixels = static_cast<std::size_t>(frame.height) * frame.width;
+    const bool cut = frame.height != frame.rows || frame.width != frame.columns;
+    const bool interleaved = g.channels > 1;
+    PictureParams pp;
+    pp.canvas = canvas;
+    pp.channels = g.channels;
+    pp.rows = g.rows;
+    pp.columns = g.columns;
+    pp.height = static_cast<int>(frame.height);
+    pp.width = static_cast<int>(frame.width);
+    pp.rgb = frame.color_space == 2 && g.channels == 3;
+    if (cut) pp.planes = allocate<double>(pixels * g.channels);
+    if (interleaved) pp.picture = allocate<double>(pixels * g.channels);
+    if (error == cudaSuccess) error = launch_picture(pp, stream);
+    auto copy = [&](HostBuffer& to, const double* from, std::size_t count) {
+      to.resize(count);
+      if (error == cudaSuccess && count > 0) {
+        error = cudaMemcpyAsync(to.data(), from, count * sizeof(double), cudaMemcpyDeviceToHost, stream);
       }
+    };
+    copy(out.canvas, canvas, size * g.channels);
+    copy(out.planes, pp.planes, cut ? pixels * g.channels : 0);
+    copy(out.picture, pp.picture, interleaved ? pixels * g.channels : 0);
+    out.coefficients.resize(components.size());
+    for (std::size_t c = 0; c < components.size(); ++c) {
+      copy(out.coefficients[c], coefficients[c], frame.components[c].coefficient_count());
     }
     if (error == cudaSuccess) error = cudaStreamSynchronize(stream);
   }

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "kernels.hpp"
+#include "host_buffer.hpp"
 #include "model.hpp"
 
 namespace urb {
@@ -42,9 +43,14 @@ struct Start {
 // What a solve made (rust/unround/src/decode.rs:70-110): the canvas C x rows x columns and
 // each component's coefficients in binary64, the records, the iterations, and why it stopped
 // (0 no solver, 1 converged, 2 iterations, 3 observer).
+// The result on the host. `planes` is the canvas cut to the picture (empty where they are the
+// same); `picture` its pixels with the channels interleaved, for YCbCr in JFIF RGB (empty where
+// it is the planes: one channel).
 struct Outcome {
-  std::vector<double> canvas;
-  std::vector<std::vector<double>> coefficients;
+  HostBuffer canvas;
+  std::vector<HostBuffer> coefficients;
+  HostBuffer planes;
+  HostBuffer picture;
   std::vector<Record> records;
   std::uint64_t iterations = 0;
   std::int32_t stop = 0;
