@@ -1,6 +1,7 @@
 // The batched solve (batch.hpp).
 #include "batch.hpp"
 
+#include <algorithm>
 #include <map>
 #include <memory>
 #include <string>
@@ -11,8 +12,6 @@
 namespace urb {
 
 namespace {
-
-constexpr int kTileRows = 128;  // rows of a tile of the batched dual sweep (a multiple of 8)
 
 std::string describe(cudaError_t error) {
   return std::string(cudaGetErrorName(error)) + ": " + cudaGetErrorString(error);
@@ -44,8 +43,51 @@ struct DualClass {
   bool tgv = false;
   int channels = 1;
   bool coupled = false;
+  std::vector<int> pictures;       // of the batch, in this class
+  std::vector<Geometry> geometry;  // theirs
   std::vector<DualTile> tiles;
   DualTile* device = nullptr;
+};
+
+// Streams to run the classes' launches of an iteration side by side: the launches of a phase
+// (the primal steps, then the dual steps) fork from `main` and join it again, so that a
+// captured iteration is a graph of parallel branches, one per class, and one class's last
+// wave of CTAs overlaps the next class's first.
+struct Branches {
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;  // [0] the fork, [1 + b] branch b's end
+  cudaError_t error = cudaSuccess;
+  explicit Branches(std::size_t count) {
+    streams.resize(count, nullptr);
+    events.resize(count + 1, nullptr);
+    for (cudaStream_t& s : streams) {
+      if (error == cudaSuccess) error = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    }
+    for (cudaEvent_t& e : events) {
+      if (error == cudaSuccess) error = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    }
+  }
+  ~Branches() {
+    for (cudaStream_t s : streams) {
+      if (s != nullptr) cudaStreamDestroy(s);
+    }
+    for (cudaEvent_t e : events) {
+      if (e != nullptr) cudaEventDestroy(e);
+    }
+  }
+  // Runs launch(b, stream) for b < count, each on its own branch of `main`.
+  template <typename Launch>
+  cudaError_t fork(cudaStream_t main, std::size_t count, Launch&& launch) {
+    if (count <= 1) return count == 1 ? launch(0, main) : cudaSuccess;
+    cudaError_t e = cudaEventRecord(events[0], main);
+    for (std::size_t b = 0; b < count && e == cudaSuccess; ++b) {
+      e = cudaStreamWaitEvent(streams[b], events[0], 0);
+      if (e == cudaSuccess) e = launch(b, streams[b]);
+      if (e == cudaSuccess) e = cudaEventRecord(events[1 + b], streams[b]);
+    }
+    for (std::size_t b = 0; b < count && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(main, events[1 + b], 0);
+    return e;
+  }
 };
 
 struct PrimalClass {
@@ -107,11 +149,8 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
     dual.tgv = plan.tgv;
     dual.channels = g.channels;
     dual.coupled = plan.coupled && g.channels > 1;
-    for (int x0 = 0; x0 < g.columns; x0 += 32) {
-      for (int i0 = 0; i0 < g.rows; i0 += kTileRows) {
-        dual.tiles.push_back({static_cast<int>(n), x0, i0, std::min(i0 + kTileRows, g.rows)});
-      }
-    }
+    dual.pictures.push_back(static_cast<int>(n));
+    dual.geometry.push_back(g);
     for (std::size_t c = 0; c < own.size(); ++c) {
       const ComponentDevice& comp = own[c].params[0].component;
       PrimalClass& primal = primals[{comp.cell_rows, comp.cell_columns}];
@@ -123,6 +162,19 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
         for (int strip = 0; strip < strips; ++strip) primal.items.push_back({z, strip, stage, 0});
       }
       components.push_back(own[c]);
+    }
+  }
+  // Each class's tiles: strips of 32 columns cut into tiles of the height that finishes the
+  // class's pictures soonest in waves of the CTAs the device holds.
+  for (auto& [key, dual] : duals) {
+    const int rows = batch_tile_rows(dual.geometry, dual_batch_slots(dual.tgv, dual.channels, dual.coupled));
+    for (std::size_t m = 0; m < dual.pictures.size(); ++m) {
+      const Geometry& g = dual.geometry[m];
+      for (int x0 = 0; x0 < g.columns; x0 += 32) {
+        for (int i0 = 0; i0 < g.rows; i0 += rows) {
+          dual.tiles.push_back({dual.pictures[m], x0, i0, std::min(i0 + rows, g.rows)});
+        }
+      }
     }
   }
   Owned owned(stream);
@@ -138,19 +190,27 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
   }
   // Iteration k (1-based): the primal steps read the state of parity (k - 1) % 2, the dual
   // steps read it and write the other.
+  std::vector<const PrimalClass*> primal_list;
+  std::vector<const DualClass*> dual_list;
+  for (auto& [key, primal] : primals) primal_list.push_back(&primal);
+  for (auto& [key, dual] : duals) dual_list.push_back(&dual);
+  Branches branches(std::max(primal_list.size(), dual_list.size()));
+  if (error == cudaSuccess) error = branches.error;
   auto iteration = [&](std::uint64_t k, cudaStream_t on) {
     const int parity = static_cast<int>((k - 1) % 2);
-    for (auto& [key, primal] : primals) {
-      if (error == cudaSuccess) {
-        error = launch_primal_batch(primal.device, static_cast<int>(primal.items.size()), components_device, parity,
-                                    primal.cell_rows, primal.cell_columns, on);
-      }
+    if (error == cudaSuccess) {
+      error = branches.fork(on, primal_list.size(), [&](std::size_t b, cudaStream_t s) {
+        const PrimalClass& primal = *primal_list[b];
+        return launch_primal_batch(primal.device, static_cast<int>(primal.items.size()), components_device, parity,
+                                   primal.cell_rows, primal.cell_columns, s);
+      });
     }
-    for (auto& [key, dual] : duals) {
-      if (error == cudaSuccess) {
-        error = launch_dual_batch(dual.device, static_cast<int>(dual.tiles.size()), images_device, parity, dual.tgv,
-                                  dual.channels, dual.coupled, on);
-      }
+    if (error == cudaSuccess) {
+      error = branches.fork(on, dual_list.size(), [&](std::size_t b, cudaStream_t s) {
+        const DualClass& dual = *dual_list[b];
+        return launch_dual_batch(dual.device, static_cast<int>(dual.tiles.size()), images_device, parity, dual.tgv,
+                                 dual.channels, dual.coupled, s);
+      });
     }
   };
   // The batch makes iterations 1 .. most - 1; each picture's last (which keeps its values for

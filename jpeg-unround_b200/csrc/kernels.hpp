@@ -7,6 +7,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -271,6 +272,10 @@ struct DualTile {
 // channels.
 cudaError_t launch_dual_batch(const DualTile* tiles, int count, const DualBatchImage* images, int parity, bool tgv,
                               int channels, bool coupled, cudaStream_t stream);
+// The CTAs of that sweep the current device holds at once (0 where it cannot tell), and the
+// tile height (a multiple of 16) that finishes a class's pictures soonest in waves of `slots`.
+int dual_batch_slots(bool tgv, int channels, bool coupled);
+int batch_tile_rows(const std::vector<Geometry>& pictures, int slots);
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,
                             bool coupled, bool keep, cudaStream_t stream);
 // A 3D tiled map of `count` float planes `stride` floats apart, boxes of `box_columns` columns

@@ -482,6 +482,33 @@ cudaError_t dual_batch_one(const DualTile* tiles, int count, const DualBatchImag
   return cudaGetLastError();
 }
 
+// The CTAs of the batched dual sweep the device holds at once (its SMs times an SM's).
+template <bool TGV, int C, bool COUPLED>
+int dual_batch_resident() {
+  auto kernel = dual_batch_kernel<TGV, C, COUPLED>;
+  const std::size_t bytes = dual_tma_shared_bytes(TGV, C);
+  int device = 0, per_sm = 0, sms = 0;
+  cudaGetDevice(&device);
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, bytes) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return per_sm * sms;
+}
+
+template <bool TGV>
+int dual_batch_resident_channels(int channels, bool coupled) {
+  switch (channels) {
+    case 1: return dual_batch_resident<TGV, 1, false>();
+    case 2: return coupled ? dual_batch_resident<TGV, 2, true>() : dual_batch_resident<TGV, 2, false>();
+    case 3: return coupled ? dual_batch_resident<TGV, 3, true>() : dual_batch_resident<TGV, 3, false>();
+    default: return 0;
+  }
+}
+
 template <bool TGV>
 cudaError_t dual_batch_channels(const DualTile* tiles, int count, const DualBatchImage* images, int parity,
                                 int channels, bool coupled, cudaStream_t s) {
@@ -501,6 +528,29 @@ cudaError_t launch_dual_batch(const DualTile* tiles, int count, const DualBatchI
                               int channels, bool coupled, cudaStream_t stream) {
   return tgv ? dual_batch_channels<true>(tiles, count, images, parity, channels, coupled, stream)
              : dual_batch_channels<false>(tiles, count, images, parity, channels, coupled, stream);
+}
+
+int dual_batch_slots(bool tgv, int channels, bool coupled) {
+  return tgv ? dual_batch_resident_channels<true>(channels, coupled)
+             : dual_batch_resident_channels<false>(channels, coupled);
+}
+
+int batch_tile_rows(const std::vector<Geometry>& pictures, int slots) {
+  int best = 128;
+  long long best_cost = -1;
+  for (int height = 64; height <= 512; height += 16) {
+    long long ctas = 0;
+    for (const Geometry& g : pictures) {
+      ctas += static_cast<long long>((g.columns + 31) / 32) * ((g.rows + height - 1) / height);
+    }
+    const long long waves = slots > 0 ? (ctas + slots - 1) / slots : ctas;
+    const long long cost = waves * (height + 2 * kChunk);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = height;
+    }
+  }
+  return best;
 }
 
 }  // namespace urb
