@@ -98,7 +98,7 @@ class UnrolledProblem:
             centre = native.model(image, options, 0, 2).reshape(by, bx, 64)
             # The start: the clipped centres' canvas (absolute coefficients).
             zeta = np.clip(centre, lower, upper).reshape(by, bx, 8, 8)
-            starts.append(_blocks_to_canvas(np.einsum("vi,abvu,un->abin", c, zeta, c)))
+            starts.append(_blocks_to_canvas(np.einsum("vi,abvu,un->abin", c, zeta, c, optimize=True)))
             # DC centred on the middle of its interval.
             middle = 0.5 * (lower[..., 0] + upper[..., 0])
             lower = lower.copy()
