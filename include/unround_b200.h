@@ -112,6 +112,12 @@ unround_status unround_b200_unrolled_backward(const unround_b200_unrolled* probl
                                               const float* checkpoints, float* workspace, const float* output_grad,
                                               double* grads, void* stream, char* message, size_t message_size);
 
+/* The blue-noise matrix of the ordered dither of 8- and 16-bit output (unround_pnm): 64 x 64
+ * ranks, row by row, into `ranks` (4096 values, each of 0 .. 4095 once), made by the
+ * void-and-cluster method as the reference's scripts/blue_noise.py makes the table of
+ * rust/unround/src/blue_noise.rs; without a device. */
+unround_status unround_b200_blue_noise(uint16_t* ranks, char* message, size_t message_size);
+
 /* What the host model makes of an input and settings, without a GPU (the reference computes the
  * same in Problem::make, cpp/src/model.cpp:134-256, and plan, cpp/src/pdhg.cpp:147-233): of
  * component `component`, `which` 0 the lower ends of the intervals, 1 the upper ends, 2 the

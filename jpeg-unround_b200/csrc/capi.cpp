@@ -5,6 +5,8 @@
 // status with its message (rust/capi/src/lib.rs:99-115, `guarded`).
 #include <cmath>
 #include <cstring>
+#include <limits>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -13,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "batch.hpp"
+#include "blue_noise.hpp"
 #include "colour.hpp"
 #include "model.hpp"
 #include "settings.hpp"
@@ -186,6 +189,88 @@ unround_result* result_of(urb::Frame&& frame, urb::Outcome&& outcome) {
     made->weights.emplace_back(c.weights.begin(), c.weights.end());
   }
   return made;
+}
+
+// The samples of a picture of height x width pixels of 1 to 4 interleaved channels, counted
+// (rust/capi/src/lib.rs:1259-1269; rust/unround/src/output.rs:232-246).
+bool picture_count(const double* samples, std::uint64_t height, std::uint64_t width, std::uint64_t channels,
+                   std::size_t& count, urb::Failure& failure) {
+  const std::uint64_t limit = std::numeric_limits<std::uint64_t>::max();
+  if ((width != 0 && height > limit / width) || (channels != 0 && height * width > limit / channels)) {
+    failure = {urb::kArgument, "a picture too large"};
+    return false;
+  }
+  if (samples == nullptr) {
+    failure = {urb::kArgument, "the samples are a null pointer"};
+    return false;
+  }
+  count = static_cast<std::size_t>(height * width * channels);
+  if (channels < 1 || channels > 4 || height == 0 || width == 0 || width > (1u << 30)) {
+    failure = {urb::kOptions, "a picture of " + std::to_string(height) + " x " + std::to_string(width) +
+                                  " x 1 to 4 samples, not empty, and not of " + std::to_string(count) + " samples in " +
+                                  std::to_string(channels) + " channels"};
+    return false;
+  }
+  return true;
+}
+
+// The 8- or 16-bit levels of the samples (output.cu), into `out` (count bytes, or 2 count
+// most significant byte first): the samples copied to the device, quantized there, and the
+// levels copied back; where a sample is not finite, the first such is named and nothing is
+// made (rust/unround/src/output.rs:220-230).
+bool quantize(const double* samples, std::size_t count, int width, int channels, bool sixteen, int dither,
+              std::uint8_t* out, urb::Failure& failure) {
+  if (!have_device(failure)) return false;
+  if (!urb::prepare_levels()) {
+    failure = {urb::kInternal, "the blue-noise matrix could not be loaded onto the device"};
+    return false;
+  }
+  Stream stream;
+  cudaError_t error = stream.error;
+  const std::size_t out_bytes = count * (sixteen ? 2 : 1);
+  void* block = nullptr;
+  const std::size_t in_bytes = (count * sizeof(double) + 255) / 256 * 256;
+  if (error == cudaSuccess) error = cudaMallocAsync(&block, in_bytes + (out_bytes + 255) / 256 * 256 + 256, stream.stream);
+  auto* in = static_cast<double*>(block);
+  auto* levels = static_cast<std::uint8_t*>(block) + in_bytes;
+  auto* flag = reinterpret_cast<int*>(levels + (out_bytes + 255) / 256 * 256);
+  int not_finite = 0;
+  if (error == cudaSuccess) error = cudaMemcpyAsync(in, samples, count * sizeof(double), cudaMemcpyHostToDevice, stream.stream);
+  if (error == cudaSuccess) error = cudaMemsetAsync(flag, 0, sizeof(int), stream.stream);
+  urb::LevelsParams p;
+  p.samples = in;
+  p.count = count;
+  p.width = width;
+  p.channels = channels;
+  p.scale = sixteen ? 257.0 : 1.0;
+  p.top = sixteen ? 65535.0 : 255.0;
+  p.dither = dither;
+  p.sixteen = sixteen;
+  p.out = levels;
+  p.not_finite = flag;
+  if (error == cudaSuccess) error = urb::launch_levels(p, stream.stream);
+  if (error == cudaSuccess) error = cudaMemcpyAsync(&not_finite, flag, sizeof(int), cudaMemcpyDeviceToHost, stream.stream);
+  if (error == cudaSuccess) error = cudaMemcpyAsync(out, levels, out_bytes, cudaMemcpyDeviceToHost, stream.stream);
+  if (block != nullptr) cudaFreeAsync(block, stream.stream);
+  const cudaError_t synced = cudaStreamSynchronize(stream.stream);
+  if (error == cudaSuccess) error = synced;
+  if (error != cudaSuccess) {
+    failure = {urb::kInternal, std::string("the device failed in the levels: ") + cudaGetErrorString(error)};
+    return false;
+  }
+  if (not_finite != 0) {
+    double first = std::numeric_limits<double>::quiet_NaN();
+    for (std::size_t k = 0; k < count; ++k) {
+      if (!std::isfinite(samples[k])) {
+        first = samples[k];
+        break;
+      }
+    }
+    failure = {urb::kOptions, std::string("a sample to quantize is not finite: ") +
+                                  (std::isnan(first) ? "NaN" : (first > 0 ? "inf" : "-inf"))};
+    return false;
+  }
+  return true;
 }
 
 bool solve_input(const unround_input* input, const unround_settings* settings, const urb::Start* start,
@@ -630,13 +715,53 @@ unround_status unround_png(const double*, uint64_t, uint64_t, uint64_t, int32_t,
   return UNROUND_ERROR_UNSUPPORTED;
 }
 
-unround_status unround_pnm(const double*, uint64_t, uint64_t, uint64_t, int32_t, int32_t, uint8_t**, uint64_t*,
-                           char* message, size_t message_size) {
-  say(message, message_size, "the PNM writer is host output outside this build's path");
-  return UNROUND_ERROR_UNSUPPORTED;
+// The PNM file (rust/unround/src/output.rs:248-271, rust/capi/src/lib.rs:1460-1488): a P5
+// (grey) or P6 (RGB) header and the levels, made on the device (quantize).
+unround_status unround_pnm(const double* samples, uint64_t height, uint64_t width, uint64_t channels, int32_t sixteen,
+                           int32_t dither, uint8_t** bytes, uint64_t* size, char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (bytes == nullptr || size == nullptr) {
+      failure = {urb::kArgument, "the bytes and the size are not null pointers"};
+      return false;
+    }
+    if (dither < 0 || dither > 2) {
+      failure = {urb::kOptions, "the dither is 0, 1 or 2, not " + std::to_string(dither)};
+      return false;
+    }
+    std::size_t count = 0;
+    if (!picture_count(samples, height, width, channels, count, failure)) return false;
+    if (channels == 2 || channels == 4) {
+      failure = {urb::kOptions, "PNM holds no alpha: write PNG or TIFF"};
+      return false;
+    }
+    const std::string header = std::string(channels == 1 ? "P5" : "P6") + "\n" + std::to_string(width) + " " +
+                               std::to_string(height) + "\n" + (sixteen != 0 ? "65535" : "255") + "\n";
+    const std::size_t body = count * (sixteen != 0 ? 2 : 1);
+    std::unique_ptr<std::uint8_t[]> file(new std::uint8_t[header.size() + body]);
+    std::memcpy(file.get(), header.data(), header.size());
+    if (!quantize(samples, count, static_cast<int>(width), static_cast<int>(channels), sixteen != 0, dither,
+                  file.get() + header.size(), failure)) {
+      return false;
+    }
+    *size = header.size() + body;
+    *bytes = file.release();
+    return true;
+  });
 }
 
 void unround_bytes_free(uint8_t* bytes, uint64_t) { delete[] bytes; }
+
+unround_status unround_b200_blue_noise(uint16_t* ranks, char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (ranks == nullptr) {
+      failure = {urb::kArgument, "the ranks are a null pointer"};
+      return false;
+    }
+    const auto& made = urb::blue_noise_ranks();
+    std::copy(made.begin(), made.end(), ranks);
+    return true;
+  });
+}
 
 unround_status unround_orient(const double*, uint64_t, uint64_t, uint64_t, int32_t, double*, uint64_t*, uint64_t*,
                               char* message, size_t message_size) {

@@ -201,6 +201,24 @@ struct PictureParams {
   double* planes = nullptr;
 };
 cudaError_t launch_picture(const PictureParams& p, cudaStream_t stream);
+// 8- or 16-bit levels (output.cu) of `count` binary64 samples, rows of `width` pixels of
+// `channels` interleaved samples: dither 0 rounds, 1 and 2 take the blue-noise matrix with the
+// channels apart or together; 16-bit levels most significant byte first. A sample that is not
+// finite sets *not_finite. prepare_levels loads the matrix onto the current device (once).
+struct LevelsParams {
+  const double* samples = nullptr;
+  std::size_t count = 0;
+  int width = 1;
+  int channels = 1;
+  double scale = 1.0;
+  double top = 255.0;
+  int dither = 1;
+  bool sixteen = false;
+  std::uint8_t* out = nullptr;
+  int* not_finite = nullptr;
+};
+bool prepare_levels();
+cudaError_t launch_levels(const LevelsParams& p, cudaStream_t stream);
 // The kept coefficients (binary32, DC centred) as binary64 absolute coefficients.
 cudaError_t launch_restore(const ComponentDevice& c, double* out, cudaStream_t stream);
 cudaError_t launch_gradient(const float* x, float* w1, float* w2, const Geometry& g, cudaStream_t stream);

@@ -204,6 +204,9 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_result_record_values": (doubles, handle, i32, u64p),
         "unround_to_rgb": (i32, doubles, u64, u64, doubles),
         "unround_to_ycbcr": (i32, doubles, u64, u64, doubles),
+        "unround_pnm": (i32, doubles, u64, u64, u64, i32, i32, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), u64p,
+                        *text),
+        "unround_bytes_free": (None, ctypes.POINTER(ctypes.c_uint8), u64),
         "unround_b200_solve_from": (i32, ctypes.POINTER(_Input), handle, ctypes.POINTER(_Start), *made),
         "unround_b200_measure": (i32, ctypes.POINTER(_Input), handle, u64, u64, ctypes.POINTER(_Timing),
                                  ctypes.POINTER(handle), *text),
@@ -724,3 +727,45 @@ def to_ycbcr(picture: npt.ArrayLike) -> Array:
     p = ctypes.POINTER(ctypes.c_double)
     _library().unround_to_ycbcr(values.ctypes.data_as(p), values.shape[0], values.shape[1], out.ctypes.data_as(p))
     return out
+
+
+# The command line's --dither and --dither-channels (docs/cli.md), as the interface's dither.
+_DITHERS = {("blue-noise", None): 1, ("blue-noise", "apart"): 1, ("blue-noise", "together"): 2, ("none", None): 0}
+
+
+def _dither(dither: str, channels: str | None) -> int:
+    """The interface's dither of the command line's --dither and --dither-channels."""
+    found = _DITHERS.get((dither, channels))
+    if found is None:
+        message = f"the dither is blue-noise, with the channels apart or together, or none, not {dither}" + (
+            "" if channels is None else f" with the channels {channels}"
+        )
+        raise ValueError(message)
+    return found
+
+
+def pnm_bytes(picture: npt.ArrayLike, *, sixteen: bool = False, dither: str = "blue-noise",
+              dither_channels: str | None = None) -> bytes:
+    """A PNM file of the picture's samples, (height, width) grey or (height, width, 3) RGB, of 8
+    bits, or of 16 (257 levels to a unit): each sample by the ordered dither of the blue-noise
+    matrix (dither "blue-noise", the channels "apart" -- the default -- or "together") or rounded
+    to the nearest level, halves away from 0 ("none"), clamped (docs/math.md 10). The levels are
+    made on the GPU (unround_pnm)."""
+    made = _dither(dither, dither_channels)
+    samples = np.ascontiguousarray(picture, dtype=np.float64)
+    if samples.ndim not in (2, 3):
+        raise ValueError(f"a picture is (height, width) or (height, width, channels), not {samples.shape}")
+    height, width = int(samples.shape[0]), int(samples.shape[1])
+    channels = 1 if samples.ndim == 2 else int(samples.shape[2])
+    library = _library()
+    pointer = ctypes.POINTER(ctypes.c_uint8)()
+    size = ctypes.c_uint64()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_pnm(samples.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), height, width, channels,
+                                 1 if sixteen else 0, made, ctypes.byref(pointer), ctypes.byref(size), message,
+                                 _MESSAGE)
+    _raise(status, message)
+    try:
+        return ctypes.string_at(pointer, int(size.value))
+    finally:
+        library.unround_bytes_free(pointer, size)
