@@ -223,6 +223,27 @@ def _call(image) -> int:
         del kept
 
 
+def _call_levels(image, out) -> int:
+    """One solve through the C interface to 8-bit levels (unround_b200_solve_levels, blue-noise
+    dither): levels in, the picture made and quantized on the device, its bytes out into `out`
+    (host memory). Returns the bytes copied from the device."""
+    import ctypes
+
+    from unround import native
+
+    library = native._library()
+    settings = native._Settings(OPTIONS)
+    given, kept = native._input_of(image)
+    sizes = (ctypes.c_uint64 * 3)()
+    message = ctypes.create_string_buffer(4096)
+    status = library.unround_b200_solve_levels(ctypes.byref(given), settings.handle, 0, 1,
+                                               out.ctypes.data_as(ctypes.c_void_p), out.nbytes, sizes, message, 4096)
+    if status != 0:
+        raise RuntimeError(message.value.decode())
+    del kept
+    return int(sizes[0] * sizes[1] * sizes[2])
+
+
 MIX_ITERATIONS = 300
 
 
@@ -572,6 +593,14 @@ def main() -> None:
         d2h = _call(image)
     e2e_seconds = max_over_ranks(time.perf_counter() - began)
     e2e = world * pixels * args.steps * ITERATIONS / e2e_seconds / 1e6
+    # The same to 8-bit levels: only the quantized picture comes back.
+    levels = np.empty(pixels * 3, dtype=np.uint8)
+    _call_levels(image, levels)  # warm the call path
+    began = time.perf_counter()
+    for _ in range(args.steps):
+        levels_d2h = _call_levels(image, levels)
+    levels_seconds = max_over_ranks(time.perf_counter() - began)
+    e2e_levels = world * pixels * args.steps * ITERATIONS / levels_seconds / 1e6
     peak, peak_kind = _peaks()
     samples = timing.samples
     dual_achieved = DUAL_BYTES * samples / (timing.dual_milliseconds / 1e3) / 1e9
@@ -594,6 +623,9 @@ def main() -> None:
                          "iteration_bytes_per_sample": ALGORITHMIC_BYTES,
                          "dual_ms": timing.dual_milliseconds, "primal_ms": timing.primal_milliseconds},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": levels_bytes, "d2h_bytes_per_step": d2h},
+            "e2e_levels": {"value": e2e_levels, "unit": UNIT, "h2d_bytes_per_step": levels_bytes,
+                           "d2h_bytes_per_step": levels_d2h,
+                           "call": "unround_b200_solve_levels, 8 bits, blue-noise dither"},
             "gpu_launches": timing.launches_per_iteration * args.steps * ITERATIONS,
             "clocks": clocks.summary(),
         }

@@ -112,6 +112,18 @@ unround_status unround_b200_unrolled_backward(const unround_b200_unrolled* probl
                                               const float* checkpoints, float* workspace, const float* output_grad,
                                               double* grads, void* stream, char* message, size_t message_size);
 
+/* unround_solve to 8- or 16-bit levels (no counterpart in the reference, whose solve returns
+ * binary64 and whose writers quantize on the host, rust/unround/src/output.rs:187-218): the
+ * picture (JFIF RGB of YCbCr, else its channels) is made and quantized on the device -- dither
+ * as unround_pnm takes it (0 rounds, halves away from 0; 1 and 2 the blue-noise matrix with the
+ * channels apart or together), 16 bits as 257 times the sample, most significant byte first --
+ * and only the levels, height x width x channels interleaved, come back into `levels`
+ * (`capacity` bytes, host memory). `sizes` (3, may be null) gets the height, the width and the
+ * channels; with `levels` null only they are made. No records are returned. */
+unround_status unround_b200_solve_levels(const unround_input* input, const unround_settings* settings, int32_t sixteen,
+                                        int32_t dither, uint8_t* levels, uint64_t capacity, uint64_t* sizes,
+                                        char* message, size_t message_size);
+
 /* The blue-noise matrix of the ordered dither of 8- and 16-bit output (unround_pnm): 64 x 64
  * ranks, row by row, into `ranks` (4096 values, each of 0 .. 4095 once), made by the
  * void-and-cluster method as the reference's scripts/blue_noise.py makes the table of

@@ -751,6 +751,59 @@ unround_status unround_pnm(const double* samples, uint64_t height, uint64_t widt
 
 void unround_bytes_free(uint8_t* bytes, uint64_t) { delete[] bytes; }
 
+unround_status unround_b200_solve_levels(const unround_input* input, const unround_settings* settings, int32_t sixteen,
+                                        int32_t dither, uint8_t* levels, uint64_t capacity, uint64_t* sizes,
+                                        char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (input == nullptr || settings == nullptr) {
+      failure = {urb::kArgument, "the input and the settings are not null pointers"};
+      return false;
+    }
+    if (dither < 0 || dither > 2) {
+      failure = {urb::kOptions, "the dither is 0, 1 or 2, not " + std::to_string(dither)};
+      return false;
+    }
+    std::vector<urb::ComponentInput> inputs;
+    if (!inputs_of(input, inputs, failure)) return false;
+    const urb::Settings& s = settings->settings;
+    auto frame = urb::make_frame(input->height, input->width, input->color_space, inputs, s, failure);
+    if (!frame) return false;
+    if (s.method == urb::Method::subgradient) {
+      failure = {urb::kUnsupported,
+                 "the subgradient method (docs/math.md 7) is not on this build's path: use mmse, tv or tgv"};
+      return false;
+    }
+    const std::uint64_t channels = frame->channels();
+    const std::uint64_t need = static_cast<std::uint64_t>(frame->height) * frame->width * channels * (sixteen ? 2 : 1);
+    if (sizes != nullptr) {
+      sizes[0] = frame->height;
+      sizes[1] = frame->width;
+      sizes[2] = channels;
+    }
+    if (levels == nullptr) return true;  // the sizes alone
+    if (capacity < need) {
+      failure = {urb::kArgument, "the levels take " + std::to_string(need) + " bytes, not " + std::to_string(capacity)};
+      return false;
+    }
+    std::optional<urb::Plan> plan;
+    if (s.method != urb::Method::mmse) {
+      plan = urb::make_plan(s, frame->channels(), failure);
+      if (!plan) return false;
+    }
+    if (!have_device(failure)) return false;
+    Stream stream;
+    if (stream.error != cudaSuccess) {
+      failure = {urb::kInternal, std::string("a CUDA stream: ") + cudaGetErrorString(stream.error)};
+      return false;
+    }
+    urb::Outcome outcome;
+    urb::Solver solver(*frame, stream.stream);
+    solver.keep_result_on_device();
+    if (!solver.solve(s.method, plan ? &*plan : nullptr, nullptr, nullptr, outcome, failure)) return false;
+    return solver.levels(sixteen != 0, dither, levels, failure);
+  });
+}
+
 unround_status unround_b200_blue_noise(uint16_t* ranks, char* message, size_t message_size) {
   return guarded(message, message_size, [&](urb::Failure& failure) {
     if (ranks == nullptr) {

@@ -70,6 +70,7 @@ struct Solver::Impl {
   Plan plan;
   bool planned = false;
   std::vector<double> host_partials;
+  bool host_result = true;  // false: the result stays on the device (levels)
 
   Impl(const Frame& f, cudaStream_t s) : frame(f), stream(s) {}
 
@@ -551,7 +552,47 @@ struct Solver::Impl {
       cp.mode = 1;
       if (error == cudaSuccess) error = launch_canvas(cp, stream);
     }
-    fetch(out);
+    if (host_result) fetch(out);
+  }
+
+  // The picture's 8- or 16-bit levels into host memory `out` (height x width x its channels,
+  // interleaved; 16 bits most significant byte first), from the binary64 canvas on the device:
+  // the picture made there (JFIF RGB of YCbCr), quantized there (output.cu), and only the
+  // levels copied out. False, with *not_finite set, where a sample of the picture is not finite.
+  void levels(bool sixteen, int dither, std::uint8_t* out, bool& not_finite) {
+    not_finite = false;
+    const std::size_t pixels = static_cast<std::size_t>(frame.height) * frame.width;
+    const bool rgb = frame.color_space == 2 && g.channels == 3;
+    PictureParams pp;
+    pp.canvas = canvas;
+    pp.channels = g.channels;
+    pp.rows = g.rows;
+    pp.columns = g.columns;
+    pp.height = static_cast<int>(frame.height);
+    pp.width = static_cast<int>(frame.width);
+    pp.rgb = rgb;
+    pp.picture = allocate<double>(pixels * g.channels);
+    if (error == cudaSuccess) error = launch_picture(pp, stream);
+    LevelsParams lp;
+    lp.samples = pp.picture;
+    lp.count = pixels * g.channels;
+    lp.width = static_cast<int>(frame.width);
+    lp.channels = g.channels;
+    lp.scale = sixteen ? 257.0 : 1.0;
+    lp.top = sixteen ? 65535.0 : 255.0;
+    lp.dither = dither;
+    lp.sixteen = sixteen;
+    const std::size_t bytes_out = lp.count * (sixteen ? 2 : 1);
+    lp.out = allocate<std::uint8_t>(bytes_out);
+    lp.not_finite = allocate<int>(1);
+    if (error == cudaSuccess && !prepare_levels()) error = cudaErrorInitializationError;
+    if (error == cudaSuccess) error = cudaMemsetAsync(lp.not_finite, 0, sizeof(int), stream);
+    if (error == cudaSuccess) error = launch_levels(lp, stream);
+    int flag = 0;
+    if (error == cudaSuccess) error = cudaMemcpyAsync(&flag, lp.not_finite, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (error == cudaSuccess) error = cudaMemcpyAsync(out, lp.out, bytes_out, cudaMemcpyDeviceToHost, stream);
+    if (error == cudaSuccess) error = cudaStreamSynchronize(stream);
+    not_finite = flag != 0;
   }
 
   // The result into host memory: the binary64 canvas and coefficients, and the picture made
@@ -613,7 +654,7 @@ bool Solver::solve(Method method, const Plan* plan, const Start* start, const Ob
     // The decoder of the centres (docs/math.md 2.3).
     m.setup(false, false);
     m.start(nullptr, false);
-    m.fetch(out);
+    if (m.host_result) m.fetch(out);
     bytes_ = m.bytes;
     out.solved = false;
     out.stop = 0;
@@ -705,7 +746,7 @@ bool Solver::run(std::uint64_t first, const Observer& observer, Outcome& out, Fa
   out.solved = true;
   if (iteration == 0) {
     // No iteration: the start itself, in binary64.
-    m.fetch(out);
+    if (m.host_result) m.fetch(out);
   } else {
     m.result(out);
   }
@@ -818,6 +859,20 @@ bool Solver::breakdown(std::uint64_t iterations, double& dual_ms, double& primal
   dual_ms = timed > 0 ? dual / static_cast<double>(timed) : 0.0;
   primal_ms = timed > 0 ? primal / static_cast<double>(timed) : 0.0;
   return m.check(failure, "the timed iterations");
+}
+
+void Solver::keep_result_on_device() { impl_->host_result = false; }
+
+bool Solver::levels(bool sixteen, int dither, std::uint8_t* out, Failure& failure) {
+  Impl& m = *impl_;
+  bool not_finite = false;
+  m.levels(sixteen, dither, out, not_finite);
+  if (!m.check(failure, "the levels")) return false;
+  if (not_finite) {
+    failure = {kOptions, "a sample to quantize is not finite"};
+    return false;
+  }
+  return true;
 }
 
 bool Solver::finish(Outcome& out, Failure& failure) {

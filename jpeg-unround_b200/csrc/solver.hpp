@@ -93,6 +93,13 @@ class Solver {
   bool batch_entries(DualBatchImage& image, std::vector<PrimalBatchComponent>& components);
   bool finish_batch(std::uint64_t done, Outcome& out, Failure& failure);
 
+  // Before solve(): keep the result on the device (the Outcome gets the records and counts,
+  // not the arrays); after it, the picture's 8- or 16-bit levels into host memory `out`
+  // (height x width x channels, interleaved; dither 0 rounds, 1 and 2 take the blue-noise
+  // matrix with the channels apart or together).
+  void keep_result_on_device();
+  bool levels(bool sixteen, int dither, std::uint8_t* out, Failure& failure);
+
   [[nodiscard]] std::size_t device_bytes() const { return bytes_; }
   [[nodiscard]] const Geometry& geometry() const { return geometry_; }
   [[nodiscard]] int launches_per_iteration() const;

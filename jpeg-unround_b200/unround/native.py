@@ -207,6 +207,8 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_pnm": (i32, doubles, u64, u64, u64, i32, i32, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), u64p,
                         *text),
         "unround_bytes_free": (None, ctypes.POINTER(ctypes.c_uint8), u64),
+        "unround_b200_solve_levels": (i32, ctypes.POINTER(_Input), handle, i32, i32, ctypes.c_void_p, u64, u64p,
+                                      *text),
         "unround_b200_solve_from": (i32, ctypes.POINTER(_Input), handle, ctypes.POINTER(_Start), *made),
         "unround_b200_measure": (i32, ctypes.POINTER(_Input), handle, u64, u64, ctypes.POINTER(_Timing),
                                  ctypes.POINTER(handle), *text),
@@ -769,3 +771,29 @@ def pnm_bytes(picture: npt.ArrayLike, *, sixteen: bool = False, dither: str = "b
         return ctypes.string_at(pointer, int(size.value))
     finally:
         library.unround_bytes_free(pointer, size)
+
+
+def solve_levels(image: jpegio.Image, settings: Settings | list[str] | None = None, *, sixteen: bool = False,
+                 dither: str = "blue-noise", dither_channels: str | None = None) -> npt.NDArray:
+    """The reconstruction as 8-bit (uint8) or 16-bit (uint16) levels, (height, width) grey or
+    (height, width, channels), quantized on the GPU as pnm_bytes quantizes a picture: only the
+    levels are copied back (include/unround_b200.h, unround_b200_solve_levels)."""
+    library = _library()
+    handle = _settings_of(settings)
+    made = _dither(dither, dither_channels)
+    given, kept = _input_of(image)
+    sizes = (ctypes.c_uint64 * 3)()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_b200_solve_levels(ctypes.byref(given), handle.handle, int(sixteen), made, None, 0, sizes,
+                                               message, _MESSAGE)
+    _raise(status, message)
+    height, width, channels = (int(v) for v in sizes)
+    out = np.empty((height, width, channels), dtype=np.uint16 if sixteen else np.uint8)
+    status = library.unround_b200_solve_levels(ctypes.byref(given), handle.handle, int(sixteen), made,
+                                               out.ctypes.data_as(ctypes.c_void_p), out.nbytes, sizes, message,
+                                               _MESSAGE)
+    _raise(status, message)
+    del kept
+    if sixteen:
+        out = out.byteswap()  # the interface's most significant byte first
+    return out[:, :, 0] if channels == 1 else out

@@ -97,3 +97,22 @@ def test_refusals():
     for dither, channels in [("ordered", None), ("none", "apart"), ("blue-noise", "mixed")]:
         with pytest.raises(ValueError, match="the dither is blue-noise"):
             native.pnm_bytes(picture, dither=dither, dither_channels=channels)
+
+
+@pytest.mark.parametrize("colour", [False, True])
+@pytest.mark.parametrize("sixteen", [False, True])
+def test_a_solve_to_levels_is_the_pnm_of_the_solve(colour, sixteen):
+    # unround_b200_solve_levels quantizes the picture on the device: the levels of the binary64
+    # picture that unround_solve returns, as unround_pnm makes them.
+    from unround import native, synthetic
+
+    made = (synthetic.colour(61, 83, quality=50, seed=4, noise=2) if colour
+            else synthetic.grey(61, 83, quality=50, seed=4, noise=2))
+    options = ["--method", "tgv", "--iterations", "20", "--tolerance", "0", "--record-every", "0"]
+    picture = native.solve(made.image, options).picture
+    for dither, channels in [("blue-noise", None), ("blue-noise", "together"), ("none", None)]:
+        levels = native.solve_levels(made.image, options, sixteen=sixteen, dither=dither, dither_channels=channels)
+        assert levels.shape == picture.shape
+        expected = _samples(native.pnm_bytes(picture, sixteen=sixteen, dither=dither, dither_channels=channels),
+                            picture.shape, sixteen)
+        np.testing.assert_array_equal(levels.reshape(expected.shape).astype(np.int64), expected)
