@@ -13,6 +13,7 @@
 #include "unround/model.hpp"
 #include "unround/operators.hpp"
 #include "unround/pdhg.hpp"
+#include "unround/samples.hpp"
 #include "unround/settings.hpp"
 
 #include <cstdint>
@@ -189,6 +190,83 @@ void* oref_solve(std::uint32_t height, std::uint32_t width, std::int32_t color_s
   out->stop = solved->stop == Stop::converged ? 1 : solved->stop == Stop::iterations ? 2 : 3;
   out->tau = solved->steps.tau;
   out->sigma = solved->steps.sigma;
+  return out;
+}
+
+// A picture of rounded samples (rust/unround/src/samples.rs; cpp/src/samples.cpp): levels of
+// `bits` bits, rows x columns x channels interleaved, reconstructed as samples::reconstruct
+// does a PNG file's (cpp/src/samples.cpp:344-405) -- the same refusals of options, the colours
+// by samples::solve and an alpha (channels 2 or 4) apart -- without reading a file. The canvas
+// is the picture's planes, C x H x W; the records, iterations and steps the colours'.
+void* oref_solve_samples(const std::uint16_t* levels, std::uint32_t rows, std::uint32_t columns,
+                         std::uint32_t channels, std::int32_t bits, std::size_t option_count,
+                         const char* const* options, char* message, std::size_t message_size) {
+  using namespace unround;
+  std::vector<std::string_view> arguments;
+  for (std::size_t i = 0; i < option_count; ++i) arguments.emplace_back(options[i]);
+  auto parsed = parse_settings(arguments);
+  if (!parsed) {
+    say(message, message_size, parsed.error().message);
+    return nullptr;
+  }
+  const Settings settings = *parsed;
+  if (settings.method != Method::tv && settings.method != Method::tgv) {
+    say(message, message_size, "a PNG file is reconstructed by tv or tgv");
+    return nullptr;
+  }
+  const DataTerm& term = settings.data.front();
+  const double mu = term.mu ? *term.mu : 0.0;
+  const pdhg::Model method = settings.method == Method::tv ? pdhg::Model::tv : pdhg::Model::tgv;
+  const Picture<const std::uint16_t> picture(levels, PictureExtents{rows, columns, channels});
+  const bool alpha = channels == 2u || channels == 4u;
+  const std::size_t colours = alpha ? channels - 1u : channels;
+  auto* out = new Outcome;
+  out->channels = channels;
+  out->rows = rows;
+  out->columns = columns;
+  auto run = [&](std::size_t first, std::size_t count, const pdhg::Regularizer& regularizer, bool keep) {
+    auto model = samples::Model::make(picture, bits, first, count, term.slack, mu);
+    if (!model) {
+      say(message, message_size, model.error().message);
+      return false;
+    }
+    auto solved = samples::solve(*model, method, regularizer, settings.pdhg);
+    if (!solved) {
+      say(message, message_size, solved.error().message);
+      return false;
+    }
+    for (const auto& plane : solved->canvas) {
+      const auto entries = plane.entries();
+      out->canvas.insert(out->canvas.end(), entries.begin(), entries.end());
+    }
+    if (keep) {
+      for (const Record& record : solved->records) {
+        out->record_iterations.push_back(record.iteration);
+        out->record_values.push_back(record.seconds);
+        out->record_values.push_back(record.primal);
+        out->record_values.push_back(record.dual);
+        out->record_values.push_back(record.scaling ? *record.scaling : __builtin_nan(""));
+        out->record_values.push_back(record.partial_gap ? *record.partial_gap : __builtin_nan(""));
+      }
+      out->iterations = solved->iterations;
+      out->stop = solved->stop == Stop::converged ? 1 : solved->stop == Stop::iterations ? 2 : 3;
+      out->tau = solved->steps.tau;
+      out->sigma = solved->steps.sigma;
+    }
+    return true;
+  };
+  if (!run(0, colours, settings.regularizer, true)) {
+    delete out;
+    return nullptr;
+  }
+  if (alpha) {
+    pdhg::Regularizer alone = settings.regularizer;
+    alone.channel_weights.clear();
+    if (!run(colours, 1, alone, false)) {
+      delete out;
+      return nullptr;
+    }
+  }
   return out;
 }
 

@@ -1,0 +1,16 @@
+// Test infrastructure of the oracle: the PNG reader that shim/unround/jpegio.hpp declares, which
+// refuses every file (the oracle gives the samples solver levels, not files).
+#include "unround/jpegio.hpp"
+
+namespace unround::jpegio {
+
+std::expected<PngImage, Error> PngImage::read(std::span<const std::uint8_t>, std::uint64_t) {
+  return std::unexpected(Error{Errc::unsupported, "the oracle reads no PNG files"});
+}
+Picture<const std::uint16_t> PngImage::levels() const { return {}; }
+int PngImage::channels() const { return 0; }
+int PngImage::bits() const { return 8; }
+std::span<const std::uint8_t> PngImage::icc_profile() const { return {}; }
+const std::string& PngImage::warning() const { return warning_; }
+
+}  // namespace unround::jpegio

@@ -74,6 +74,11 @@ def _library() -> ctypes.CDLL:
     lib.oref_records.restype = ctypes.c_uint64
     lib.oref_records.argtypes = (ctypes.c_void_p, ctypes.POINTER(u64p), ctypes.POINTER(dp))
     lib.oref_solver.argtypes = (ctypes.c_void_p, u64p, ctypes.POINTER(ctypes.c_int32), dp, dp)
+    lib.oref_solve_samples.restype = ctypes.c_void_p
+    lib.oref_solve_samples.argtypes = (
+        ctypes.POINTER(ctypes.c_uint16), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32,
+        ctypes.c_size_t, ctypes.POINTER(ctypes.c_char_p), ctypes.c_char_p, ctypes.c_size_t,
+    )
     return lib
 
 
@@ -171,5 +176,51 @@ def solve(
             record_iterations=record_iterations.astype(np.int64), records=records,
             iterations=iterations.value, stop=stop.value, tau=tau.value, sigma=sigma.value,
         )
+    finally:
+        lib.oref_free(handle)
+
+
+@dataclass
+class SolvedSamples:
+    """What the reference made of a picture of rounded samples: its planes (C, H, W), the
+    colours' records (iteration; seconds, primal, dual, scaling, partial gap), iterations, stop
+    (1 converged, 2 iterations) and steps."""
+
+    canvas: np.ndarray
+    record_iterations: np.ndarray
+    records: np.ndarray
+    iterations: int
+    stop: int
+    tau: float
+    sigma: float
+
+
+def solve_samples(levels: np.ndarray, bits: int, options: list[str]) -> SolvedSamples:
+    """Runs the reference's solver of rounded samples (cpp/src/samples.cpp) on levels (H, W) or
+    (H, W, C) of `bits` bits, as it reconstructs a PNG file's."""
+    lib = _library()
+    values = np.ascontiguousarray(levels, dtype=np.uint16)
+    if values.ndim == 2:
+        values = values[:, :, np.newaxis]
+    rows, columns, channels = values.shape
+    encoded = [option.encode() for option in options]
+    array = (ctypes.c_char_p * max(len(encoded), 1))(*encoded)
+    message = ctypes.create_string_buffer(4096)
+    handle = lib.oref_solve_samples(values.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), rows, columns, channels,
+                                    bits, len(encoded), array, message, 4096)
+    if not handle:
+        raise ValueError(message.value.decode())
+    try:
+        canvas = np.ctypeslib.as_array(lib.oref_canvas(handle), shape=(channels, rows, columns)).copy()
+        iterations_p = ctypes.POINTER(ctypes.c_uint64)()
+        values_p = ctypes.POINTER(ctypes.c_double)()
+        n = lib.oref_records(handle, ctypes.byref(iterations_p), ctypes.byref(values_p))
+        record_iterations = np.ctypeslib.as_array(iterations_p, shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+        records = np.ctypeslib.as_array(values_p, shape=(n, 5)).copy() if n else np.zeros((0, 5))
+        iterations, stop = ctypes.c_uint64(), ctypes.c_int32()
+        tau, sigma = ctypes.c_double(), ctypes.c_double()
+        lib.oref_solver(handle, ctypes.byref(iterations), ctypes.byref(stop), ctypes.byref(tau), ctypes.byref(sigma))
+        return SolvedSamples(canvas=canvas, record_iterations=record_iterations.astype(np.int64), records=records,
+                             iterations=iterations.value, stop=stop.value, tau=tau.value, sigma=sigma.value)
     finally:
         lib.oref_free(handle)
