@@ -124,6 +124,24 @@ unround_status unround_b200_solve_levels(const unround_input* input, const unrou
                                         int32_t dither, uint8_t* levels, uint64_t capacity, uint64_t* sizes,
                                         char* message, size_t message_size);
 
+/* A picture of rounded samples reconstructed on the device -- what the reference does to a PNG
+ * file in unround_decode (rust/unround/src/samples.rs, cpp/src/samples.cpp:344-405), here from
+ * its levels, since this build reads no PNG files: `levels` rows x columns x channels (1 to 4:
+ * grey, grey and alpha, RGB, RGB and alpha) interleaved, of `bits` bits (1 to 16). Each sample is
+ * held within the values that round to its level (docs/math.md 11), TV or TGV as the settings
+ * say with the defaults of PNG files (a gap per sample of 1e-4, 10000 iterations, TGV's ratio of
+ * the steps 0.3); an alpha is reconstructed apart, as one channel. The result is as
+ * unround_solve's: the picture, its planes and canvas, the records; no coefficients. */
+unround_status unround_b200_solve_samples(const uint16_t* levels, uint64_t rows, uint64_t columns, uint64_t channels,
+                                         int32_t bits, const unround_settings* settings, unround_observer observer,
+                                         void* user, unround_result** result, char* message, size_t message_size);
+
+/* The interval and centre of a level of `bits` bits as unround_b200_solve_samples models it
+ * (cpp/src/samples.cpp:86-105): ends[0] the least value held, ends[1] the greatest, ends[2] the
+ * level's centre; without a device. */
+unround_status unround_b200_sample_interval(uint32_t level, int32_t bits, double slack, double* ends, char* message,
+                                           size_t message_size);
+
 /* The blue-noise matrix of the ordered dither of 8- and 16-bit output (unround_pnm): 64 x 64
  * ranks, row by row, into `ranks` (4096 values, each of 0 .. 4095 once), made by the
  * void-and-cluster method as the reference's scripts/blue_noise.py makes the table of

@@ -18,6 +18,7 @@
 #include "blue_noise.hpp"
 #include "colour.hpp"
 #include "model.hpp"
+#include "samples_model.hpp"
 #include "settings.hpp"
 #include "solver.hpp"
 #include "unround.h"
@@ -801,6 +802,125 @@ unround_status unround_b200_solve_levels(const unround_input* input, const unrou
     solver.keep_result_on_device();
     if (!solver.solve(s.method, plan ? &*plan : nullptr, nullptr, nullptr, outcome, failure)) return false;
     return solver.levels(sixteen != 0, dither, levels, failure);
+  });
+}
+
+// A picture of rounded samples reconstructed (rust/unround/src/samples.rs; cpp/src/samples.cpp:
+// 344-405, samples::reconstruct without the file): the colours by TV or TGV within their
+// samples' intervals, an alpha (2 or 4 channels) apart, one channel, without channel weights.
+unround_status unround_b200_solve_samples(const uint16_t* levels, uint64_t rows, uint64_t columns, uint64_t channels,
+                                         int32_t bits, const unround_settings* settings, unround_observer observer,
+                                         void* user, unround_result** result, char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (levels == nullptr || settings == nullptr || result == nullptr) {
+      failure = {urb::kArgument, "the levels, the settings and the result are not null pointers"};
+      return false;
+    }
+    if (channels < 1 || channels > 4 || rows == 0 || columns == 0 || rows > (1u << 24) || columns > (1u << 24)) {
+      failure = {urb::kOptions, "a picture of " + std::to_string(rows) + " x " + std::to_string(columns) + " x " +
+                                    std::to_string(channels) + " samples: 1 to 4 channels, not empty"};
+      return false;
+    }
+    const urb::Settings& s = settings->settings;
+    if (!urb::check_samples_settings(s, failure)) return false;
+    const urb::DataTerm& term = s.data.front();
+    const double mu = term.mu ? *term.mu : 0.0;
+    const bool alpha = channels == 2 || channels == 4;
+    const std::size_t colours = alpha ? channels - 1 : channels;
+    auto colour_model = urb::make_samples_model(levels, rows, columns, channels, bits, 0, colours, term.slack, mu,
+                                                failure);
+    if (!colour_model) return false;
+    std::optional<urb::SamplesModel> alpha_model;
+    if (alpha) {
+      alpha_model = urb::make_samples_model(levels, rows, columns, channels, bits, colours, 1, term.slack, mu, failure);
+      if (!alpha_model) return false;
+    }
+    auto plan = urb::make_plan(s, colours, failure, urb::samples_plan_defaults());
+    if (!plan) return false;
+    urb::Settings alone = s;
+    alone.regularizer.channel_weights.clear();
+    std::optional<urb::Plan> alpha_plan;
+    if (alpha) {
+      alpha_plan = urb::make_plan(alone, 1, failure, urb::samples_plan_defaults());
+      if (!alpha_plan) return false;
+    }
+    if (!have_device(failure)) return false;
+    // The solvers' frame: the picture's size and colours, no components (the samples are the
+    // data term); the result's gets a component (with no blocks) per channel.
+    urb::Frame frame;
+    frame.height = static_cast<std::uint32_t>(rows);
+    frame.width = static_cast<std::uint32_t>(columns);
+    frame.rows = static_cast<std::uint32_t>(rows);
+    frame.columns = static_cast<std::uint32_t>(columns);
+    frame.color_space = colours == 3 ? 3 : 1;
+    urb::Observer watch;
+    if (observer != nullptr) {
+      watch = [&](const urb::Record& r, double gap, const double* canvas) {
+        unround_record raw{r.iteration, gap, r.primal, r.dual, colours, rows, columns, canvas};
+        return observer(user, &raw) != 0;
+      };
+    }
+    Stream stream;
+    if (stream.error != cudaSuccess) {
+      failure = {urb::kInternal, std::string("a CUDA stream: ") + cudaGetErrorString(stream.error)};
+      return false;
+    }
+    urb::Outcome outcome;
+    {
+      urb::Solver solver(frame, *colour_model, stream.stream);
+      if (!solver.solve(s.method, &*plan, nullptr, watch, outcome, failure)) return false;
+    }
+    if (!alpha) {
+      frame.components.resize(colours);
+      *result = result_of(std::move(frame), std::move(outcome));
+      return true;
+    }
+    urb::Frame alpha_frame = frame;
+    alpha_frame.color_space = 1;
+    urb::Outcome alpha_outcome;
+    {
+      urb::Solver solver(alpha_frame, *alpha_model, stream.stream);
+      if (!solver.solve(s.method, &*alpha_plan, nullptr, watch, alpha_outcome, failure)) return false;
+    }
+    // The colours' planes and the alpha's, and the picture interleaved, in one result.
+    const std::size_t plane = static_cast<std::size_t>(rows) * columns;
+    urb::Outcome merged;
+    merged.canvas.resize(channels * plane);
+    std::memcpy(merged.canvas.data(), outcome.canvas.data(), colours * plane * sizeof(double));
+    std::memcpy(merged.canvas.data() + colours * plane, alpha_outcome.canvas.data(), plane * sizeof(double));
+    merged.picture.resize(channels * plane);
+    for (std::size_t k = 0; k < plane; ++k) {
+      for (std::size_t c = 0; c < channels; ++c) merged.picture.data()[k * channels + c] = merged.canvas.data()[c * plane + k];
+    }
+    merged.records = std::move(outcome.records);
+    merged.iterations = outcome.iterations;
+    merged.stop = outcome.stop;
+    merged.solved = outcome.solved;
+    merged.tau = outcome.tau;
+    merged.sigma = outcome.sigma;
+    frame.components.resize(channels);
+    frame.color_space = colours == 3 ? 3 : 1;
+    *result = result_of(std::move(frame), std::move(merged));
+    return true;
+  });
+}
+
+unround_status unround_b200_sample_interval(uint32_t level, int32_t bits, double slack, double* ends, char* message,
+                                           size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (ends == nullptr) {
+      failure = {urb::kArgument, "the ends are a null pointer"};
+      return false;
+    }
+    if (bits < 1 || bits > 16 || level >= (1u << bits) || !(slack >= 0.0 && std::isfinite(slack))) {
+      failure = {urb::kOptions, "a level below 2^bits, bits 1 to 16, and a slack at least 0"};
+      return false;
+    }
+    const urb::SampleInterval made = urb::sample_interval(level, bits, slack);
+    ends[0] = made.lower;
+    ends[1] = made.upper;
+    ends[2] = made.centre;
+    return true;
   });
 }
 

@@ -219,6 +219,52 @@ struct LevelsParams {
 };
 bool prepare_levels();
 cudaError_t launch_levels(const LevelsParams& p, cudaStream_t stream);
+
+// Pictures of rounded samples (samples.cu): the primal step with its sample-by-sample proximal
+// map, G* at a field, and the start or the result canvas. Binary32 planes are pitched like the
+// state (channel-major); binary64 ones packed, channel-major, rows x columns each.
+struct SamplesPrimalParams {
+  Geometry g;
+  const float* x = nullptr;
+  const float* p1 = nullptr;
+  const float* p2 = nullptr;
+  float* xt = nullptr;
+  const float* lower = nullptr;  // the intervals and centres in binary32, pitched
+  const float* upper = nullptr;
+  const float* centre = nullptr;
+  const double* centre64 = nullptr;  // binary64, packed
+  float descent[kMaxChannels] = {};  // tau gamma_c
+  float t = 0.0f;                    // tau mu
+  float r = 1.0f;                    // 1 / (1 + tau mu)
+  double half_mu = 0.0;
+  double* partials = nullptr;  // with keep: mu/2 sum (x~ - c)^2, one per CTA
+};
+struct SamplesConjugateParams {
+  Geometry g;  // one channel's
+  const float* q1 = nullptr;
+  const float* q2 = nullptr;
+  double scale = 1.0;
+  double gamma = 1.0;
+  double mu = 0.0;
+  const double* lower64 = nullptr;  // the channel's, packed
+  const double* upper64 = nullptr;
+  const double* centre64 = nullptr;
+  double* partials = nullptr;  // one per CTA
+};
+struct SamplesCanvasParams {
+  Geometry g;
+  int mode = 0;  // 0: the start from the centres; 1: the result from x~
+  float* x = nullptr;
+  const float* xt = nullptr;
+  const double* lower64 = nullptr;
+  const double* upper64 = nullptr;
+  const double* centre64 = nullptr;
+  double* canvas = nullptr;  // C x rows x columns
+};
+int samples_grid_blocks(const Geometry& g, int channels);
+cudaError_t launch_samples_primal(const SamplesPrimalParams& p, bool keep, cudaStream_t stream);
+cudaError_t launch_samples_conjugate(const SamplesConjugateParams& p, cudaStream_t stream);
+cudaError_t launch_samples_canvas(const SamplesCanvasParams& p, cudaStream_t stream);
 // The kept coefficients (binary32, DC centred) as binary64 absolute coefficients.
 cudaError_t launch_restore(const ComponentDevice& c, double* out, cudaStream_t stream);
 cudaError_t launch_gradient(const float* x, float* w1, float* w2, const Geometry& g, cudaStream_t stream);

@@ -327,7 +327,8 @@ std::optional<Frame> make_frame(std::uint32_t height, std::uint32_t width, std::
   return frame;
 }
 
-std::optional<Plan> make_plan(const Settings& settings, std::size_t channels, Failure& failure) {
+std::optional<Plan> make_plan(const Settings& settings, std::size_t channels, Failure& failure,
+                              const PlanDefaults& defaults) {
   const Regularizer& reg = settings.regularizer;
   const PdhgOptions& o = settings.pdhg;
   const bool tv = settings.method == Method::tv;
@@ -357,12 +358,12 @@ std::optional<Plan> make_plan(const Settings& settings, std::size_t channels, Fa
   const double bound = tv ? 8.0 : (17.0 + std::sqrt(33.0)) / 2.0;
   const double norm_squared = o.norm_squared ? *o.norm_squared : bound * (largest * largest);
   const double weight = tv ? reg.alpha : reg.alpha1;
-  const double default_ratio = tv ? 10.0 : 3.0;
-  const double default_tolerance = tv ? 2e-4 : 2e-3;
+  const double default_ratio = tv ? defaults.tv_ratio : defaults.tgv_ratio;
+  const double default_tolerance = tv ? defaults.tv_tolerance : defaults.tgv_tolerance;
   const double ratio = o.step_ratio ? *o.step_ratio : o.weight_scaling ? default_ratio / (weight * weight)
                                                                         : default_ratio;
   plan.tolerance = o.tolerance ? *o.tolerance : o.weight_scaling ? default_tolerance * weight : default_tolerance;
-  plan.iterations = o.iterations ? *o.iterations : tv ? 5000u : 10000u;
+  plan.iterations = o.iterations ? *o.iterations : tv ? defaults.tv_iterations : defaults.tgv_iterations;
   const double product = o.step_product;
   plan.tau = std::sqrt((ratio * product) / norm_squared);
   plan.sigma = std::sqrt(product / (ratio * norm_squared));

@@ -122,7 +122,19 @@ struct Plan {
   double alpha0 = 2.0;
 };
 
-std::optional<Plan> make_plan(const Settings& settings, std::size_t channels, Failure& failure);
+// The defaults of a plan where the options give none: JPEG files' (cpp/include/unround/pdhg.hpp)
+// unless a caller gives others (pictures of rounded samples).
+struct PlanDefaults {
+  double tv_ratio = 10.0;
+  double tgv_ratio = 3.0;
+  double tv_tolerance = 2e-4;
+  double tgv_tolerance = 2e-3;
+  std::uint64_t tv_iterations = 5000;
+  std::uint64_t tgv_iterations = 10000;
+};
+
+std::optional<Plan> make_plan(const Settings& settings, std::size_t channels, Failure& failure,
+                              const PlanDefaults& defaults = PlanDefaults{});
 
 // The Laplace scale of a frequency from its counts (docs/math.md 2.1,
 // cpp/src/laplace.cpp:81-107), and delta / Q of a bin's mean (2.2, laplace.cpp:132-146).

@@ -1,6 +1,8 @@
 // The device solve. See solver.hpp.
 #include "solver.hpp"
 
+#include "samples_model.hpp"
+
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -71,6 +73,17 @@ struct Solver::Impl {
   bool planned = false;
   std::vector<double> host_partials;
   bool host_result = true;  // false: the result stays on the device (levels)
+  // A picture of rounded samples in place of a JPEG file's components (samples.cu): its
+  // intervals and centres, binary32 pitched for the iterations, binary64 packed for the
+  // records and the result.
+  const SamplesModel* samples = nullptr;
+  float* s_lower = nullptr;
+  float* s_upper = nullptr;
+  float* s_centre = nullptr;
+  double* s_lower64 = nullptr;
+  double* s_upper64 = nullptr;
+  double* s_centre64 = nullptr;
+  int samples_written = 0;  // the CTAs of the last kept primal step's sums of G
 
   Impl(const Frame& f, cudaStream_t s) : frame(f), stream(s) {}
 
@@ -138,9 +151,38 @@ struct Solver::Impl {
   }
 
   // Device copies of the model: levels, flat blocks, binary64 constants.
+  // The samples' intervals and centres on the device.
+  void setup_samples() {
+    const std::size_t n = g.plane * g.channels, packed = static_cast<std::size_t>(g.channels) * g.rows * g.columns;
+    s_lower64 = upload(samples->lower.data(), packed);
+    s_upper64 = upload(samples->upper.data(), packed);
+    s_centre64 = upload(samples->centre.data(), packed);
+    // Binary32 ends rounded inward (the result is clipped to the binary64 ones), pitched.
+    std::vector<float> lower(n, 0.0f), upper(n, 0.0f), centre(n, 0.0f);
+    for (int c = 0; c < g.channels; ++c) {
+      for (int i = 0; i < g.rows; ++i) {
+        for (int j = 0; j < g.columns; ++j) {
+          const std::size_t k = (static_cast<std::size_t>(c) * g.rows + i) * g.columns + j;
+          const std::size_t at = c * g.plane + static_cast<std::size_t>(i) * g.pitch + j;
+          float a = static_cast<float>(samples->lower[k]), b = static_cast<float>(samples->upper[k]);
+          if (static_cast<double>(a) < samples->lower[k]) a = std::nextafter(a, 256.0f);
+          if (static_cast<double>(b) > samples->upper[k]) b = std::nextafter(b, -1.0f);
+          lower[at] = a;
+          upper[at] = b;
+          centre[at] = static_cast<float>(samples->centre[k]);
+        }
+      }
+    }
+    s_lower = upload(lower.data(), n);
+    s_upper = upload(upper.data(), n);
+    s_centre = upload(centre.data(), n);
+    if (error == cudaSuccess) error = cudaStreamSynchronize(stream);  // the staged copies' sources
+  }
+
   void setup(bool with_tgv, bool solving = true) {
     tgv = with_tgv;
     const std::size_t n = g.plane * g.channels;
+    if (samples != nullptr) setup_samples();
     for (const Component& c : frame.components) {
       ComponentDevice d;
       d.block_rows = static_cast<int>(c.block_rows);
@@ -174,7 +216,7 @@ struct Solver::Impl {
     xt = allocate<float>(n);
     xts[0] = xt;
     xt_id = 0;
-    fusable = solving && fused_kernels() &&
+    fusable = solving && samples == nullptr && fused_kernels() &&
               iteration_takes(g, components.data(), static_cast<int>(components.size()));
     if (fusable) {
       xts[1] = allocate<float>(n);
@@ -206,6 +248,7 @@ struct Solver::Impl {
     if (with_tgv) div2 = allocate<float>(2 * n);
     canvas = allocate<double>(static_cast<std::size_t>(g.channels) * g.rows * g.columns);
     std::size_t most = 3u * norms_grid_blocks(g);
+    if (samples != nullptr) most = std::max<std::size_t>(most, samples_grid_blocks(g, g.channels));
     for (const ComponentDevice& d : components) {
       most = std::max<std::size_t>(most, conjugate_grid_blocks(g, d));
       most = std::max<std::size_t>(most, start_grid_blocks(d));
@@ -217,6 +260,7 @@ struct Solver::Impl {
     partials = allocate<double>(most);
     std::size_t values = 0;
     for (int count : value_counts) values += count;
+    if (samples != nullptr) values += samples_grid_blocks(g, g.channels);
     value_partials = allocate<double>(values);
     host_partials.resize(std::max(most, values));
   }
@@ -279,6 +323,7 @@ struct Solver::Impl {
   }
 
   double data_value() {
+    if (samples != nullptr) return sum_of(value_partials, samples_written);
     double total = 0.0;
     for (std::size_t c = 0; c < components.size(); ++c) total += sum_of(value_slot(c), value_written[c]);
     return total;
@@ -288,6 +333,17 @@ struct Solver::Impl {
   // coefficients), 128 past the blocks; w = grad x; the duals 0 or given, projected. The
   // start is the first tilde point.
   void start(const Start* given, bool for_solver) {
+    if (samples != nullptr) {
+      // The centres: x0 and the binary64 canvas; G there is 0.
+      SamplesCanvasParams sp;
+      sp.g = g;
+      sp.mode = 0;
+      sp.x = state[0].x;
+      sp.centre64 = s_centre64;
+      sp.canvas = canvas;
+      if (error == cudaSuccess) error = launch_samples_canvas(sp, stream);
+      samples_written = 0;
+    }
     for (std::size_t c = 0; c < components.size(); ++c) {
       StartParams sp;
       sp.component = components[c];
@@ -397,6 +453,28 @@ struct Solver::Impl {
   // The primal step of every component; the TMA path takes two components of the same cells
   // (Cb and Cr) in one launch.
   void primal(bool keep) {
+    if (samples != nullptr) {
+      const Fields& st = state[current];
+      SamplesPrimalParams sp;
+      sp.g = g;
+      sp.x = st.x;
+      sp.p1 = st.p1;
+      sp.p2 = st.p2;
+      sp.xt = xt;
+      sp.lower = s_lower;
+      sp.upper = s_upper;
+      sp.centre = s_centre;
+      sp.centre64 = s_centre64;
+      for (int c = 0; c < g.channels; ++c) sp.descent[c] = static_cast<float>(plan.tau * plan.channel_weights[c]);
+      const double t = plan.tau * samples->mu;
+      sp.t = static_cast<float>(t);
+      sp.r = static_cast<float>(1.0 / (1.0 + t));
+      sp.half_mu = 0.5 * samples->mu;
+      sp.partials = value_partials;
+      if (error == cudaSuccess) error = launch_samples_primal(sp, keep, stream);
+      if (keep) samples_written = samples_grid_blocks(g, g.channels);
+      return;
+    }
     for (std::size_t c = 0; c < components.size();) {
       if (!primal_swept[c]) {
         const PrimalParams pp = primal_params(c);
@@ -467,6 +545,23 @@ struct Solver::Impl {
 
   // G* of channel c at xi = gamma div(scale q) (cpp/src/frames.cpp:428-493).
   double conjugate(std::size_t c, const float* q1, const float* q2, double scale) {
+    if (samples != nullptr) {
+      SamplesConjugateParams sp;
+      sp.g = g;
+      sp.g.channels = 1;
+      sp.q1 = q1;
+      sp.q2 = q2;
+      sp.scale = scale;
+      sp.gamma = plan.channel_weights[c];
+      sp.mu = samples->mu;
+      const std::size_t packed = c * static_cast<std::size_t>(g.rows) * g.columns;
+      sp.lower64 = s_lower64 + packed;
+      sp.upper64 = s_upper64 + packed;
+      sp.centre64 = s_centre64 + packed;
+      sp.partials = partials;
+      if (error == cudaSuccess) error = launch_samples_conjugate(sp, stream);
+      return sum_of(partials, samples_grid_blocks(sp.g, 1));
+    }
     ConjugateParams cp;
     cp.g = g;
     cp.component = components[c];
@@ -480,6 +575,9 @@ struct Solver::Impl {
     if (error == cudaSuccess) error = launch_conjugate(cp, stream);
     return sum_of(partials, conjugate_grid_blocks(g, components[c]));
   }
+
+  // The channels of the data term: the components, or the samples' channels.
+  std::size_t data_channels() const { return samples != nullptr ? samples->channels : components.size(); }
 
   // The record of the tilde point (cpp/src/primal_dual.hpp:446-501).
   Record record(std::uint64_t iteration) {
@@ -501,7 +599,7 @@ struct Solver::Impl {
     if (!tgv) {
       r.primal = plan.alpha * first + data;
       double conjugates = 0.0;
-      for (std::size_t c = 0; c < components.size(); ++c) {
+      for (std::size_t c = 0; c < data_channels(); ++c) {
         conjugates += conjugate(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0);
       }
       r.dual = -conjugates;
@@ -513,14 +611,14 @@ struct Solver::Impl {
     const double theta = most > plan.alpha1 ? plan.alpha1 / most : 1.0;
     r.scaling = theta;
     double conjugates = 0.0;
-    for (std::size_t c = 0; c < components.size(); ++c) {
+    for (std::size_t c = 0; c < data_channels(); ++c) {
       const std::size_t base = 2 * c * g.plane;
       conjugates += conjugate(c, div2 + base, div2 + base + g.plane, -theta);
     }
     r.dual = -conjugates;
     if (plan.partial_radius) {
       double partial = 0.0, residual = 0.0;
-      for (std::size_t c = 0; c < components.size(); ++c) {
+      for (std::size_t c = 0; c < data_channels(); ++c) {
         partial += conjugate(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0);
         ResidualParams rp;
         rp.g = g;
@@ -541,6 +639,17 @@ struct Solver::Impl {
   // coefficients are zeta).
   void result(Outcome& out) {
     const std::size_t size = static_cast<std::size_t>(g.rows) * g.columns;
+    if (samples != nullptr) {
+      // The last tilde point in binary64, each sample clipped to its interval.
+      SamplesCanvasParams sp;
+      sp.g = g;
+      sp.mode = 1;
+      sp.xt = xt;
+      sp.lower64 = s_lower64;
+      sp.upper64 = s_upper64;
+      sp.canvas = canvas;
+      if (error == cudaSuccess) error = launch_samples_canvas(sp, stream);
+    }
     for (std::size_t c = 0; c < components.size(); ++c) {
       if (error == cudaSuccess) error = launch_restore(components[c], coefficients[c], stream);
       CanvasParams cp;
@@ -640,9 +749,21 @@ Solver::Solver(const Frame& frame, cudaStream_t stream) : impl_(std::make_unique
   impl_->g = geometry_;
 }
 
+Solver::Solver(const Frame& frame, const SamplesModel& samples, cudaStream_t stream)
+    : impl_(std::make_unique<Impl>(frame, stream)) {
+  geometry_.rows = static_cast<int>(samples.rows);
+  geometry_.columns = static_cast<int>(samples.columns);
+  geometry_.pitch = static_cast<int>((samples.columns + 31) / 32 * 32);
+  geometry_.channels = static_cast<int>(samples.channels);
+  geometry_.plane = static_cast<std::size_t>(geometry_.rows) * geometry_.pitch;
+  impl_->g = geometry_;
+  impl_->samples = &samples;
+}
+
 Solver::~Solver() = default;
 
 int Solver::launches_per_iteration() const {
+  if (impl_->samples != nullptr) return 2;
   return impl_->fusable ? 1 : 1 + static_cast<int>(impl_->components.size());
 }
 

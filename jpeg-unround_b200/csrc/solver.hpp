@@ -63,9 +63,14 @@ struct Outcome {
 // (C x rows x columns binary64, valid for the call); true stops the solver.
 using Observer = std::function<bool(const Record&, double gap, const double* canvas)>;
 
+struct SamplesModel;
+
 class Solver {
  public:
   Solver(const Frame& frame, cudaStream_t stream);
+  // A picture of rounded samples (samples_model.hpp): `frame` gives only its size and colour
+  // space (no components); the model outlives the solver.
+  Solver(const Frame& frame, const SamplesModel& samples, cudaStream_t stream);
   ~Solver();
   Solver(const Solver&) = delete;
   Solver& operator=(const Solver&) = delete;

@@ -209,6 +209,7 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_bytes_free": (None, ctypes.POINTER(ctypes.c_uint8), u64),
         "unround_b200_solve_levels": (i32, ctypes.POINTER(_Input), handle, i32, i32, ctypes.c_void_p, u64, u64p,
                                       *text),
+        "unround_b200_solve_samples": (i32, ctypes.POINTER(ctypes.c_uint16), u64, u64, u64, i32, handle, *made),
         "unround_b200_solve_from": (i32, ctypes.POINTER(_Input), handle, ctypes.POINTER(_Start), *made),
         "unround_b200_measure": (i32, ctypes.POINTER(_Input), handle, u64, u64, ctypes.POINTER(_Timing),
                                  ctypes.POINTER(handle), *text),
@@ -797,3 +798,28 @@ def solve_levels(image: jpegio.Image, settings: Settings | list[str] | None = No
     if sixteen:
         out = out.byteswap()  # the interface's most significant byte first
     return out[:, :, 0] if channels == 1 else out
+
+
+def solve_samples(levels: npt.ArrayLike, bits: int = 8, settings: Settings | list[str] | None = None) -> Decoded:
+    """A picture of rounded samples -- a PNG file's levels, (height, width) grey or (height, width,
+    channels) with 2 to 4 channels (an alpha last) -- reconstructed on the GPU within the
+    intervals of its samples (include/unround_b200.h, unround_b200_solve_samples; docs/math.md
+    11): TV or TGV as the settings say, with the defaults of PNG files."""
+    values = np.ascontiguousarray(levels, dtype=np.uint16)
+    if values.ndim == 2:
+        values = values[:, :, np.newaxis]
+    if values.ndim != 3:
+        raise ValueError(f"levels are (height, width) or (height, width, channels), not {values.shape}")
+    library = _library()
+    handle = _settings_of(settings)
+    result = ctypes.c_void_p()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    rows, columns, channels = values.shape
+    status = library.unround_b200_solve_samples(values.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), rows, columns,
+                                                channels, int(bits), handle.handle, _OBSERVER(), None,
+                                                ctypes.byref(result), message, _MESSAGE)
+    _raise(status, message)
+    try:
+        return _decoded(library, result, problems=False)
+    finally:
+        library.unround_result_free(result)
