@@ -352,6 +352,84 @@ def _mix_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     print(json.dumps(line))
 
 
+SAMPLES_BYTES = 18.0  # the samples' primal step: x, p1, p2 and the 16-bit level read, x~ written
+
+
+def _samples_arm(args: argparse.Namespace, rank: int, world: int) -> None:
+    """Pictures of rounded samples (the PNG path, unround_b200_solve_samples): the bench's
+    4032x3024 colour picture as 8-bit RGB levels, TGV (alpha1 1, alpha0 2), 500 iterations.
+    value: the iteration loop's device time (unround_b200_measure_samples, CUDA events); e2e:
+    the C call with host levels in and the binary64 result out; roofline: the dual sweep and
+    the samples' primal step, each against its algorithmic bytes."""
+    import ctypes
+
+    import numpy as np
+
+    from unround import native, synthetic
+    from unround.sharding import max_over_ranks
+
+    rgb = synthetic.colour(HEIGHT, WIDTH, quality=75, seed=rank, noise=3.0).samples
+    levels = np.ascontiguousarray(np.clip(np.rint(rgb), 0, 255).astype(np.uint16))
+    options = [*OPTIONS[:6], "--iterations", str(ITERATIONS), "--tolerance", "0", "--record-every", "0"]
+    with Clocks(0) as clocks:
+        timing = native.measure_samples(levels, 8, options, warmup=max(3, args.warmup) * 10,
+                                        iterations=args.steps * ITERATIONS)
+    seconds = max_over_ranks(timing.milliseconds / 1e3)
+    pixels = timing.pixels
+    value = world * pixels * args.steps * ITERATIONS / seconds / 1e6
+    library = native._library()
+    settings = native._Settings(options)
+
+    def call() -> int:
+        result = ctypes.c_void_p()
+        message = ctypes.create_string_buffer(4096)
+        status = library.unround_b200_solve_samples(levels.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), HEIGHT,
+                                                    WIDTH, 3, 8, settings.handle, native._OBSERVER(), None,
+                                                    ctypes.byref(result), message, 4096)
+        if status != 0:
+            raise RuntimeError(message.value.decode())
+        try:
+            c, h, w = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+            pointer = library.unround_result_picture(result, ctypes.byref(h), ctypes.byref(w), ctypes.byref(c))
+            picture = np.ctypeslib.as_array(pointer, shape=(h.value * w.value * c.value,))
+            if not np.isfinite(picture[:: max(1, picture.size // 4096)]).all():
+                raise RuntimeError("the result holds values that are not finite")
+            return 2 * picture.nbytes  # the canvas and the interleaved picture
+        finally:
+            library.unround_result_free(result)
+
+    call()  # warm the call path
+    began = time.perf_counter()
+    for _ in range(args.steps):
+        d2h = call()
+    e2e_seconds = max_over_ranks(time.perf_counter() - began)
+    peak, peak_kind = _peaks()
+    dual = DUAL_BYTES * timing.samples / (timing.dual_milliseconds / 1e3) / 1e9
+    primal = SAMPLES_BYTES * timing.samples / (timing.primal_milliseconds / 1e3) / 1e9
+    iteration = (DUAL_BYTES + SAMPLES_BYTES) * timing.samples / (seconds / (args.steps * ITERATIONS)) / 1e9
+    if rank != 0:
+        return
+    line = {
+        "metric": "TGV PDHG of rounded samples Mpx*iter/s on 1 B200 (4032x3024 RGB 8-bit, 500 iterations)",
+        "value": value, "unit": "Mpx*iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": seconds / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (the bench's colour picture, RGB, 8-bit levels)",
+        "config": {"workload": "samples-rgb8-4032x3024", "iterations_per_step": ITERATIONS, "alpha1": 1.0,
+                   "alpha0": 2.0, "samples": timing.samples, "l2": "state larger than L2, no flush"},
+        "roofline": {"bound": "hbm", "kernel": "dual_kernel<tgv,3,coupled>", "achieved": dual, "peak": peak,
+                     "unit": "GB/s", "frac": dual / peak, "peak_kind": peak_kind,
+                     "samples_primal_achieved": primal, "samples_primal_frac": primal / peak,
+                     "samples_primal_bytes_per_sample": SAMPLES_BYTES, "iteration_achieved": iteration,
+                     "iteration_frac": iteration / peak, "dual_ms": timing.dual_milliseconds,
+                     "primal_ms": timing.primal_milliseconds},
+        "e2e": {"value": world * pixels * args.steps * ITERATIONS / e2e_seconds / 1e6, "unit": "Mpx*iter/s",
+                "h2d_bytes_per_step": int(levels.nbytes), "d2h_bytes_per_step": d2h},
+        "gpu_launches": timing.launches_per_iteration * args.steps * ITERATIONS,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
 LARGE_OPTIONS = ["--method", "tgv", "--alpha1", "1.5", "--alpha0", "3", "--iterations", "1000", "--tolerance", "0",
                  "--record-every", "50"]
 
@@ -533,7 +611,7 @@ def main() -> None:
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--height", type=int, default=HEIGHT, help="a smaller picture for profiling")
     parser.add_argument("--width", type=int, default=WIDTH)
-    parser.add_argument("--workload", default="tgv-colour", choices=["tgv-colour", "mix", "unrolled", "large"],
+    parser.add_argument("--workload", default="tgv-colour", choices=["tgv-colour", "mix", "unrolled", "large", "samples"],
                         help="mix: the batched solve of 64 uneven pictures against image-at-a-time launches; "
                              "unrolled: the differentiable unrolled TGV solve, forward and forward+adjoint")
     parser.add_argument("--pictures", type=int, default=64, help="pictures of the mix")
@@ -553,6 +631,9 @@ def main() -> None:
         return
     if args.workload == "large":
         _large_arm(args, rank, world)
+        return
+    if args.workload == "samples":
+        _samples_arm(args, rank, world)
         return
     group = None
     if world > 1:

@@ -136,6 +136,14 @@ unround_status unround_b200_solve_samples(const uint16_t* levels, uint64_t rows,
                                          int32_t bits, const unround_settings* settings, unround_observer observer,
                                          void* user, unround_result** result, char* message, size_t message_size);
 
+/* unround_b200_measure for pictures of rounded samples (grey or RGB levels): the iteration loop
+ * alone, `warmup` iterations and then `iterations` timed by CUDA events, and the dual and primal
+ * steps timed apart. */
+unround_status unround_b200_measure_samples(const uint16_t* levels, uint64_t rows, uint64_t columns, uint64_t channels,
+                                           int32_t bits, const unround_settings* settings, uint64_t warmup,
+                                           uint64_t iterations, unround_b200_timing* timing, char* message,
+                                           size_t message_size);
+
 /* The interval and centre of a level of `bits` bits as unround_b200_solve_samples models it
  * (cpp/src/samples.cpp:86-105): ends[0] the least value held, ends[1] the greatest, ends[2] the
  * level's centre; without a device. */

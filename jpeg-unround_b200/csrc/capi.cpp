@@ -905,6 +905,63 @@ unround_status unround_b200_solve_samples(const uint16_t* levels, uint64_t rows,
   });
 }
 
+unround_status unround_b200_measure_samples(const uint16_t* levels, uint64_t rows, uint64_t columns, uint64_t channels,
+                                           int32_t bits, const unround_settings* settings, uint64_t warmup,
+                                           uint64_t iterations, unround_b200_timing* timing, char* message,
+                                           size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (levels == nullptr || settings == nullptr || timing == nullptr) {
+      failure = {urb::kArgument, "the levels, the settings and the timing are not null pointers"};
+      return false;
+    }
+    if (channels != 1 && channels != 3) {
+      failure = {urb::kOptions, "the measurement takes grey or RGB levels (1 or 3 channels)"};
+      return false;
+    }
+    const urb::Settings& s = settings->settings;
+    if (!urb::check_samples_settings(s, failure)) return false;
+    const urb::DataTerm& term = s.data.front();
+    auto model = urb::make_samples_model(levels, rows, columns, channels, bits, 0, channels, term.slack,
+                                         term.mu ? *term.mu : 0.0, failure);
+    if (!model) return false;
+    auto plan = urb::make_plan(s, channels, failure, urb::samples_plan_defaults());
+    if (!plan) return false;
+    if (!have_device(failure)) return false;
+    urb::Frame frame;
+    frame.height = frame.rows = static_cast<std::uint32_t>(rows);
+    frame.width = frame.columns = static_cast<std::uint32_t>(columns);
+    frame.color_space = channels == 3 ? 3 : 1;
+    Stream stream;
+    urb::Solver solver(frame, *model, stream.stream);
+    if (!solver.prepare(*plan, failure)) return false;
+    if (warmup > 0 && !solver.iterate(warmup, failure)) return false;
+    cudaEvent_t begin, end;
+    cudaEventCreate(&begin);
+    cudaEventCreate(&end);
+    cudaStreamSynchronize(stream.stream);
+    cudaEventRecord(begin, stream.stream);
+    const bool ok = solver.iterate(iterations, failure);
+    cudaEventRecord(end, stream.stream);
+    cudaEventSynchronize(end);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, begin, end);
+    cudaEventDestroy(begin);
+    cudaEventDestroy(end);
+    if (!ok) return false;
+    double dual_ms = 0.0, primal_ms = 0.0;
+    if (!solver.breakdown(20, dual_ms, primal_ms, failure)) return false;
+    timing->milliseconds = ms;
+    timing->dual_milliseconds = dual_ms;
+    timing->primal_milliseconds = primal_ms;
+    timing->iterations = iterations;
+    timing->launches_per_iteration = static_cast<std::uint64_t>(solver.launches_per_iteration());
+    timing->samples = channels * rows * columns;
+    timing->pixels = rows * columns;
+    timing->device_bytes = solver.device_bytes();
+    return true;
+  });
+}
+
 unround_status unround_b200_sample_interval(uint32_t level, int32_t bits, double slack, double* ends, char* message,
                                            size_t message_size) {
   return guarded(message, message_size, [&](urb::Failure& failure) {

@@ -221,18 +221,33 @@ bool prepare_levels();
 cudaError_t launch_levels(const LevelsParams& p, cudaStream_t stream);
 
 // Pictures of rounded samples (samples.cu): the primal step with its sample-by-sample proximal
-// map, G* at a field, and the start or the result canvas. Binary32 planes are pitched like the
-// state (channel-major); binary64 ones packed, channel-major, rows x columns each.
+// map, G* at a field, and the start or the result canvas. A sample's level (16 bits) sits in a
+// plane pitched like the state (channel-major); its interval and centre are looked up by level
+// in a table, in binary32 (the ends rounded inward, the centre to nearest) for the iterations
+// and in binary64 for the records and the result. Binary64 canvases are packed, channel-major,
+// rows x columns each.
+struct alignas(16) SampleEnds32 {
+  float lower, upper, centre, unused;
+};
+struct alignas(32) SampleEnds64 {
+  double lower, upper, centre, unused;
+};
+struct SamplesLevelsParams {
+  Geometry g;
+  const std::uint16_t* source = nullptr;  // rows x columns x stride, interleaved
+  int stride = 1;
+  int first = 0;
+  std::uint16_t* levels = nullptr;  // the channels' planes, pitched
+};
 struct SamplesPrimalParams {
   Geometry g;
   const float* x = nullptr;
   const float* p1 = nullptr;
   const float* p2 = nullptr;
   float* xt = nullptr;
-  const float* lower = nullptr;  // the intervals and centres in binary32, pitched
-  const float* upper = nullptr;
-  const float* centre = nullptr;
-  const double* centre64 = nullptr;  // binary64, packed
+  const std::uint16_t* levels = nullptr;
+  const SampleEnds32* ends = nullptr;
+  const SampleEnds64* ends64 = nullptr;
   float descent[kMaxChannels] = {};  // tau gamma_c
   float t = 0.0f;                    // tau mu
   float r = 1.0f;                    // 1 / (1 + tau mu)
@@ -246,9 +261,8 @@ struct SamplesConjugateParams {
   double scale = 1.0;
   double gamma = 1.0;
   double mu = 0.0;
-  const double* lower64 = nullptr;  // the channel's, packed
-  const double* upper64 = nullptr;
-  const double* centre64 = nullptr;
+  const std::uint16_t* levels = nullptr;  // the channel's plane
+  const SampleEnds64* ends64 = nullptr;
   double* partials = nullptr;  // one per CTA
 };
 struct SamplesCanvasParams {
@@ -256,15 +270,15 @@ struct SamplesCanvasParams {
   int mode = 0;  // 0: the start from the centres; 1: the result from x~
   float* x = nullptr;
   const float* xt = nullptr;
-  const double* lower64 = nullptr;
-  const double* upper64 = nullptr;
-  const double* centre64 = nullptr;
+  const std::uint16_t* levels = nullptr;
+  const SampleEnds64* ends64 = nullptr;
   double* canvas = nullptr;  // C x rows x columns
 };
 int samples_grid_blocks(const Geometry& g, int channels);
 cudaError_t launch_samples_primal(const SamplesPrimalParams& p, bool keep, cudaStream_t stream);
 cudaError_t launch_samples_conjugate(const SamplesConjugateParams& p, cudaStream_t stream);
 cudaError_t launch_samples_canvas(const SamplesCanvasParams& p, cudaStream_t stream);
+cudaError_t launch_samples_levels(const SamplesLevelsParams& p, cudaStream_t stream);
 // The kept coefficients (binary32, DC centred) as binary64 absolute coefficients.
 cudaError_t launch_restore(const ComponentDevice& c, double* out, cudaStream_t stream);
 cudaError_t launch_gradient(const float* x, float* w1, float* w2, const Geometry& g, cudaStream_t stream);

@@ -13,9 +13,13 @@
 //                             max(xi a, xi b) at mu = 0 (samples.cpp:205-227), in binary64
 //   samples_canvas_kernel     the start (x = c in binary32 and the binary64 canvas of the
 //                             centres), or the result: x~ in binary64, clipped to its interval
+//   samples_levels_kernel     the levels of the picture's channels, interleaved as given, into
+//                             planes pitched like the state
 //
 // A thread per sample, CTAs of 32 x 8 samples of one channel; binary32 iterations, binary64
-// records and result, as the JPEG path.
+// records and result, as the JPEG path. A sample's ends and centre come from a table indexed
+// by its level (2^bits entries: 4 KB at 8 bits, read through L1), so the primal step moves
+// 18 bytes a sample: x, p1, p2 and the level read, x~ written.
 #include "kernels.hpp"
 
 namespace urb {
@@ -41,10 +45,20 @@ __device__ __forceinline__ void block_sum(double value, double* out) {
   }
 }
 
+// descent[c] by a chain of selects: indexing the parameter array with a register would copy
+// the whole parameter block to local memory, thread by thread.
+__device__ __forceinline__ float descent_of(const SamplesPrimalParams& P, int c) {
+  float d = P.descent[0];
+#pragma unroll
+  for (int k = 1; k < kMaxChannels; ++k) d = c == k ? P.descent[k] : d;
+  return d;
+}
+
 template <bool KEEP>
 __global__ void __launch_bounds__(256) samples_primal_kernel(const SamplesPrimalParams P) {
   const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, c = blockIdx.z;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
+  const float descent = descent_of(P, c);
   double term = 0.0;
   if (i < rows && j < columns) {
     const std::size_t at = c * P.g.plane + static_cast<std::size_t>(i) * pitch + j;
@@ -54,12 +68,13 @@ __global__ void __launch_bounds__(256) samples_primal_kernel(const SamplesPrimal
     // div p = dy' p2 + dx' p1, backward differences with Neumann ends.
     const float dy = (i + 1 < rows ? p2 : 0.0f) - (i > 0 ? above : 0.0f);
     const float dx = (j + 1 < columns ? p1 : 0.0f) - (j > 0 ? before : 0.0f);
-    const float v = P.x[at] + P.descent[c] * (dy + dx);
-    const float z = fminf(fmaxf((v + P.t * P.centre[at]) * P.r, P.lower[at]), P.upper[at]);
+    const float v = P.x[at] + descent * (dy + dx);
+    const unsigned level = P.levels[at];
+    const float4 ends = __ldg(reinterpret_cast<const float4*>(P.ends) + level);  // lower, upper, centre
+    const float z = fminf(fmaxf((v + P.t * ends.z) * P.r, ends.x), ends.y);
     P.xt[at] = z;
     if constexpr (KEEP) {
-      const std::size_t k = (static_cast<std::size_t>(c) * rows + i) * columns + j;
-      const double away = static_cast<double>(z) - P.centre64[k];
+      const double away = static_cast<double>(z) - P.ends64[level].centre;
       term = P.half_mu * (away * away);
     }
   }
@@ -77,8 +92,8 @@ __global__ void __launch_bounds__(256) samples_conjugate_kernel(const SamplesCon
     const double dy = (i + 1 < rows ? q_at(P.q2, i, j) : 0.0) - (i > 0 ? q_at(P.q2, i - 1, j) : 0.0);
     const double dx = (j + 1 < columns ? q_at(P.q1, i, j) : 0.0) - (j > 0 ? q_at(P.q1, i, j - 1) : 0.0);
     const double s = P.gamma * (dy + dx);
-    const std::size_t k = static_cast<std::size_t>(i) * columns + j;
-    const double low = P.lower64[k], high = P.upper64[k], centre = P.centre64[k], m = P.mu;
+    const SampleEnds64& ends = P.ends64[P.levels[static_cast<std::size_t>(i) * pitch + j]];
+    const double low = ends.lower, high = ends.upper, centre = ends.centre, m = P.mu;
     if (m > 0.0) {
       const double best = fmin(fmax(centre + s / m, low), high);
       const double away = best - centre;
@@ -95,12 +110,20 @@ __global__ void __launch_bounds__(256) samples_canvas_kernel(const SamplesCanvas
   if (i >= P.g.rows || j >= P.g.columns) return;
   const std::size_t at = c * P.g.plane + static_cast<std::size_t>(i) * P.g.pitch + j;
   const std::size_t k = (static_cast<std::size_t>(c) * P.g.rows + i) * P.g.columns + j;
+  const SampleEnds64& ends = P.ends64[P.levels[at]];
   if (P.mode == 0) {
-    P.x[at] = static_cast<float>(P.centre64[k]);
-    P.canvas[k] = P.centre64[k];
+    P.x[at] = static_cast<float>(ends.centre);
+    P.canvas[k] = ends.centre;
   } else {
-    P.canvas[k] = fmin(fmax(static_cast<double>(P.xt[at]), P.lower64[k]), P.upper64[k]);
+    P.canvas[k] = fmin(fmax(static_cast<double>(P.xt[at]), ends.lower), ends.upper);
   }
+}
+
+__global__ void __launch_bounds__(256) samples_levels_kernel(const SamplesLevelsParams P) {
+  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, c = blockIdx.z;
+  if (i >= P.g.rows || j >= P.g.columns) return;
+  const std::size_t from = (static_cast<std::size_t>(i) * P.g.columns + j) * P.stride + P.first + c;
+  P.levels[c * P.g.plane + static_cast<std::size_t>(i) * P.g.pitch + j] = P.source[from];
 }
 
 dim3 sample_grid(const Geometry& g, int channels) {
@@ -131,6 +154,11 @@ cudaError_t launch_samples_conjugate(const SamplesConjugateParams& p, cudaStream
 
 cudaError_t launch_samples_canvas(const SamplesCanvasParams& p, cudaStream_t stream) {
   samples_canvas_kernel<<<sample_grid(p.g, p.g.channels), dim3(32, 8), 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_samples_levels(const SamplesLevelsParams& p, cudaStream_t stream) {
+  samples_levels_kernel<<<sample_grid(p.g, p.g.channels), dim3(32, 8), 0, stream>>>(p);
   return cudaGetLastError();
 }
 

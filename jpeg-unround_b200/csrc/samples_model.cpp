@@ -97,30 +97,28 @@ std::optional<SamplesModel> make_samples_model(const std::uint16_t* levels, std:
     return std::nullopt;
   }
   const std::size_t level_count = std::size_t{1} << bits;
-  std::vector<SampleInterval> table(level_count);
-  for (std::size_t v = 0; v < level_count; ++v) table[v] = sample_interval(static_cast<std::uint32_t>(v), bits, slack);
+  const std::size_t plane = rows * columns;
+  std::uint16_t highest = 0;
+  for (std::size_t k = 0; k < plane; ++k) {
+    const std::uint16_t* sample = levels + k * channels + first;
+    for (std::size_t c = 0; c < count; ++c) highest = sample[c] > highest ? sample[c] : highest;
+  }
+  if (highest >= level_count) {
+    failure = {kOptions, "a level of " + std::to_string(bits) + " bits is below 2^" + std::to_string(bits)};
+    return std::nullopt;
+  }
   SamplesModel model;
   model.rows = rows;
   model.columns = columns;
   model.channels = count;
   model.bits = bits;
   model.mu = mu;
-  const std::size_t plane = rows * columns;
-  model.lower.resize(count * plane);
-  model.upper.resize(count * plane);
-  model.centre.resize(count * plane);
-  for (std::size_t c = 0; c < count; ++c) {
-    for (std::size_t k = 0; k < plane; ++k) {
-      const std::uint16_t level = levels[k * channels + first + c];
-      if (level >= level_count) {
-        failure = {kOptions, "a level of " + std::to_string(bits) + " bits is below 2^" + std::to_string(bits)};
-        return std::nullopt;
-      }
-      const SampleInterval& ends = table[level];
-      model.lower[c * plane + k] = ends.lower;
-      model.upper[c * plane + k] = ends.upper;
-      model.centre[c * plane + k] = ends.centre;
-    }
+  model.levels = levels;
+  model.stride = channels;
+  model.first = first;
+  model.intervals.resize(level_count);
+  for (std::size_t v = 0; v < level_count; ++v) {
+    model.intervals[v] = sample_interval(static_cast<std::uint32_t>(v), bits, slack);
   }
   return model;
 }

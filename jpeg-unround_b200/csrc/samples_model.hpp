@@ -5,7 +5,8 @@
 // rounded inward -- the lower one up to the least double at or above it, the upper one down to
 // the greatest double below it; with a slack in levels, max(0, ((v - 1/2) - slack) s) and
 // min(255, ((v + 1/2) + slack) s) in floating point with s the nearest double. The centre is
-// the double nearest to v s. Channel-major planes, rows x columns each, in binary64.
+// the double nearest to v s. The model is the levels themselves and a table of the 2^b
+// intervals: the device expands neither, each kernel looks a sample's ends up by its level.
 #pragma once
 
 #include <cstddef>
@@ -31,11 +32,16 @@ struct SamplesModel {
   std::size_t rows = 0, columns = 0, channels = 0;
   int bits = 8;
   double mu = 0.0;
-  std::vector<double> lower, upper, centre;  // channels x rows x columns
+  // Borrowed: rows x columns x stride levels interleaved, of which channels first ..
+  // first + channels - 1 are the model's. They outlive the model's use.
+  const std::uint16_t* levels = nullptr;
+  std::size_t stride = 1, first = 0;
+  std::vector<SampleInterval> intervals;  // one per level, 2^bits
 };
 
 // The model of channels first .. first + count - 1 of levels (rows x columns x `channels`
-// interleaved) of `bits` bits, with a slack and mu at least 0 (cpp/src/samples.cpp:107-151).
+// interleaved) of `bits` bits, with a slack and mu at least 0 (cpp/src/samples.cpp:107-151):
+// every level of those channels below 2^bits, the table of their intervals.
 std::optional<SamplesModel> make_samples_model(const std::uint16_t* levels, std::size_t rows, std::size_t columns,
                                                std::size_t channels, int bits, std::size_t first, std::size_t count,
                                                double slack, double mu, Failure& failure);

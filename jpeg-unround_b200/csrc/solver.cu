@@ -77,12 +77,9 @@ struct Solver::Impl {
   // intervals and centres, binary32 pitched for the iterations, binary64 packed for the
   // records and the result.
   const SamplesModel* samples = nullptr;
-  float* s_lower = nullptr;
-  float* s_upper = nullptr;
-  float* s_centre = nullptr;
-  double* s_lower64 = nullptr;
-  double* s_upper64 = nullptr;
-  double* s_centre64 = nullptr;
+  std::uint16_t* s_levels = nullptr;  // the channels' levels, pitched like the state
+  SampleEnds32* s_ends = nullptr;       // per level: binary32 ends rounded inward, the centre
+  SampleEnds64* s_ends64 = nullptr;     // per level: binary64 ends and centre
   int samples_written = 0;  // the CTAs of the last kept primal step's sums of G
 
   Impl(const Frame& f, cudaStream_t s) : frame(f), stream(s) {}
@@ -153,29 +150,27 @@ struct Solver::Impl {
   // Device copies of the model: levels, flat blocks, binary64 constants.
   // The samples' intervals and centres on the device.
   void setup_samples() {
-    const std::size_t n = g.plane * g.channels, packed = static_cast<std::size_t>(g.channels) * g.rows * g.columns;
-    s_lower64 = upload(samples->lower.data(), packed);
-    s_upper64 = upload(samples->upper.data(), packed);
-    s_centre64 = upload(samples->centre.data(), packed);
-    // Binary32 ends rounded inward (the result is clipped to the binary64 ones), pitched.
-    std::vector<float> lower(n, 0.0f), upper(n, 0.0f), centre(n, 0.0f);
-    for (int c = 0; c < g.channels; ++c) {
-      for (int i = 0; i < g.rows; ++i) {
-        for (int j = 0; j < g.columns; ++j) {
-          const std::size_t k = (static_cast<std::size_t>(c) * g.rows + i) * g.columns + j;
-          const std::size_t at = c * g.plane + static_cast<std::size_t>(i) * g.pitch + j;
-          float a = static_cast<float>(samples->lower[k]), b = static_cast<float>(samples->upper[k]);
-          if (static_cast<double>(a) < samples->lower[k]) a = std::nextafter(a, 256.0f);
-          if (static_cast<double>(b) > samples->upper[k]) b = std::nextafter(b, -1.0f);
-          lower[at] = a;
-          upper[at] = b;
-          centre[at] = static_cast<float>(samples->centre[k]);
-        }
-      }
+    const std::size_t count = samples->intervals.size();
+    std::vector<SampleEnds32> ends(count);
+    std::vector<SampleEnds64> ends64(count);
+    for (std::size_t v = 0; v < count; ++v) {
+      // Binary32 ends rounded inward (the result is clipped to the binary64 ones).
+      const SampleInterval& e = samples->intervals[v];
+      float a = static_cast<float>(e.lower), b = static_cast<float>(e.upper);
+      if (static_cast<double>(a) < e.lower) a = std::nextafter(a, 256.0f);
+      if (static_cast<double>(b) > e.upper) b = std::nextafter(b, -1.0f);
+      ends[v] = SampleEnds32{a, b, static_cast<float>(e.centre), 0.0f};
+      ends64[v] = SampleEnds64{e.lower, e.upper, e.centre, 0.0};
     }
-    s_lower = upload(lower.data(), n);
-    s_upper = upload(upper.data(), n);
-    s_centre = upload(centre.data(), n);
+    s_ends = upload(ends.data(), count);
+    s_ends64 = upload(ends64.data(), count);
+    SamplesLevelsParams lp;
+    lp.g = g;
+    lp.source = upload(samples->levels, samples->rows * samples->columns * samples->stride);
+    lp.stride = static_cast<int>(samples->stride);
+    lp.first = static_cast<int>(samples->first);
+    lp.levels = s_levels = allocate<std::uint16_t>(g.plane * g.channels);
+    if (error == cudaSuccess) error = launch_samples_levels(lp, stream);
     if (error == cudaSuccess) error = cudaStreamSynchronize(stream);  // the staged copies' sources
   }
 
@@ -339,7 +334,8 @@ struct Solver::Impl {
       sp.g = g;
       sp.mode = 0;
       sp.x = state[0].x;
-      sp.centre64 = s_centre64;
+      sp.levels = s_levels;
+      sp.ends64 = s_ends64;
       sp.canvas = canvas;
       if (error == cudaSuccess) error = launch_samples_canvas(sp, stream);
       samples_written = 0;
@@ -461,10 +457,9 @@ struct Solver::Impl {
       sp.p1 = st.p1;
       sp.p2 = st.p2;
       sp.xt = xt;
-      sp.lower = s_lower;
-      sp.upper = s_upper;
-      sp.centre = s_centre;
-      sp.centre64 = s_centre64;
+      sp.levels = s_levels;
+      sp.ends = s_ends;
+      sp.ends64 = s_ends64;
       for (int c = 0; c < g.channels; ++c) sp.descent[c] = static_cast<float>(plan.tau * plan.channel_weights[c]);
       const double t = plan.tau * samples->mu;
       sp.t = static_cast<float>(t);
@@ -554,10 +549,8 @@ struct Solver::Impl {
       sp.scale = scale;
       sp.gamma = plan.channel_weights[c];
       sp.mu = samples->mu;
-      const std::size_t packed = c * static_cast<std::size_t>(g.rows) * g.columns;
-      sp.lower64 = s_lower64 + packed;
-      sp.upper64 = s_upper64 + packed;
-      sp.centre64 = s_centre64 + packed;
+      sp.levels = s_levels + c * g.plane;
+      sp.ends64 = s_ends64;
       sp.partials = partials;
       if (error == cudaSuccess) error = launch_samples_conjugate(sp, stream);
       return sum_of(partials, samples_grid_blocks(sp.g, 1));
@@ -645,8 +638,8 @@ struct Solver::Impl {
       sp.g = g;
       sp.mode = 1;
       sp.xt = xt;
-      sp.lower64 = s_lower64;
-      sp.upper64 = s_upper64;
+      sp.levels = s_levels;
+      sp.ends64 = s_ends64;
       sp.canvas = canvas;
       if (error == cudaSuccess) error = launch_samples_canvas(sp, stream);
     }

@@ -210,6 +210,8 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_b200_solve_levels": (i32, ctypes.POINTER(_Input), handle, i32, i32, ctypes.c_void_p, u64, u64p,
                                       *text),
         "unround_b200_solve_samples": (i32, ctypes.POINTER(ctypes.c_uint16), u64, u64, u64, i32, handle, *made),
+        "unround_b200_measure_samples": (i32, ctypes.POINTER(ctypes.c_uint16), u64, u64, u64, i32, handle, u64, u64,
+                                         ctypes.POINTER(_Timing), *text),
         "unround_b200_solve_from": (i32, ctypes.POINTER(_Input), handle, ctypes.POINTER(_Start), *made),
         "unround_b200_measure": (i32, ctypes.POINTER(_Input), handle, u64, u64, ctypes.POINTER(_Timing),
                                  ctypes.POINTER(handle), *text),
@@ -823,3 +825,23 @@ def solve_samples(levels: npt.ArrayLike, bits: int = 8, settings: Settings | lis
         return _decoded(library, result, problems=False)
     finally:
         library.unround_result_free(result)
+
+
+def measure_samples(levels: npt.ArrayLike, bits: int = 8, settings: Settings | list[str] | None = None, *,
+                    warmup: int = 3, iterations: int = 100) -> Timing:
+    """The iteration loop of solve_samples alone on the GPU, timed by CUDA events
+    (unround_b200_measure_samples): grey (height, width) or RGB (height, width, 3) levels."""
+    values = np.ascontiguousarray(levels, dtype=np.uint16)
+    if values.ndim == 2:
+        values = values[:, :, np.newaxis]
+    library = _library()
+    handle = _settings_of(settings)
+    timing = _Timing()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    rows, columns, channels = values.shape
+    status = library.unround_b200_measure_samples(values.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), rows,
+                                                  columns, channels, int(bits), handle.handle, warmup, iterations,
+                                                  ctypes.byref(timing), message, _MESSAGE)
+    _raise(status, message)
+    return Timing(timing.milliseconds, timing.dual_milliseconds, timing.primal_milliseconds, int(timing.iterations),
+                  int(timing.launches_per_iteration), int(timing.samples), int(timing.pixels), int(timing.device_bytes))

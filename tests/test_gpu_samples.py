@@ -119,3 +119,17 @@ def test_refusals():
         native.solve_samples(levels, 17, ["--method", "tgv"])
     with pytest.raises(native.UnroundError, match="below 2"):
         native.solve_samples(np.full((4, 4), 300, dtype=np.uint16), 8, ["--method", "tgv"])
+
+
+def test_the_measured_loop():
+    """unround_b200_measure_samples times the loop of the same solver: its counts are the
+    picture's, both kernels took time, and a colour picture with an alpha is refused."""
+    from unround import native
+
+    levels = _picture(64, 96, 3, 8, seed=4)
+    timing = native.measure_samples(levels, 8, ["--method", "tgv"], warmup=3, iterations=20)
+    assert timing.iterations == 20 and timing.pixels == 64 * 96 and timing.samples == 3 * 64 * 96
+    assert timing.launches_per_iteration == 2
+    assert timing.milliseconds > 0 and timing.dual_milliseconds > 0 and timing.primal_milliseconds > 0
+    with pytest.raises(native.UnroundError):
+        native.measure_samples(_picture(8, 8, 4, 8, seed=1), 8, ["--method", "tgv"])
