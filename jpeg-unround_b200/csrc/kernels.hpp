@@ -274,7 +274,8 @@ struct SamplesCanvasParams {
   const SampleEnds64* ends64 = nullptr;
   double* canvas = nullptr;  // C x rows x columns
 };
-int samples_grid_blocks(const Geometry& g, int channels);
+int samples_grid_blocks(const Geometry& g, int channels);  // a sample per thread
+int samples_primal_blocks(const Geometry& g);              // the primal step's CTAs
 cudaError_t launch_samples_primal(const SamplesPrimalParams& p, bool keep, cudaStream_t stream);
 cudaError_t launch_samples_conjugate(const SamplesConjugateParams& p, cudaStream_t stream);
 cudaError_t launch_samples_canvas(const SamplesCanvasParams& p, cudaStream_t stream);

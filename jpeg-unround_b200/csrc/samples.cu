@@ -54,28 +54,59 @@ __device__ __forceinline__ float descent_of(const SamplesPrimalParams& P, int c)
   return d;
 }
 
+// Four consecutive samples of a row per thread (16-byte loads of x, p1, p2 and x~ stores, an
+// 8-byte load of the levels; the pitch is a multiple of 32 samples), a warp per 128 columns of
+// a row, CTAs of 128 columns x 8 rows. p1 at the column before comes from the lane before by
+// a shuffle (lane 0 loads it); p2 at the row above by a 16-byte load, mostly from L1.
 template <bool KEEP>
 __global__ void __launch_bounds__(256) samples_primal_kernel(const SamplesPrimalParams P) {
-  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y, c = blockIdx.z;
+  const int lane = threadIdx.x;
+  const int j = blockIdx.x * 128 + 4 * lane, i = blockIdx.y * 8 + threadIdx.y, c = blockIdx.z;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
   const float descent = descent_of(P, c);
+  const bool row_in = i < rows;
   double term = 0.0;
-  if (i < rows && j < columns) {
-    const std::size_t at = c * P.g.plane + static_cast<std::size_t>(i) * pitch + j;
-    const float p1 = P.p1[at], p2 = P.p2[at];
-    const float above = i > 0 ? P.p2[at - pitch] : 0.0f;
-    const float before = j > 0 ? P.p1[at - 1] : 0.0f;
-    // div p = dy' p2 + dx' p1, backward differences with Neumann ends.
-    const float dy = (i + 1 < rows ? p2 : 0.0f) - (i > 0 ? above : 0.0f);
-    const float dx = (j + 1 < columns ? p1 : 0.0f) - (j > 0 ? before : 0.0f);
-    const float v = P.x[at] + descent * (dy + dx);
-    const unsigned level = P.levels[at];
-    const float4 ends = __ldg(reinterpret_cast<const float4*>(P.ends) + level);  // lower, upper, centre
-    const float z = fminf(fmaxf((v + P.t * ends.z) * P.r, ends.x), ends.y);
-    P.xt[at] = z;
-    if constexpr (KEEP) {
-      const double away = static_cast<double>(z) - P.ends64[level].centre;
-      term = P.half_mu * (away * away);
+  const std::size_t at = c * P.g.plane + static_cast<std::size_t>(row_in ? i : 0) * pitch + (j < pitch ? j : 0);
+  float4 p1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (row_in && j < columns) p1 = *reinterpret_cast<const float4*>(P.p1 + at);
+  // The p1 of the column before this thread's first: the lane before's last, or a load.
+  float before = __shfl_up_sync(kAll, p1.w, 1);
+  if (lane == 0) before = row_in && j > 0 && j < columns ? P.p1[at - 1] : 0.0f;
+  if (row_in && j < columns) {
+    const float4 p2 = *reinterpret_cast<const float4*>(P.p2 + at);
+    const float4 above = i > 0 ? *reinterpret_cast<const float4*>(P.p2 + at - pitch) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 x = *reinterpret_cast<const float4*>(P.x + at);
+    const ushort4 level = *reinterpret_cast<const ushort4*>(P.levels + at);
+    const bool last_row = i + 1 == rows;
+    const float pv[4] = {p1.x, p1.y, p1.z, p1.w}, qv[4] = {p2.x, p2.y, p2.z, p2.w};
+    const float av[4] = {above.x, above.y, above.z, above.w}, xv[4] = {x.x, x.y, x.z, x.w};
+    const unsigned lv[4] = {level.x, level.y, level.z, level.w};
+    float zv[4];
+    float left = before;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      // div p = dy' p2 + dx' p1, backward differences with Neumann ends.
+      const int jj = j + u;
+      const float dy = (last_row ? 0.0f : qv[u]) - (i > 0 ? av[u] : 0.0f);
+      const float dx = (jj + 1 < columns ? pv[u] : 0.0f) - (jj > 0 ? left : 0.0f);
+      left = pv[u];
+      const float v = xv[u] + descent * (dy + dx);
+      const float4 ends = __ldg(reinterpret_cast<const float4*>(P.ends) + (jj < columns ? lv[u] : 0u));
+      zv[u] = fminf(fmaxf((v + P.t * ends.z) * P.r, ends.x), ends.y);
+      if constexpr (KEEP) {
+        if (jj < columns) {
+          const double away = static_cast<double>(zv[u]) - P.ends64[lv[u]].centre;
+          term += P.half_mu * (away * away);
+        }
+      }
+    }
+    if (j + 4 <= columns) {
+      *reinterpret_cast<float4*>(P.xt + at) = make_float4(zv[0], zv[1], zv[2], zv[3]);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (j + u < columns) P.xt[at + u] = zv[u];
+      }
     }
   }
   if constexpr (KEEP) block_sum(term, P.partials);
@@ -130,6 +161,10 @@ dim3 sample_grid(const Geometry& g, int channels) {
   return dim3((g.columns + 31) / 32, (g.rows + 7) / 8, channels);
 }
 
+dim3 primal_grid(const Geometry& g) {
+  return dim3((g.columns + 127) / 128, (g.rows + 7) / 8, g.channels);
+}
+
 }  // namespace
 
 int samples_grid_blocks(const Geometry& g, int channels) {
@@ -137,8 +172,13 @@ int samples_grid_blocks(const Geometry& g, int channels) {
   return static_cast<int>(grid.x * grid.y * grid.z);
 }
 
+int samples_primal_blocks(const Geometry& g) {
+  const dim3 grid = primal_grid(g);
+  return static_cast<int>(grid.x * grid.y * grid.z);
+}
+
 cudaError_t launch_samples_primal(const SamplesPrimalParams& p, bool keep, cudaStream_t stream) {
-  const dim3 grid = sample_grid(p.g, p.g.channels);
+  const dim3 grid = primal_grid(p.g);
   if (keep) {
     samples_primal_kernel<true><<<grid, dim3(32, 8), 0, stream>>>(p);
   } else {

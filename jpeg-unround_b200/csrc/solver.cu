@@ -467,7 +467,7 @@ struct Solver::Impl {
       sp.half_mu = 0.5 * samples->mu;
       sp.partials = value_partials;
       if (error == cudaSuccess) error = launch_samples_primal(sp, keep, stream);
-      if (keep) samples_written = samples_grid_blocks(g, g.channels);
+      if (keep) samples_written = samples_primal_blocks(g);
       return;
     }
     for (std::size_t c = 0; c < components.size();) {
