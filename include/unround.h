@@ -12,9 +12,10 @@
  * used on different threads at once: each call has its own CUDA stream and device buffers.
  *
  * Each declaration cites the reference declaration it replaces (rust/capi/include/unround.h,
- * line numbers of that file). The file-level paths that need libjpeg-turbo or libpng
- * (decode, project, the PNG/PNM/TIFF writers, the C layer) are exported and return
- * UNROUND_ERROR_UNSUPPORTED: this build has no such library. */
+ * line numbers of that file). Files are read and written on the host by this build's own JPEG
+ * reader (ITU-T T.81: baseline, extended and progressive Huffman files) and PNG reader and writer
+ * (zlib), in place of libjpeg-turbo and libpng; the projection onto a file's intervals
+ * (unround_project) and the TIFF writer are exported and return UNROUND_ERROR_UNSUPPORTED. */
 #ifndef UNROUND_H
 #define UNROUND_H
 

@@ -55,7 +55,7 @@ def build(force: bool = False) -> Path:
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
         objects = list(pool.map(lambda source: _compile(source, force), sources))
     if force or _stale(OUTPUT, objects):
-        command = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(OUTPUT), *map(str, objects), "-lpthread"]
+        command = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(OUTPUT), *map(str, objects), "-lpthread", "-lz"]
         subprocess.run(command, check=True)
     return OUTPUT
 

@@ -3,7 +3,9 @@
 // (rust/capi/src/lib.rs:617-660), results are owned by the library until unround_result_free,
 // and no exception crosses the interface: each entry point catches everything and returns a
 // status with its message (rust/capi/src/lib.rs:99-115, `guarded`).
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <memory>
@@ -13,11 +15,14 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <zlib.h>
 
 #include "batch.hpp"
 #include "blue_noise.hpp"
+#include "jpeg_reader.hpp"
 #include "colour.hpp"
 #include "model.hpp"
+#include "png_io.hpp"
 #include "samples_model.hpp"
 #include "settings.hpp"
 #include "solver.hpp"
@@ -46,6 +51,12 @@ struct unround_result {
   mutable std::once_flag problem_once;
   mutable std::vector<std::vector<double>> problem[3];
   std::vector<std::vector<double>> steps, weights;
+  // What the file held besides its picture (unround_result_format and the rest).
+  std::int32_t format = UNROUND_FORMAT_JPEG;
+  std::int32_t bits = 8;
+  std::int32_t exif_orientation = 0;
+  std::vector<std::uint8_t> icc;
+  std::string warning;
 };
 
 namespace {
@@ -337,6 +348,107 @@ bool solve_input(const unround_input* input, const unround_settings* settings, c
 
 }  // namespace
 
+// The solve of unround_b200_solve_samples, and of a PNG file's levels in unround_decode: the
+// result's format is PNG, of the levels' bits.
+static bool solve_samples_into(const uint16_t* levels, uint64_t rows, uint64_t columns, uint64_t channels, int32_t bits,
+                               const unround_settings* settings, unround_observer observer, void* user,
+                               unround_result** result, urb::Failure& failure) {
+  if (levels == nullptr || settings == nullptr || result == nullptr) {
+    failure = {urb::kArgument, "the levels, the settings and the result are not null pointers"};
+    return false;
+  }
+  if (channels < 1 || channels > 4 || rows == 0 || columns == 0 || rows > (1u << 24) || columns > (1u << 24)) {
+    failure = {urb::kOptions, "a picture of " + std::to_string(rows) + " x " + std::to_string(columns) + " x " +
+                                  std::to_string(channels) + " samples: 1 to 4 channels, not empty"};
+    return false;
+  }
+  const urb::Settings& s = settings->settings;
+  if (!urb::check_samples_settings(s, failure)) return false;
+  const urb::DataTerm& term = s.data.front();
+  const double mu = term.mu ? *term.mu : 0.0;
+  const bool alpha = channels == 2 || channels == 4;
+  const std::size_t colours = alpha ? channels - 1 : channels;
+  auto colour_model = urb::make_samples_model(levels, rows, columns, channels, bits, 0, colours, term.slack, mu,
+                                              failure);
+  if (!colour_model) return false;
+  std::optional<urb::SamplesModel> alpha_model;
+  if (alpha) {
+    alpha_model = urb::make_samples_model(levels, rows, columns, channels, bits, colours, 1, term.slack, mu, failure);
+    if (!alpha_model) return false;
+  }
+  auto plan = urb::make_plan(s, colours, failure, urb::samples_plan_defaults());
+  if (!plan) return false;
+  urb::Settings alone = s;
+  alone.regularizer.channel_weights.clear();
+  std::optional<urb::Plan> alpha_plan;
+  if (alpha) {
+    alpha_plan = urb::make_plan(alone, 1, failure, urb::samples_plan_defaults());
+    if (!alpha_plan) return false;
+  }
+  if (!have_device(failure)) return false;
+  // The solvers' frame: the picture's size and colours, no components (the samples are the
+  // data term); the result's gets a component (with no blocks) per channel.
+  urb::Frame frame;
+  frame.height = static_cast<std::uint32_t>(rows);
+  frame.width = static_cast<std::uint32_t>(columns);
+  frame.rows = static_cast<std::uint32_t>(rows);
+  frame.columns = static_cast<std::uint32_t>(columns);
+  frame.color_space = colours == 3 ? 3 : 1;
+  urb::Observer watch;
+  if (observer != nullptr) {
+    watch = [&](const urb::Record& r, double gap, const double* canvas) {
+      unround_record raw{r.iteration, gap, r.primal, r.dual, colours, rows, columns, canvas};
+      return observer(user, &raw) != 0;
+    };
+  }
+  Stream stream;
+  if (stream.error != cudaSuccess) {
+    failure = {urb::kInternal, std::string("a CUDA stream: ") + cudaGetErrorString(stream.error)};
+    return false;
+  }
+  urb::Outcome outcome;
+  {
+    urb::Solver solver(frame, *colour_model, stream.stream);
+    if (!solver.solve(s.method, &*plan, nullptr, watch, outcome, failure)) return false;
+  }
+  if (!alpha) {
+    frame.components.resize(colours);
+    *result = result_of(std::move(frame), std::move(outcome));
+    (*result)->format = UNROUND_FORMAT_PNG;
+    (*result)->bits = bits;
+    return true;
+  }
+  urb::Frame alpha_frame = frame;
+  alpha_frame.color_space = 1;
+  urb::Outcome alpha_outcome;
+  {
+    urb::Solver solver(alpha_frame, *alpha_model, stream.stream);
+    if (!solver.solve(s.method, &*alpha_plan, nullptr, watch, alpha_outcome, failure)) return false;
+  }
+  // The colours' planes and the alpha's, and the picture interleaved, in one result.
+  const std::size_t plane = static_cast<std::size_t>(rows) * columns;
+  urb::Outcome merged;
+  merged.canvas.resize(channels * plane);
+  std::memcpy(merged.canvas.data(), outcome.canvas.data(), colours * plane * sizeof(double));
+  std::memcpy(merged.canvas.data() + colours * plane, alpha_outcome.canvas.data(), plane * sizeof(double));
+  merged.picture.resize(channels * plane);
+  for (std::size_t k = 0; k < plane; ++k) {
+    for (std::size_t c = 0; c < channels; ++c) merged.picture.data()[k * channels + c] = merged.canvas.data()[c * plane + k];
+  }
+  merged.records = std::move(outcome.records);
+  merged.iterations = outcome.iterations;
+  merged.stop = outcome.stop;
+  merged.solved = outcome.solved;
+  merged.tau = outcome.tau;
+  merged.sigma = outcome.sigma;
+  frame.components.resize(channels);
+  frame.color_space = colours == 3 ? 3 : 1;
+  *result = result_of(std::move(frame), std::move(merged));
+  (*result)->format = UNROUND_FORMAT_PNG;
+  (*result)->bits = bits;
+  return true;
+}
+
 extern "C" {
 
 int32_t unround_abi_version(void) { return UNROUND_ABI_VERSION; }
@@ -385,12 +497,69 @@ size_t unround_settings_options(const unround_settings* settings, char* buffer, 
   }
 }
 
-unround_status unround_decode(const uint8_t*, size_t, const unround_settings*, unround_observer, void*,
-                              unround_result**, char* message, size_t message_size) {
-  say(message, message_size,
-      "reading a JPEG file needs libjpeg-turbo, which this build does not carry: give the components as arrays "
-      "to unround_solve");
-  return UNROUND_ERROR_UNSUPPORTED;
+// A file reconstructed (rust/capi/src/lib.rs, unround_decode; rust/unround/src/decode.rs and
+// rounded.rs): a PNG file, known by its signature, within the intervals of its rounded samples
+// (the levels read on the host, solved as unround_b200_solve_samples does); any other file as a
+// JPEG file, its coefficients read on the host (jpeg_reader.hpp) and solved as unround_solve
+// does. The reading's refusals map as the reference maps them: UNSUPPORTED stays, a limit is
+// OPTIONS, anything else READ.
+unround_status unround_decode(const uint8_t* data, size_t size, const unround_settings* settings,
+                              unround_observer observer, void* user, unround_result** result, char* message,
+                              size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (data == nullptr || settings == nullptr || result == nullptr) {
+      failure = {urb::kArgument, "the data, the settings and the result are not null pointers"};
+      return false;
+    }
+    const urb::Settings& s = settings->settings;
+    auto read_failure = [&](int status, const std::string& text) {
+      const urb::Status mapped = status == urb::kJpegUnsupported ? urb::kUnsupported
+                                  : status == urb::kJpegLimit     ? urb::kOptions
+                                                                  : urb::kRead;
+      failure = {mapped, text};
+      return false;
+    };
+    if (urb::is_png(data, size)) {
+      urb::PngPicture picture;
+      std::string text;
+      const int status = urb::read_png(data, size, s.reading.max_pixels, picture, text);
+      if (status != urb::kPngOk) return read_failure(status, text);
+      if (!solve_samples_into(picture.samples.data(), picture.height, picture.width,
+                              static_cast<std::uint64_t>(picture.channels), picture.bits, settings, observer, user,
+                              result, failure)) {
+        return false;
+      }
+      (*result)->icc = std::move(picture.icc);
+      (*result)->warning = picture.warning;
+      return true;
+    }
+    urb::JpegLimits limits;
+    limits.max_pixels = s.reading.max_pixels;
+    limits.max_scans = s.reading.max_scans;
+    limits.warnings_are_errors = s.reading.warnings_are_errors;
+    urb::JpegFile file;
+    std::string text;
+    const int status = urb::read_jpeg(data, size, limits, file, text);
+    if (status != urb::kJpegOk) return read_failure(status, text);
+    std::vector<unround_component> components(file.components.size());
+    for (std::size_t c = 0; c < components.size(); ++c) {
+      const urb::JpegComponent& from = file.components[c];
+      unround_component& to = components[c];
+      to.levels = from.coefficients.data();
+      to.rows = from.height_in_blocks;
+      to.columns = from.width_in_blocks;
+      to.h_samp_factor = from.h;
+      to.v_samp_factor = from.v;
+      std::copy(from.table, from.table + 64, to.quant_table);
+    }
+    unround_input input{file.height, file.width, file.color_space, static_cast<std::uint32_t>(components.size()),
+                        components.data()};
+    if (!solve_input(&input, settings, nullptr, observer, user, result, failure, nullptr)) return false;
+    (*result)->exif_orientation = file.exif_orientation;
+    (*result)->icc = std::move(file.icc);
+    (*result)->warning = file.warning;
+    return true;
+  });
 }
 
 unround_status unround_solve(const unround_input* input, const unround_settings* settings, unround_observer observer,
@@ -697,11 +866,22 @@ const double* unround_result_record_values(const unround_result* result, int32_t
 int32_t unround_result_alpha_solver(const unround_result*, uint64_t*, int32_t*) { return 0; }
 const uint64_t* unround_result_alpha_record_iterations(const unround_result*, uint64_t*) { return nullptr; }
 const double* unround_result_alpha_record_values(const unround_result*, int32_t, uint64_t*) { return nullptr; }
-const uint8_t* unround_result_icc_profile(const unround_result*, uint64_t*) { return nullptr; }
-int32_t unround_result_exif_orientation(const unround_result*) { return 0; }
-int32_t unround_result_format(const unround_result* result) { return result == nullptr ? 0 : UNROUND_FORMAT_JPEG; }
-int32_t unround_result_bits(const unround_result* result) { return result == nullptr ? 0 : 8; }
-const char* unround_result_warning(const unround_result* result) { return result == nullptr ? nullptr : ""; }
+const uint8_t* unround_result_icc_profile(const unround_result* result, uint64_t* size) {
+  if (result == nullptr || result->icc.empty()) {
+    put(size, 0);
+    return nullptr;
+  }
+  put(size, result->icc.size());
+  return result->icc.data();
+}
+int32_t unround_result_exif_orientation(const unround_result* result) {
+  return result == nullptr ? 0 : result->exif_orientation;
+}
+int32_t unround_result_format(const unround_result* result) { return result == nullptr ? 0 : result->format; }
+int32_t unround_result_bits(const unround_result* result) { return result == nullptr ? 0 : result->bits; }
+const char* unround_result_warning(const unround_result* result) {
+  return result == nullptr ? nullptr : result->warning.c_str();
+}
 const double* unround_result_excess(const unround_result*, uint64_t, uint64_t*) { return nullptr; }
 
 unround_status unround_tiff(const double*, uint64_t, uint64_t, uint64_t, int32_t, const uint8_t*, uint64_t, uint8_t**,
@@ -710,10 +890,53 @@ unround_status unround_tiff(const double*, uint64_t, uint64_t, uint64_t, int32_t
   return UNROUND_ERROR_UNSUPPORTED;
 }
 
-unround_status unround_png(const double*, uint64_t, uint64_t, uint64_t, int32_t, int32_t, int32_t, const uint8_t*,
-                           uint64_t, uint8_t**, uint64_t*, char* message, size_t message_size) {
-  say(message, message_size, "writing PNG needs libpng, which this build does not carry");
-  return UNROUND_ERROR_UNSUPPORTED;
+// The bytes of a PNG file (rust/capi/src/lib.rs, unround_png; c/jpegio/src/png.c): the levels
+// made on the device as unround_pnm makes them, 8 or 16 bits, 1 to 4 channels, written by
+// png_io.hpp with zlib's compression level (-1 its default) and the ICC profile where it goes
+// with the picture (the message says why where it does not).
+unround_status unround_png(const double* samples, uint64_t height, uint64_t width, uint64_t channels, int32_t sixteen,
+                           int32_t dither, int32_t compression, const uint8_t* icc, uint64_t icc_size, uint8_t** bytes,
+                           uint64_t* size, char* message, size_t message_size) {
+  std::string warning;
+  const unround_status status = guarded(message, message_size, [&](urb::Failure& failure) {
+    if (bytes == nullptr || size == nullptr) {
+      failure = {urb::kArgument, "the bytes and the size are not null pointers"};
+      return false;
+    }
+    if (dither < 0 || dither > 2 || compression < -1 || compression > 9) {
+      failure = {urb::kOptions, "the dither is 0, 1 or 2 and the compression -1 to 9"};
+      return false;
+    }
+    std::size_t count = 0;
+    if (!picture_count(samples, height, width, channels, count, failure)) return false;
+    std::vector<std::uint8_t> levels(count * (sixteen != 0 ? 2 : 1));
+    if (!quantize(samples, count, static_cast<int>(width), static_cast<int>(channels), sixteen != 0, dither,
+                  levels.data(), failure)) {
+      return false;
+    }
+    std::vector<std::uint16_t> wide;
+    if (sixteen != 0) {  // the levels most significant byte first, as PNM holds them
+      wide.resize(count);
+      for (std::size_t i = 0; i < count; ++i) wide[i] = static_cast<std::uint16_t>((levels[2 * i] << 8) | levels[2 * i + 1]);
+    }
+    std::vector<std::uint8_t> file;
+    std::string text;
+    const int written = urb::write_png(sixteen != 0 ? static_cast<const void*>(wide.data()) : levels.data(),
+                                       static_cast<std::uint32_t>(width), static_cast<std::uint32_t>(height),
+                                       static_cast<int>(channels), sixteen != 0 ? 16 : 8, compression, icc,
+                                       static_cast<std::size_t>(icc_size), file, warning, text);
+    if (written != urb::kPngOk) {
+      failure = {written == urb::kPngArgument ? urb::kOptions : urb::kIo, text};
+      return false;
+    }
+    std::unique_ptr<std::uint8_t[]> out(new std::uint8_t[file.size()]);
+    std::memcpy(out.get(), file.data(), file.size());
+    *size = file.size();
+    *bytes = out.release();
+    return true;
+  });
+  if (status == UNROUND_OK) say(message, message_size, warning);
+  return status;
 }
 
 // The PNM file (rust/unround/src/output.rs:248-271, rust/capi/src/lib.rs:1460-1488): a P5
@@ -812,96 +1035,7 @@ unround_status unround_b200_solve_samples(const uint16_t* levels, uint64_t rows,
                                          int32_t bits, const unround_settings* settings, unround_observer observer,
                                          void* user, unround_result** result, char* message, size_t message_size) {
   return guarded(message, message_size, [&](urb::Failure& failure) {
-    if (levels == nullptr || settings == nullptr || result == nullptr) {
-      failure = {urb::kArgument, "the levels, the settings and the result are not null pointers"};
-      return false;
-    }
-    if (channels < 1 || channels > 4 || rows == 0 || columns == 0 || rows > (1u << 24) || columns > (1u << 24)) {
-      failure = {urb::kOptions, "a picture of " + std::to_string(rows) + " x " + std::to_string(columns) + " x " +
-                                    std::to_string(channels) + " samples: 1 to 4 channels, not empty"};
-      return false;
-    }
-    const urb::Settings& s = settings->settings;
-    if (!urb::check_samples_settings(s, failure)) return false;
-    const urb::DataTerm& term = s.data.front();
-    const double mu = term.mu ? *term.mu : 0.0;
-    const bool alpha = channels == 2 || channels == 4;
-    const std::size_t colours = alpha ? channels - 1 : channels;
-    auto colour_model = urb::make_samples_model(levels, rows, columns, channels, bits, 0, colours, term.slack, mu,
-                                                failure);
-    if (!colour_model) return false;
-    std::optional<urb::SamplesModel> alpha_model;
-    if (alpha) {
-      alpha_model = urb::make_samples_model(levels, rows, columns, channels, bits, colours, 1, term.slack, mu, failure);
-      if (!alpha_model) return false;
-    }
-    auto plan = urb::make_plan(s, colours, failure, urb::samples_plan_defaults());
-    if (!plan) return false;
-    urb::Settings alone = s;
-    alone.regularizer.channel_weights.clear();
-    std::optional<urb::Plan> alpha_plan;
-    if (alpha) {
-      alpha_plan = urb::make_plan(alone, 1, failure, urb::samples_plan_defaults());
-      if (!alpha_plan) return false;
-    }
-    if (!have_device(failure)) return false;
-    // The solvers' frame: the picture's size and colours, no components (the samples are the
-    // data term); the result's gets a component (with no blocks) per channel.
-    urb::Frame frame;
-    frame.height = static_cast<std::uint32_t>(rows);
-    frame.width = static_cast<std::uint32_t>(columns);
-    frame.rows = static_cast<std::uint32_t>(rows);
-    frame.columns = static_cast<std::uint32_t>(columns);
-    frame.color_space = colours == 3 ? 3 : 1;
-    urb::Observer watch;
-    if (observer != nullptr) {
-      watch = [&](const urb::Record& r, double gap, const double* canvas) {
-        unround_record raw{r.iteration, gap, r.primal, r.dual, colours, rows, columns, canvas};
-        return observer(user, &raw) != 0;
-      };
-    }
-    Stream stream;
-    if (stream.error != cudaSuccess) {
-      failure = {urb::kInternal, std::string("a CUDA stream: ") + cudaGetErrorString(stream.error)};
-      return false;
-    }
-    urb::Outcome outcome;
-    {
-      urb::Solver solver(frame, *colour_model, stream.stream);
-      if (!solver.solve(s.method, &*plan, nullptr, watch, outcome, failure)) return false;
-    }
-    if (!alpha) {
-      frame.components.resize(colours);
-      *result = result_of(std::move(frame), std::move(outcome));
-      return true;
-    }
-    urb::Frame alpha_frame = frame;
-    alpha_frame.color_space = 1;
-    urb::Outcome alpha_outcome;
-    {
-      urb::Solver solver(alpha_frame, *alpha_model, stream.stream);
-      if (!solver.solve(s.method, &*alpha_plan, nullptr, watch, alpha_outcome, failure)) return false;
-    }
-    // The colours' planes and the alpha's, and the picture interleaved, in one result.
-    const std::size_t plane = static_cast<std::size_t>(rows) * columns;
-    urb::Outcome merged;
-    merged.canvas.resize(channels * plane);
-    std::memcpy(merged.canvas.data(), outcome.canvas.data(), colours * plane * sizeof(double));
-    std::memcpy(merged.canvas.data() + colours * plane, alpha_outcome.canvas.data(), plane * sizeof(double));
-    merged.picture.resize(channels * plane);
-    for (std::size_t k = 0; k < plane; ++k) {
-      for (std::size_t c = 0; c < channels; ++c) merged.picture.data()[k * channels + c] = merged.canvas.data()[c * plane + k];
-    }
-    merged.records = std::move(outcome.records);
-    merged.iterations = outcome.iterations;
-    merged.stop = outcome.stop;
-    merged.solved = outcome.solved;
-    merged.tau = outcome.tau;
-    merged.sigma = outcome.sigma;
-    frame.components.resize(channels);
-    frame.color_space = colours == 3 ? 3 : 1;
-    *result = result_of(std::move(frame), std::move(merged));
-    return true;
+    return solve_samples_into(levels, rows, columns, channels, bits, settings, observer, user, result, failure);
   });
 }
 
@@ -993,10 +1127,50 @@ unround_status unround_b200_blue_noise(uint16_t* ranks, char* message, size_t me
   });
 }
 
-unround_status unround_orient(const double*, uint64_t, uint64_t, uint64_t, int32_t, double*, uint64_t*, uint64_t*,
+// A picture turned upright by its EXIF orientation (rust/capi/src/lib.rs, unround_orient;
+// rust/unround/src/orientation.rs:67-150; EXIF 2.3 tag 0x0112): 0 or 1 as stored, 2 mirrored, 3 turned half round, 4 flipped, 5 transposed,
+// 6 turned a quarter clockwise, 7 transversed, 8 turned a quarter anticlockwise; 5 to 8 swap
+// the height and the width. turned holds height * width * channels samples.
+unround_status unround_orient(const double* samples, uint64_t height, uint64_t width, uint64_t channels,
+                              int32_t orientation, double* turned, uint64_t* turned_height, uint64_t* turned_width,
                               char* message, size_t message_size) {
-  say(message, message_size, "turning a picture upright is host output outside this build's path");
-  return UNROUND_ERROR_UNSUPPORTED;
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (samples == nullptr || turned == nullptr) {
+      failure = {urb::kArgument, "the samples and the turned picture are not null pointers"};
+      return false;
+    }
+    if (orientation < 0 || orientation > 8) {
+      failure = {urb::kOptions, "an EXIF orientation is 1 to 8, or 0 for none, not " + std::to_string(orientation)};
+      return false;
+    }
+    if (height == 0 || width == 0 || channels == 0) {
+      failure = {urb::kArgument, "the picture is empty"};
+      return false;
+    }
+    const bool swap = orientation >= 5;
+    const std::uint64_t out_h = swap ? width : height, out_w = swap ? height : width;
+    for (std::uint64_t y = 0; y < out_h; ++y) {
+      for (std::uint64_t x = 0; x < out_w; ++x) {
+        std::uint64_t sy = 0, sx = 0;  // the stored pixel shown at (y, x)
+        switch (orientation) {
+          case 0:
+          case 1: sy = y; sx = x; break;
+          case 2: sy = y; sx = width - 1 - x; break;
+          case 3: sy = height - 1 - y; sx = width - 1 - x; break;
+          case 4: sy = height - 1 - y; sx = x; break;
+          case 5: sy = x; sx = y; break;
+          case 6: sy = height - 1 - x; sx = y; break;
+          case 7: sy = height - 1 - x; sx = width - 1 - y; break;
+          default: sy = x; sx = width - 1 - y; break;
+        }
+        std::memcpy(turned + (y * out_w + x) * channels, samples + (sy * width + sx) * channels,
+                    channels * sizeof(double));
+      }
+    }
+    if (turned_height != nullptr) *turned_height = out_h;
+    if (turned_width != nullptr) *turned_width = out_w;
+    return true;
+  });
 }
 
 unround_status unround_to_rgb(const double* planes, uint64_t height, uint64_t width, double* picture) {
@@ -1014,28 +1188,192 @@ unround_status unround_to_ycbcr(const double* picture, uint64_t height, uint64_t
 int32_t unround_main(size_t, const char* const*) { return 3; }
 
 int32_t unround_jpeg_abi_version(void) { return UNROUND_JPEGIO_ABI_VERSION; }
-const char* unround_jpeg_libjpeg_version(void) { return "none (this build reads no JPEG files)"; }
-const char* unround_jpeg_libpng_version(void) { return "none (this build writes no PNG files)"; }
+const char* unround_jpeg_libjpeg_version(void) { return "unround JPEG reader (ITU-T T.81, Huffman)"; }
+const char* unround_jpeg_libpng_version(void) { return "unround PNG reader and writer, zlib " ZLIB_VERSION; }
 
-int32_t unround_jpeg_check_icc(const uint8_t*, uint64_t, int32_t, char* reason, size_t reason_size) {
-  say(reason, reason_size, "this build carries no libpng to check a profile");
-  return 0;
+int32_t unround_jpeg_check_icc(const uint8_t* profile, uint64_t size, int32_t channels, char* reason,
+                               size_t reason_size) {
+  std::string why;
+  const bool taken = urb::check_icc(profile, size, channels, why);
+  say(reason, reason_size, why);
+  return taken ? 1 : 0;
 }
 
-unround_jpegio_status unround_jpeg_read(const uint8_t*, size_t, const unround_jpegio_options*, unround_jpegio_image*,
-                                        char* message, size_t message_size) {
-  say(message, message_size, "reading a JPEG file needs libjpeg-turbo, which this build does not carry");
-  return 3;
+// The C layer's reading of a JPEG file (c/jpegio/include/unround/jpegio.h:188-211): the
+// coefficients and the metadata, by this build's own reader (jpeg_reader.hpp). The arrays are
+// allocated with malloc and freed by unround_jpeg_image_free, as the reference's are.
+unround_jpegio_status unround_jpeg_read(const uint8_t* data, size_t size, const unround_jpegio_options* options,
+                                        unround_jpegio_image* image, char* message, size_t message_size) {
+  if (image == nullptr || (message == nullptr && message_size > 0)) return urb::kJpegArgument;
+  *image = unround_jpegio_image{};
+  urb::JpegLimits limits;
+  if (options != nullptr) {
+    if (options->max_pixels != 0) limits.max_pixels = options->max_pixels;
+    if (options->max_scans > 0) limits.max_scans = options->max_scans;
+    limits.warnings_are_errors = options->warnings_are_errors != 0;
+  }
+  urb::JpegFile file;
+  std::string text;
+  const int status = urb::read_jpeg(data, size, limits, file, text);
+  say(message, message_size, text);
+  if (status != urb::kJpegOk) return status;
+  image->width = file.width;
+  image->height = file.height;
+  image->color_space = file.color_space;
+  image->num_components = static_cast<int32_t>(file.components.size());
+  image->max_h_samp_factor = file.hmax;
+  image->max_v_samp_factor = file.vmax;
+  image->progressive = file.progressive ? 1 : 0;
+  image->arithmetic = 0;
+  image->exif_orientation = file.exif_orientation;
+  image->warnings = file.warnings;
+  for (std::size_t c = 0; c < file.components.size(); ++c) {
+    const urb::JpegComponent& from = file.components[c];
+    unround_jpegio_component& to = image->components[c];
+    to.id = from.id;
+    to.h_samp_factor = from.h;
+    to.v_samp_factor = from.v;
+    to.quant_table_slot = from.slot;
+    to.width = from.width;
+    to.height = from.height;
+    to.width_in_blocks = from.width_in_blocks;
+    to.height_in_blocks = from.height_in_blocks;
+    std::copy(from.table, from.table + 64, to.quant_table);
+    const std::size_t bytes = std::max<std::size_t>(from.coefficients.size() * sizeof(int16_t), 1);
+    to.coefficients = static_cast<int16_t*>(std::malloc(bytes));
+    if (to.coefficients == nullptr) {
+      unround_jpeg_image_free(image);
+      say(message, message_size, "out of memory");
+      return urb::kJpegMemory;
+    }
+    std::memcpy(to.coefficients, from.coefficients.data(), from.coefficients.size() * sizeof(int16_t));
+  }
+  if (!file.icc.empty()) {
+    image->icc_profile = static_cast<uint8_t*>(std::malloc(file.icc.size()));
+    if (image->icc_profile == nullptr) {
+      unround_jpeg_image_free(image);
+      say(message, message_size, "out of memory");
+      return urb::kJpegMemory;
+    }
+    std::memcpy(image->icc_profile, file.icc.data(), file.icc.size());
+    image->icc_profile_size = file.icc.size();
+  }
+  return urb::kJpegOk;
 }
 
-void unround_jpeg_image_free(unround_jpegio_image*) {}
-
-unround_jpegio_status unround_jpeg_decode_planes(const uint8_t*, size_t, const unround_jpegio_options*,
-                                                 unround_jpegio_planes*, char* message, size_t message_size) {
-  say(message, message_size, "decoding a JPEG file needs libjpeg-turbo, which this build does not carry");
-  return 3;
+void unround_jpeg_image_free(unround_jpegio_image* image) {
+  if (image == nullptr) return;
+  for (unround_jpegio_component& c : image->components) std::free(c.coefficients);
+  std::free(image->icc_profile);
+  *image = unround_jpegio_image{};
 }
 
-void unround_jpeg_planes_free(unround_jpegio_planes*) {}
+// Each component's samples (c/jpegio/include/unround/jpegio.h:116-132, 203-211): the inverse DCT
+// of its dequantized coefficients, level-shifted and clamped to 0-255, padded to whole blocks, no
+// upsampling or colour conversion. The reference's are libjpeg's integer inverse DCT; these are
+// the exact transform rounded, within 1 of it.
+unround_jpegio_status unround_jpeg_decode_planes(const uint8_t* data, size_t size, const unround_jpegio_options* options,
+                                                 unround_jpegio_planes* planes, char* message, size_t message_size) {
+  if (planes == nullptr || (message == nullptr && message_size > 0)) return urb::kJpegArgument;
+  *planes = unround_jpegio_planes{};
+  urb::JpegLimits limits;
+  if (options != nullptr) {
+    if (options->max_pixels != 0) limits.max_pixels = options->max_pixels;
+    if (options->max_scans > 0) limits.max_scans = options->max_scans;
+    limits.warnings_are_errors = options->warnings_are_errors != 0;
+  }
+  urb::JpegFile file;
+  std::string text;
+  const int status = urb::read_jpeg(data, size, limits, file, text);
+  say(message, message_size, text);
+  if (status != urb::kJpegOk) return status;
+  planes->num_components = static_cast<int32_t>(file.components.size());
+  for (std::size_t c = 0; c < file.components.size(); ++c) {
+    const std::vector<std::uint8_t> plane = urb::component_plane(file.components[c]);
+    unround_jpegio_plane& to = planes->planes[c];
+    to.width = file.components[c].width_in_blocks * 8;
+    to.height = file.components[c].height_in_blocks * 8;
+    to.stride = to.width;
+    to.samples = static_cast<uint8_t*>(std::malloc(std::max<std::size_t>(plane.size(), 1)));
+    if (to.samples == nullptr) {
+      unround_jpeg_planes_free(planes);
+      say(message, message_size, "out of memory");
+      return urb::kJpegMemory;
+    }
+    std::memcpy(to.samples, plane.data(), plane.size());
+  }
+  return urb::kJpegOk;
+}
+
+void unround_jpeg_planes_free(unround_jpegio_planes* planes) {
+  if (planes == nullptr) return;
+  for (unround_jpegio_plane& p : planes->planes) std::free(p.samples);
+  *planes = unround_jpegio_planes{};
+}
+
+// The C layer's PNG reading and writing (c/jpegio/include/unround/jpegio.h:225-256), by png_io.hpp.
+unround_jpegio_status unround_jpegio_read_png(const uint8_t* data, size_t size, uint64_t max_pixels,
+                                              unround_jpegio_png_image* image, char* message, size_t message_size) {
+  if (image == nullptr || (message == nullptr && message_size > 0)) return urb::kPngArgument;
+  *image = unround_jpegio_png_image{};
+  urb::PngPicture picture;
+  std::string text;
+  const int status = urb::read_png(data, size, max_pixels, picture, text);
+  say(message, message_size, text);
+  if (status != urb::kPngOk) return status;
+  image->samples = static_cast<uint16_t*>(std::malloc(std::max<std::size_t>(picture.samples.size() * 2, 1)));
+  image->icc_profile = picture.icc.empty() ? nullptr : static_cast<uint8_t*>(std::malloc(picture.icc.size()));
+  if (image->samples == nullptr || (!picture.icc.empty() && image->icc_profile == nullptr)) {
+    unround_jpegio_png_image_free(image);
+    say(message, message_size, "out of memory");
+    return urb::kPngMemory;
+  }
+  std::memcpy(image->samples, picture.samples.data(), picture.samples.size() * 2);
+  if (!picture.icc.empty()) std::memcpy(image->icc_profile, picture.icc.data(), picture.icc.size());
+  image->icc_profile_size = picture.icc.size();
+  image->width = picture.width;
+  image->height = picture.height;
+  image->channels = picture.channels;
+  image->bits = picture.bits;
+  return urb::kPngOk;
+}
+
+void unround_jpegio_png_image_free(unround_jpegio_png_image* image) {
+  if (image == nullptr) return;
+  std::free(image->samples);
+  std::free(image->icc_profile);
+  *image = unround_jpegio_png_image{};
+}
+
+unround_jpegio_status unround_jpegio_write_png(const unround_jpegio_png* png, unround_jpegio_bytes* file, char* message,
+                                               size_t message_size) {
+  if (file == nullptr || (message == nullptr && message_size > 0)) return urb::kPngArgument;
+  *file = unround_jpegio_bytes{};
+  if (png == nullptr) {
+    say(message, message_size, "no picture is given");
+    return urb::kPngArgument;
+  }
+  std::vector<std::uint8_t> bytes;
+  std::string warning, text;
+  const int status = urb::write_png(png->samples, png->width, png->height, png->channels, png->bits, png->compression,
+                                    png->icc_profile, static_cast<std::size_t>(png->icc_profile_size), bytes, warning,
+                                    text);
+  say(message, message_size, text);
+  if (status != urb::kPngOk) return status;
+  file->data = static_cast<uint8_t*>(std::malloc(bytes.size()));
+  if (file->data == nullptr) {
+    say(message, message_size, "out of memory");
+    return urb::kPngMemory;
+  }
+  std::memcpy(file->data, bytes.data(), bytes.size());
+  file->size = bytes.size();
+  return urb::kPngOk;
+}
+
+void unround_jpegio_bytes_free(unround_jpegio_bytes* bytes) {
+  if (bytes == nullptr) return;
+  std::free(bytes->data);
+  *bytes = unround_jpegio_bytes{};
+}
 
 }  // extern "C"

@@ -1,14 +1,15 @@
 """A JPEG file's quantized components, as the reference package's unround.jpegio gives them.
 
 The reference reads them with its C layer over libjpeg-turbo (python/src/unround/jpegio.py of
-JPEG-Unround). This build carries no libjpeg-turbo: the entropy decoding that produces the
-levels stays on the host, outside the GPU path, and `read` refuses with JpegioError. The data
-classes are the same, so that a caller that has levels and tables (from libjpeg-turbo
-elsewhere, or made in memory) builds an Image and passes it to unround.native.solve.
+JPEG-Unround). This build reads them with its own reader in the same library as the solver
+(unround_jpeg_read, unround_jpeg_decode_planes; a Huffman decoder of baseline, extended and
+progressive files written from ITU-T T.81): the same structures, statuses and data classes, so
+that read() and decode_planes() are drop-ins. image_of builds an Image of levels made in memory.
 """
 
 from __future__ import annotations
 
+import ctypes
 import enum
 from dataclasses import dataclass
 from typing import Final
@@ -139,11 +140,183 @@ def image_of(
     )
 
 
-def read(data: bytes | bytearray | memoryview, **_: object) -> Image:
-    """Refuses: reading a JPEG file needs libjpeg-turbo, which this build does not carry."""
-    raise JpegioError(ErrorKind.UNSUPPORTED, "reading a JPEG file needs libjpeg-turbo, which this build does not carry")
+class _Options(ctypes.Structure):
+    _fields_ = [("max_pixels", ctypes.c_uint64), ("max_scans", ctypes.c_int32), ("warnings_are_errors", ctypes.c_int32)]
 
 
-def decode_planes(data: bytes | bytearray | memoryview, **_: object) -> Planes:
-    """Refuses, as read() does."""
-    raise JpegioError(ErrorKind.UNSUPPORTED, "decoding a JPEG file needs libjpeg-turbo, which this build does not carry")
+class _Component(ctypes.Structure):
+    _fields_ = [
+        ("id", ctypes.c_int32),
+        ("h_samp_factor", ctypes.c_int32),
+        ("v_samp_factor", ctypes.c_int32),
+        ("quant_table_slot", ctypes.c_int32),
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("width_in_blocks", ctypes.c_uint32),
+        ("height_in_blocks", ctypes.c_uint32),
+        ("quant_table", ctypes.c_uint16 * 64),
+        ("coefficients", ctypes.POINTER(ctypes.c_int16)),
+    ]
+
+
+class _Image(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("color_space", ctypes.c_int32),
+        ("num_components", ctypes.c_int32),
+        ("max_h_samp_factor", ctypes.c_int32),
+        ("max_v_samp_factor", ctypes.c_int32),
+        ("progressive", ctypes.c_int32),
+        ("arithmetic", ctypes.c_int32),
+        ("exif_orientation", ctypes.c_int32),
+        ("warnings", ctypes.c_int32),
+        ("components", _Component * 4),
+        ("icc_profile", ctypes.POINTER(ctypes.c_uint8)),
+        ("icc_profile_size", ctypes.c_uint64),
+    ]
+
+
+class _Plane(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("stride", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("samples", ctypes.POINTER(ctypes.c_uint8)),
+    ]
+
+
+class _Planes(ctypes.Structure):
+    _fields_ = [("num_components", ctypes.c_int32), ("reserved", ctypes.c_int32), ("planes", _Plane * 4)]
+
+
+_MESSAGE: Final = 512
+_UINT64_MAX: Final = 2**64 - 1
+_INT32_MAX: Final = 2**31 - 1
+
+
+def _c_library() -> ctypes.CDLL:
+    from unround import native  # the library is loaded (and its functions bound) there
+
+    library = native._library()
+    library.unround_jpeg_read.restype = ctypes.c_int32
+    library.unround_jpeg_read.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_Options),
+                                          ctypes.POINTER(_Image), ctypes.c_char_p, ctypes.c_size_t]
+    library.unround_jpeg_image_free.restype = None
+    library.unround_jpeg_image_free.argtypes = [ctypes.POINTER(_Image)]
+    library.unround_jpeg_decode_planes.restype = ctypes.c_int32
+    library.unround_jpeg_decode_planes.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_Options),
+                                                   ctypes.POINTER(_Planes), ctypes.c_char_p, ctypes.c_size_t]
+    library.unround_jpeg_planes_free.restype = None
+    library.unround_jpeg_planes_free.argtypes = [ctypes.POINTER(_Planes)]
+    return library
+
+
+def _options(max_pixels: int, max_scans: int, *, warnings_are_errors: bool) -> _Options:
+    if not 0 <= max_pixels <= _UINT64_MAX:
+        raise JpegioError(ErrorKind.ARGUMENT, f"max_pixels is {max_pixels}, not 0 to 2**64 - 1")
+    if not 0 <= max_scans <= _INT32_MAX:
+        raise JpegioError(ErrorKind.ARGUMENT, f"max_scans is {max_scans}, not 0 to 2**31 - 1")
+    return _Options(max_pixels, max_scans, 1 if warnings_are_errors else 0)
+
+
+def _raise_for(status: int, message: str) -> None:
+    if status != 0:
+        try:
+            kind = ErrorKind(status)
+        except ValueError:
+            kind = ErrorKind.DECODE
+        raise JpegioError(kind, message)
+
+
+def _read_only[T: np.generic](array: npt.NDArray[T]) -> npt.NDArray[T]:
+    array.flags.writeable = False
+    return array
+
+
+def read(
+    data: bytes | bytearray | memoryview,
+    *,
+    max_pixels: int = 0,
+    max_scans: int = 0,
+    warnings_are_errors: bool = False,
+) -> Image:
+    """The coefficients and metadata of a JPEG file in memory (unround_jpeg_read).
+
+    max_pixels and max_scans limit what the file may declare (0 means the C layer's defaults,
+    1 << 28 pixels and 500 scans), and warnings_are_errors makes corrupt data that the reader
+    works around fail the read. The arrays are copies, read-only."""
+    options = _options(max_pixels, max_scans, warnings_are_errors=warnings_are_errors)
+    payload = bytes(data)
+    library = _c_library()
+    raw = _Image()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_jpeg_read(payload, len(payload), ctypes.byref(options), ctypes.byref(raw), message,
+                                       _MESSAGE)
+    text = message.value.decode("utf-8", "replace")
+    _raise_for(status, text)
+    try:
+        components = []
+        for index in range(raw.num_components):
+            c = raw.components[index]
+            count = c.height_in_blocks * c.width_in_blocks * 64
+            levels = np.ctypeslib.as_array(c.coefficients, shape=(count,)).copy() if count else np.zeros(0, np.int16)
+            components.append(
+                Component(
+                    id=int(c.id),
+                    h_samp_factor=int(c.h_samp_factor),
+                    v_samp_factor=int(c.v_samp_factor),
+                    quant_table_slot=int(c.quant_table_slot),
+                    width=int(c.width),
+                    height=int(c.height),
+                    quant_table=_read_only(np.array(c.quant_table, dtype=np.uint16).reshape(8, 8)),
+                    coefficients=_read_only(levels.reshape(c.height_in_blocks, c.width_in_blocks, 8, 8)),
+                )
+            )
+        icc = bytes(ctypes.string_at(raw.icc_profile, raw.icc_profile_size)) if raw.icc_profile_size else None
+        return Image(
+            width=int(raw.width),
+            height=int(raw.height),
+            color_space=ColorSpace(raw.color_space),
+            max_h_samp_factor=int(raw.max_h_samp_factor),
+            max_v_samp_factor=int(raw.max_v_samp_factor),
+            progressive=bool(raw.progressive),
+            arithmetic=bool(raw.arithmetic),
+            exif_orientation=int(raw.exif_orientation),
+            warnings=int(raw.warnings),
+            warning=text,
+            components=tuple(components),
+            icc_profile=icc,
+        )
+    finally:
+        library.unround_jpeg_image_free(ctypes.byref(raw))
+
+
+def decode_planes(
+    data: bytes | bytearray | memoryview,
+    *,
+    max_pixels: int = 0,
+    max_scans: int = 0,
+    warnings_are_errors: bool = False,
+) -> Planes:
+    """Each component's 8-bit samples (unround_jpeg_decode_planes): the inverse DCT of its
+    dequantized coefficients, level-shifted and clamped, padded to whole blocks."""
+    options = _options(max_pixels, max_scans, warnings_are_errors=warnings_are_errors)
+    payload = bytes(data)
+    library = _c_library()
+    raw = _Planes()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_jpeg_decode_planes(payload, len(payload), ctypes.byref(options), ctypes.byref(raw),
+                                                message, _MESSAGE)
+    text = message.value.decode("utf-8", "replace")
+    _raise_for(status, text)
+    try:
+        planes = []
+        for index in range(raw.num_components):
+            p = raw.planes[index]
+            flat = np.ctypeslib.as_array(p.samples, shape=(p.height * p.stride,)).copy()
+            planes.append(_read_only(flat.reshape(p.height, p.stride)[:, : p.width].copy()))
+        return Planes(tuple(planes), text)
+    finally:
+        library.unround_jpeg_planes_free(ctypes.byref(raw))

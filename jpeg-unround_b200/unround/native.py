@@ -19,8 +19,11 @@ from __future__ import annotations
 import ctypes
 import enum
 import functools
+import os
+import warnings
 from collections.abc import Callable
 from dataclasses import dataclass
+from pathlib import Path
 from typing import Final
 
 import numpy as np
@@ -207,6 +210,14 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_pnm": (i32, doubles, u64, u64, u64, i32, i32, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), u64p,
                         *text),
         "unround_bytes_free": (None, ctypes.POINTER(ctypes.c_uint8), u64),
+        "unround_png": (i32, doubles, u64, u64, u64, i32, i32, i32, ctypes.POINTER(ctypes.c_uint8), u64,
+                        ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), u64p, *text),
+        "unround_orient": (i32, doubles, u64, u64, u64, i32, doubles, u64p, u64p, *text),
+        "unround_result_icc_profile": (ctypes.POINTER(ctypes.c_uint8), handle, u64p),
+        "unround_result_exif_orientation": (i32, handle),
+        "unround_result_format": (i32, handle),
+        "unround_result_bits": (i32, handle),
+        "unround_result_warning": (ctypes.c_char_p, handle),
         "unround_b200_solve_levels": (i32, ctypes.POINTER(_Input), handle, i32, i32, ctypes.c_void_p, u64, u64p,
                                       *text),
         "unround_b200_solve_samples": (i32, ctypes.POINTER(ctypes.c_uint16), u64, u64, u64, i32, handle, *made),
@@ -471,11 +482,16 @@ def _decoded(library: ctypes.CDLL, result: ctypes.c_void_p, problems: bool = Tru
         values = [_copy(library.unround_result_record_values(result, which, ctypes.byref(n)), (int(n.value),))
                   for which in range(5)]
         solution = Solution(int(iterations.value), Stop(int(stop.value)), History(steps, *values))
+    icc_size = ctypes.c_uint64()
+    icc = library.unround_result_icc_profile(result, ctypes.byref(icc_size))
     return Decoded(
         picture=picture, planes=planes, canvas=canvas,
         color_space=jpegio.ColorSpace(int(library.unround_result_color_space(result))),
         coefficients=tuple(coefficients), problems=tuple(models), result=solution,
-        icc_profile=None, exif_orientation=0,
+        icc_profile=ctypes.string_at(icc, int(icc_size.value)) if icc and icc_size.value else None,
+        exif_orientation=int(library.unround_result_exif_orientation(result)),
+        input_format="png" if int(library.unround_result_format(result)) == 2 else "jpeg",
+        bits=int(library.unround_result_bits(result)),
     )
 
 
@@ -676,18 +692,49 @@ def model(image: jpegio.Image, settings: Settings | list[str] | None = None, com
     return out
 
 
-def decode(source: object, settings: Settings | None = None, **_: object) -> Decoded:
-    """Reading a JPEG file needs libjpeg-turbo: the library refuses with UNSUPPORTED."""
+def decode(source: object, settings: Settings | list[str] | None = None, *, observer: Observer | None = None,
+           max_pixels: int = 0, max_scans: int = 0, warnings_are_errors: bool = False) -> Decoded:
+    """Reconstructs a JPEG file or a PNG file: its bytes or its path; or a JPEG file's components as
+    unround.jpegio.read gives them (rust/capi/src/lib.rs, unround_decode).
+
+    A PNG file, known by its signature, is reconstructed within the intervals of its rounded
+    samples by TV or TGV, its colours together and its alpha alone; any other file as a JPEG file,
+    its coefficients read on the host and the iterations run on the GPU. The limits of reading are
+    those of unround.jpegio.read (a PNG file takes max_pixels alone). A warning of the reading (a
+    JPEG file's corrupt data, a PNG file's transparent colour that is not taken) is said as an
+    UnroundWarning; a file that is not reconstructed raises UnroundError."""
+    if isinstance(source, jpegio.Image):
+        if max_pixels or max_scans or warnings_are_errors:
+            raise ValueError("an image read already takes no limits of reading")
+        return solve(source, settings, observer=observer)
+    if isinstance(settings, list):
+        given = list(settings)
+        if max_pixels:
+            given += ["--max-pixels", str(max_pixels)]
+        if max_scans:
+            given += ["--max-scans", str(max_scans)]
+        if warnings_are_errors:
+            given.append("--warnings-are-errors")
+    else:
+        given = options(settings, max_pixels=max_pixels, max_scans=max_scans, warnings_are_errors=warnings_are_errors)
     library = _library()
-    handle = _settings_of(settings)
-    data = source if isinstance(source, (bytes, bytearray)) else b""
+    handle = _Settings(given)
+    data = Path(source).read_bytes() if isinstance(source, (str, os.PathLike)) else bytes(source)  # type: ignore[arg-type]
+    watcher = _Watcher(observer)
     result = ctypes.c_void_p()
     message = ctypes.create_string_buffer(_MESSAGE)
-    status = library.unround_decode(bytes(data), len(data), handle.handle, _OBSERVER(), None, ctypes.byref(result),
+    status = library.unround_decode(data, len(data), handle.handle, watcher.callback, None, ctypes.byref(result),
                                     message, _MESSAGE)
+    if watcher.error is not None:
+        if status == 0:
+            library.unround_result_free(result)
+        raise watcher.error
     _raise(status, message)
     try:
-        return _decoded(library, result)
+        warning = library.unround_result_warning(result)
+        if warning:
+            warnings.warn(warning.decode("utf-8", "replace"), UnroundWarning, stacklevel=2)
+        return _decoded(library, result, problems=int(library.unround_result_format(result)) != 2)
     finally:
         library.unround_result_free(result)
 
@@ -774,6 +821,65 @@ def pnm_bytes(picture: npt.ArrayLike, *, sixteen: bool = False, dither: str = "b
         return ctypes.string_at(pointer, int(size.value))
     finally:
         library.unround_bytes_free(pointer, size)
+
+
+def png_bytes(picture: npt.ArrayLike, *, sixteen: bool = False, dither: str = "blue-noise",
+              dither_channels: str | None = None, compression: int | None = None,
+              icc_profile: bytes | None = None) -> bytes:
+    """A PNG file of the picture's samples, (height, width) or (height, width, channels) with 1 to 4
+    channels, of 8 bits or 16, the levels made on the GPU as pnm_bytes makes them (unround_png).
+    compression is zlib's level, 0 to 9, or None for its default; the ICC profile is written where
+    it goes with the picture, and otherwise left out with an UnroundWarning."""
+    level = -1 if compression is None else compression
+    if not -1 <= level <= 9:
+        raise ValueError(f"zlib's level is 0 to 9, or None, not {compression}")
+    made = _dither(dither, dither_channels)
+    samples = np.ascontiguousarray(picture, dtype=np.float64)
+    if samples.ndim not in (2, 3):
+        raise ValueError(f"a picture is (height, width) or (height, width, channels), not {samples.shape}")
+    height, width = int(samples.shape[0]), int(samples.shape[1])
+    channels = 1 if samples.ndim == 2 else int(samples.shape[2])
+    profile = b"" if icc_profile is None else bytes(icc_profile)
+    profile_buffer = (ctypes.c_uint8 * max(len(profile), 1)).from_buffer_copy(profile or b"\0")
+    library = _library()
+    pointer = ctypes.POINTER(ctypes.c_uint8)()
+    size = ctypes.c_uint64()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_png(samples.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), height, width, channels,
+                                 1 if sixteen else 0, made, level,
+                                 profile_buffer if icc_profile is not None else None, len(profile),
+                                 ctypes.byref(pointer), ctypes.byref(size), message, _MESSAGE)
+    _raise(status, message)
+    try:
+        if message.value:
+            warnings.warn(message.value.decode("utf-8", "replace"), UnroundWarning, stacklevel=2)
+        return ctypes.string_at(pointer, int(size.value))
+    finally:
+        library.unround_bytes_free(pointer, size)
+
+
+def oriented(picture: npt.ArrayLike, orientation: int) -> Array:
+    """The picture, (height, width) or (height, width, channels), turned upright as EXIF's
+    orientation says (unround_orient): 1 to 8, or 0 where the file has none, which is 1; from 5 on,
+    the rows become columns. Every sample of the result is one of the picture's, bit for bit."""
+    samples = np.ascontiguousarray(picture, dtype=np.float64)
+    if samples.ndim not in (2, 3):
+        raise ValueError(f"a picture is (height, width) or (height, width, channels), not {samples.shape}")
+    if not -(2**31) <= orientation < 2**31:
+        raise ValueError(f"an EXIF orientation is 1 to 8, or 0 for none, not {orientation}")
+    height, width = int(samples.shape[0]), int(samples.shape[1])
+    channels = 1 if samples.ndim == 2 else int(samples.shape[2])
+    turned = np.empty(samples.size, dtype=np.float64)
+    rows, columns = ctypes.c_uint64(), ctypes.c_uint64()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    doubles = ctypes.POINTER(ctypes.c_double)
+    library = _library()
+    status = library.unround_orient(samples.ctypes.data_as(doubles), height, width, channels, orientation,
+                                    turned.ctypes.data_as(doubles), ctypes.byref(rows), ctypes.byref(columns), message,
+                                    _MESSAGE)
+    _raise(status, message)
+    shape = (int(rows.value), int(columns.value)) + (() if samples.ndim == 2 else (channels,))
+    return turned.reshape(shape)
 
 
 def solve_levels(image: jpegio.Image, settings: Settings | list[str] | None = None, *, sixteen: bool = False,

@@ -84,9 +84,14 @@ def test_every_refusal_at_once():
     assert "--mu" in raised.value.message and "--relaxation" in raised.value.message
 
 
-def test_unsupported_file_paths():
+def test_file_paths_refuse_what_they_cannot_read():
+    # A JPEG file cut after its first marker holds no image: READ, before any device is needed.
     with pytest.raises(native.UnroundError) as raised:
         native.decode(b"\xff\xd8\xff")
+    assert raised.value.status == native.Status.READ
+    # The projection onto a file's intervals is not on this build's path.
+    with pytest.raises(native.UnroundError) as raised:
+        native.project(np.zeros((8, 8)), b"\xff\xd8\xff\xd9")
     assert raised.value.status == native.Status.UNSUPPORTED
 
 
@@ -106,3 +111,23 @@ def test_solve_fails_loudly_without_a_device():
         native.solve(image, ["--method", "tv", "--iterations", "2"])
     assert raised.value.status == native.Status.INTERNAL
     assert "CUDA" in raised.value.message
+
+
+@pytest.mark.parametrize("orientation", range(9))
+def test_oriented_turns_as_exif_says(orientation):
+    # EXIF 2.3 tag 0x0112 (the reference's rust/unround/src/orientation.rs): 0 or 1 as stored,
+    # 2 mirrored, 3 half round, 4 flipped, 5 transposed, 6 a quarter clockwise, 7 transversed,
+    # 8 a quarter anticlockwise.
+    picture = np.arange(3 * 5 * 2, dtype=np.float64).reshape(3, 5, 2)
+    expected = {
+        0: picture, 1: picture, 2: picture[:, ::-1], 3: picture[::-1, ::-1], 4: picture[::-1],
+        5: picture.transpose(1, 0, 2), 6: np.rot90(picture, -1), 7: np.rot90(picture, -1)[::-1],
+        8: np.rot90(picture, 1),
+    }[orientation]
+    np.testing.assert_array_equal(native.oriented(picture, orientation), expected)
+    np.testing.assert_array_equal(native.oriented(picture[..., 0], orientation), expected[..., 0])
+
+
+def test_oriented_refuses_what_is_no_orientation():
+    with pytest.raises(native.UnroundError):
+        native.oriented(np.zeros((2, 3)), 9)
