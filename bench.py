@@ -180,6 +180,57 @@ def _traffic() -> float | None:
         return None
 
 
+def _jpeg_file(seed: int) -> bytes:
+    """The workload's picture (the same generator, size and noise) as a JPEG file, quality 75, 4:2:0,
+    written by Pillow's libjpeg-turbo: the file path's input."""
+    import io
+
+    import numpy as np
+    from PIL import Image
+
+    from unround import synthetic
+
+    rgb = synthetic.colour(HEIGHT, WIDTH, quality=75, seed=seed, noise=3.0).samples
+    buffer = io.BytesIO()
+    Image.fromarray(np.clip(np.rint(rgb), 0, 255).astype(np.uint8)).save(buffer, format="JPEG", quality=75,
+                                                                         subsampling=2)
+    return buffer.getvalue()
+
+
+def _call_file(data: bytes) -> int:
+    """One solve of a JPEG file through unround_decode: the file's bytes in (the coefficients read
+    on the host by the library), the binary64 canvas and picture out and read on the host."""
+    import ctypes
+
+    import numpy as np
+
+    from unround import native
+
+    library = native._library()
+    settings = native._Settings(OPTIONS)
+    result = ctypes.c_void_p()
+    message = ctypes.create_string_buffer(4096)
+    status = library.unround_decode(data, len(data), settings.handle, native._OBSERVER(), None, ctypes.byref(result),
+                                    message, 4096)
+    if status != 0:
+        raise RuntimeError(message.value.decode())
+    try:
+        c, h, w = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        canvas = np.ctypeslib.as_array(library.unround_result_canvas(result, ctypes.byref(c), ctypes.byref(h),
+                                                                     ctypes.byref(w)),
+                                       shape=(c.value * h.value * w.value,))
+        ph, pw, pc = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        picture = np.ctypeslib.as_array(library.unround_result_picture(result, ctypes.byref(ph), ctypes.byref(pw),
+                                                                       ctypes.byref(pc)),
+                                        shape=(ph.value * pw.value * pc.value,))
+        if not (np.isfinite(canvas[:: max(1, canvas.size // 4096)]).all()
+                and np.isfinite(picture[:: max(1, picture.size // 4096)]).all()):
+            raise RuntimeError("the result holds values that are not finite")
+        return canvas.nbytes + picture.nbytes
+    finally:
+        library.unround_result_free(result)
+
+
 def _call(image) -> int:
     """One solve through the C interface, as a C or cgo caller makes it: unround_solve on host
     arrays (levels in; the binary64 canvas, coefficients and RGB picture out, into the result),
@@ -682,6 +733,14 @@ def main() -> None:
         levels_d2h = _call_levels(image, levels)
     levels_seconds = max_over_ranks(time.perf_counter() - began)
     e2e_levels = world * pixels * args.steps * ITERATIONS / levels_seconds / 1e6
+    # From a JPEG file's bytes: the host reads the coefficients, the rest as e2e.
+    jpeg = _jpeg_file(seed=rank)
+    _call_file(jpeg)  # warm the call path
+    began = time.perf_counter()
+    for _ in range(args.steps):
+        file_d2h = _call_file(jpeg)
+    file_seconds = max_over_ranks(time.perf_counter() - began)
+    e2e_file = world * pixels * args.steps * ITERATIONS / file_seconds / 1e6
     peak, peak_kind = _peaks()
     samples = timing.samples
     dual_achieved = DUAL_BYTES * samples / (timing.dual_milliseconds / 1e3) / 1e9
@@ -707,6 +766,10 @@ def main() -> None:
             "e2e_levels": {"value": e2e_levels, "unit": UNIT, "h2d_bytes_per_step": levels_bytes,
                            "d2h_bytes_per_step": levels_d2h,
                            "call": "unround_b200_solve_levels, 8 bits, blue-noise dither"},
+            "e2e_file": {"value": e2e_file, "unit": UNIT, "h2d_bytes_per_step": len(jpeg),
+                         "d2h_bytes_per_step": file_d2h,
+                         "call": "unround_decode of a JPEG file (quality 75, 4:2:0, Pillow-written) of the "
+                                 "workload's picture; coefficients read on the host"},
             "gpu_launches": timing.launches_per_iteration * args.steps * ITERATIONS,
             "clocks": clocks.summary(),
         }
