@@ -69,6 +69,9 @@ typedef struct unround_b200_batch_timing {
   uint64_t launches_per_iteration;
   uint64_t samples;
   uint64_t pixels;
+  /* The autotuner's measurements of the classes' tile heights, before the timed part (0 when a
+   * batch of the same shapes was measured before in the process, or UNROUND_B200_AUTOTUNE=0). */
+  double tuning_milliseconds;
 } unround_b200_batch_timing;
 
 unround_status unround_b200_solve_batch(uint64_t count, const unround_input* inputs,

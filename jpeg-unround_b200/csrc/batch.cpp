@@ -2,8 +2,10 @@
 #include "batch.hpp"
 
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 
@@ -46,6 +48,7 @@ struct DualClass {
   std::vector<int> pictures;       // of the batch, in this class
   std::vector<Geometry> geometry;  // theirs
   std::vector<DualTile> tiles;
+  int tile_rows = 0;
   DualTile* device = nullptr;
 };
 
@@ -89,6 +92,86 @@ struct Branches {
     return e;
   }
 };
+
+// A class's tiles: strips of 32 columns of each of its pictures, cut into tiles of `rows` rows.
+std::vector<DualTile> tiles_of(const DualClass& dual, int rows) {
+  std::vector<DualTile> tiles;
+  for (std::size_t m = 0; m < dual.pictures.size(); ++m) {
+    const Geometry& g = dual.geometry[m];
+    for (int x0 = 0; x0 < g.columns; x0 += 32) {
+      for (int i0 = 0; i0 < g.rows; i0 += rows) tiles.push_back({dual.pictures[m], x0, i0, std::min(i0 + rows, g.rows)});
+    }
+  }
+  return tiles;
+}
+
+// The autotuner's record: per device, class and the sizes of its pictures, the tile height its
+// measurement chose, so that a batch of the same shapes is measured once in a process.
+using TuneKey = std::tuple<int, bool, int, bool, std::vector<std::pair<int, int>>>;
+std::mutex tune_mutex;
+std::map<TuneKey, int>& tuned() {
+  static auto* record = new std::map<TuneKey, int>();  // never destroyed: used until exit
+  return *record;
+}
+
+bool autotune_enabled() {
+  const char* given = std::getenv("UNROUND_B200_AUTOTUNE");
+  return given == nullptr || std::string(given) != "0";
+}
+
+// Measures a class's dual sweep at candidate tile heights and returns the fastest: the wave
+// model's choice (batch_tile_rows), the heights beside it, and a spread from 96 to 512. Each
+// candidate's table is launched once to warm up and timed over three launches by CUDA events;
+// a candidate replaces the model's choice only when it is at least 2% faster. The launches read
+// the state of parity 0 and the start's tilde point and write the state of parity 1, which the
+// first iteration writes again: they change nothing the solve reads.
+int tune_dual(const DualClass& dual, const DualBatchImage* images_device, cudaStream_t stream, cudaError_t& error) {
+  const int model = batch_tile_rows(dual.geometry, dual_batch_slots(dual.tgv, dual.channels, dual.coupled));
+  std::vector<int> candidates = {model};
+  for (int h : {model - 32, model + 32, 96, 128, 192, 256, 320, 384, 512}) {
+    if (h >= 64 && h <= 512 && std::find(candidates.begin(), candidates.end(), h) == candidates.end()) {
+      candidates.push_back(h);
+    }
+  }
+  cudaEvent_t begin = nullptr, end = nullptr;
+  if (error == cudaSuccess) error = cudaEventCreate(&begin);
+  if (error == cudaSuccess) error = cudaEventCreate(&end);
+  int best = model;
+  float best_ms = -1.0f, model_ms = -1.0f;
+  for (int rows : candidates) {
+    if (error != cudaSuccess) break;
+    const std::vector<DualTile> tiles = tiles_of(dual, rows);
+    void* table = nullptr;
+    error = cudaMallocAsync(&table, tiles.size() * sizeof(DualTile), stream);
+    if (error != cudaSuccess) break;
+    error = cudaMemcpyAsync(table, tiles.data(), tiles.size() * sizeof(DualTile), cudaMemcpyHostToDevice, stream);
+    const int count = static_cast<int>(tiles.size());
+    auto launch = [&] {
+      if (error == cudaSuccess) {
+        error = launch_dual_batch(static_cast<const DualTile*>(table), count, images_device, 0, dual.tgv, dual.channels,
+                                  dual.coupled, stream);
+      }
+    };
+    launch();
+    if (error == cudaSuccess) error = cudaEventRecord(begin, stream);
+    for (int r = 0; r < 3; ++r) launch();
+    if (error == cudaSuccess) error = cudaEventRecord(end, stream);
+    if (error == cudaSuccess) error = cudaEventSynchronize(end);
+    float ms = 0.0f;
+    if (error == cudaSuccess) error = cudaEventElapsedTime(&ms, begin, end);
+    cudaFreeAsync(table, stream);
+    if (error != cudaSuccess) break;
+    if (rows == model) model_ms = ms;
+    if (best_ms < 0.0f || ms < best_ms) {
+      best_ms = ms;
+      best = rows;
+    }
+  }
+  if (begin != nullptr) cudaEventDestroy(begin);
+  if (end != nullptr) cudaEventDestroy(end);
+  if (error != cudaSuccess || model_ms < 0.0f) return model;
+  return best_ms < 0.98f * model_ms ? best : model;
+}
 
 struct PrimalClass {
   int cell_rows = 1;
@@ -164,27 +247,52 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
       components.push_back(own[c]);
     }
   }
-  // Each class's tiles: strips of 32 columns cut into tiles of the height that finishes the
-  // class's pictures soonest in waves of the CTAs the device holds.
-  for (auto& [key, dual] : duals) {
-    const int rows = batch_tile_rows(dual.geometry, dual_batch_slots(dual.tgv, dual.channels, dual.coupled));
-    for (std::size_t m = 0; m < dual.pictures.size(); ++m) {
-      const Geometry& g = dual.geometry[m];
-      for (int x0 = 0; x0 < g.columns; x0 += 32) {
-        for (int i0 = 0; i0 < g.rows; i0 += rows) {
-          dual.tiles.push_back({dual.pictures[m], x0, i0, std::min(i0 + rows, g.rows)});
-        }
-      }
-    }
-  }
   Owned owned(stream);
   DualBatchImage* images_device = nullptr;
   PrimalBatchComponent* components_device = nullptr;
   cudaError_t error = owned.upload(images, &images_device);
   if (error == cudaSuccess) error = owned.upload(components, &components_device);
+  // Each class's tiles: strips of 32 columns cut into tiles of the height that finishes the
+  // class's pictures soonest in waves of the CTAs the device holds (the wave model), or, with
+  // the autotuner (on unless UNROUND_B200_AUTOTUNE=0), the height its measurement chose.
+  int device = 0;
+  if (error == cudaSuccess) error = cudaGetDevice(&device);
+  cudaEvent_t tune_begin = nullptr, tune_end = nullptr;
+  const bool tuning = autotune_enabled();
+  if (tuning && error == cudaSuccess) error = cudaEventCreate(&tune_begin);
+  if (tuning && error == cudaSuccess) error = cudaEventCreate(&tune_end);
+  if (tuning && error == cudaSuccess) error = cudaEventRecord(tune_begin, stream);
   for (auto& [key, dual] : duals) {
+    int rows = batch_tile_rows(dual.geometry, dual_batch_slots(dual.tgv, dual.channels, dual.coupled));
+    if (tuning && error == cudaSuccess) {
+      std::vector<std::pair<int, int>> sizes;
+      for (const Geometry& g : dual.geometry) sizes.emplace_back(g.rows, g.columns);
+      std::sort(sizes.begin(), sizes.end());
+      const TuneKey tune_key{device, dual.tgv, dual.channels, dual.coupled, sizes};
+      std::unique_lock<std::mutex> lock(tune_mutex);
+      const auto found = tuned().find(tune_key);
+      if (found != tuned().end()) {
+        rows = found->second;
+      } else {
+        lock.unlock();
+        rows = tune_dual(dual, images_device, stream, error);
+        lock.lock();
+        if (error == cudaSuccess) tuned()[tune_key] = rows;
+      }
+    }
+    dual.tile_rows = rows;
+    dual.tiles = tiles_of(dual, rows);
     if (error == cudaSuccess) error = owned.upload(dual.tiles, &dual.device);
   }
+  if (tuning && error == cudaSuccess) error = cudaEventRecord(tune_end, stream);
+  if (tuning && error == cudaSuccess) error = cudaEventSynchronize(tune_end);
+  if (tuning && error == cudaSuccess) {
+    float ms = 0.0f;
+    error = cudaEventElapsedTime(&ms, tune_begin, tune_end);
+    timing.tuning_milliseconds = ms;
+  }
+  if (tune_begin != nullptr) cudaEventDestroy(tune_begin);
+  if (tune_end != nullptr) cudaEventDestroy(tune_end);
   for (auto& [key, primal] : primals) {
     if (error == cudaSuccess) error = owned.upload(primal.items, &primal.device);
   }

@@ -33,6 +33,7 @@ struct BatchTiming {
   std::uint64_t launches_per_iteration = 0;
   std::uint64_t samples = 0;
   std::uint64_t pixels = 0;
+  double tuning_milliseconds = 0.0;  // the autotuner's measurements, before the timed part
 };
 
 // All entries' plans have the same number of iterations and record at the last only

@@ -693,6 +693,7 @@ unround_status unround_b200_solve_batch(uint64_t count, const unround_input* inp
       timing->launches_per_iteration = measured.launches_per_iteration;
       timing->samples = measured.samples;
       timing->pixels = measured.pixels;
+      timing->tuning_milliseconds = measured.tuning_milliseconds;
     }
     for (uint64_t n = 0; n < count; ++n) results[n] = result_of(std::move(frames[n]), std::move(outcomes[n]));
     return true;

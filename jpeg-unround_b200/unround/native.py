@@ -131,6 +131,7 @@ class _BatchTiming(ctypes.Structure):
         ("launches_per_iteration", ctypes.c_uint64),
         ("samples", ctypes.c_uint64),
         ("pixels", ctypes.c_uint64),
+        ("tuning_milliseconds", ctypes.c_double),
     )
 
 
@@ -624,13 +625,14 @@ def measure(image: jpegio.Image, settings: Settings | list[str] | None = None, *
 class BatchTiming:
     """solve_batch(): the device milliseconds of the batched iterations (CUDA events), their
     count, the launches an iteration of the whole batch takes, and all pictures' samples and
-    pixels."""
+    pixels; and the milliseconds the autotuner measured the tile heights for, before them."""
 
     milliseconds: float
     iterations: int
     launches_per_iteration: int
     samples: int
     pixels: int
+    tuning_milliseconds: float = 0.0
 
 
 def solve_batch(images: list[jpegio.Image], settings: Settings | list[str] | list | None = None
@@ -662,7 +664,7 @@ def solve_batch(images: list[jpegio.Image], settings: Settings | list[str] | lis
         _raise(status, message)
         decoded = [_decoded(library, results[n]) for n in range(count)]
         return decoded, BatchTiming(timing.milliseconds, int(timing.iterations), int(timing.launches_per_iteration),
-                                    int(timing.samples), int(timing.pixels))
+                                    int(timing.samples), int(timing.pixels), float(timing.tuning_milliseconds))
     finally:
         for n in range(count):
             if results[n]:

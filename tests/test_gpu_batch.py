@@ -84,3 +84,26 @@ def test_few_iterations(iterations):
     assert timing.iterations == iterations - 1
     for n, (b, a) in enumerate(zip(decoded, alone)):
         _same(b, a, f"picture {n}")
+
+
+def test_the_autotuner_measures_once_and_changes_no_result(monkeypatch):
+    # The autotuner times each class's dual sweep at candidate tile heights before the loop
+    # (launches that write only what the first iteration writes again): a batch of new shapes is
+    # measured, the same shapes again are not, and the results agree with the wave model's tiles
+    # and with each picture alone.
+    from unround import native, synthetic
+
+    entries = synthetic.mix(8, seed=21, smallest=64, largest=400, iterations=20)
+    images, options = [e.image for e in entries], [e.options for e in entries]
+    first, timing = native.solve_batch(images, options)
+    assert timing.tuning_milliseconds > 0
+    again, timing = native.solve_batch(images, options)
+    assert timing.tuning_milliseconds == 0
+    monkeypatch.setenv("UNROUND_B200_AUTOTUNE", "0")
+    modelled, timing = native.solve_batch(images, options)
+    assert timing.tuning_milliseconds == 0
+    for n, entry in enumerate(entries):
+        alone = native.solve(entry.image, entry.options)
+        np.testing.assert_array_equal(first[n].canvas, again[n].canvas)
+        _same(first[n], alone, f"picture {n} tuned")
+        _same(modelled[n], alone, f"picture {n} modelled")
