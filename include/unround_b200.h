@@ -69,8 +69,9 @@ typedef struct unround_b200_batch_timing {
   uint64_t launches_per_iteration;
   uint64_t samples;
   uint64_t pixels;
-  /* The autotuner's measurements of the classes' tile heights, before the timed part (0 when a
-   * batch of the same shapes was measured before in the process, or UNROUND_B200_AUTOTUNE=0). */
+  /* The autotuner's measurements of the classes' tile heights, before the timed part: with
+   * UNROUND_B200_AUTOTUNE=1 in the environment, 0 when a batch of the same shapes was measured
+   * before in the process; without it the wave model chooses and this is 0. */
   double tuning_milliseconds;
 } unround_b200_batch_timing;
 

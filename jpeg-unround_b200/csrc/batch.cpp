@@ -116,7 +116,7 @@ std::map<TuneKey, int>& tuned() {
 
 bool autotune_enabled() {
   const char* given = std::getenv("UNROUND_B200_AUTOTUNE");
-  return given == nullptr || std::string(given) != "0";
+  return given != nullptr && std::string(given) == "1";
 }
 
 // Measures a class's dual sweep at candidate tile heights and returns the fastest: the wave
@@ -254,11 +254,12 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
   if (error == cudaSuccess) error = owned.upload(components, &components_device);
   // Each class's tiles: strips of 32 columns cut into tiles of the height that finishes the
   // class's pictures soonest in waves of the CTAs the device holds (the wave model), or, with
-  // the autotuner (on unless UNROUND_B200_AUTOTUNE=0), the height its measurement chose.
+  // the autotuner (UNROUND_B200_AUTOTUNE=1), the height its measurement chose.
   int device = 0;
   if (error == cudaSuccess) error = cudaGetDevice(&device);
   cudaEvent_t tune_begin = nullptr, tune_end = nullptr;
   const bool tuning = autotune_enabled();
+  bool measured = false;  // a class was measured in this call (not found in the record)
   if (tuning && error == cudaSuccess) error = cudaEventCreate(&tune_begin);
   if (tuning && error == cudaSuccess) error = cudaEventCreate(&tune_end);
   if (tuning && error == cudaSuccess) error = cudaEventRecord(tune_begin, stream);
@@ -276,6 +277,7 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
       } else {
         lock.unlock();
         rows = tune_dual(dual, images_device, stream, error);
+        measured = true;
         lock.lock();
         if (error == cudaSuccess) tuned()[tune_key] = rows;
       }
@@ -289,7 +291,7 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
   if (tuning && error == cudaSuccess) {
     float ms = 0.0f;
     error = cudaEventElapsedTime(&ms, tune_begin, tune_end);
-    timing.tuning_milliseconds = ms;
+    timing.tuning_milliseconds = measured ? ms : 0.0;
   }
   if (tune_begin != nullptr) cudaEventDestroy(tune_begin);
   if (tune_end != nullptr) cudaEventDestroy(tune_end);

@@ -95,11 +95,12 @@ def test_the_autotuner_measures_once_and_changes_no_result(monkeypatch):
 
     entries = synthetic.mix(8, seed=21, smallest=64, largest=400, iterations=20)
     images, options = [e.image for e in entries], [e.options for e in entries]
+    monkeypatch.setenv("UNROUND_B200_AUTOTUNE", "1")
     first, timing = native.solve_batch(images, options)
     assert timing.tuning_milliseconds > 0
     again, timing = native.solve_batch(images, options)
     assert timing.tuning_milliseconds == 0
-    monkeypatch.setenv("UNROUND_B200_AUTOTUNE", "0")
+    monkeypatch.delenv("UNROUND_B200_AUTOTUNE")
     modelled, timing = native.solve_batch(images, options)
     assert timing.tuning_milliseconds == 0
     for n, entry in enumerate(entries):
