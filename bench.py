@@ -404,6 +404,7 @@ def _mix_arm(args: argparse.Namespace, rank: int, world: int) -> None:
 
 
 SAMPLES_BYTES = 18.0  # the samples' primal step: x, p1, p2 and the 16-bit level read, x~ written
+SAMPLES_FUSED_BYTES = DUAL_BYTES + 6.0  # the fused sweep: the dual step's, the level read, x~ written
 
 
 def _samples_arm(args: argparse.Namespace, rank: int, world: int) -> None:
@@ -425,6 +426,12 @@ def _samples_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     with Clocks(0) as clocks:
         timing = native.measure_samples(levels, 8, options, warmup=max(3, args.warmup) * 10,
                                         iterations=args.steps * ITERATIONS)
+    # The loop as one fused sweep an iteration (UNROUND_B200_KERNELS=fused), beside.
+    os.environ["UNROUND_B200_KERNELS"] = "fused"
+    try:
+        other = native.measure_samples(levels, 8, options, warmup=30, iterations=ITERATIONS)
+    finally:
+        del os.environ["UNROUND_B200_KERNELS"]
     seconds = max_over_ranks(timing.milliseconds / 1e3)
     pixels = timing.pixels
     value = world * pixels * args.steps * ITERATIONS / seconds / 1e6
@@ -458,6 +465,7 @@ def _samples_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     dual = DUAL_BYTES * timing.samples / (timing.dual_milliseconds / 1e3) / 1e9
     primal = SAMPLES_BYTES * timing.samples / (timing.primal_milliseconds / 1e3) / 1e9
     iteration = (DUAL_BYTES + SAMPLES_BYTES) * timing.samples / (seconds / (args.steps * ITERATIONS)) / 1e9
+    fused = SAMPLES_FUSED_BYTES * other.samples / (other.dual_milliseconds / 1e3) / 1e9
     if rank != 0:
         return
     line = {
@@ -469,10 +477,14 @@ def _samples_arm(args: argparse.Namespace, rank: int, world: int) -> None:
                    "alpha0": 2.0, "samples": timing.samples, "l2": "state larger than L2, no flush"},
         "roofline": {"bound": "hbm", "kernel": "dual_kernel<tgv,3,coupled>", "achieved": dual, "peak": peak,
                      "unit": "GB/s", "frac": dual / peak, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_sample": DUAL_BYTES, "dual_ms": timing.dual_milliseconds,
                      "samples_primal_achieved": primal, "samples_primal_frac": primal / peak,
-                     "samples_primal_bytes_per_sample": SAMPLES_BYTES, "iteration_achieved": iteration,
-                     "iteration_frac": iteration / peak, "dual_ms": timing.dual_milliseconds,
-                     "primal_ms": timing.primal_milliseconds},
+                     "samples_primal_bytes_per_sample": SAMPLES_BYTES, "primal_ms": timing.primal_milliseconds,
+                     "iteration_achieved": iteration, "iteration_frac": iteration / peak,
+                     "fused_sweep": {"kernel": "samples_iteration_kernel<tgv,3,coupled>",
+                                     "iteration_ms": other.milliseconds / other.iterations,
+                                     "bytes_per_sample": SAMPLES_FUSED_BYTES, "achieved": fused,
+                                     "frac": fused / peak}},
         "e2e": {"value": world * pixels * args.steps * ITERATIONS / e2e_seconds / 1e6, "unit": "Mpx*iter/s",
                 "h2d_bytes_per_step": int(levels.nbytes), "d2h_bytes_per_step": d2h},
         "gpu_launches": timing.launches_per_iteration * args.steps * ITERATIONS,

@@ -651,6 +651,266 @@ __global__ void __launch_bounds__(32 * kWarps, 2)
   }
 }
 
+// Pictures of rounded samples in one sweep (samples.cu has the split kernels): the dual step D_n
+// as iteration_kernel's phase A makes it, then in phase B the r step and the primal step
+// P_{n+1} sample by sample -- v = x_n + tau gamma div p_n and x~ = clip((v + t c) r, a, b), the
+// ends and centre by the sample's level from the binary32 table -- so that x_n and p_n go from
+// registers into the proximal map and x~ is written once: 68 bytes a sample of the dual sweep
+// plus the level read and x~ written, against 86 for the two launches. Ragged last chunks are
+// taken (rows past the picture write nothing).
+template <bool TGV, int C, bool COUPLED>
+__global__ void __launch_bounds__(32 * kWarps, 2)
+    samples_iteration_kernel(const __grid_constant__ CUtensorMap state_map,
+                             const __grid_constant__ CUtensorMap tilde_map, const SamplesIterationParams P) {
+  constexpr int F = TGV ? 8 : 3;
+  constexpr int PLANE = kBox * kSpan;
+  constexpr int TOFF = (F * C * PLANE + 31) / 32 * 32;
+  constexpr int STRIDE = (TOFF + C * PLANE + 31) / 32 * 32;
+  extern __shared__ __align__(128) float ring[];
+  __shared__ __align__(8) std::uint64_t bars[2];
+  __shared__ float wbar[TGV ? C : 1][2][kRows][32];
+  __shared__ float wcarry[TGV ? C : 1][2][32];
+  __shared__ float p2rows[C][kRows][32];
+  __shared__ float p2carry[C][32];
+  __shared__ float wleft[TGV ? C : 1][2][kRows];
+  __shared__ float pleft[C][kRows];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const Geometry& g = P.dual.g;
+  const int rows = g.rows, columns = g.columns, pitch = g.pitch;
+  const std::size_t plane = g.plane;
+  const int x0 = blockIdx.x * 32;
+  const int i0 = blockIdx.y * P.strip_rows;
+  const int i1 = min(i0 + P.strip_rows, rows);
+  const int chunks = (i1 - i0 + kRows - 1) / kRows;
+  const float rho = P.dual.rho, rest = P.dual.rest;
+
+  if (tid == 0) {
+    barrier_init(&bars[0], 1);
+    barrier_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int k) {
+    if (tid == 0 && k < chunks) {
+      float* to = ring + (k & 1) * STRIDE;
+      const int chunk_row = i0 + k * kRows;
+      barrier_expect(&bars[k & 1], (F * C + C) * PLANE * 4);
+      load_box(to, &state_map, &bars[k & 1], x0 - kHalo, chunk_row, 0);
+      load_box(to + TOFF, &tilde_map, &bars[k & 1], x0 - kHalo, chunk_row, 0);
+    }
+  };
+  issue(0);
+  issue(1);
+
+  const int j = x0 + lane;
+  const bool valid = j < columns;
+  const int jc = valid ? j : columns - 1;
+  const bool has_left = j > 0, has_right = j + 1 < columns;
+
+  // The row above the strip, made from global memory by the first row warp.
+  if (warp == 0) {
+    if (i0 > 0) {
+      const int u = i0 - 1;
+      PixelDual d[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const std::size_t base = c * plane;
+        const Fields& in = P.dual.in;
+        const float* planes[8] = {in.x, in.p1, in.p2, in.w1, in.w2, in.r11, in.r22, in.r12};
+        auto at = [&](int field, int dr, int dc) -> float {
+          return __ldg(planes[field] + base + static_cast<std::size_t>(u + dr) * pitch + jc + dc);
+        };
+        auto xt = [&](int dr, int dc) -> float {
+          return __ldg(P.dual.xt + base + static_cast<std::size_t>(u + dr) * pitch + jc + dc);
+        };
+        d[c] = pixel_dual<TGV>(at, xt, has_right, true, P.dual.sigma[c], P.dual.tau[c]);
+      }
+      float scale[C];
+      p_scales<C, COUPLED>(d, P.dual.radius, scale);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        if constexpr (TGV) {
+          wcarry[c][0][lane] = d[c].wb1;
+          wcarry[c][1][lane] = d[c].wb2;
+        }
+        p2carry[c][lane] = rho * (d[c].s2 * scale[c]) + rest * d[c].p2;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        if constexpr (TGV) {
+          wcarry[c][0][lane] = 0.0f;
+          wcarry[c][1][lane] = 0.0f;
+        }
+        p2carry[c][lane] = 0.0f;
+      }
+    }
+  }
+  __syncthreads();
+
+  bool failed = false;
+  int stopped = chunks;
+  for (int k = 0; k < chunks; ++k) {
+    const bool ready = barrier_wait(&bars[k & 1], (k >> 1) & 1);
+    if (__syncthreads_or(!ready)) {
+      failed = true;
+      stopped = k;
+      break;
+    }
+    const float* slot = ring + (k & 1) * STRIDE;
+    const int chunk_row = i0 + k * kRows;
+    const int r = warp;
+    const int i = chunk_row + r;
+    const bool row_in = i < i1;  // warp-uniform
+    // ---- A: the dual step at the warp's pixel (row warps), at column x0 - 1 (side warp).
+    float xn[C], pn1[C], pn2[C], wb1[C], wb2[C];
+    if (warp < kRows) {
+      const bool has_down = i + 1 < rows;
+      const int own = kHalo + lane;
+      PixelDual d[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        auto at = [&](int field, int dr, int dc) -> float {
+          return slot[((field * C + c) * kBox + r + dr) * kSpan + own + dc];
+        };
+        auto xt = [&](int dr, int dc) -> float { return slot[TOFF + (c * kBox + r + dr) * kSpan + own + dc]; };
+        d[c] = pixel_dual<TGV>(at, xt, has_right, has_down, P.dual.sigma[c], P.dual.tau[c]);
+      }
+      float scale[C];
+      p_scales<C, COUPLED>(d, P.dual.radius, scale);
+      const std::size_t here = static_cast<std::size_t>(row_in ? i : i0) * pitch + jc;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const std::size_t at = c * plane + here;
+        xn[c] = rho * d[c].xt + rest * d[c].x;
+        pn1[c] = rho * (d[c].s1 * scale[c]) + rest * d[c].p1;
+        pn2[c] = rho * (d[c].s2 * scale[c]) + rest * d[c].p2;
+        wb1[c] = d[c].wb1;
+        wb2[c] = d[c].wb2;
+        if (valid && row_in) {
+          P.dual.out.x[at] = xn[c];
+          P.dual.out.p1[at] = pn1[c];
+          P.dual.out.p2[at] = pn2[c];
+          if constexpr (TGV) {
+            P.dual.out.w1[at] = rho * d[c].t1 + rest * d[c].w1;
+            P.dual.out.w2[at] = rho * d[c].t2 + rest * d[c].w2;
+          }
+        }
+        if constexpr (TGV) {
+          wbar[c][0][r][lane] = wb1[c];
+          wbar[c][1][r][lane] = wb2[c];
+        }
+        p2rows[c][r][lane] = pn2[c];
+      }
+    } else if (lane < kRows && x0 > 0) {
+      const int rr = lane, ii = chunk_row + rr;
+      const int col = kHalo - 1;
+      PixelDual e[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        auto at = [&](int field, int dr, int dc) -> float {
+          return slot[((field * C + c) * kBox + rr + dr) * kSpan + col + dc];
+        };
+        auto xt = [&](int dr, int dc) -> float { return slot[TOFF + (c * kBox + rr + dr) * kSpan + col + dc]; };
+        e[c] = pixel_dual<TGV>(at, xt, true, ii + 1 < rows, P.dual.sigma[c], P.dual.tau[c]);
+      }
+      float scale[C];
+      p_scales<C, COUPLED>(e, P.dual.radius, scale);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        if constexpr (TGV) {
+          wleft[c][0][rr] = e[c].wb1;
+          wleft[c][1][rr] = e[c].wb2;
+        }
+        pleft[c][rr] = rho * (e[c].s1 * scale[c]) + rest * e[c].p1;
+      }
+    }
+    __syncthreads();
+
+    // ---- B: the r step; v; the proximal map of the samples' boxes; x~_{n+1}.
+    if (warp < kRows && row_in) {
+      const bool has_down = i + 1 < rows, has_up = i > 0;
+      const std::size_t here = static_cast<std::size_t>(i) * pitch + jc;
+      if constexpr (TGV) {
+        float s11[C], s22[C], s12[C], o11[C], o22[C], o12[C];
+        float square = 0.0f;
+        const int own = kHalo + lane;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          float wl1 = __shfl_up_sync(kAll, wb1[c], 1), wl2 = __shfl_up_sync(kAll, wb2[c], 1);
+          if (lane == 0) {
+            wl1 = wleft[c][0][r];
+            wl2 = wleft[c][1][r];
+          }
+          if (!has_left) wl1 = wl2 = 0.0f;
+          float wu1 = r > 0 ? wbar[c][0][r - 1][lane] : wcarry[c][0][lane];
+          float wu2 = r > 0 ? wbar[c][1][r - 1][lane] : wcarry[c][1][lane];
+          if (!has_up) wu1 = wu2 = 0.0f;
+          const float own1x = has_right ? wb1[c] : 0.0f, own2x = has_right ? wb2[c] : 0.0f;
+          const float own1y = has_down ? wb1[c] : 0.0f, own2y = has_down ? wb2[c] : 0.0f;
+          const float exx = own1x - wl1;
+          const float eyy = own2y - wu2;
+          const float exy = 0.5f * ((own1y - wu1) + (own2x - wl2));
+          o11[c] = slot[((5 * C + c) * kBox + r) * kSpan + own];
+          o22[c] = slot[((6 * C + c) * kBox + r) * kSpan + own];
+          o12[c] = slot[((7 * C + c) * kBox + r) * kSpan + own];
+          const float sigma = P.dual.sigma[c];
+          s11[c] = o11[c] + sigma * exx;
+          s22[c] = o22[c] + sigma * eyy;
+          s12[c] = o12[c] + sigma * exy;
+          if constexpr (COUPLED) square += s11[c] * s11[c] + s22[c] * s22[c] + 2.0f * (s12[c] * s12[c]);
+        }
+        const float coupled_scale = COUPLED ? ball_of(square, P.dual.radius0) : 1.0f;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          float sr = coupled_scale;
+          if constexpr (!COUPLED) {
+            sr = ball_of(s11[c] * s11[c] + s22[c] * s22[c] + 2.0f * (s12[c] * s12[c]), P.dual.radius0);
+          }
+          if (valid) {
+            const std::size_t at = c * plane + here;
+            P.dual.out.r11[at] = rho * (s11[c] * sr) + rest * o11[c];
+            P.dual.out.r22[at] = rho * (s22[c] * sr) + rest * o22[c];
+            P.dual.out.r12[at] = rho * (s12[c] * sr) + rest * o12[c];
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        float before = __shfl_up_sync(kAll, pn1[c], 1);
+        if (lane == 0) before = pleft[c][r];
+        const float above = r > 0 ? p2rows[c][r - 1][lane] : p2carry[c][lane];
+        const float dy = (has_down ? pn2[c] : 0.0f) - (has_up ? above : 0.0f);
+        const float dx = (has_right ? pn1[c] : 0.0f) - (has_left ? before : 0.0f);
+        const float v = xn[c] + P.dual.tau[c] * (dy + dx);
+        if (valid) {
+          const std::size_t at = c * plane + here;
+          const float4 ends = __ldg(reinterpret_cast<const float4*>(P.ends) + P.levels[at]);  // lower, upper, centre
+          P.next[at] = fminf(fmaxf((v + P.t * ends.z) * P.r, ends.x), ends.y);
+        }
+      }
+    }
+    __syncthreads();
+    issue(k + 2);  // every read of the slot is done
+    if (warp == kRows - 1) {
+      // The last row's w- and p2_n: the row above the next chunk.
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        if constexpr (TGV) {
+          wcarry[c][0][lane] = wb1[c];
+          wcarry[c][1][lane] = wb2[c];
+        }
+        p2carry[c][lane] = pn2[c];
+      }
+    }
+  }
+  if (failed && tid == 0 && P.dual.error != nullptr) atomicExch(P.dual.error, 1);
+  if (failed) {
+    for (int k = stopped; k < min(stopped + 2, chunks); ++k) barrier_wait(&bars[k & 1], (k >> 1) & 1);
+  }
+}
+
 template <bool TGV, int C>
 constexpr std::size_t shared_bytes() {
   constexpr int F = TGV ? 8 : 3;
@@ -713,6 +973,33 @@ cudaError_t launch_channels(const CUtensorMap& state, const CUtensorMap& tilde, 
   }
 }
 
+template <bool TGV, int C, bool COUPLED>
+cudaError_t launch_samples_one(const CUtensorMap& state, const CUtensorMap& tilde, const SamplesIterationParams& p,
+                               cudaStream_t s) {
+  auto kernel = samples_iteration_kernel<TGV, C, COUPLED>;
+  constexpr std::size_t bytes = shared_bytes<TGV, C>();
+  static std::atomic<int> resident[64] = {};
+  int device = 0;
+  cudaGetDevice(&device);
+  int slots = resident[device & 63].load();
+  if (slots == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    int per_sm = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * kWarps, bytes);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    slots = std::max(1, per_sm * sms);
+    resident[device & 63].store(slots);
+  }
+  const int strips = (p.dual.g.columns + 31) / 32;
+  const int best = strip_rows_for(p.dual.g, slots);
+  SamplesIterationParams q = p;
+  q.strip_rows = best;
+  const dim3 grid(strips, (p.dual.g.rows + best - 1) / best, 1);
+  kernel<<<grid, 32 * kWarps, bytes, s>>>(state, tilde, q);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 bool iteration_takes(const Geometry& g, const ComponentDevice* components, int count) {
@@ -742,6 +1029,24 @@ cudaError_t launch_iteration(const CUtensorMap& state, const CUtensorMap& tilde,
                              bool coupled, int cell_rows, int cell_columns, cudaStream_t stream) {
   return tgv ? launch_channels<true>(state, tilde, p, coupled, cell_rows, cell_columns, stream)
              : launch_channels<false>(state, tilde, p, coupled, cell_rows, cell_columns, stream);
+}
+
+bool samples_iteration_takes(const Geometry& g) { return g.channels == 1 || g.channels == 3; }
+
+cudaError_t launch_samples_iteration(const CUtensorMap& state, const CUtensorMap& tilde,
+                                     const SamplesIterationParams& p, bool tgv, bool coupled, cudaStream_t stream) {
+  const int channels = p.dual.g.channels;
+  if (channels == 1) {
+    return tgv ? launch_samples_one<true, 1, false>(state, tilde, p, stream)
+               : launch_samples_one<false, 1, false>(state, tilde, p, stream);
+  }
+  if (channels != 3) return cudaErrorInvalidValue;
+  if (tgv) {
+    return coupled ? launch_samples_one<true, 3, true>(state, tilde, p, stream)
+                   : launch_samples_one<true, 3, false>(state, tilde, p, stream);
+  }
+  return coupled ? launch_samples_one<false, 3, true>(state, tilde, p, stream)
+                 : launch_samples_one<false, 3, false>(state, tilde, p, stream);
 }
 
 }  // namespace urb

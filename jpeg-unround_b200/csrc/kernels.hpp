@@ -386,6 +386,21 @@ bool make_iteration_map(CUtensorMap& map, const float* planes, const Geometry& g
 cudaError_t launch_iteration(const CUtensorMap& state, const CUtensorMap& tilde, const IterationParams& p, bool tgv,
                              bool coupled, int cell_rows, int cell_columns, cudaStream_t stream);
 
+// Pictures of rounded samples in one sweep per iteration (iteration.cu): the dual step and the
+// next primal step with its sample-by-sample proximal map; maps as make_iteration_map makes them.
+struct SamplesIterationParams {
+  DualParams dual;
+  const std::uint16_t* levels = nullptr;  // the channels' levels, pitched like the state
+  const SampleEnds32* ends = nullptr;      // per level
+  float t = 0.0f;                          // tau mu
+  float r = 1.0f;                          // 1 / (1 + tau mu)
+  float* next = nullptr;                   // x~ of the next iteration
+  int strip_rows = 256;                    // set by the launcher
+};
+bool samples_iteration_takes(const Geometry& g);  // 1 or 3 channels
+cudaError_t launch_samples_iteration(const CUtensorMap& state, const CUtensorMap& tilde,
+                                     const SamplesIterationParams& p, bool tgv, bool coupled, cudaStream_t stream);
+
 cudaError_t launch_widen(const float* from, double* to, const Geometry& g, cudaStream_t stream);
 cudaError_t launch_narrow(const double* from, float* to, const Geometry& g, cudaStream_t stream);
 

@@ -28,6 +28,9 @@ bool fused_kernels() {
   return value != nullptr && std::strcmp(value, "fused") == 0;
 }
 
+// Pictures of rounded samples take the fused sweep with UNROUND_B200_KERNELS=fused too.
+bool samples_fused() { return fused_kernels(); }
+
 }  // namespace
 
 struct Solver::Impl {
@@ -211,8 +214,9 @@ struct Solver::Impl {
     xt = allocate<float>(n);
     xts[0] = xt;
     xt_id = 0;
-    fusable = solving && samples == nullptr && fused_kernels() &&
-              iteration_takes(g, components.data(), static_cast<int>(components.size()));
+    fusable = solving && (samples != nullptr ? samples_fused() && samples_iteration_takes(g)
+                                             : fused_kernels() && iteration_takes(g, components.data(),
+                                                                                  static_cast<int>(components.size())));
     if (fusable) {
       xts[1] = allocate<float>(n);
       cell_rows = components.size() > 1 ? components[1].cell_rows : 1;
@@ -525,6 +529,24 @@ struct Solver::Impl {
   // The dual step of iteration n and the primal step of iteration n + 1 as one sweep
   // (iteration.cu), keeping nothing: from x~_n and s_{n-1} to s_n and x~_{n+1}.
   void fused() {
+    if (samples != nullptr) {
+      SamplesIterationParams sp;
+      sp.dual = dual_params();
+      sp.levels = s_levels;
+      sp.ends = s_ends;
+      const double t = plan.tau * samples->mu;
+      sp.t = static_cast<float>(t);
+      sp.r = static_cast<float>(1.0 / (1.0 + t));
+      sp.next = xts[1 - xt_id];
+      if (error == cudaSuccess) {
+        error = launch_samples_iteration(iteration_state_maps[current], iteration_tilde_maps[xt_id], sp, tgv,
+                                         plan.coupled, stream);
+      }
+      current = 1 - current;
+      xt_id = 1 - xt_id;
+      xt = xts[xt_id];
+      return;
+    }
     IterationParams ip;
     ip.dual = dual_params();
     for (std::size_t c = 0; c < components.size(); ++c) ip.component[c] = components[c];
@@ -756,7 +778,7 @@ Solver::Solver(const Frame& frame, const SamplesModel& samples, cudaStream_t str
 Solver::~Solver() = default;
 
 int Solver::launches_per_iteration() const {
-  if (impl_->samples != nullptr) return 2;
+  if (impl_->samples != nullptr) return impl_->fusable ? 1 : 2;
   return impl_->fusable ? 1 : 1 + static_cast<int>(impl_->components.size());
 }
 

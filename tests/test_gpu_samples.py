@@ -133,3 +133,28 @@ def test_the_measured_loop():
     assert timing.milliseconds > 0 and timing.dual_milliseconds > 0 and timing.primal_milliseconds > 0
     with pytest.raises(native.UnroundError):
         native.measure_samples(_picture(8, 8, 4, 8, seed=1), 8, ["--method", "tgv"])
+
+
+@pytest.mark.parametrize("shape, options", [
+    ((45, 61, 3), ["--method", "tgv"]),
+    ((37, 29, 1), ["--method", "tv", "--mu", "0.05"]),
+    ((52, 70, 3), ["--method", "tv", "--channels", "apart"]),
+    ((19, 100, 3), ["--method", "tgv", "--channels", "apart", "--slack", "0.3"]),
+])
+def test_the_fused_sweep_equals_the_two_launches(monkeypatch, shape, options):
+    """The fused sweep of the samples (dual step and the next primal step in one launch,
+    UNROUND_B200_KERNELS=fused) against the dual sweep and the primal kernel apart (the default),
+    on ragged sizes: the same iterations, the canvases to binary32 rounding."""
+    from unround import native
+
+    levels = _picture(*shape, 8, seed=shape[0])
+    given = [*options, "--iterations", "90", "--tolerance", "0"]
+    split = native.solve_samples(levels, 8, given)
+    assert native.measure_samples(levels, 8, options, warmup=2, iterations=5).launches_per_iteration == 2
+    monkeypatch.setenv("UNROUND_B200_KERNELS", "fused")
+    fused = native.solve_samples(levels, 8, given)
+    assert native.measure_samples(levels, 8, options, warmup=2, iterations=5).launches_per_iteration == 1
+    assert fused.result.iterations == split.result.iterations == 90
+    difference = fused.canvas - split.canvas
+    assert np.linalg.norm(difference) / np.linalg.norm(split.canvas) <= 1e-5
+    assert np.abs(difference).max() <= 1e-3
