@@ -426,12 +426,16 @@ def _samples_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     with Clocks(0) as clocks:
         timing = native.measure_samples(levels, 8, options, warmup=max(3, args.warmup) * 10,
                                         iterations=args.steps * ITERATIONS)
-    # The loop as one fused sweep an iteration (UNROUND_B200_KERNELS=fused), beside.
-    os.environ["UNROUND_B200_KERNELS"] = "fused"
-    try:
-        other = native.measure_samples(levels, 8, options, warmup=30, iterations=ITERATIONS)
-    finally:
-        del os.environ["UNROUND_B200_KERNELS"]
+    # Beside: the loop as one launch an iteration, the primal step in the fused sweep of
+    # iteration.cu (UNROUND_B200_KERNELS=fused) or in the dual sweep (=sweep).
+    others = {}
+    for mode in ("fused", "sweep"):
+        os.environ["UNROUND_B200_KERNELS"] = mode
+        try:
+            others[mode] = native.measure_samples(levels, 8, options, warmup=30, iterations=ITERATIONS)
+        finally:
+            del os.environ["UNROUND_B200_KERNELS"]
+
     seconds = max_over_ranks(timing.milliseconds / 1e3)
     pixels = timing.pixels
     value = world * pixels * args.steps * ITERATIONS / seconds / 1e6
@@ -465,7 +469,6 @@ def _samples_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     dual = DUAL_BYTES * timing.samples / (timing.dual_milliseconds / 1e3) / 1e9
     primal = SAMPLES_BYTES * timing.samples / (timing.primal_milliseconds / 1e3) / 1e9
     iteration = (DUAL_BYTES + SAMPLES_BYTES) * timing.samples / (seconds / (args.steps * ITERATIONS)) / 1e9
-    fused = SAMPLES_FUSED_BYTES * other.samples / (other.dual_milliseconds / 1e3) / 1e9
     if rank != 0:
         return
     line = {
@@ -481,10 +484,11 @@ def _samples_arm(args: argparse.Namespace, rank: int, world: int) -> None:
                      "samples_primal_achieved": primal, "samples_primal_frac": primal / peak,
                      "samples_primal_bytes_per_sample": SAMPLES_BYTES, "primal_ms": timing.primal_milliseconds,
                      "iteration_achieved": iteration, "iteration_frac": iteration / peak,
-                     "fused_sweep": {"kernel": "samples_iteration_kernel<tgv,3,coupled>",
-                                     "iteration_ms": other.milliseconds / other.iterations,
-                                     "bytes_per_sample": SAMPLES_FUSED_BYTES, "achieved": fused,
-                                     "frac": fused / peak}},
+                     "one_launch": {mode: {"iteration_ms": t.milliseconds / t.iterations,
+                                           "bytes_per_sample": SAMPLES_FUSED_BYTES,
+                                           "achieved": SAMPLES_FUSED_BYTES * t.samples / (t.milliseconds / t.iterations)
+                                           / 1e6}
+                                    for mode, t in others.items()}},
         "e2e": {"value": world * pixels * args.steps * ITERATIONS / e2e_seconds / 1e6, "unit": "Mpx*iter/s",
                 "h2d_bytes_per_step": int(levels.nbytes), "d2h_bytes_per_step": d2h},
         "gpu_launches": timing.launches_per_iteration * args.steps * ITERATIONS,

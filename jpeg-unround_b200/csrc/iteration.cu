@@ -749,6 +749,12 @@ __global__ void __launch_bounds__(32 * kWarps, 2)
   }
   __syncthreads();
 
+  // The levels of the first chunk's pixels (then each chunk loads the next's).
+  unsigned level[C] = {};
+  if (warp < kRows && i0 + warp < i1 && valid) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) level[c] = __ldg(P.levels + c * plane + static_cast<std::size_t>(i0 + warp) * pitch + jc);
+  }
   bool failed = false;
   int stopped = chunks;
   for (int k = 0; k < chunks; ++k) {
@@ -763,6 +769,19 @@ __global__ void __launch_bounds__(32 * kWarps, 2)
     const int r = warp;
     const int i = chunk_row + r;
     const bool row_in = i < i1;  // warp-uniform
+    // The pixel's ends (by the level loaded a chunk ago), looked up now so that the dual step
+    // hides the lookup, and the level of the pixel a chunk below, for the next chunk.
+    float4 ends[C];
+    {
+      const int below = i + kRows;
+      const bool ahead = warp < kRows && below < i1 && valid;
+      const std::size_t there = static_cast<std::size_t>(ahead ? below : 0) * pitch + jc;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        ends[c] = __ldg(reinterpret_cast<const float4*>(P.ends) + level[c]);  // lower, upper, centre
+        level[c] = ahead ? __ldg(P.levels + c * plane + there) : 0u;
+      }
+    }
     // ---- A: the dual step at the warp's pixel (row warps), at column x0 - 1 (side warp).
     float xn[C], pn1[C], pn2[C], wb1[C], wb2[C];
     if (warp < kRows) {
@@ -884,11 +903,7 @@ __global__ void __launch_bounds__(32 * kWarps, 2)
         const float dy = (has_down ? pn2[c] : 0.0f) - (has_up ? above : 0.0f);
         const float dx = (has_right ? pn1[c] : 0.0f) - (has_left ? before : 0.0f);
         const float v = xn[c] + P.dual.tau[c] * (dy + dx);
-        if (valid) {
-          const std::size_t at = c * plane + here;
-          const float4 ends = __ldg(reinterpret_cast<const float4*>(P.ends) + P.levels[at]);  // lower, upper, centre
-          P.next[at] = fminf(fmaxf((v + P.t * ends.z) * P.r, ends.x), ends.y);
-        }
+        if (valid) P.next[c * plane + here] = fminf(fmaxf((v + P.t * ends[c].z) * P.r, ends[c].x), ends[c].y);
       }
     }
     __syncthreads();

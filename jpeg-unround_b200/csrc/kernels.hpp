@@ -398,6 +398,17 @@ struct SamplesIterationParams {
   int strip_rows = 256;                    // set by the launcher
 };
 bool samples_iteration_takes(const Geometry& g);  // 1 or 3 channels
+// The same in the dual sweep's layout (sweep.cu: 8-row boxes in a ring of three slots, the
+// sweep's maps): the primal step of pictures of rounded samples after the dual step, per chunk.
+struct SamplesStep {
+  const std::uint16_t* levels = nullptr;  // the channels' levels, pitched like the state
+  const SampleEnds32* ends = nullptr;      // per level
+  float t = 0.0f;                          // tau mu
+  float r = 1.0f;                          // 1 / (1 + tau mu)
+  float* next = nullptr;                   // x~ of the next iteration
+};
+cudaError_t launch_dual_samples(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p,
+                                const SamplesStep& q, bool tgv, bool coupled, cudaStream_t stream);
 cudaError_t launch_samples_iteration(const CUtensorMap& state, const CUtensorMap& tilde,
                                      const SamplesIterationParams& p, bool tgv, bool coupled, cudaStream_t stream);
 

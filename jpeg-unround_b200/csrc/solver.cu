@@ -28,8 +28,16 @@ bool fused_kernels() {
   return value != nullptr && std::strcmp(value, "fused") == 0;
 }
 
-// Pictures of rounded samples take the fused sweep with UNROUND_B200_KERNELS=fused too.
-bool samples_fused() { return fused_kernels(); }
+// How pictures of rounded samples iterate: 0 two launches (the dual sweep, then the primal
+// kernel: the default, the fastest measured); 1 the fused sweep of iteration.cu
+// (UNROUND_B200_KERNELS=fused); 2 the dual sweep with the primal step in it (=sweep).
+int samples_kernels() {
+  const char* value = std::getenv("UNROUND_B200_KERNELS");
+  if (value == nullptr) return 0;
+  if (std::strcmp(value, "fused") == 0) return 1;
+  if (std::strcmp(value, "sweep") == 0) return 2;
+  return 0;
+}
 
 }  // namespace
 
@@ -81,6 +89,7 @@ struct Solver::Impl {
   // records and the result.
   const SamplesModel* samples = nullptr;
   std::uint16_t* s_levels = nullptr;  // the channels' levels, pitched like the state
+  int samples_layout = 0;              // samples_kernels() when the solve began
   SampleEnds32* s_ends = nullptr;       // per level: binary32 ends rounded inward, the centre
   SampleEnds64* s_ends64 = nullptr;     // per level: binary64 ends and centre
   int samples_written = 0;  // the CTAs of the last kept primal step's sums of G
@@ -214,7 +223,8 @@ struct Solver::Impl {
     xt = allocate<float>(n);
     xts[0] = xt;
     xt_id = 0;
-    fusable = solving && (samples != nullptr ? samples_fused() && samples_iteration_takes(g)
+    samples_layout = samples != nullptr ? samples_kernels() : 0;
+    fusable = solving && (samples != nullptr ? samples_layout != 0 && samples_iteration_takes(g)
                                              : fused_kernels() && iteration_takes(g, components.data(),
                                                                                   static_cast<int>(components.size())));
     if (fusable) {
@@ -529,6 +539,23 @@ struct Solver::Impl {
   // The dual step of iteration n and the primal step of iteration n + 1 as one sweep
   // (iteration.cu), keeping nothing: from x~_n and s_{n-1} to s_n and x~_{n+1}.
   void fused() {
+    if (samples != nullptr && samples_layout == 2) {
+      SamplesStep q;
+      q.levels = s_levels;
+      q.ends = s_ends;
+      const double t = plan.tau * samples->mu;
+      q.t = static_cast<float>(t);
+      q.r = static_cast<float>(1.0 / (1.0 + t));
+      q.next = xts[1 - xt_id];
+      if (error == cudaSuccess) {
+        error = launch_dual_samples(state_maps[current], tilde_maps[xt_id], dual_params(), q, tgv, plan.coupled,
+                                    stream);
+      }
+      current = 1 - current;
+      xt_id = 1 - xt_id;
+      xt = xts[xt_id];
+      return;
+    }
     if (samples != nullptr) {
       SamplesIterationParams sp;
       sp.dual = dual_params();

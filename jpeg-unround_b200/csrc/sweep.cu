@@ -48,9 +48,10 @@ __device__ __forceinline__ T ball(T square, T radius) {
 
 // One CTA's strip: columns x0 .. x0 + 31, rows i0 .. i1 - 1 (a whole number of chunks, or the
 // canvas's last rows), of the image whose maps and parameters these are.
-template <bool TGV, int C, bool COUPLED, bool KEEP>
+template <bool TGV, int C, bool COUPLED, bool KEEP, bool SAMPLES = false>
 __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const CUtensorMap* tilde_map,
-                                           const DualParams& P, int x0, int i0, int i1) {
+                                           const DualParams& P, int x0, int i0, int i1,
+                                           const SamplesStep* Q = nullptr) {
   constexpr int F = TGV ? 8 : 3;  // state planes per channel: x, p1, p2 (+ w1, w2, r11, r22, r12)
   constexpr int PLANE = kChunk * kSpan;
   constexpr int SLOT = (F + 1) * C * PLANE;  // floats: the state planes, then x~'s
@@ -60,6 +61,11 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
   __shared__ float carry[2][W][2][32];      // w- of the row above a chunk, own columns
   __shared__ float wbar[W][2][kChunk][32];  // w- of each row of the chunk
   __shared__ float wleft[W][2][kChunk];     // w- at column x0 - 1
+  // With SAMPLES: p2_n of each row of the chunk, of the row above it, and p1_n at column x0 - 1.
+  constexpr int PS = SAMPLES ? C : 1;
+  __shared__ float p2rows[PS][kChunk][32];
+  __shared__ float p2carry[2][PS][32];
+  __shared__ float pleft[PS][kChunk];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
   const std::size_t plane = P.g.plane;
@@ -114,8 +120,51 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
       carry[0][c][1][lane] = wb2;
     }
   }
+  if (SAMPLES && warp == 0) {
+    // p2_n of the row above the strip: the dual step at (i0 - 1, j), from global memory.
+    float step1[C], step2[C], old2[C];
+    float square = 0.0f;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      step1[c] = step2[c] = old2[c] = 0.0f;
+      if (i0 > 0) {
+        const std::size_t base = c * plane;
+        const std::size_t a = static_cast<std::size_t>(i0 - 1) * pitch + jc;
+        auto bar_at = [&](std::size_t at) { return 2.0f * __ldg(P.xt + base + at) - __ldg(P.in.x + base + at); };
+        const float bar = bar_at(a);
+        const float gx = has_right ? bar_at(a + 1) - bar : 0.0f;
+        const float gy = bar_at(a + pitch) - bar;
+        const float p1 = __ldg(P.in.p1 + base + a), p2 = __ldg(P.in.p2 + base + a);
+        float wb1 = 0.0f, wb2 = 0.0f;
+        if constexpr (TGV) {
+          wb1 = carry[0][c][0][lane];  // written above by this warp
+          wb2 = carry[0][c][1][lane];
+        }
+        step1[c] = p1 + P.sigma[c] * (gx - wb1);
+        step2[c] = p2 + P.sigma[c] * (gy - wb2);
+        old2[c] = p2;
+        if constexpr (COUPLED) square += step1[c] * step1[c] + step2[c] * step2[c];
+      }
+    }
+    const float coupled_scale = COUPLED ? ball(square, P.radius) : 1.0f;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      float sp = coupled_scale;
+      if constexpr (!COUPLED) sp = ball(step1[c] * step1[c] + step2[c] * step2[c], P.radius);
+      p2carry[0][c][lane] = i0 > 0 ? rho * (step2[c] * sp) + rest * old2[c] : 0.0f;
+    }
+  }
   __syncthreads();
 
+  // With SAMPLES: the levels of the first chunk's pixels (then each chunk loads the next's).
+  unsigned level[SAMPLES ? C : 1] = {};
+  if constexpr (SAMPLES) {
+    const int first = i0 + warp;
+    if (warp < kChunk && first < i1 && valid) {
+#pragma unroll
+      for (int c = 0; c < C; ++c) level[c] = __ldg(Q->levels + c * plane + static_cast<std::size_t>(first) * pitch + jc);
+    }
+  }
   bool failed = false;
   int stopped = chunks;
   for (int k = 0; k < chunks; ++k) {
@@ -157,6 +206,20 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
     const bool row = warp < kChunk && i < i1;
     const std::size_t here = static_cast<std::size_t>(row ? i : 0) * pitch + jc;
     float wb1[C], wb2[C];
+    float xn[C], pn1[C], pn2[C];  // with SAMPLES: x_n and p_n at the pixel
+    // With SAMPLES: the pixel's ends (by the level loaded a chunk ago), looked up now so that the
+    // dual step hides the lookup, and the level of the pixel a chunk below, for the next chunk.
+    float4 ends[SAMPLES ? C : 1];
+    if constexpr (SAMPLES) {
+      const int below = i + kChunk;
+      const bool ahead = warp < kChunk && below < i1 && valid;
+      const std::size_t there = static_cast<std::size_t>(ahead ? below : 0) * pitch + jc;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        ends[c] = __ldg(reinterpret_cast<const float4*>(Q->ends) + level[c]);  // a, b, centre
+        level[c] = ahead ? __ldg(Q->levels + c * plane + there) : 0u;
+      }
+    }
     // ---- The row warps: x, w and p at the pixel; w- left in shared memory.
     if (row) {
       const bool has_down = i + 1 < rows;
@@ -169,6 +232,7 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
         const float bar = 2.0f * xt0 - x0v;
         const float gx = has_right ? (2.0f * XT(c, r, own + 1) - S(0, c, r, own + 1)) - bar : 0.0f;
         const float gy = has_down ? (2.0f * XT(c, r + 1, own) - S(0, c, r + 1, own)) - bar : 0.0f;
+        if constexpr (SAMPLES) xn[c] = rho * xt0 + rest * x0v;
         if (valid) P.out.x[base + here] = rho * xt0 + rest * x0v;
         const float p1 = S(1, c, r, own), p2 = S(2, c, r, own);
         old_p1[c] = p1;
@@ -204,7 +268,23 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
       }
       float scale_p = 1.0f;
       if constexpr (COUPLED) scale_p = ball(square_p, P.radius);
-      if (valid) {
+      if constexpr (SAMPLES) {
+        // p_n at every lane (the divergence of the primal step reads the neighbours'), kept.
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const std::size_t base = c * plane;
+          float sp = scale_p;
+          if constexpr (!COUPLED) sp = ball(step_p1[c] * step_p1[c] + step_p2[c] * step_p2[c], P.radius);
+          pn1[c] = rho * (step_p1[c] * sp) + rest * old_p1[c];
+          pn2[c] = rho * (step_p2[c] * sp) + rest * old_p2[c];
+          if (valid) {
+            P.out.p1[base + here] = pn1[c];
+            P.out.p2[base + here] = pn2[c];
+          }
+          p2rows[c][r][lane] = pn2[c];
+          if (r == kChunk - 1) p2carry[(k + 1) & 1][c][lane] = pn2[c];
+        }
+      } else if (valid) {
 #pragma unroll
         for (int c = 0; c < C; ++c) {
           const std::size_t base = c * plane;
@@ -219,17 +299,47 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
           }
         }
       }
-    } else if (TGV && warp == kChunk && lane < kChunk && x0 > 0 && i0 + k * kChunk + lane < i1) {
-      // ---- The side warp: w- at column x0 - 1 of the chunk's rows (a lane each).
+    } else if ((TGV || SAMPLES) && warp == kChunk && lane < kChunk && x0 > 0 && i0 + k * kChunk + lane < i1) {
+      // ---- The side warp: w- at column x0 - 1 of the chunk's rows (a lane each); with SAMPLES
+      // p1_n there too (the divergence's left neighbour of the strip's first column).
       const int rr = lane, ii = i0 + k * kChunk + rr;
+      float lb1[C], lb2[C];
 #pragma unroll
       for (int c = 0; c < C; ++c) {
-        float t1, t2, w1, w2;
-        w_tilde(c, rr, kHalo - 1, ii, x0 - 1, t1, t2, w1, w2);
-        wleft[c][0][rr] = 2.0f * t1 - w1;
-        wleft[c][1][rr] = 2.0f * t2 - w2;
+        lb1[c] = lb2[c] = 0.0f;
+        if constexpr (TGV) {
+          float t1, t2, w1, w2;
+          w_tilde(c, rr, kHalo - 1, ii, x0 - 1, t1, t2, w1, w2);
+          lb1[c] = 2.0f * t1 - w1;
+          lb2[c] = 2.0f * t2 - w2;
+          wleft[c][0][rr] = lb1[c];
+          wleft[c][1][rr] = lb2[c];
+        }
+      }
+      if constexpr (SAMPLES) {
+        constexpr int L = kHalo - 1;  // column x0 - 1 in the box
+        float step1[C], step2[C], old1[C];
+        float square = 0.0f;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const float bar = 2.0f * XT(c, rr, L) - S(0, c, rr, L);
+          const float gx = (2.0f * XT(c, rr, L + 1) - S(0, c, rr, L + 1)) - bar;  // x0 < columns
+          const float gy = ii + 1 < rows ? (2.0f * XT(c, rr + 1, L) - S(0, c, rr + 1, L)) - bar : 0.0f;
+          old1[c] = S(1, c, rr, L);
+          step1[c] = old1[c] + P.sigma[c] * (gx - lb1[c]);
+          step2[c] = S(2, c, rr, L) + P.sigma[c] * (gy - lb2[c]);
+          if constexpr (COUPLED) square += step1[c] * step1[c] + step2[c] * step2[c];
+        }
+        const float coupled_scale = COUPLED ? ball(square, P.radius) : 1.0f;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          float sp = coupled_scale;
+          if constexpr (!COUPLED) sp = ball(step1[c] * step1[c] + step2[c] * step2[c], P.radius);
+          pleft[c][rr] = rho * (step1[c] * sp) + rest * old1[c];
+        }
       }
     }
+    if constexpr (!TGV && SAMPLES) __syncthreads();
     if constexpr (TGV) {
       __syncthreads();
       // ---- The r step from w- of the pixel and of its left and upper neighbours.
@@ -289,6 +399,23 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
         }
       }
     }
+    if constexpr (SAMPLES) {
+      // ---- The primal step of the next iteration at the pixel: v = x_n + tau gamma div p_n
+      // (backward differences, Neumann ends) and its proximal map, the box of the sample's level.
+      if (row) {
+        const bool has_down = i + 1 < rows, has_up = i > 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          float before = __shfl_up_sync(kAll, pn1[c], 1);
+          if (lane == 0) before = x0 > 0 ? pleft[c][r] : 0.0f;
+          const float above = r > 0 ? p2rows[c][r - 1][lane] : p2carry[k & 1][c][lane];
+          const float dy = (has_down ? pn2[c] : 0.0f) - (has_up ? above : 0.0f);
+          const float dx = (has_right ? pn1[c] : 0.0f) - (has_left ? before : 0.0f);
+          const float v = xn[c] + P.tau[c] * (dy + dx);
+          if (valid) Q->next[c * plane + here] = fminf(fmaxf((v + Q->t * ends[c].z) * Q->r, ends[c].x), ends[c].y);
+        }
+      }
+    }
     __syncthreads();  // every warp is done with slot k
     issue(k + kSlots);
   }
@@ -306,6 +433,16 @@ __global__ void __launch_bounds__(kThreads, 2) dual_tma_kernel(const __grid_cons
                                                                 const DualParams P) {
   const int i0 = blockIdx.y * P.strip_rows;
   dual_strip<TGV, C, COUPLED, KEEP>(&state_map, &tilde_map, P, blockIdx.x * 32, i0, min(i0 + P.strip_rows, P.g.rows));
+}
+
+// The dual step and the next primal step of a picture of rounded samples (SamplesStep).
+template <bool TGV, int C, bool COUPLED>
+__global__ void __launch_bounds__(kThreads, 2) dual_samples_kernel(const __grid_constant__ CUtensorMap state_map,
+                                                                    const __grid_constant__ CUtensorMap tilde_map,
+                                                                    const DualParams P, const SamplesStep Q) {
+  const int i0 = blockIdx.y * P.strip_rows;
+  dual_strip<TGV, C, COUPLED, false, true>(&state_map, &tilde_map, P, blockIdx.x * 32, i0,
+                                           min(i0 + P.strip_rows, P.g.rows), &Q);
 }
 
 // The dual step of a batch: a CTA a tile of the table, of the image whose entry (maps and
@@ -452,6 +589,53 @@ bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, in
 
 bool make_primal_map(CUtensorMap& map, const float* x, const Geometry& g, std::size_t stride) {
   return make_box_map(map, x, g, 3, stride, 65, 36);
+}
+
+namespace {
+
+template <bool TGV, int C, bool COUPLED>
+cudaError_t launch_samples_one(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p,
+                               const SamplesStep& q, cudaStream_t s) {
+  auto kernel = dual_samples_kernel<TGV, C, COUPLED>;
+  const std::size_t bytes = dual_tma_shared_bytes(TGV, C);
+  static std::atomic<int> resident[64] = {};
+  int device = 0;
+  cudaGetDevice(&device);
+  int slots = resident[device & 63].load();
+  if (slots == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    int per_sm = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, bytes);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    slots = std::max(1, per_sm * sms);
+    resident[device & 63].store(slots);
+  }
+  DualParams d = p;
+  d.strip_rows = strip_rows_for(p.g, slots);
+  const dim3 grid((p.g.columns + 31) / 32, (p.g.rows + d.strip_rows - 1) / d.strip_rows, 1);
+  kernel<<<grid, kThreads, bytes, s>>>(state, tilde, d, q);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_dual_samples(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p,
+                                const SamplesStep& q, bool tgv, bool coupled, cudaStream_t stream) {
+  switch (p.g.channels) {
+    case 1:
+      return tgv ? launch_samples_one<true, 1, false>(state, tilde, p, q, stream)
+                 : launch_samples_one<false, 1, false>(state, tilde, p, q, stream);
+    case 3:
+      if (tgv) {
+        return coupled ? launch_samples_one<true, 3, true>(state, tilde, p, q, stream)
+                       : launch_samples_one<true, 3, false>(state, tilde, p, q, stream);
+      }
+      return coupled ? launch_samples_one<false, 3, true>(state, tilde, p, q, stream)
+                     : launch_samples_one<false, 3, false>(state, tilde, p, q, stream);
+    default:
+      return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_dual_tma(const CUtensorMap& state, const CUtensorMap& tilde, const DualParams& p, bool tgv,

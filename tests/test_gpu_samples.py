@@ -141,20 +141,29 @@ def test_the_measured_loop():
     ((52, 70, 3), ["--method", "tv", "--channels", "apart"]),
     ((19, 100, 3), ["--method", "tgv", "--channels", "apart", "--slack", "0.3"]),
 ])
-def test_the_fused_sweep_equals_the_two_launches(monkeypatch, shape, options):
-    """The fused sweep of the samples (dual step and the next primal step in one launch,
-    UNROUND_B200_KERNELS=fused) against the dual sweep and the primal kernel apart (the default),
-    on ragged sizes: the same iterations, the canvases to binary32 rounding."""
+def test_the_fused_sweeps_equal_the_two_launches(monkeypatch, shape, options):
+    """The samples' primal step inside the dual sweep (UNROUND_B200_KERNELS=sweep) and in the
+    fused sweep of iteration.cu (=fused), one launch an iteration each, against the dual sweep and
+    the primal kernel apart (the default), on ragged sizes: the same iterations, the canvases to
+    binary32 rounding."""
     from unround import native
 
     levels = _picture(*shape, 8, seed=shape[0])
     given = [*options, "--iterations", "90", "--tolerance", "0"]
-    split = native.solve_samples(levels, 8, given)
-    assert native.measure_samples(levels, 8, options, warmup=2, iterations=5).launches_per_iteration == 2
-    monkeypatch.setenv("UNROUND_B200_KERNELS", "fused")
-    fused = native.solve_samples(levels, 8, given)
-    assert native.measure_samples(levels, 8, options, warmup=2, iterations=5).launches_per_iteration == 1
-    assert fused.result.iterations == split.result.iterations == 90
-    difference = fused.canvas - split.canvas
-    assert np.linalg.norm(difference) / np.linalg.norm(split.canvas) <= 1e-5
-    assert np.abs(difference).max() <= 1e-3
+    launches = {}
+    made = {}
+    for mode in ("split", "fused", "sweep", None):
+        if mode is None:
+            monkeypatch.delenv("UNROUND_B200_KERNELS", raising=False)
+        else:
+            monkeypatch.setenv("UNROUND_B200_KERNELS", mode)
+        made[mode] = native.solve_samples(levels, 8, given)
+        launches[mode] = native.measure_samples(levels, 8, options, warmup=2, iterations=5).launches_per_iteration
+    assert launches == {"split": 2, "fused": 1, "sweep": 1, None: 2}
+    split = made["split"]
+    np.testing.assert_array_equal(made[None].canvas, split.canvas)
+    for mode in ("fused", "sweep"):
+        assert made[mode].result.iterations == split.result.iterations == 90
+        difference = made[mode].canvas - split.canvas
+        assert np.linalg.norm(difference) / np.linalg.norm(split.canvas) <= 1e-5, mode
+        assert np.abs(difference).max() <= 1e-3, mode
