@@ -374,6 +374,17 @@ class Reader {
   // Tops the accumulator up to at least 57 bits: data bytes (0xFF 0x00 is 0xFF), and zeros once
   // a marker or the end is reached.
   void fill() {
+    // Four bytes at once where none of them is 0xFF (no stuffing, no marker).
+    while (bits_ <= 32 && !stopped_ && size_ - pos_ >= 4) {
+      const std::uint32_t word = (std::uint32_t{data_[pos_]} << 24) | (std::uint32_t{data_[pos_ + 1]} << 16) |
+                                 (std::uint32_t{data_[pos_ + 2]} << 8) | std::uint32_t{data_[pos_ + 3]};
+      // A byte of the word is 0xFF where its complement has a zero byte.
+      const std::uint32_t inverse = ~word;
+      if (((inverse - 0x01010101u) & ~inverse & 0x80808080u) != 0) break;
+      acc_ |= std::uint64_t{word} << (32 - bits_);
+      bits_ += 32;
+      pos_ += 4;
+    }
     while (bits_ <= 56) {
       std::uint64_t byte = 0;
       if (!stopped_ && pos_ < size_) {
@@ -745,10 +756,14 @@ class Reader {
     for (Working& w : comps_) {
       if (!w.out.latched) fail(kJpegDecode, "the file ends before the data of every component");
       JpegComponent out = w.out;
-      const std::size_t row = static_cast<std::size_t>(out.width_in_blocks) * 64;
-      out.coefficients.resize(row * out.height_in_blocks);
-      for (std::uint32_t r = 0; r < out.height_in_blocks; ++r) {
-        std::memcpy(out.coefficients.data() + r * row, w.block(r, 0), row * sizeof(std::int16_t));
+      if (w.padded_columns == out.width_in_blocks && w.padded_rows == out.height_in_blocks) {
+        out.coefficients = std::move(w.blocks);  // no dummy blocks: the arrays are the picture's
+      } else {
+        const std::size_t row = static_cast<std::size_t>(out.width_in_blocks) * 64;
+        out.coefficients.resize(row * out.height_in_blocks);
+        for (std::uint32_t r = 0; r < out.height_in_blocks; ++r) {
+          std::memcpy(out.coefficients.data() + r * row, w.block(r, 0), row * sizeof(std::int16_t));
+        }
       }
       std::vector<std::int16_t>().swap(w.blocks);
       file_.components.push_back(std::move(out));
