@@ -53,6 +53,32 @@ def _peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
+def _copy_gbs() -> float:
+    """The device's copy bandwidth on this box, now: a 2 GiB device-to-device copy (read and
+    write counted), the best of 10 timed by CUDA events after 3 warm-up copies. Reported beside
+    the peak, so a fraction can be read against the same box and clocks."""
+    import torch
+
+    n = (2 << 30) // 4
+    source = torch.empty(n, dtype=torch.float32, device="cuda")
+    target = torch.empty_like(source)
+    source.fill_(1.0)
+    for _ in range(3):
+        target.copy_(source)
+    best = None
+    for _ in range(10):
+        begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        begin.record()
+        target.copy_(source)
+        end.record()
+        end.synchronize()
+        ms = begin.elapsed_time(end)
+        best = ms if best is None else min(best, ms)
+    del source, target
+    torch.cuda.empty_cache()
+    return 2 * n * 4 / (best / 1e3) / 1e9
+
+
 class Clocks:
     """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
 
@@ -758,6 +784,7 @@ def main() -> None:
     file_seconds = max_over_ranks(time.perf_counter() - began)
     e2e_file = world * pixels * args.steps * ITERATIONS / file_seconds / 1e6
     peak, peak_kind = _peaks()
+    copy = _copy_gbs()
     samples = timing.samples
     dual_achieved = DUAL_BYTES * samples / (timing.dual_milliseconds / 1e3) / 1e9
     iteration_seconds = seconds / (args.steps * ITERATIONS)
@@ -777,7 +804,9 @@ def main() -> None:
                          "traffic": traffic, "algorithmic_bytes_per_sample": DUAL_BYTES,
                          "iteration_achieved": iteration_achieved, "iteration_frac": iteration_achieved / peak,
                          "iteration_bytes_per_sample": ALGORITHMIC_BYTES,
-                         "dual_ms": timing.dual_milliseconds, "primal_ms": timing.primal_milliseconds},
+                         "dual_ms": timing.dual_milliseconds, "primal_ms": timing.primal_milliseconds,
+                         "copy_gbs_this_box": copy, "frac_of_copy_this_box": dual_achieved / copy,
+                         "iteration_frac_of_copy_this_box": iteration_achieved / copy},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": levels_bytes, "d2h_bytes_per_step": d2h},
             "e2e_levels": {"value": e2e_levels, "unit": UNIT, "h2d_bytes_per_step": levels_bytes,
                            "d2h_bytes_per_step": levels_d2h,

@@ -17,7 +17,8 @@ from typing import Final
 import numpy as np
 import numpy.typing as npt
 
-__all__ = ["ABI_VERSION", "ColorSpace", "Component", "ErrorKind", "Image", "JpegioError", "Planes", "decode_planes", "read"]
+__all__ = ["ABI_VERSION", "ColorSpace", "Component", "ErrorKind", "Image", "JpegioError", "LibraryNotFoundError",
+           "Planes", "abi_version", "check_icc", "decode_planes", "libjpeg_version", "libpng_version", "read"]
 
 ABI_VERSION: Final = 3
 
@@ -48,6 +49,10 @@ class JpegioError(Exception):
         super().__init__(f"{message} ({kind.name.lower()})")
         self.kind = kind
         self.message = message
+
+
+class LibraryNotFoundError(RuntimeError):
+    """The shared library is not where this package looks for it."""
 
 
 @dataclass(frozen=True, slots=True, eq=False)
@@ -210,7 +215,43 @@ def _c_library() -> ctypes.CDLL:
                                                    ctypes.POINTER(_Planes), ctypes.c_char_p, ctypes.c_size_t]
     library.unround_jpeg_planes_free.restype = None
     library.unround_jpeg_planes_free.argtypes = [ctypes.POINTER(_Planes)]
+    library.unround_jpeg_abi_version.restype = ctypes.c_int32
+    library.unround_jpeg_abi_version.argtypes = []
+    library.unround_jpeg_libjpeg_version.restype = ctypes.c_char_p
+    library.unround_jpeg_libjpeg_version.argtypes = []
+    library.unround_jpeg_libpng_version.restype = ctypes.c_char_p
+    library.unround_jpeg_libpng_version.argtypes = []
+    library.unround_jpeg_check_icc.restype = ctypes.c_int32
+    library.unround_jpeg_check_icc.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_char_p,
+                                               ctypes.c_size_t]
     return library
+
+
+def abi_version() -> int:
+    """UNROUND_JPEGIO_ABI_VERSION of the library that is loaded."""
+    return int(_c_library().unround_jpeg_abi_version())
+
+
+def libjpeg_version() -> str:
+    """What reads JPEG files in the library: this build's own reader (no libjpeg is carried)."""
+    return _c_library().unround_jpeg_libjpeg_version().decode("ascii")
+
+
+def libpng_version() -> str:
+    """What reads and writes PNG files in the library: this build's own, and the zlib it uses."""
+    return _c_library().unround_jpeg_libpng_version().decode("ascii")
+
+
+def check_icc(profile: bytes, channels: int) -> str | None:
+    """Why an ICC profile does not go with a picture of that many channels (1 or 2 grey, 3 or 4
+    RGB), or None: the checks a reader makes of the profile of an iCCP chunk before it takes it;
+    the PNG writer leaves out a profile that fails them."""
+    if not 0 <= channels <= _INT32_MAX:
+        raise ValueError(f"channels is {channels}, not 0 to 2**31 - 1")
+    reason = ctypes.create_string_buffer(_MESSAGE)
+    data = bytes(profile)
+    accepted = _c_library().unround_jpeg_check_icc(data, len(data), channels, reason, _MESSAGE)
+    return None if accepted == 1 else reason.value.decode("utf-8", "replace")
 
 
 def _options(max_pixels: int, max_scans: int, *, warnings_are_errors: bool) -> _Options:

@@ -214,6 +214,9 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_png": (i32, doubles, u64, u64, u64, i32, i32, i32, ctypes.POINTER(ctypes.c_uint8), u64,
                         ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), u64p, *text),
         "unround_orient": (i32, doubles, u64, u64, u64, i32, doubles, u64p, u64p, *text),
+        "unround_tiff": (i32, doubles, u64, u64, u64, i32, ctypes.POINTER(ctypes.c_uint8), u64,
+                         ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), u64p, *text),
+        "unround_main": (i32, size, ctypes.POINTER(ctypes.c_char_p)),
         "unround_result_icc_profile": (ctypes.POINTER(ctypes.c_uint8), handle, u64p),
         "unround_result_exif_orientation": (i32, handle),
         "unround_result_format": (i32, handle),
@@ -858,6 +861,38 @@ def png_bytes(picture: npt.ArrayLike, *, sixteen: bool = False, dither: str = "b
         return ctypes.string_at(pointer, int(size.value))
     finally:
         library.unround_bytes_free(pointer, size)
+
+
+def tiff_bytes(picture: npt.ArrayLike, *, ycbcr: bool = False, icc_profile: bytes | None = None) -> bytes:
+    """The TIFF writer of the reference (unround_tiff): outside this build's path, it raises
+    UnroundError with UNSUPPORTED."""
+    samples = np.ascontiguousarray(picture, dtype=np.float64)
+    if samples.ndim not in (2, 3):
+        raise ValueError(f"a picture is (height, width) or (height, width, channels), not {samples.shape}")
+    height, width = int(samples.shape[0]), int(samples.shape[1])
+    channels = 1 if samples.ndim == 2 else int(samples.shape[2])
+    library = _library()
+    pointer = ctypes.POINTER(ctypes.c_uint8)()
+    size = ctypes.c_uint64()
+    message = ctypes.create_string_buffer(_MESSAGE)
+    status = library.unround_tiff(samples.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), height, width, channels,
+                                  1 if ycbcr else 0, None, 0 if icc_profile is None else len(icc_profile),
+                                  ctypes.byref(pointer), ctypes.byref(size), message, _MESSAGE)
+    _raise(status, message)
+    try:
+        return ctypes.string_at(pointer, int(size.value))
+    finally:
+        library.unround_bytes_free(pointer, size)
+
+
+def main(arguments: list[str] | None = None) -> int:
+    """The reference's command line (unround_main): outside this build's path, its exit status is
+    3 (unsupported)."""
+    import sys
+
+    given = [argument.encode("utf-8") for argument in (sys.argv[1:] if arguments is None else arguments)]
+    array = (ctypes.c_char_p * max(len(given), 1))(*given)
+    return int(_library().unround_main(len(given), array))
 
 
 def oriented(picture: npt.ArrayLike, orientation: int) -> Array:

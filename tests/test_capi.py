@@ -131,3 +131,18 @@ def test_oriented_turns_as_exif_says(orientation):
 def test_oriented_refuses_what_is_no_orientation():
     with pytest.raises(native.UnroundError):
         native.oriented(np.zeros((2, 3)), 9)
+
+
+def test_the_c_layer_s_metadata_and_the_profile_check():
+    from unround import jpegio
+
+    assert jpegio.abi_version() == jpegio.ABI_VERSION
+    assert "JPEG reader" in jpegio.libjpeg_version() and "zlib" in jpegio.libpng_version()
+    assert jpegio.check_icc(b"\0" * 200, 3) is not None  # no 'acsp', no length
+
+
+def test_the_paths_outside_this_build_refuse():
+    with pytest.raises(native.UnroundError) as raised:
+        native.tiff_bytes(np.zeros((4, 4)))
+    assert raised.value.status == native.Status.UNSUPPORTED
+    assert native.main(["--help"]) == 3
