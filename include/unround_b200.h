@@ -195,6 +195,30 @@ unround_status unround_b200_decode_centres_noalloc(const unround_input* input, c
                                                    uint64_t coefficient_capacity, uint64_t* sizes, void* stream,
                                                    char* message, size_t message_size);
 
+/* One picture solved in row strips across ranks (no counterpart in the reference; its strip
+ * decomposition is the threads' of docs/math.md, here across GPUs): each rank makes the solver
+ * of its strip -- the picture's MCU bands it owns and two halo bands either side, given as an
+ * unround_input of those bands -- and drives it iteration by iteration, exchanging between the
+ * steps the halo rows of the state with its neighbours (the python package's strips module, over
+ * NCCL). The plan must record at its last iteration only (--record-every 0 --tolerance 0).
+ *   _new     the strip's solver, started (the start s_0 on the device);
+ *   _step    `iterations` iterations keeping nothing, waited for; the last one is _finish's;
+ *   _state   the device planes of the current state (x, p1, p2, and for TGV w1, w2, r11, r22,
+ *            r12, each channel after channel), rows x columns each, rows `pitch` floats apart:
+ *            returns the count, up to `most` written;
+ *   _finish  the last iteration and the result, as unround_solve makes it, of the strip's canvas;
+ *   _free    frees the strip. */
+typedef struct unround_b200_strip unround_b200_strip;
+unround_status unround_b200_strip_new(const unround_input* input, const unround_settings* settings,
+                                      unround_b200_strip** strip, char* message, size_t message_size);
+unround_status unround_b200_strip_step(unround_b200_strip* strip, uint64_t iterations, char* message,
+                                       size_t message_size);
+uint64_t unround_b200_strip_state(const unround_b200_strip* strip, float** planes, uint64_t most, uint64_t* rows,
+                                  uint64_t* columns, uint64_t* pitch);
+unround_status unround_b200_strip_finish(unround_b200_strip* strip, unround_result** result, char* message,
+                                         size_t message_size);
+void unround_b200_strip_free(unround_b200_strip* strip);
+
 #ifdef __cplusplus
 }
 #endif

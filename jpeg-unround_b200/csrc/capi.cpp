@@ -1312,6 +1312,102 @@ void unround_jpeg_planes_free(unround_jpegio_planes* planes) {
   *planes = unround_jpegio_planes{};
 }
 
+// One strip of a picture solved in row strips across ranks (strips.py): the solver of the
+// strip's own canvas (its bands and the halo bands either side), driven iteration by iteration
+// so that the caller can exchange the halo rows of the state between the steps.
+struct unround_b200_strip {
+  urb::Frame frame;
+  urb::Plan plan;
+  Stream stream;
+  std::unique_ptr<urb::Solver> solver;
+  std::uint64_t done = 0;
+};
+
+unround_status unround_b200_strip_new(const unround_input* input, const unround_settings* settings,
+                                      unround_b200_strip** strip, char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (input == nullptr || settings == nullptr || strip == nullptr) {
+      failure = {urb::kArgument, "the input, the settings and the strip are not null pointers"};
+      return false;
+    }
+    *strip = nullptr;
+    std::vector<urb::ComponentInput> inputs;
+    if (!inputs_of(input, inputs, failure)) return false;
+    const urb::Settings& s = settings->settings;
+    if (s.method != urb::Method::tv && s.method != urb::Method::tgv) {
+      failure = {urb::kOptions, "a picture is solved in strips by tv or tgv"};
+      return false;
+    }
+    auto frame = urb::make_frame(input->height, input->width, input->color_space, inputs, s, failure);
+    if (!frame) return false;
+    auto plan = urb::make_plan(s, frame->channels(), failure);
+    if (!plan) return false;
+    if (plan->record_every != 0 || plan->tolerance > 0.0 || plan->relative_tolerance > 0.0 ||
+        plan->partial_tolerance > 0.0) {
+      failure = {urb::kOptions, "a picture solved in strips records at its last iteration only and stops there: "
+                                "give --record-every 0 and --tolerance 0"};
+      return false;
+    }
+    if (!have_device(failure)) return false;
+    auto made = std::make_unique<unround_b200_strip>();
+    if (made->stream.error != cudaSuccess) {
+      failure = {urb::kInternal, std::string("a CUDA stream: ") + cudaGetErrorString(made->stream.error)};
+      return false;
+    }
+    made->frame = std::move(*frame);
+    made->plan = *plan;
+    made->solver = std::make_unique<urb::Solver>(made->frame, made->stream.stream);
+    if (!made->solver->begin_batch(made->plan, failure)) return false;
+    *strip = made.release();
+    return true;
+  });
+}
+
+unround_status unround_b200_strip_step(unround_b200_strip* strip, uint64_t iterations, char* message,
+                                       size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (strip == nullptr) {
+      failure = {urb::kArgument, "the strip is a null pointer"};
+      return false;
+    }
+    if (strip->done + iterations >= strip->plan.iterations && iterations > 0) {
+      failure = {urb::kArgument, "the strip's last iteration is made by unround_b200_strip_finish"};
+      return false;
+    }
+    if (!strip->solver->step(iterations, failure)) return false;
+    strip->done += iterations;
+    return true;
+  });
+}
+
+uint64_t unround_b200_strip_state(const unround_b200_strip* strip, float** planes, uint64_t most, uint64_t* rows,
+                                  uint64_t* columns, uint64_t* pitch) {
+  if (strip == nullptr || !strip->solver) return 0;
+  const urb::Geometry& g = strip->solver->geometry();
+  put(rows, static_cast<uint64_t>(g.rows));
+  put(columns, static_cast<uint64_t>(g.columns));
+  put(pitch, static_cast<uint64_t>(g.pitch));
+  const int bound = most > 64 ? 64 : static_cast<int>(most);
+  return static_cast<uint64_t>(strip->solver->state_planes(planes, planes == nullptr ? 0 : bound));
+}
+
+unround_status unround_b200_strip_finish(unround_b200_strip* strip, unround_result** result, char* message,
+                                         size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (strip == nullptr || result == nullptr) {
+      failure = {urb::kArgument, "the strip and the result are not null pointers"};
+      return false;
+    }
+    urb::Outcome outcome;
+    if (!strip->solver->finish_batch(strip->done, outcome, failure)) return false;
+    strip->solver.reset();
+    *result = result_of(std::move(strip->frame), std::move(outcome));
+    return true;
+  });
+}
+
+void unround_b200_strip_free(unround_b200_strip* strip) { delete strip; }
+
 // The C layer's PNG reading and writing (c/jpegio/include/unround/jpegio.h:225-256), by png_io.hpp.
 unround_jpegio_status unround_jpegio_read_png(const uint8_t* data, size_t size, uint64_t max_pixels,
                                               unround_jpegio_png_image* image, char* message, size_t message_size) {

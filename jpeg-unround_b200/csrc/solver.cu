@@ -961,6 +961,28 @@ bool Solver::finish_batch(std::uint64_t done, Outcome& out, Failure& failure) {
   return run(done, Observer{}, out, failure);
 }
 
+bool Solver::step(std::uint64_t iterations, Failure& failure) {
+  Impl& m = *impl_;
+  for (std::uint64_t n = 0; n < iterations && m.error == cudaSuccess; ++n) {
+    m.primal(false);
+    m.dual(false);
+  }
+  if (m.error == cudaSuccess) m.error = cudaStreamSynchronize(m.stream);
+  return m.check(failure, "the strip's iterations");
+}
+
+int Solver::state_planes(float** planes, int most) const {
+  const Impl& m = *impl_;
+  const Fields& f = m.state[m.current];
+  const float* fields[8] = {f.x, f.p1, f.p2, f.w1, f.w2, f.r11, f.r22, f.r12};
+  const int channels = m.g.channels;
+  const int count = (m.tgv ? 8 : 3) * channels;
+  for (int k = 0; k < count && k < most; ++k) {
+    planes[k] = const_cast<float*>(fields[k / channels]) + static_cast<std::size_t>(k % channels) * m.g.plane;
+  }
+  return count;
+}
+
 bool Solver::prepare(const Plan& plan, Failure& failure) {
   Impl& m = *impl_;
   m.plan = plan;

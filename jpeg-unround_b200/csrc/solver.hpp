@@ -98,6 +98,14 @@ class Solver {
   bool batch_entries(DualBatchImage& image, std::vector<PrimalBatchComponent>& components);
   bool finish_batch(std::uint64_t done, Outcome& out, Failure& failure);
 
+  // For a strip of a picture solved in row strips (strips.py; begin_batch first, finish_batch
+  // last): `iterations` iterations keeping nothing -- the primal step P_k, then the dual step
+  // D_k -- waited for; and the device planes of the current state s_k, field by field (x, p1,
+  // p2, and for TGV w1, w2, r11, r22, r12), each channel after channel, rows `pitch` floats apart.
+  // Returns how many planes there are (up to `most` written).
+  bool step(std::uint64_t iterations, Failure& failure);
+  int state_planes(float** planes, int most) const;
+
   // Before solve(): keep the result on the device (the Outcome gets the records and counts,
   // not the arrays); after it, the picture's 8- or 16-bit levels into host memory `out`
   // (height x width x channels, interleaved; dither 0 rounds, 1 and 2 take the blue-noise

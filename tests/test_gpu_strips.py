@@ -1,0 +1,32 @@
+"""One picture in row strips (unround.strips.solve_in_strips): the strips' solvers on one GPU with
+their halo rows swapped after every iteration, against the whole picture solved at once
+(unround_solve): the canvas to binary32 rounding (rel L2 <= 1e-5, max |difference| <= 1e-3 on
+0-255), grey and colour, TV and TGV, heights that are not whole bands, two to four strips."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("grey-tgv-2", "grey", (150, 96), ["--method", "tgv"], 2),
+    ("grey-tv-3", "grey", (203, 77), ["--method", "tv", "--alpha", "1.5"], 3),
+    ("colour420-tgv-2", "colour", (161, 120), ["--method", "tgv"], 2),
+    ("colour420-tv-apart-4", "colour", (290, 88), ["--method", "tv", "--channels", "apart"], 4),
+]
+
+
+@pytest.mark.parametrize("name, kind, shape, options, strips", CASES, ids=[c[0] for c in CASES])
+def test_strips_equal_the_whole_solve(name, kind, shape, options, strips):
+    from unround import native, synthetic
+    from unround.strips import solve_in_strips
+
+    make = synthetic.grey if kind == "grey" else synthetic.colour
+    image = make(*shape, quality=60, seed=len(name), noise=2.0).image
+    given = [*options, "--iterations", "60", "--tolerance", "0", "--record-every", "0"]
+    whole = native.solve(image, given).canvas
+    parts = solve_in_strips(image, given, strips)
+    assert parts.shape == whole.shape
+    difference = parts - whole
+    assert np.linalg.norm(difference) / np.linalg.norm(whole) <= 1e-5, name
+    assert np.abs(difference).max() <= 1e-3, name
