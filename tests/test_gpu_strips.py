@@ -30,3 +30,31 @@ def test_strips_equal_the_whole_solve(name, kind, shape, options, strips):
     difference = parts - whole
     assert np.linalg.norm(difference) / np.linalg.norm(whole) <= 1e-5, name
     assert np.abs(difference).max() <= 1e-3, name
+
+
+def test_the_distributed_form_on_one_rank():
+    # solve_strip under torch.distributed with NCCL at one rank (this pool gives one GPU a call):
+    # the driver, the state's planes aliased as device tensors and the swap's (empty) schedule.
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from unround import native, synthetic
+    from unround.strips import solve_strip
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    image = synthetic.grey(120, 64, quality=50, seed=9, noise=2.0).image
+    given = ["--method", "tgv", "--iterations", "30", "--tolerance", "0", "--record-every", "0"]
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        mine = solve_strip(image, given)
+    finally:
+        dist.destroy_process_group()
+    whole = native.solve(image, given).canvas
+    np.testing.assert_allclose(mine, whole, rtol=0, atol=1e-3)
+    assert np.linalg.norm(mine - whole) / np.linalg.norm(whole) <= 1e-5
