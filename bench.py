@@ -528,7 +528,7 @@ LARGE_OPTIONS = ["--method", "tgv", "--alpha1", "1.5", "--alpha0", "3", "--itera
 
 
 def _large_arm(args: argparse.Namespace, rank: int, world: int) -> None:
-    """BASELINE's large single solve: 8192^2 TGV (alpha0 3, alpha1 1.5), 1000 iterations. value:
+    """The large single solve: 8192^2 TGV (alpha0 3, alpha1 1.5), 1000 iterations. value:
     the iteration loop's device time (CUDA events, no records); e2e: the drop-in solve with the
     primal-dual gap recorded every 50 iterations, host arrays in and out; and the binary64 check
     that every coefficient of all 1,048,576 blocks lies in its interval."""

@@ -1,6 +1,6 @@
 """The CUDA path against the reference's conformance cases (golden fixtures), through the C
 interface. The iterations compute in binary32, the cases in binary64 within tolerances of
-binary64 rounding; the bar here is north_star's: relative L2 <= 1e-4 and max |difference|
+binary64 rounding; the bar here is the parity bar: relative L2 <= 1e-4 and max |difference|
 <= 2e-3 (0..255 scale) of the canvas, the same records and stop, every coefficient within its
 interval in binary64, and the decoder of the centres (binary64 end to end) within the case's
 own tolerance."""
