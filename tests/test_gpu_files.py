@@ -88,22 +88,28 @@ def test_a_cut_jpeg_file_warns():
     assert raised.value.status == native.Status.READ
 
 
-@pytest.mark.parametrize("mode", ["L", "RGB", "RGBA"])
+@pytest.mark.parametrize("mode", ["L", "LA", "RGB", "RGBA", "I;16"])
 def test_a_png_file_against_the_reference_solver(mode):
     from unround import native
 
-    channels = {"L": 1, "RGB": 3, "RGBA": 4}[mode]
+    channels = {"L": 1, "LA": 2, "RGB": 3, "RGBA": 4, "I;16": 1}[mode]
     pixels = _picture(5, 36, 44, channels)
+    bits = 8
+    if mode == "I;16":  # 16 bits: the 8-bit picture spread over the levels, with a little noise
+        bits = 16
+        noise = np.random.default_rng(6).integers(0, 200, size=pixels.shape)
+        pixels = (pixels.astype(np.int64) * 257 + noise).clip(0, 65535).astype(np.uint16)
     buffer = io.BytesIO()
     PILImage.fromarray(pixels).save(buffer, format="PNG")
+    assert PILImage.open(io.BytesIO(buffer.getvalue())).mode == mode
     options = ["--method", "tgv", "--iterations", "120", "--tolerance", "0"]
     ours = native.decode(buffer.getvalue(), options)
-    assert ours.input_format == "png" and ours.bits == 8
-    theirs = reference.solve_samples(pixels, 8, options)
+    assert ours.input_format == "png" and ours.bits == bits
+    theirs = reference.solve_samples(pixels, bits, options)
     got = ours.canvas.reshape(theirs.canvas.shape)
     assert np.linalg.norm(got - theirs.canvas) / np.linalg.norm(theirs.canvas) <= 1e-4
     assert np.max(np.abs(got - theirs.canvas)) <= 2e-3
-    np.testing.assert_array_equal(native.solve_samples(pixels, 8, options).canvas, ours.canvas)
+    np.testing.assert_array_equal(native.solve_samples(pixels, bits, options).canvas, ours.canvas)
 
 
 @pytest.mark.parametrize("sixteen", [False, True])
