@@ -14,8 +14,9 @@
  * Each declaration cites the reference declaration it replaces (rust/capi/include/unround.h,
  * line numbers of that file). Files are read and written on the host by this build's own JPEG
  * reader (ITU-T T.81: baseline, extended and progressive Huffman files) and PNG reader and writer
- * (zlib), in place of libjpeg-turbo and libpng; the projection onto a file's intervals
- * (unround_project) and the TIFF writer are exported and return UNROUND_ERROR_UNSUPPORTED. */
+ * (zlib), in place of libjpeg-turbo and libpng; a picture's projection onto a file's intervals
+ * (unround_project) is computed on the host in binary64; the TIFF writer and the command line
+ * are exported and refuse (UNROUND_ERROR_UNSUPPORTED; unround_main returns 3). */
 #ifndef UNROUND_H
 #define UNROUND_H
 
@@ -103,7 +104,9 @@ unround_status unround_decode(const uint8_t* data, size_t size, const unround_se
 unround_status unround_solve(const unround_input* input, const unround_settings* settings, unround_observer observer,
                              void* user, unround_result** result, char* message, size_t message_size);
 
-/* unround.h:148-150: needs libjpeg-turbo; UNROUND_ERROR_UNSUPPORTED here. */
+/* unround.h:142-150: a picture measured against a JPEG file's intervals and projected onto them,
+ * on the host in binary64; the result has no solver, and unround_result_excess gives each
+ * component's excess in steps. */
 unround_status unround_project(const uint8_t* data, size_t size, const unround_settings* settings,
                                const double* picture, uint64_t height, uint64_t width, uint64_t channels,
                                unround_result** result, char* message, size_t message_size);

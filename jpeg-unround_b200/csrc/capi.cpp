@@ -21,6 +21,7 @@
 #include "blue_noise.hpp"
 #include "jpeg_reader.hpp"
 #include "colour.hpp"
+#include "dct.cuh"
 #include "model.hpp"
 #include "png_io.hpp"
 #include "samples_model.hpp"
@@ -57,6 +58,7 @@ struct unround_result {
   std::int32_t exif_orientation = 0;
   std::vector<std::uint8_t> icc;
   std::string warning;
+  std::vector<std::vector<double>> excess;  // of a projection: each component's, in steps
 };
 
 namespace {
@@ -176,6 +178,156 @@ void to_ycbcr(const double* picture, std::size_t size, double* planes) {
     planes[size + k] = 128.0 + kToCb * (b - y);
     planes[2 * size + k] = 128.0 + kToCr * (r - y);
   }
+}
+
+// The projection of a picture made elsewhere onto a frame's intervals (docs/math.md 12;
+// cpp/src/picture.cpp:70-148, rust/unround/src/picture.rs:130), on the host in binary64. The
+// canvas is made as an encoder makes the file's: of a file in YCbCr JFIF's YCbCr of the picture's
+// RGB, of a grey or RGB file its own channels, each extended over the canvas's whole MCUs by
+// repeating its last column and then its last row. Then channel by channel and block by block:
+// the cell means (each cell's samples summed down its columns, those sums across, divided by the
+// cell's samples), their DCT e (rows, then columns), each coefficient's excess
+// max(0, a - e, e - b) / Q, zeta = clip(e, a, b), and the canvas moved: with cells of one sample
+// the inverse DCT of zeta, else each cell's samples by the change of its mean; the samples beyond
+// the blocks as they are. Into `out` (the projected canvas, zeta, the planes and the picture)
+// and `excess` (component by component, 64 a block).
+bool project_picture(const urb::Frame& frame, const double* picture, urb::Outcome& out,
+                     std::vector<std::vector<double>>& excess, urb::Failure& failure) {
+  const std::size_t height = frame.height, width = frame.width, rows = frame.rows, columns = frame.columns;
+  const std::size_t channels = frame.channels(), count = height * width, plane = frame.plane();
+  const std::size_t given = frame.color_space == 1 ? 1 : 3;
+  for (std::size_t k = 0; k < count * given; ++k) {
+    if (!std::isfinite(picture[k])) {
+      failure = {urb::kOptions, "a picture's samples are finite"};
+      return false;
+    }
+  }
+  std::vector<double> planes(channels * count);
+  if (frame.color_space == 2) {
+    to_ycbcr(picture, count, planes.data());
+  } else {
+    for (std::size_t k = 0; k < count; ++k) {
+      for (std::size_t c = 0; c < channels; ++c) planes[c * count + k] = picture[k * given + c];
+    }
+  }
+  out.canvas.resize(channels * plane);
+  double* canvas = out.canvas.data();
+  for (std::size_t c = 0; c < channels; ++c) {
+    double* grid = canvas + c * plane;
+    for (std::size_t i = 0; i < rows; ++i) {
+      const double* from = planes.data() + c * count + std::min(i, height - 1) * width;
+      double* to = grid + i * columns;
+      std::copy(from, from + width, to);
+      std::fill(to + width, to + columns, from[width - 1]);
+    }
+  }
+  double basis[8][8];
+  for (int k = 0; k < 8; ++k) {
+    for (int n = 0; n < 8; ++n) basis[k][n] = urb::basis(k, n);
+  }
+  excess.assign(channels, {});
+  out.coefficients.clear();
+  for (std::size_t c = 0; c < channels; ++c) {
+    const urb::Component& comp = frame.components[c];
+    const std::size_t down = comp.cell_rows, across = comp.cell_columns;
+    const double cells = static_cast<double>(down * across);
+    double* grid = canvas + c * plane;
+    std::vector<double>& beyond = excess[c];
+    beyond.assign(comp.coefficient_count(), 0.0);
+    urb::HostBuffer kept;
+    kept.resize(comp.coefficient_count());
+    for (std::size_t by = 0; by < comp.block_rows; ++by) {
+      for (std::size_t bx = 0; bx < comp.block_columns; ++bx) {
+        // The block's samples of the component: the cell means.
+        double m[8][8];
+        for (std::size_t y = 0; y < 8; ++y) {
+          for (std::size_t x = 0; x < 8; ++x) {
+            const std::size_t i0 = (8 * by + y) * down, j0 = (8 * bx + x) * across;
+            double total = 0.0;
+            for (std::size_t b = 0; b < across; ++b) {
+              double column = grid[i0 * columns + j0 + b];
+              for (std::size_t a = 1; a < down; ++a) column += grid[(i0 + a) * columns + j0 + b];
+              total = b == 0 ? column : total + column;
+            }
+            m[y][x] = cells == 1.0 ? total : total / cells;
+          }
+        }
+        double t[8][8], e[8][8];
+        for (int y = 0; y < 8; ++y) {
+          for (int u = 0; u < 8; ++u) {
+            double sum = 0.0;
+            for (int x = 0; x < 8; ++x) sum += basis[u][x] * m[y][x];
+            t[y][u] = sum;
+          }
+        }
+        for (int v = 0; v < 8; ++v) {
+          for (int u = 0; u < 8; ++u) {
+            double sum = 0.0;
+            for (int y = 0; y < 8; ++y) sum += basis[v][y] * t[y][u];
+            e[v][u] = sum;
+          }
+        }
+        const std::size_t block = by * comp.block_columns + bx;
+        const std::int16_t* levels = comp.levels.data() + block * 64;
+        double z[8][8];
+        for (int k = 0; k < 64; ++k) {
+          const double value = e[k / 8][k % 8];
+          const double low = comp.lower(levels[k], k), high = comp.upper(levels[k], k);
+          beyond[block * 64 + k] = std::max(std::max(low - value, value - high), 0.0) / comp.steps[k];
+          z[k / 8][k % 8] = std::min(std::max(value, low), high);
+          kept.data()[block * 64 + k] = z[k / 8][k % 8];
+        }
+        for (int y = 0; y < 8; ++y) {
+          for (int u = 0; u < 8; ++u) {
+            double sum = 0.0;
+            for (int v = 0; v < 8; ++v) sum += basis[v][y] * z[v][u];
+            t[y][u] = sum;
+          }
+        }
+        for (std::size_t y = 0; y < 8; ++y) {
+          for (std::size_t x = 0; x < 8; ++x) {
+            double back = 0.0;
+            for (int u = 0; u < 8; ++u) back += basis[u][x] * t[y][u];
+            const std::size_t i0 = (8 * by + y) * down, j0 = (8 * bx + x) * across;
+            if (cells == 1.0) {
+              grid[i0 * columns + j0] = back;
+            } else {
+              const double change = back - m[y][x];
+              for (std::size_t a = 0; a < down; ++a) {
+                for (std::size_t b = 0; b < across; ++b) grid[(i0 + a) * columns + j0 + b] += change;
+              }
+            }
+          }
+        }
+      }
+    }
+    out.coefficients.push_back(std::move(kept));
+  }
+  // The planes cut to the picture, and of colour the picture interleaved (of YCbCr, its RGB).
+  if (height != rows || width != columns) {
+    out.planes.resize(channels * count);
+    for (std::size_t c = 0; c < channels; ++c) {
+      for (std::size_t i = 0; i < height; ++i) {
+        std::copy(canvas + c * plane + i * columns, canvas + c * plane + i * columns + width,
+                  out.planes.data() + c * count + i * width);
+      }
+    }
+  }
+  if (channels == 3) {
+    const double* cut = out.planes.empty() ? canvas : out.planes.data();
+    out.picture.resize(3 * count);
+    if (frame.color_space == 2) {
+      to_rgb(cut, count, out.picture.data());
+    } else {
+      for (std::size_t k = 0; k < count; ++k) {
+        for (std::size_t c = 0; c < 3; ++c) out.picture.data()[3 * k + c] = cut[c * count + k];
+      }
+    }
+  }
+  out.iterations = 0;
+  out.stop = 0;
+  out.solved = false;
+  return true;
 }
 
 // The result of a solve (rust/unround/src/decode.rs:306-364): the canvas cut to the picture,
@@ -749,11 +901,63 @@ unround_status unround_b200_model(const unround_input* input, const unround_sett
   });
 }
 
-unround_status unround_project(const uint8_t*, size_t, const unround_settings*, const double*, uint64_t, uint64_t,
-                               uint64_t, unround_result**, char* message, size_t message_size) {
-  say(message, message_size, "projecting onto a JPEG file's intervals needs libjpeg-turbo, which this build does "
-                             "not carry");
-  return UNROUND_ERROR_UNSUPPORTED;
+// A picture made elsewhere measured against a JPEG file's intervals and projected onto them
+// (rust/capi/src/lib.rs, unround_project; docs/math.md 12): the file's coefficients read on the
+// host as unround_decode reads them, its frame with the settings' slack, and the projection of
+// project_picture. The picture is the file's size as it stores it, grey or RGB.
+unround_status unround_project(const uint8_t* data, size_t size, const unround_settings* settings,
+                               const double* picture, uint64_t height, uint64_t width, uint64_t channels,
+                               unround_result** result, char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (data == nullptr || settings == nullptr || picture == nullptr || result == nullptr) {
+      failure = {urb::kArgument, "the data, the settings, the picture and the result are not null pointers"};
+      return false;
+    }
+    const urb::Settings& s = settings->settings;
+    urb::JpegLimits limits;
+    limits.max_pixels = s.reading.max_pixels;
+    limits.max_scans = s.reading.max_scans;
+    limits.warnings_are_errors = s.reading.warnings_are_errors;
+    urb::JpegFile file;
+    std::string text;
+    const int status = urb::read_jpeg(data, size, limits, file, text);
+    if (status != urb::kJpegOk) {
+      failure = {status == urb::kJpegUnsupported ? urb::kUnsupported : status == urb::kJpegLimit ? urb::kOptions
+                                                                                                 : urb::kRead,
+                 text};
+      return false;
+    }
+    const std::uint64_t expected = file.color_space == 1 ? 1 : 3;
+    if (height != file.height || width != file.width || channels != expected) {
+      failure = {urb::kOptions, "a picture of the file is " + std::to_string(file.height) + " x " +
+                                    std::to_string(file.width) + " x " + std::to_string(expected) + " samples, not " +
+                                    std::to_string(height) + " x " + std::to_string(width) + " x " +
+                                    std::to_string(channels)};
+      return false;
+    }
+    std::vector<urb::ComponentInput> inputs;
+    for (const urb::JpegComponent& c : file.components) {
+      urb::ComponentInput in;
+      in.levels = c.coefficients.data();
+      in.rows = c.height_in_blocks;
+      in.columns = c.width_in_blocks;
+      in.h = c.h;
+      in.v = c.v;
+      std::copy(c.table, c.table + 64, in.table.begin());
+      inputs.push_back(in);
+    }
+    auto frame = urb::make_frame(file.height, file.width, file.color_space, inputs, s, failure);
+    if (!frame) return false;
+    urb::Outcome outcome;
+    std::vector<std::vector<double>> excess;
+    if (!project_picture(*frame, picture, outcome, excess, failure)) return false;
+    *result = result_of(std::move(*frame), std::move(outcome));
+    (*result)->excess = std::move(excess);
+    (*result)->exif_orientation = file.exif_orientation;
+    (*result)->icc = std::move(file.icc);
+    (*result)->warning = file.warning;
+    return true;
+  });
 }
 
 void unround_result_free(unround_result* result) { delete result; }
@@ -883,7 +1087,14 @@ int32_t unround_result_bits(const unround_result* result) { return result == nul
 const char* unround_result_warning(const unround_result* result) {
   return result == nullptr ? nullptr : result->warning.c_str();
 }
-const double* unround_result_excess(const unround_result*, uint64_t, uint64_t*) { return nullptr; }
+const double* unround_result_excess(const unround_result* result, uint64_t component, uint64_t* count) {
+  if (result == nullptr || component >= result->excess.size()) {
+    put(count, 0);
+    return nullptr;
+  }
+  put(count, result->excess[component].size());
+  return result->excess[component].data();
+}
 
 unround_status unround_tiff(const double*, uint64_t, uint64_t, uint64_t, int32_t, const uint8_t*, uint64_t, uint8_t**,
                             uint64_t*, char* message, size_t message_size) {

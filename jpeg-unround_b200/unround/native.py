@@ -222,6 +222,7 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_result_format": (i32, handle),
         "unround_result_bits": (i32, handle),
         "unround_result_warning": (ctypes.c_char_p, handle),
+        "unround_result_excess": (doubles, handle, u64, u64p),
         "unround_b200_solve_levels": (i32, ctypes.POINTER(_Input), handle, i32, i32, ctypes.c_void_p, u64, u64p,
                                       *text),
         "unround_b200_solve_samples": (i32, ctypes.POINTER(ctypes.c_uint16), u64, u64, u64, i32, handle, *made),
@@ -486,6 +487,12 @@ def _decoded(library: ctypes.CDLL, result: ctypes.c_void_p, problems: bool = Tru
         values = [_copy(library.unround_result_record_values(result, which, ctypes.byref(n)), (int(n.value),))
                   for which in range(5)]
         solution = Solution(int(iterations.value), Stop(int(stop.value)), History(steps, *values))
+    excess = []
+    for index in range(len(coefficients)):
+        pointer = library.unround_result_excess(result, index, ctypes.byref(count))
+        if not pointer:
+            break
+        excess.append(_copy(pointer, coefficients[index].shape))
     icc_size = ctypes.c_uint64()
     icc = library.unround_result_icc_profile(result, ctypes.byref(icc_size))
     return Decoded(
@@ -496,6 +503,7 @@ def _decoded(library: ctypes.CDLL, result: ctypes.c_void_p, problems: bool = Tru
         exif_orientation=int(library.unround_result_exif_orientation(result)),
         input_format="png" if int(library.unround_result_format(result)) == 2 else "jpeg",
         bits=int(library.unround_result_bits(result)),
+        excess=tuple(excess) if excess else None,
     )
 
 
@@ -744,19 +752,37 @@ def decode(source: object, settings: Settings | list[str] | None = None, *, obse
         library.unround_result_free(result)
 
 
-def project(picture: npt.ArrayLike, source: object, settings: Settings | None = None, **_: object) -> Decoded:
-    """Projecting onto a JPEG file's intervals needs libjpeg-turbo: the library refuses."""
+def project(picture: npt.ArrayLike, source: object, settings: Settings | list[str] | None = None, *,
+            max_pixels: int = 0, max_scans: int = 0, warnings_are_errors: bool = False) -> Decoded:
+    """Measures a picture against a JPEG file's intervals and projects it onto them
+    (unround_project; docs/math.md 12 of the reference). picture is of the file's size as the file
+    stores it, before its EXIF orientation: (height, width) of a greyscale file, or (height,
+    width, 3) of RGB of a file in colour, made elsewhere, by another decoder, say; source is the
+    file's bytes or path. The result is the projection, as a reconstruction without a solver
+    (result is None), and its excess holds the picture's: how far each coefficient lay outside its
+    interval, in steps. A picture of another size or of other channels raises UnroundError."""
+    if isinstance(settings, list):
+        given = list(settings)
+        if max_pixels:
+            given += ["--max-pixels", str(max_pixels)]
+        if max_scans:
+            given += ["--max-scans", str(max_scans)]
+        if warnings_are_errors:
+            given.append("--warnings-are-errors")
+    else:
+        given = options(settings, max_pixels=max_pixels, max_scans=max_scans, warnings_are_errors=warnings_are_errors)
     library = _library()
-    handle = _settings_of(settings)
+    handle = _Settings(given)
     samples = np.ascontiguousarray(picture, dtype=np.float64)
+    if samples.ndim not in (2, 3):
+        raise ValueError(f"a picture is (height, width) or (height, width, channels), not {samples.shape}")
+    data = Path(source).read_bytes() if isinstance(source, (str, os.PathLike)) else bytes(source)  # type: ignore[arg-type]
     result = ctypes.c_void_p()
     message = ctypes.create_string_buffer(_MESSAGE)
-    data = source if isinstance(source, (bytes, bytearray)) else b""
-    status = library.unround_project(bytes(data), len(data), handle.handle,
+    status = library.unround_project(data, len(data), handle.handle,
                                      samples.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), samples.shape[0],
-                                     samples.shape[1] if samples.ndim > 1 else 1,
-                                     samples.shape[2] if samples.ndim > 2 else 1, ctypes.byref(result), message,
-                                     _MESSAGE)
+                                     samples.shape[1], samples.shape[2] if samples.ndim > 2 else 1,
+                                     ctypes.byref(result), message, _MESSAGE)
     _raise(status, message)
     try:
         return _decoded(library, result)

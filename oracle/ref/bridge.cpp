@@ -13,6 +13,7 @@
 #include "unround/model.hpp"
 #include "unround/operators.hpp"
 #include "unround/pdhg.hpp"
+#include "unround/picture.hpp"
 #include "unround/samples.hpp"
 #include "unround/settings.hpp"
 
@@ -327,6 +328,62 @@ void oref_solver(const void* handle, std::uint64_t* iterations, std::int32_t* st
   *stop = out->stop;
   *tau = out->tau;
   *sigma = out->sigma;
+}
+
+// The projection of a picture onto the intervals of components given as arrays, as the
+// reference's picture::project makes it (cpp/src/picture.cpp:70-148: canvas_of, excess, and
+// Frame::project per channel), without the picture of the result: into `canvas` (C x rows x
+// columns), `zeta` (every component's blocks, 64 a block) and `excess` (the same, in steps).
+// Returns 0, or 1 with the reason in message.
+int oref_project(std::uint32_t height, std::uint32_t width, std::int32_t color_space, std::uint32_t count,
+                 const Component* components, std::size_t option_count, const char* const* options,
+                 const double* picture, std::size_t channels, double* canvas, double* zeta, double* excess,
+                 char* message, std::size_t message_size) {
+  using namespace unround;
+  std::vector<std::string_view> arguments;
+  for (std::size_t i = 0; i < option_count; ++i) arguments.emplace_back(options[i]);
+  auto parsed = parse_settings(arguments);
+  if (!parsed) {
+    say(message, message_size, parsed.error().message);
+    return 1;
+  }
+  const ColourSpace space = color_space == 1 ? ColourSpace::grayscale
+                            : color_space == 2 ? ColourSpace::ycbcr
+                                               : ColourSpace::rgb;
+  std::vector<ComponentInput> inputs;
+  for (std::uint32_t c = 0; c < count; ++c) {
+    ComponentInput in;
+    in.levels = Blocks<const std::int16_t>(components[c].levels, block_extents(components[c].rows, components[c].columns));
+    for (int k = 0; k < 64; ++k) in.table[k] = components[c].table[k];
+    in.h = static_cast<std::uint32_t>(components[c].h);
+    in.v = static_cast<std::uint32_t>(components[c].v);
+    inputs.push_back(in);
+  }
+  auto frame = Frame::make(height, width, space, inputs, data_of(*parsed));
+  if (!frame) {
+    say(message, message_size, frame.error().message);
+    return 1;
+  }
+  auto made = picture::canvas_of(*frame, Picture<const double>(picture, PictureExtents{height, width, channels}));
+  if (!made) {
+    say(message, message_size, made.error().message);
+    return 1;
+  }
+  const std::vector<BlocksArray<double>> beyond = picture::excess(*frame, *made);
+  std::size_t offset = 0;
+  for (std::size_t c = 0; c < frame->channels(); ++c) {
+    GridArray<double>& grid = (*made)[c];
+    BlocksArray<double> kept(frame->component(c).problem.extents());
+    Room room = frame->room(c);
+    frame->project(c, std::as_const(grid).view(), grid.view(), kept.view(), room);
+    const std::size_t plane = frame->rows() * frame->columns();
+    std::memcpy(canvas + c * plane, grid.view().data_handle(), plane * sizeof(double));
+    const std::size_t entries = kept.entries().size();
+    std::memcpy(zeta + offset, kept.entries().data(), entries * sizeof(double));
+    std::memcpy(excess + offset, beyond[c].entries().data(), entries * sizeof(double));
+    offset += entries;
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -63,6 +63,12 @@ def _library() -> ctypes.CDLL:
         ctypes.c_size_t, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_Start), ctypes.c_char_p, ctypes.c_size_t,
     )
     lib.oref_free.argtypes = (ctypes.c_void_p,)
+    lib.oref_project.restype = ctypes.c_int
+    lib.oref_project.argtypes = (
+        ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_uint32, ctypes.POINTER(_Component),
+        ctypes.c_size_t, ctypes.POINTER(ctypes.c_char_p), dp, ctypes.c_size_t, dp, dp, dp, ctypes.c_char_p,
+        ctypes.c_size_t,
+    )
     lib.oref_shape.argtypes = (ctypes.c_void_p, u64p, u64p, u64p)
     lib.oref_canvas.restype = dp
     lib.oref_canvas.argtypes = (ctypes.c_void_p,)
@@ -224,3 +230,56 @@ def solve_samples(levels: np.ndarray, bits: int, options: list[str]) -> SolvedSa
                              iterations=iterations.value, stop=stop.value, tau=tau.value, sigma=sigma.value)
     finally:
         lib.oref_free(handle)
+
+
+@dataclass
+class Projected:
+    """The reference's projection of a picture onto a file's intervals (cpp/src/picture.cpp:
+    70-148): the projected canvas (C, rows, columns), each component's clipped coefficients and
+    the picture's excess in steps (rows, columns, 8, 8)."""
+
+    canvas: np.ndarray
+    coefficients: list[np.ndarray]
+    excess: list[np.ndarray]
+
+
+def project(height: int, width: int, color_space: int, components: list[tuple[np.ndarray, np.ndarray, int, int]],
+            options: list[str], picture: np.ndarray) -> Projected:
+    """Runs the reference's projection of `picture` ((height, width) grey or (height, width, 3)
+    RGB, binary64) onto the intervals of the components (as solve takes them)."""
+    lib = _library()
+    kept = []
+    raw = (_Component * len(components))()
+    for index, (levels, table, h, v) in enumerate(components):
+        levels = np.ascontiguousarray(levels, dtype=np.int16)
+        kept.append(levels)
+        raw[index].levels = levels.ctypes.data_as(ctypes.POINTER(ctypes.c_int16))
+        raw[index].rows, raw[index].columns = levels.shape[0], levels.shape[1]
+        raw[index].h, raw[index].v = h, v
+        raw[index].table = (ctypes.c_uint16 * 64)(*(int(step) for step in np.asarray(table).reshape(64)))
+    encoded = [option.encode() for option in options]
+    array = (ctypes.c_char_p * max(len(encoded), 1))(*encoded)
+    samples = np.ascontiguousarray(picture, dtype=np.float64)
+    channels = 1 if samples.ndim == 2 else samples.shape[2]
+    v_max = max(v for _, _, _, v in components)
+    h_max = max(h for _, _, h, _ in components)
+    rows = -(-height // (8 * v_max)) * 8 * v_max
+    columns = -(-width // (8 * h_max)) * 8 * h_max
+    canvas = np.zeros((len(components), rows, columns))
+    blocks = [np.asarray(levels).shape[:2] for levels, _, _, _ in components]
+    total = sum(r * c * 64 for r, c in blocks)
+    zeta, excess = np.zeros(total), np.zeros(total)
+    dp = ctypes.POINTER(ctypes.c_double)
+    message = ctypes.create_string_buffer(4096)
+    status = lib.oref_project(height, width, color_space, len(components), raw, len(encoded), array,
+                              samples.ctypes.data_as(dp), channels, canvas.ctypes.data_as(dp),
+                              zeta.ctypes.data_as(dp), excess.ctypes.data_as(dp), message, 4096)
+    if status != 0:
+        raise ValueError(message.value.decode())
+    out_z, out_e, offset = [], [], 0
+    for r, c in blocks:
+        n = r * c * 64
+        out_z.append(zeta[offset : offset + n].reshape(r, c, 8, 8))
+        out_e.append(excess[offset : offset + n].reshape(r, c, 8, 8))
+        offset += n
+    return Projected(canvas, out_z, out_e)

@@ -89,10 +89,10 @@ def test_file_paths_refuse_what_they_cannot_read():
     with pytest.raises(native.UnroundError) as raised:
         native.decode(b"\xff\xd8\xff")
     assert raised.value.status == native.Status.READ
-    # The projection onto a file's intervals is not on this build's path.
+    # Nor can a picture be projected onto the intervals of a file that holds no image.
     with pytest.raises(native.UnroundError) as raised:
         native.project(np.zeros((8, 8)), b"\xff\xd8\xff\xd9")
-    assert raised.value.status == native.Status.UNSUPPORTED
+    assert raised.value.status == native.Status.READ
 
 
 def test_colour_conversions_invert():
