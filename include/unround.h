@@ -15,8 +15,8 @@
  * line numbers of that file). Files are read and written on the host by this build's own JPEG
  * reader (ITU-T T.81: baseline, extended and progressive Huffman files) and PNG reader and writer
  * (zlib), in place of libjpeg-turbo and libpng; a picture's projection onto a file's intervals
- * (unround_project) is computed on the host in binary64; the TIFF writer and the command line
- * are exported and refuse (UNROUND_ERROR_UNSUPPORTED; unround_main returns 3). */
+ * (unround_project) is computed on the host in binary64, and the TIFF writer holds binary64
+ * samples bit for bit; the command line is exported and refuses (unround_main returns 3). */
 #ifndef UNROUND_H
 #define UNROUND_H
 

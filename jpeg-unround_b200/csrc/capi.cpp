@@ -1096,10 +1096,134 @@ const double* unround_result_excess(const unround_result* result, uint64_t compo
   return result->excess[component].data();
 }
 
-unround_status unround_tiff(const double*, uint64_t, uint64_t, uint64_t, int32_t, const uint8_t*, uint64_t, uint8_t**,
-                            uint64_t*, char* message, size_t message_size) {
-  say(message, message_size, "the TIFF writer is host output outside this build's path");
-  return UNROUND_ERROR_UNSUPPORTED;
+// A TIFF of the picture's binary64 samples, bit for bit (rust/capi/src/lib.rs, unround_tiff; the
+// TIFF 6.0 specification): little-endian, one uncompressed strip, the samples of a pixel together,
+// SampleFormat IEEE floating point of 64 bits; grey (BlackIsZero) or RGB, with an alpha last
+// declared unassociated (ExtraSamples 2); with ycbcr, three samples declared as JFIF's Y, Cb and
+// Cr (YCbCrCoefficients 0.299, 0.587, 0.114; no subsampling; ReferenceBlackWhite 0-255 and
+// 128-centred); the ICC profile (tag 34675) where it goes with the picture's colours (as
+// unround_jpeg_check_icc checks it; of YCbCr, its RGB), otherwise left out and the message says why.
+unround_status unround_tiff(const double* samples, uint64_t height, uint64_t width, uint64_t channels, int32_t ycbcr,
+                            const uint8_t* icc, uint64_t icc_size, uint8_t** bytes, uint64_t* size, char* message,
+                            size_t message_size) {
+  std::string warning;
+  const unround_status status = guarded(message, message_size, [&](urb::Failure& failure) {
+    if (bytes == nullptr || size == nullptr) {
+      failure = {urb::kArgument, "the bytes and the size are not null pointers"};
+      return false;
+    }
+    std::size_t count = 0;
+    if (!picture_count(samples, height, width, channels, count, failure)) return false;
+    if (ycbcr != 0 && channels != 3) {
+      failure = {urb::kOptions, "YCbCr is three samples a pixel, not " + std::to_string(channels)};
+      return false;
+    }
+    const std::uint64_t data_bytes = static_cast<std::uint64_t>(count) * 8u;
+    if (height > 0xFFFFFFFFull || width > 0xFFFFFFFFull || data_bytes > 0xFFFF0000ull) {
+      failure = {urb::kOptions, "a TIFF of this build holds at most 4 GB of samples"};
+      return false;
+    }
+    bool with_icc = false;
+    if (icc != nullptr) {
+      std::string reason;
+      with_icc = urb::check_icc(icc, icc_size, static_cast<int>(channels), reason);
+      if (!with_icc) warning = "the ICC profile is not written: " + reason;
+    }
+    // The IFD's entries (tag, type, count, value or offset), in tag order; values of more than
+    // 4 bytes go after the IFD.
+    struct Entry {
+      std::uint16_t tag, type;
+      std::uint32_t count;
+      std::vector<std::uint8_t> value;
+    };
+    auto shorts = [](std::initializer_list<std::uint32_t> values) {
+      std::vector<std::uint8_t> v;
+      for (std::uint32_t x : values) {
+        v.push_back(static_cast<std::uint8_t>(x));
+        v.push_back(static_cast<std::uint8_t>(x >> 8));
+      }
+      return v;
+    };
+    auto longs = [](std::initializer_list<std::uint32_t> values) {
+      std::vector<std::uint8_t> v;
+      for (std::uint32_t x : values) {
+        for (int b = 0; b < 4; ++b) v.push_back(static_cast<std::uint8_t>(x >> (8 * b)));
+      }
+      return v;
+    };
+    auto repeated_short = [&](std::uint32_t value, std::size_t n) {
+      std::vector<std::uint8_t> v;
+      for (std::size_t k = 0; k < n; ++k) {
+        const auto one = shorts({value});
+        v.insert(v.end(), one.begin(), one.end());
+      }
+      return v;
+    };
+    const std::uint32_t spp = static_cast<std::uint32_t>(channels);
+    const std::uint32_t photometric = ycbcr != 0 ? 6 : (spp <= 2 ? 1 : 2);
+    std::vector<Entry> entries = {
+        {256, 4, 1, longs({static_cast<std::uint32_t>(width)})},
+        {257, 4, 1, longs({static_cast<std::uint32_t>(height)})},
+        {258, 3, spp, repeated_short(64, spp)},
+        {259, 3, 1, shorts({1})},
+        {262, 3, 1, shorts({photometric})},
+        {273, 4, 1, longs({0})},  // the strip's offset, set below
+        {277, 3, 1, shorts({spp})},
+        {278, 4, 1, longs({static_cast<std::uint32_t>(height)})},
+        {279, 4, 1, longs({static_cast<std::uint32_t>(data_bytes)})},
+        {284, 3, 1, shorts({1})},
+    };
+    if (spp == 2 || spp == 4) entries.push_back({338, 3, 1, shorts({2})});
+    entries.push_back({339, 3, spp, repeated_short(3, spp)});
+    if (ycbcr != 0) {
+      entries.push_back({529, 5, 3, longs({299, 1000, 587, 1000, 114, 1000})});
+      entries.push_back({530, 3, 2, shorts({1, 1})});
+      entries.push_back({532, 5, 6, longs({0, 1, 255, 1, 128, 1, 255, 1, 128, 1, 255, 1})});
+    }
+    if (with_icc) entries.push_back({34675, 7, static_cast<std::uint32_t>(icc_size), std::vector<std::uint8_t>(icc, icc + icc_size)});
+    // Layout: header (8), IFD (2 + 12 n + 4), the values that do not fit, then the samples at an
+    // offset that is a multiple of 8.
+    const std::uint32_t ifd_bytes = 2 + 12 * static_cast<std::uint32_t>(entries.size()) + 4;
+    std::uint32_t extra = 8 + ifd_bytes;
+    std::vector<std::uint32_t> offsets(entries.size(), 0);
+    for (std::size_t e = 0; e < entries.size(); ++e) {
+      if (entries[e].value.size() > 4) {
+        offsets[e] = extra;
+        extra += static_cast<std::uint32_t>((entries[e].value.size() + 1) / 2 * 2);
+      }
+    }
+    const std::uint32_t data_offset = (extra + 7) / 8 * 8;
+    entries[5].value = longs({data_offset});
+    const std::size_t total = data_offset + static_cast<std::size_t>(data_bytes);
+    std::unique_ptr<std::uint8_t[]> file(new std::uint8_t[total]());
+    std::uint8_t* out = file.get();
+    const std::uint8_t header[8] = {'I', 'I', 42, 0, 8, 0, 0, 0};
+    std::memcpy(out, header, 8);
+    std::uint8_t* at = out + 8;
+    const std::uint16_t n = static_cast<std::uint16_t>(entries.size());
+    std::memcpy(at, &n, 2);
+    at += 2;
+    for (std::size_t e = 0; e < entries.size(); ++e) {
+      const Entry& entry = entries[e];
+      std::memcpy(at, &entry.tag, 2);
+      std::memcpy(at + 2, &entry.type, 2);
+      std::memcpy(at + 4, &entry.count, 4);
+      if (entry.value.size() > 4) {
+        std::memcpy(at + 8, &offsets[e], 4);
+        std::memcpy(out + offsets[e], entry.value.data(), entry.value.size());
+      } else {
+        std::memcpy(at + 8, entry.value.data(), entry.value.size());
+      }
+      at += 12;
+    }
+    std::memset(at, 0, 4);  // no next IFD
+    std::memcpy(out + data_offset, samples, static_cast<std::size_t>(data_bytes));  // little-endian host
+    *size = total;
+    *bytes = file.release();
+    return true;
+  });
+  if (status == UNROUND_OK) say(message, message_size, warning);
+  return status;
 }
 
 // The bytes of a PNG file (rust/capi/src/lib.rs, unround_png; c/jpegio/src/png.c): the levels

@@ -890,22 +890,28 @@ def png_bytes(picture: npt.ArrayLike, *, sixteen: bool = False, dither: str = "b
 
 
 def tiff_bytes(picture: npt.ArrayLike, *, ycbcr: bool = False, icc_profile: bytes | None = None) -> bytes:
-    """The TIFF writer of the reference (unround_tiff): outside this build's path, it raises
-    UnroundError with UNSUPPORTED."""
+    """A TIFF of the picture's samples in binary64, bit for bit (unround_tiff): (height, width) or
+    (height, width, channels) with 1 to 4 channels, an alpha last. With ycbcr, the three samples of
+    a pixel are JFIF's Y, Cb and Cr, and the file says so. The ICC profile is embedded where it goes
+    with the picture (jpegio.check_icc); otherwise it is left out, with an UnroundWarning."""
     samples = np.ascontiguousarray(picture, dtype=np.float64)
     if samples.ndim not in (2, 3):
         raise ValueError(f"a picture is (height, width) or (height, width, channels), not {samples.shape}")
     height, width = int(samples.shape[0]), int(samples.shape[1])
     channels = 1 if samples.ndim == 2 else int(samples.shape[2])
+    profile = None if icc_profile is None else bytes(icc_profile)
+    buffer = (ctypes.c_uint8 * len(profile)).from_buffer_copy(profile) if profile else None
     library = _library()
     pointer = ctypes.POINTER(ctypes.c_uint8)()
     size = ctypes.c_uint64()
     message = ctypes.create_string_buffer(_MESSAGE)
     status = library.unround_tiff(samples.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), height, width, channels,
-                                  1 if ycbcr else 0, None, 0 if icc_profile is None else len(icc_profile),
+                                  1 if ycbcr else 0, buffer, 0 if profile is None else len(profile),
                                   ctypes.byref(pointer), ctypes.byref(size), message, _MESSAGE)
     _raise(status, message)
     try:
+        if message.value:
+            warnings.warn(message.value.decode("utf-8", "replace"), UnroundWarning, stacklevel=2)
         return ctypes.string_at(pointer, int(size.value))
     finally:
         library.unround_bytes_free(pointer, size)
