@@ -27,7 +27,7 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++20", "-I", str(INCLUDE), "-I", str(SOURCES)]
 CUDA_FLAGS = [*ARCH, "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-O3"]
-HOST_FLAGS = ["-x", "c++", "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall"]
+HOST_FLAGS = [*ARCH, "-x", "c++", "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall"]
 
 
 def _stale(target: Path, sources: list[Path]) -> bool:
