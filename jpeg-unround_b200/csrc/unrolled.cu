@@ -27,6 +27,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -291,7 +292,7 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
                                                            const __grid_constant__ CUtensorMap bar_map, Problem q,
                                                            Planes b, float* xt_bar, double* grads) {
   extern __shared__ __align__(128) float shared[];
-  __shared__ __align__(8) std::uint64_t loaded;
+  __shared__ __align__(8) std::uint64_t loaded[2];  // [0] s_{k-1} and x~_k, [1] the adjoint
   float* const S = shared;                       // [field][row][column], row i0 - 2 + r, column j0 - 4 + c
   float* const A = S + kStateFloats;             // [field][row][column], row i0 - 1 + r, column j0 - 4 + c
   float* const T = A + kBarFloats;               // (1) w~, then (3) the adjoint of w~
@@ -302,25 +303,35 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
   const float rho = q.rho, rest = 1.0f - q.rho, tau = q.tau[z], sigma = q.sigma[z];
   const float alpha0 = q.alpha0[z], alpha1 = q.alpha1[z];
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(shared_address(&loaded)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(shared_address(&loaded[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(shared_address(&loaded[1])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  // Two copies on two barriers: (1) needs only the first, which lands while the second is
+  // still on its way.
   if (tid == 0) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(shared_address(&loaded)),
-                 "r"(static_cast<unsigned>((kStateFloats + kBarFloats) * sizeof(float)))
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(shared_address(&loaded[0])),
+                 "r"(static_cast<unsigned>(kStateFloats * sizeof(float)))
                  : "memory");
-    load_fields(S, &state_map, &loaded, j0 - 4, i0 - 2, z);
-    load_fields(A, &bar_map, &loaded, j0 - 4, i0 - 1, z);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(shared_address(&loaded[1])),
+                 "r"(static_cast<unsigned>(kBarFloats * sizeof(float)))
+                 : "memory");
+    load_fields(S, &state_map, &loaded[0], j0 - 4, i0 - 2, z);
+    load_fields(A, &bar_map, &loaded[1], j0 - 4, i0 - 1, z);
   }
-  const bool ready = wait_phase(&loaded, 0);
-  if (__syncthreads_or(!ready)) {
-    // The loads did not land: the gradients say so, and no copy may still be writing into the
-    // CTA's shared memory when it leaves.
+  // A copy that did not land: the gradients say so, and no copy may still be writing into the
+  // CTA's shared memory when it leaves (each barrier waited for once more, bounded).
+  auto give_up = [&]() {
     if (tid == 0) {
       atomicAdd(grads + 3 * q.images + z, static_cast<double>(__int_as_float(0x7fc00000)));
-      wait_phase(&loaded, 0);
+      wait_phase(&loaded[0], 0);
+      wait_phase(&loaded[1], 0);
     }
+  };
+  const bool ready = wait_phase(&loaded[0], 0);
+  if (__syncthreads_or(!ready)) {
+    give_up();
     return;
   }
   auto s_at = [&](int f, int i, int j) -> float { return S[(f * kStateRows + i - i0 + 2) * kAdjointSpan + j - j0 + 4]; };
@@ -329,163 +340,184 @@ __global__ void __launch_bounds__(256) dual_adjoint_kernel(const __grid_constant
   auto l_at = [&](int f, int i, int j) -> float& { return L[(f * kPointRows + i - i0 + 1) * kAdjointSpan + j - j0 + 1]; };
   auto tb_at = [&](int f, int i, int j) -> float& { return T[(f * kBackRows + i - i0 + 1) * kAdjointSpan + j - j0 + 1]; };
   enum { X = 0, P1, P2, W1, W2, R11, R22, R12, EXTRA };  // EXTRA: x~ in S, v^ in A
+  float g_alpha0 = 0.0f, g_alpha1 = 0.0f, g_sigma = 0.0f, g_tau = 0.0f;
+  // A tile whose halos lie inside the picture (rows i0 - 2 .. i0 + 17, columns j0 - 2 .. j0 + 34)
+  // passes every bounds test below: IN states that, and the tests fold away.
+  const bool interior = i0 >= 2 && j0 >= 2 && i0 + 17 < H && j0 + 34 < W;
+  bool failed = false;  // the same in every thread: set after a CTA-wide vote
+  auto tile = [&](auto kind) {
+    constexpr bool IN = decltype(kind)::value;
 
-  // (1) w~ = w + tau (p + div2 r), div2 r by forward differences.
-  for (int n = tid; n < kTildeRows * kAdjointSpan; n += 256) {
-    if (n % kAdjointSpan >= kTildeColumns) continue;
-    const int i = i0 - 2 + n / kAdjointSpan, j = j0 - 2 + n % kAdjointSpan;
-    const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
-    float d1 = j + 1 < W ? s_at(R11, i, j + 1) - r11 : 0.0f;
-    float d2 = j + 1 < W ? s_at(R12, i, j + 1) - r12 : 0.0f;
-    d1 = d1 + (i + 1 < H ? s_at(R12, i + 1, j) - r12 : 0.0f);
-    d2 = d2 + (i + 1 < H ? s_at(R22, i + 1, j) - r22 : 0.0f);
-    t_at(0, i, j) = s_at(W1, i, j) + tau * (s_at(P1, i, j) + d1);
-    t_at(1, i, j) = s_at(W2, i, j) + tau * (s_at(P2, i, j) + d2);
-  }
-  __syncthreads();
+    // (1) w~ = w + tau (p + div2 r), div2 r by forward differences, and w- = 2 w~ - w.
+    for (int n = tid; n < kTildeRows * kAdjointSpan; n += 256) {
+      if (n % kAdjointSpan >= kTildeColumns) continue;
+      const int i = i0 - 2 + n / kAdjointSpan, j = j0 - 2 + n % kAdjointSpan;
+      const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
+      float d1 = IN || j + 1 < W ? s_at(R11, i, j + 1) - r11 : 0.0f;
+      float d2 = IN || j + 1 < W ? s_at(R12, i, j + 1) - r12 : 0.0f;
+      d1 = d1 + (IN || i + 1 < H ? s_at(R12, i + 1, j) - r12 : 0.0f);
+      d2 = d2 + (IN || i + 1 < H ? s_at(R22, i + 1, j) - r22 : 0.0f);
+      // Kept as w- = 2 w~ - w, the only form (2) reads.
+      const float w1 = s_at(W1, i, j), w2 = s_at(W2, i, j);
+      const float tilde1 = w1 + tau * (s_at(P1, i, j) + d1), tilde2 = w2 + tau * (s_at(P2, i, j) + d2);
+      t_at(0, i, j) = 2.0f * tilde1 - w1;
+      t_at(1, i, j) = 2.0f * tilde2 - w2;
+    }
+    const bool adjoint_ready = wait_phase(&loaded[1], 0);
+    if (__syncthreads_or(!adjoint_ready)) {
+      failed = true;
+      return;
+    }
 
-  // (2) The points q = p + sigma (grad x- - w-) and s = r + sigma E w-, and the adjoints of q
-  // and s through the projections onto the balls (d/d alpha1, d/d alpha0 and d/d sigma beside).
-  float g_alpha0 = 0.0f, g_alpha1 = 0.0f, g_sigma = 0.0f;
-  for (int n = tid; n < kPointRows * kAdjointSpan; n += 256) {
-    if (n % kAdjointSpan >= kPointColumns) continue;
-    const int i = i0 - 1 + n / kAdjointSpan, j = j0 - 1 + n % kAdjointSpan;
-    const bool right = j + 1 < W, down = i + 1 < H;
-    const float bar = 2.0f * s_at(EXTRA, i, j) - s_at(X, i, j);
-    const float g1 = right ? (2.0f * s_at(EXTRA, i, j + 1) - s_at(X, i, j + 1)) - bar : 0.0f;
-    const float g2 = down ? (2.0f * s_at(EXTRA, i + 1, j) - s_at(X, i + 1, j)) - bar : 0.0f;
-    const float b1 = 2.0f * t_at(0, i, j) - s_at(W1, i, j);
-    const float b2 = 2.0f * t_at(1, i, j) - s_at(W2, i, j);
-    const float q1 = s_at(P1, i, j) + sigma * (g1 - b1);
-    const float q2 = s_at(P2, i, j) + sigma * (g2 - b2);
-    float l1 = 0.0f, l2 = 0.0f, u1 = 0.0f, u2 = 0.0f;
-    if (j > 0) {
-      l1 = 2.0f * t_at(0, i, j - 1) - s_at(W1, i, j - 1);
-      l2 = 2.0f * t_at(1, i, j - 1) - s_at(W2, i, j - 1);
+    // (2) The points q = p + sigma (grad x- - w-) and s = r + sigma E w-, and the adjoints of q
+    // and s through the projections onto the balls (d/d alpha1, d/d alpha0 and d/d sigma beside).
+    for (int n = tid; n < kPointRows * kAdjointSpan; n += 256) {
+      if (n % kAdjointSpan >= kPointColumns) continue;
+      const int i = i0 - 1 + n / kAdjointSpan, j = j0 - 1 + n % kAdjointSpan;
+      const bool right = IN || j + 1 < W, down = IN || i + 1 < H;
+      const float bar = 2.0f * s_at(EXTRA, i, j) - s_at(X, i, j);
+      const float g1 = right ? (2.0f * s_at(EXTRA, i, j + 1) - s_at(X, i, j + 1)) - bar : 0.0f;
+      const float g2 = down ? (2.0f * s_at(EXTRA, i + 1, j) - s_at(X, i + 1, j)) - bar : 0.0f;
+      const float b1 = t_at(0, i, j);
+      const float b2 = t_at(1, i, j);
+      const float q1 = s_at(P1, i, j) + sigma * (g1 - b1);
+      const float q2 = s_at(P2, i, j) + sigma * (g2 - b2);
+      float l1 = 0.0f, l2 = 0.0f, u1 = 0.0f, u2 = 0.0f;
+      if (IN || j > 0) {
+        l1 = t_at(0, i, j - 1);
+        l2 = t_at(1, i, j - 1);
+      }
+      if (IN || i > 0) {
+        u1 = t_at(0, i - 1, j);
+        u2 = t_at(1, i - 1, j);
+      }
+      const float own1x = right ? b1 : 0.0f, own2x = right ? b2 : 0.0f;
+      const float own1y = down ? b1 : 0.0f, own2y = down ? b2 : 0.0f;
+      const float e11 = own1x - l1, e22 = own2y - u2, e12 = 0.5f * ((own1y - u1) + (own2x - l2));
+      const float s11 = s_at(R11, i, j) + sigma * e11;
+      const float s22 = s_at(R22, i, j) + sigma * e22;
+      const float s12 = s_at(R12, i, j) + sigma * e12;
+      // The adjoint of p of s_k: that of the relaxation's p and of P_{k+1}'s v = x + tau div p,
+      // p^ += tau div^T v^ = -tau grad v^.
+      const float v = a_at(EXTRA, i, j);
+      float ap1 = a_at(P1, i, j), ap2 = a_at(P2, i, j);
+      if (right) ap1 += -tau * (a_at(EXTRA, i, j + 1) - v);
+      if (down) ap2 += -tau * (a_at(EXTRA, i + 1, j) - v);
+      const float pb1 = rho * ap1, pb2 = rho * ap2;
+      // The projections' branches compare squares: |q| > alpha where |q|^2 > alpha^2, but for
+      // ties within rounding, where the map is continuous; 1 / |q| by the approximate rsqrt.
+      float qb1 = pb1, qb2 = pb2, ga1 = 0.0f;
+      const float sq = q1 * q1 + q2 * q2;
+      if (sq > alpha1 * alpha1) {
+        const float dot = q1 * pb1 + q2 * pb2, inverse = rsqrtf(sq);
+        const float f = alpha1 * inverse, h = dot * inverse * inverse;
+        qb1 = f * (pb1 - q1 * h);
+        qb2 = f * (pb2 - q2 * h);
+        ga1 = dot * inverse;
+      }
+      const float rb11 = rho * a_at(R11, i, j), rb22 = rho * a_at(R22, i, j), rb12 = rho * a_at(R12, i, j);
+      float sb11 = rb11, sb22 = rb22, sb12 = rb12, ga0 = 0.0f;
+      const float ss = s11 * s11 + s22 * s22 + 2.0f * (s12 * s12);
+      if (ss > alpha0 * alpha0) {
+        const float dot = s11 * rb11 + s22 * rb22 + s12 * rb12, inverse = rsqrtf(ss);
+        const float f = alpha0 * inverse, h = dot * inverse * inverse;
+        sb11 = f * (rb11 - s11 * h);
+        sb22 = f * (rb22 - s22 * h);
+        sb12 = f * (rb12 - 2.0f * s12 * h);
+        ga0 = dot * inverse;
+      }
+      l_at(0, i, j) = qb1;
+      l_at(1, i, j) = qb2;
+      l_at(2, i, j) = sb11;
+      l_at(3, i, j) = sb22;
+      l_at(4, i, j) = sb12;
+      if (i >= i0 && i < i0 + kAdjointRows && j >= j0 && j < j0 + 32 && (IN || (i < H && j < W))) {
+        g_alpha0 += ga0;
+        g_alpha1 += ga1;
+        g_sigma += qb1 * (g1 - b1) + qb2 * (g2 - b2) + sb11 * e11 + sb22 * e22 + sb12 * e12;
+      }
     }
-    if (i > 0) {
-      u1 = 2.0f * t_at(0, i - 1, j) - s_at(W1, i - 1, j);
-      u2 = 2.0f * t_at(1, i - 1, j) - s_at(W2, i - 1, j);
-    }
-    const float own1x = right ? b1 : 0.0f, own2x = right ? b2 : 0.0f;
-    const float own1y = down ? b1 : 0.0f, own2y = down ? b2 : 0.0f;
-    const float e11 = own1x - l1, e22 = own2y - u2, e12 = 0.5f * ((own1y - u1) + (own2x - l2));
-    const float s11 = s_at(R11, i, j) + sigma * e11;
-    const float s22 = s_at(R22, i, j) + sigma * e22;
-    const float s12 = s_at(R12, i, j) + sigma * e12;
-    // The adjoint of p of s_k: that of the relaxation's p and of P_{k+1}'s v = x + tau div p,
-    // p^ += tau div^T v^ = -tau grad v^.
-    const float v = a_at(EXTRA, i, j);
-    float ap1 = a_at(P1, i, j), ap2 = a_at(P2, i, j);
-    if (right) ap1 += -tau * (a_at(EXTRA, i, j + 1) - v);
-    if (down) ap2 += -tau * (a_at(EXTRA, i + 1, j) - v);
-    const float pb1 = rho * ap1, pb2 = rho * ap2;
-    // The projections' branches compare squares: |q| > alpha where |q|^2 > alpha^2, but for
-    // ties within rounding, where the map is continuous; 1 / |q| by the approximate rsqrt.
-    float qb1 = pb1, qb2 = pb2, ga1 = 0.0f;
-    const float sq = q1 * q1 + q2 * q2;
-    if (sq > alpha1 * alpha1) {
-      const float dot = q1 * pb1 + q2 * pb2, inverse = rsqrtf(sq);
-      const float f = alpha1 * inverse, h = dot * inverse * inverse;
-      qb1 = f * (pb1 - q1 * h);
-      qb2 = f * (pb2 - q2 * h);
-      ga1 = dot * inverse;
-    }
-    const float rb11 = rho * a_at(R11, i, j), rb22 = rho * a_at(R22, i, j), rb12 = rho * a_at(R12, i, j);
-    float sb11 = rb11, sb22 = rb22, sb12 = rb12, ga0 = 0.0f;
-    const float ss = s11 * s11 + s22 * s22 + 2.0f * (s12 * s12);
-    if (ss > alpha0 * alpha0) {
-      const float dot = s11 * rb11 + s22 * rb22 + s12 * rb12, inverse = rsqrtf(ss);
-      const float f = alpha0 * inverse, h = dot * inverse * inverse;
-      sb11 = f * (rb11 - s11 * h);
-      sb22 = f * (rb22 - s22 * h);
-      sb12 = f * (rb12 - 2.0f * s12 * h);
-      ga0 = dot * inverse;
-    }
-    l_at(0, i, j) = qb1;
-    l_at(1, i, j) = qb2;
-    l_at(2, i, j) = sb11;
-    l_at(3, i, j) = sb22;
-    l_at(4, i, j) = sb12;
-    if (i >= i0 && i < i0 + kAdjointRows && j >= j0 && j < j0 + 32 && i < H && j < W) {
-      g_alpha0 += ga0;
-      g_alpha1 += ga1;
-      g_sigma += qb1 * (g1 - b1) + qb2 * (g2 - b2) + sb11 * e11 + sb22 * e22 + sb12 * e12;
-    }
-  }
-  __syncthreads();
+    __syncthreads();
 
-  // (3) The adjoint of w~: that of w- is -sigma q^ + sigma E^T s^ (E^T gathering s^ of the pixel
-  // and of its right and lower ones), and w~ = (w- + w) / 2 gives it twice, beside the
-  // relaxation's rho w'^. Over the tile and the column to its left and the row above it.
-  auto w_minus_bar = [&](int i, int j, float& wb1, float& wb2) {
-    wb1 = -sigma * l_at(0, i, j);
-    wb2 = -sigma * l_at(1, i, j);
-    float e1 = 0.0f, e2 = 0.0f;
-    if (j + 1 < W) {
-      e1 += l_at(2, i, j) - l_at(2, i, j + 1);
-      e2 += 0.5f * (l_at(4, i, j) - l_at(4, i, j + 1));
+    // (3) The adjoint of w~: that of w- is -sigma q^ + sigma E^T s^ (E^T gathering s^ of the pixel
+    // and of its right and lower ones), and w~ = (w- + w) / 2 gives it twice, beside the
+    // relaxation's rho w'^. Over the tile and the column to its left and the row above it.
+    auto w_minus_bar = [&](int i, int j, float& wb1, float& wb2) {
+      wb1 = -sigma * l_at(0, i, j);
+      wb2 = -sigma * l_at(1, i, j);
+      float e1 = 0.0f, e2 = 0.0f;
+      if (IN || j + 1 < W) {
+        e1 += l_at(2, i, j) - l_at(2, i, j + 1);
+        e2 += 0.5f * (l_at(4, i, j) - l_at(4, i, j + 1));
+      }
+      if (IN || i + 1 < H) {
+        e2 += l_at(3, i, j) - l_at(3, i + 1, j);
+        e1 += 0.5f * (l_at(4, i, j) - l_at(4, i + 1, j));
+      }
+      wb1 += sigma * e1;
+      wb2 += sigma * e2;
+    };
+    for (int n = tid; n < kBackRows * kAdjointSpan; n += 256) {
+      if (n % kAdjointSpan >= kBackColumns) continue;
+      const int i = i0 - 1 + n / kAdjointSpan, j = j0 - 1 + n % kAdjointSpan;
+      float wb1, wb2;
+      w_minus_bar(i, j, wb1, wb2);
+      tb_at(0, i, j) = rho * a_at(W1, i, j) + 2.0f * wb1;
+      tb_at(1, i, j) = rho * a_at(W2, i, j) + 2.0f * wb2;
     }
-    if (i + 1 < H) {
-      e2 += l_at(3, i, j) - l_at(3, i + 1, j);
-      e1 += 0.5f * (l_at(4, i, j) - l_at(4, i + 1, j));
+    __syncthreads();
+
+    // (4) The tile's adjoints of s_{k-1} and of x~_k.
+    for (int n = tid; n < kAdjointRows * 32; n += 256) {
+      const int i = i0 + n / 32, j = j0 + n % 32;
+      if (!IN && (i >= H || j >= W)) continue;
+      const std::size_t k = at(q, z, i, j);
+      const bool right = IN || j + 1 < W, down = IN || i + 1 < H;
+      const float tb1 = tb_at(0, i, j), tb2 = tb_at(1, i, j);
+      const float v = a_at(EXTRA, i, j);
+      float ap1 = a_at(P1, i, j), ap2 = a_at(P2, i, j);
+      if (right) ap1 += -tau * (a_at(EXTRA, i, j + 1) - v);
+      if (down) ap2 += -tau * (a_at(EXTRA, i + 1, j) - v);
+      // w^ = (1 - rho) w'^ - w-^ + w~^, and w~^ = rho w'^ + 2 w-^ gives w-^ from w~^.
+      b.w1[k] = fmaf(rest + 0.5f * rho, a_at(W1, i, j), 0.5f * tb1);
+      b.w2[k] = fmaf(rest + 0.5f * rho, a_at(W2, i, j), 0.5f * tb2);
+      b.p1[k] = rest * ap1 + l_at(0, i, j) + tau * tb1;
+      b.p2[k] = rest * ap2 + l_at(1, i, j) + tau * tb2;
+      // r^: the relaxation's, s^, and div2^T of d^ = tau w~^ (w~^ of the pixel and of its left
+      // and upper ones).
+      const float l1 = IN || j > 0 ? tb_at(0, i, j - 1) : 0.0f, l2 = IN || j > 0 ? tb_at(1, i, j - 1) : 0.0f;
+      const float u1 = IN || i > 0 ? tb_at(0, i - 1, j) : 0.0f, u2 = IN || i > 0 ? tb_at(1, i - 1, j) : 0.0f;
+      const float db1 = tau * tb1, db2 = tau * tb2;
+      const float div11 = tau * l1 - (right ? db1 : 0.0f);
+      const float div12 = tau * u1 - (down ? db1 : 0.0f) + tau * l2 - (right ? db2 : 0.0f);
+      const float div22 = tau * u2 - (down ? db2 : 0.0f);
+      b.r11[k] = rest * a_at(R11, i, j) + l_at(2, i, j) + div11;
+      b.r22[k] = rest * a_at(R22, i, j) + l_at(3, i, j) + div22;
+      b.r12[k] = rest * a_at(R12, i, j) + l_at(4, i, j) + div12;
+      // d/dtau of w~ = p + div2 r.
+      const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
+      float d1 = right ? s_at(R11, i, j + 1) - r11 : 0.0f;
+      float d2 = right ? s_at(R12, i, j + 1) - r12 : 0.0f;
+      d1 = d1 + (down ? s_at(R12, i + 1, j) - r12 : 0.0f);
+      d2 = d2 + (down ? s_at(R22, i + 1, j) - r22 : 0.0f);
+      g_tau += tb1 * (s_at(P1, i, j) + d1) + tb2 * (s_at(P2, i, j) + d2);
+      // The adjoint of x- : grad^T (sigma q^) = -div (sigma q^).
+      const float div = (right ? l_at(0, i, j) : 0.0f) - (IN || j > 0 ? l_at(0, i, j - 1) : 0.0f) +
+                        (down ? l_at(1, i, j) : 0.0f) - (IN || i > 0 ? l_at(1, i - 1, j) : 0.0f);
+      const float xbb = -sigma * div;
+      const float ax = a_at(X, i, j) + v;
+      xt_bar[k] = rho * ax + 2.0f * xbb;
+      b.x[k] = rest * ax - xbb;
     }
-    wb1 += sigma * e1;
-    wb2 += sigma * e2;
   };
-  for (int n = tid; n < kBackRows * kAdjointSpan; n += 256) {
-    if (n % kAdjointSpan >= kBackColumns) continue;
-    const int i = i0 - 1 + n / kAdjointSpan, j = j0 - 1 + n % kAdjointSpan;
-    float wb1, wb2;
-    w_minus_bar(i, j, wb1, wb2);
-    tb_at(0, i, j) = rho * a_at(W1, i, j) + 2.0f * wb1;
-    tb_at(1, i, j) = rho * a_at(W2, i, j) + 2.0f * wb2;
+  if (interior) {
+    tile(std::true_type{});
+  } else {
+    tile(std::false_type{});
   }
-  __syncthreads();
-
-  // (4) The tile's adjoints of s_{k-1} and of x~_k.
-  float g_tau = 0.0f;
-  for (int n = tid; n < kAdjointRows * 32; n += 256) {
-    const int i = i0 + n / 32, j = j0 + n % 32;
-    if (i >= H || j >= W) continue;
-    const std::size_t k = at(q, z, i, j);
-    const bool right = j + 1 < W, down = i + 1 < H;
-    const float tb1 = tb_at(0, i, j), tb2 = tb_at(1, i, j);
-    float wb1, wb2;
-    w_minus_bar(i, j, wb1, wb2);
-    const float v = a_at(EXTRA, i, j);
-    float ap1 = a_at(P1, i, j), ap2 = a_at(P2, i, j);
-    if (right) ap1 += -tau * (a_at(EXTRA, i, j + 1) - v);
-    if (down) ap2 += -tau * (a_at(EXTRA, i + 1, j) - v);
-    b.w1[k] = rest * a_at(W1, i, j) - wb1 + tb1;
-    b.w2[k] = rest * a_at(W2, i, j) - wb2 + tb2;
-    b.p1[k] = rest * ap1 + l_at(0, i, j) + tau * tb1;
-    b.p2[k] = rest * ap2 + l_at(1, i, j) + tau * tb2;
-    // r^: the relaxation's, s^, and div2^T of d^ = tau w~^ (w~^ of the pixel and of its left
-    // and upper ones).
-    const float l1 = j > 0 ? tb_at(0, i, j - 1) : 0.0f, l2 = j > 0 ? tb_at(1, i, j - 1) : 0.0f;
-    const float u1 = i > 0 ? tb_at(0, i - 1, j) : 0.0f, u2 = i > 0 ? tb_at(1, i - 1, j) : 0.0f;
-    const float db1 = tau * tb1, db2 = tau * tb2;
-    const float div11 = tau * l1 - (right ? db1 : 0.0f);
-    const float div12 = tau * u1 - (down ? db1 : 0.0f) + tau * l2 - (right ? db2 : 0.0f);
-    const float div22 = tau * u2 - (down ? db2 : 0.0f);
-    b.r11[k] = rest * a_at(R11, i, j) + l_at(2, i, j) + div11;
-    b.r22[k] = rest * a_at(R22, i, j) + l_at(3, i, j) + div22;
-    b.r12[k] = rest * a_at(R12, i, j) + l_at(4, i, j) + div12;
-    // d/dtau of w~ = p + div2 r.
-    const float r11 = s_at(R11, i, j), r22 = s_at(R22, i, j), r12 = s_at(R12, i, j);
-    float d1 = right ? s_at(R11, i, j + 1) - r11 : 0.0f;
-    float d2 = right ? s_at(R12, i, j + 1) - r12 : 0.0f;
-    d1 = d1 + (down ? s_at(R12, i + 1, j) - r12 : 0.0f);
-    d2 = d2 + (down ? s_at(R22, i + 1, j) - r22 : 0.0f);
-    g_tau += tb1 * (s_at(P1, i, j) + d1) + tb2 * (s_at(P2, i, j) + d2);
-    // The adjoint of x- : grad^T (sigma q^) = -div (sigma q^).
-    const float div = (right ? l_at(0, i, j) : 0.0f) - (j > 0 ? l_at(0, i, j - 1) : 0.0f) +
-                      (down ? l_at(1, i, j) : 0.0f) - (i > 0 ? l_at(1, i - 1, j) : 0.0f);
-    const float xbb = -sigma * div;
-    const float ax = a_at(X, i, j) + v;
-    xt_bar[k] = rho * ax + 2.0f * xbb;
-    b.x[k] = rest * ax - xbb;
+  if (failed) {
+    give_up();
+    return;
   }
   add_sum(g_alpha0, grads + 0 * q.images + z);
   add_sum(g_alpha1, grads + 1 * q.images + z);

@@ -59,6 +59,19 @@ def test_forward_and_gradients_against_the_reference():
         assert np.abs(g - r).max() <= 2e-3 * scale + 1e-6, f"parameter {k}: {g} vs {r}"
 
 
+def test_interior_tiles_against_the_reference():
+    """Pictures of 96 x 160: most tiles of the dual step's adjoint have their halos inside the
+    picture (the kernel's path without bounds tests), beside the edge tiles."""
+    problem, clean, base = _case(iterations=12, every=5, rows=96, columns=160)
+    out, _, grads = _device_loss_and_grads(problem, clean, base)
+    ref_out, ref_grads = _reference_grads(problem, clean, base)
+    got = out.double().cpu().numpy()
+    assert np.linalg.norm(got - ref_out) / np.linalg.norm(ref_out) <= 1e-5
+    for k, (g, r) in enumerate(zip(grads, ref_grads)):
+        scale = np.abs(r).max()
+        assert np.abs(g - r).max() <= 2e-3 * scale + 1e-6, f"parameter {k}: {g} vs {r}"
+
+
 def test_gradients_against_finite_differences():
     from unround.unrolled import unrolled_tgv
 
