@@ -2,7 +2,7 @@
 
 nvcc compiles the CUDA kernels and the host driver (csrc/*.cu) and g++ the host model,
 settings and C interface (csrc/*.cpp), all into unround/_native/libunround_capi.so, where
-unround._loading finds it (the reference's Python package looks in the same place). Objects
+unround.native loads it (unless UNROUND_LIBRARY names another). Objects
 go to _build/. The library links the CUDA runtime statically, so that it loads wherever the
 driver is, and needs no torch.
 

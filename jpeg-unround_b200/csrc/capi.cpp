@@ -30,10 +30,6 @@
 #include "unround.h"
 #include "unround_b200.h"
 
-struct unround_settings {
-  urb::Settings settings;
-};
-
 struct unround_result {
   urb::Frame frame;
   urb::Outcome outcome;  // the canvas, the planes and the picture (made on the device)

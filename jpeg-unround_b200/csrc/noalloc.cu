@@ -12,10 +12,11 @@
 // pool on every call; this entry point takes none.
 //
 // The first call on a device also looks up the array's device address there (cudaGetSymbolAddress,
-// once per device, kept for later calls), which loads this library's device code on that device if
-// it is not loaded yet. Every call uses the one array, which keeps what the last call left there:
-// calls whose work overlaps on the same GPU (two streams, two host threads at once) race on it, so
-// the caller serializes them.
+// with that device current; kept for later calls once it succeeds), which loads this library's
+// device code on that device if it is not loaded yet. Every call uses the one array, which keeps
+// what the last call left there: calls whose work overlaps on the same GPU (two streams, two host
+// threads at once) race on it, so the caller serializes them. Every call waits for its own work
+// on the stream before it returns, whether it succeeds or fails.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -42,10 +43,6 @@ constexpr int kDevices = 64;
 // The scratch of every call, on every device that uses this entry point.
 static __device__ __align__(256) unsigned char scratch[kScratchBytes];
 
-struct unround_settings {
-  urb::Settings settings;
-};
-
 namespace {
 
 void tell(char* buffer, std::size_t size, const std::string& text) {
@@ -56,26 +53,34 @@ void tell(char* buffer, std::size_t size, const std::string& text) {
   buffer[end] = 0;
 }
 
-// The device address of the scratch array on the current device, looked up once per device.
+// The device address of the scratch array on the current device, looked up on the first call
+// on that device that finds it and kept for later calls. A lookup that fails is not kept: the
+// next call tries again.
 bool scratch_of(unsigned char*& address, std::string& why) {
-  static std::once_flag once[kDevices];
+  static std::mutex guard;
   static unsigned char* found[kDevices] = {};
-  static cudaError_t errors[kDevices] = {};
   int device = 0;
   const cudaError_t error = cudaGetDevice(&device);
-  if (error != cudaSuccess || device < 0 || device >= kDevices) {
-    why = std::string("no CUDA device for the decoder of the centres: ") + cudaGetErrorString(error);
+  if (error != cudaSuccess) {
+    why = std::string("no CUDA device for the decoder of the centres: ") + cudaGetErrorName(error) + ": " +
+          cudaGetErrorString(error);
     return false;
   }
-  std::call_once(once[device], [device] {
-    void* p = nullptr;
-    errors[device] = cudaGetSymbolAddress(&p, scratch);
-    found[device] = static_cast<unsigned char*>(p);
-  });
-  if (errors[device] != cudaSuccess || found[device] == nullptr) {
-    why = std::string("the device address of the decoder's scratch: ") + cudaGetErrorName(errors[device]) + ": " +
-          cudaGetErrorString(errors[device]);
+  if (device < 0 || device >= kDevices) {
+    why = "the decoder of the centres serves devices 0 to " + std::to_string(kDevices - 1) + ", not device " +
+          std::to_string(device);
     return false;
+  }
+  std::lock_guard<std::mutex> lock(guard);
+  if (found[device] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t looked = cudaGetSymbolAddress(&p, scratch);
+    if (looked != cudaSuccess || p == nullptr) {
+      why = std::string("the device address of the decoder's scratch: ") + cudaGetErrorName(looked) + ": " +
+            cudaGetErrorString(looked);
+      return false;
+    }
+    found[device] = static_cast<unsigned char*>(p);
   }
   address = found[device];
   return true;
@@ -234,8 +239,11 @@ extern "C" unround_status unround_b200_decode_centres_noalloc(const unround_inpu
       if (error == cudaSuccess) error = urb::launch_canvas(cp, on);
       coefficient_offset += comp.coefficient_count();
     }
-    // The host copies above read `frame` and `constants`, which end with this call.
-    if (error == cudaSuccess) error = cudaStreamSynchronize(on);
+    // The host copies above read `frame` and `constants`, which end with this call; and on a
+    // failure part of the way, nothing queued for the components before it may still be writing
+    // the caller's buffers or the scratch when the call returns.
+    const cudaError_t drained = cudaStreamSynchronize(on);
+    if (error == cudaSuccess) error = drained;
     if (error != cudaSuccess) {
       tell(message, message_size, std::string("the device failed in the decoder of the centres: ") +
                                       cudaGetErrorName(error) + ": " + cudaGetErrorString(error));

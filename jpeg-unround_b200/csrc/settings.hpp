@@ -100,3 +100,9 @@ std::vector<std::string> options_of(const Settings& settings);
 std::string shortest(double value);
 
 }  // namespace urb
+
+// The opaque settings handle of the C interface (unround.h's unround_settings), shared by every
+// source that takes one.
+struct unround_settings {
+  urb::Settings settings;
+};

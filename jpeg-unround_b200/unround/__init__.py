@@ -3,10 +3,12 @@
 The drop-in for the reference package unround (python/src/unround of JPEG-Unround): the same
 modules and names -- settings, native (solve, options, Decoded, UnroundError ...), jpegio
 (Image, Component) -- over the same C interface (include/unround.h), whose library here runs
-the TV/TGV primal-dual solve as CUDA kernels on the GPU. Reading JPEG files (libjpeg-turbo)
-is not part of this build: give the levels and tables as arrays (jpegio.image_of) to
-native.solve. synthetic makes seeded test pictures and their levels; batch solves many
-pictures at once; unrolled differentiates an unrolled TGV solve with torch.
+the TV/TGV primal-dual solve as CUDA kernels on the GPU. Files are read on the host by this
+build's own JPEG and PNG readers (jpegio.read, native.decode), whose coefficients and levels
+go to the same solve; levels and tables given as arrays (jpegio.image_of) go to native.solve.
+synthetic makes seeded test pictures and their levels; native.solve_batch solves many pictures
+at once; unrolled differentiates an unrolled TGV solve with torch; strips solves one picture in
+row strips across ranks.
 """
 
 from unround import jpegio, native, settings

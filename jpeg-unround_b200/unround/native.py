@@ -9,9 +9,15 @@ shortest decimal that reads back as the same double (repr); the results come bac
 arrays, copied, and the library's memory is freed before a function returns.
 
 solve() is the path: levels and tables in, the TV/TGV primal-dual solve on the GPU, the
-binary64 result out. decode() and project(), which need libjpeg-turbo to read a file, raise
-UnroundError with the library's UNSUPPORTED status. solve_from() and measure() are this
-build's extensions (include/unround_b200.h).
+binary64 result out. decode() reads a JPEG file's coefficients (or a PNG file's levels) on the
+host with this build's own readers and solves them the same way; project() measures a picture
+against a file's intervals on the host. solve_from(), measure(), solve_batch() and the other
+functions without a counterpart in the reference are this build's extensions
+(include/unround_b200.h).
+
+The library is the file that the environment variable UNROUND_LIBRARY names, where it is set,
+as the reference's package looks it up; otherwise libunround_capi.so in this package's _native
+folder, where jpeg-unround_b200/build.py writes it.
 """
 
 from __future__ import annotations
@@ -29,7 +35,7 @@ from typing import Final
 import numpy as np
 import numpy.typing as npt
 
-from unround import _loading, jpegio
+from unround import jpegio
 from unround.settings import TGV, TV, DataTerm, PdhgOptions, Settings, SubgradientOptions
 
 __all__ = [
@@ -243,7 +249,12 @@ def _bind(library: ctypes.CDLL) -> None:
 
 def library_path() -> str:
     """The path of the library this module loads."""
-    path = _loading.configured("UNROUND_LIBRARY") or _loading.bundled(_loading.RUST)
+    named = os.environ.get("UNROUND_LIBRARY")
+    if named:
+        path: Path | None = Path(named)
+    else:
+        built = Path(__file__).parent / "_native" / "libunround_capi.so"
+        path = built if built.is_file() else None
     if path is None or not path.is_file():
         where = f"UNROUND_LIBRARY names {path}, where there is no file" if path else "the package holds no library"
         raise LibraryNotFoundError(f"{where}: build it with python jpeg-unround_b200/build.py")

@@ -3,11 +3,13 @@ dither (64 x 64 ranks, row by row), made by running the reference's own generato
 (scripts/blue_noise.py of JPEG-Unround, its matrix()) where the reference checkout lies. The
 tests compare the library's own void-and-cluster ranks with it, and read only the .npy.
 
-Run: python tests/golden/make_blue_noise.py [path to the reference checkout]
+Run: python tests/golden/make_blue_noise.py <path to the reference checkout>
+(or with the environment variable UNROUND_REFERENCE naming it)
 """
 
 from __future__ import annotations
 
+import os
 import sys
 import types
 from pathlib import Path
@@ -18,7 +20,10 @@ HERE = Path(__file__).resolve().parent
 
 
 def main() -> None:
-    reference = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    named = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("UNROUND_REFERENCE")
+    if not named:
+        raise SystemExit("name the reference checkout: make_blue_noise.py <path>, or UNROUND_REFERENCE=<path>")
+    reference = Path(named)
     # Its annotations name its own class before the class is made (evaluated lazily by newer
     # Pythons): run its source with postponed annotations.
     path = reference / "scripts" / "blue_noise.py"

@@ -10,18 +10,19 @@ mmse, tv and tgv; the subgradient case is a comparison method outside it), the a
 tests compare with, in one compressed .npz per case. The tests read only the .npz files,
 so they run where the reference is not present.
 
-Run: python tests/golden/make_golden.py [path to the reference checkout]
+Run: python tests/golden/make_golden.py <path to the reference checkout>
+(or with the environment variable UNROUND_REFERENCE naming it)
 """
 
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-DEFAULT_REFERENCE = Path("/root/reference")
 
 
 def _floats(items: list[str]) -> np.ndarray:
@@ -112,7 +113,10 @@ def parse_case(path: Path) -> dict[str, np.ndarray]:
 
 
 def main() -> None:
-    reference = Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_REFERENCE
+    named = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("UNROUND_REFERENCE")
+    if not named:
+        raise SystemExit("name the reference checkout: make_golden.py <path>, or UNROUND_REFERENCE=<path>")
+    reference = Path(named)
     cases = sorted((reference / "conformance" / "cases").glob("*.txt"))
     written = 0
     for path in cases:

@@ -1,7 +1,9 @@
 """unround_b200_decode_centres_noalloc, the decoder of the centres that allocates no device
 memory: its output in caller-owned device buffers against unround_solve's with --method=mmse on
-the same input, call after call (the scratch array keeps what the last call left there), and its
-refusals. The file is named to be collected last, after the tests that load the library."""
+the same input, call after call (the scratch array keeps what the last call left there); that a
+warm call leaves the device's free memory, its stream-ordered pool and torch's allocator exactly
+as they were; and its refusals. The file is named to be collected last, after the tests that load
+the library."""
 
 import ctypes
 
@@ -89,6 +91,53 @@ def test_against_unround_solve_call_after_call():
         if name in outputs:
             np.testing.assert_array_equal(got_canvas, outputs[name])
         outputs[name] = got_canvas
+
+
+def _device_memory():
+    """(free bytes of the device, the default pool's reserved and used bytes, torch's reserved and
+    allocated bytes): what a device allocation by anyone in this process would change."""
+    import torch
+    from cuda.bindings import driver
+
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info()
+    (error,) = driver.cuInit(0)
+    assert error == driver.CUresult.CUDA_SUCCESS
+    error, device = driver.cuDeviceGet(torch.cuda.current_device())
+    assert error == driver.CUresult.CUDA_SUCCESS
+    error, pool = driver.cuDeviceGetDefaultMemPool(device)
+    assert error == driver.CUresult.CUDA_SUCCESS
+    attributes = driver.CUmemPool_attribute
+    pooled = []
+    for attribute in (attributes.CU_MEMPOOL_ATTR_RESERVED_MEM_CURRENT, attributes.CU_MEMPOOL_ATTR_USED_MEM_CURRENT):
+        error, value = driver.cuMemPoolGetAttribute(pool, attribute)
+        assert error == driver.CUresult.CUDA_SUCCESS
+        pooled.append(int(value))
+    return (int(free), *pooled, torch.cuda.memory_reserved(), torch.cuda.memory_allocated())
+
+
+@pytest.mark.gpu
+def test_allocates_nothing():
+    import torch
+
+    from unround import synthetic
+
+    image = synthetic.colour(517, 389, quality=55, seed=21).image
+    status, message, (channels, rows, columns, count) = _call(image)
+    assert status == 0, message
+    canvas = torch.empty((channels, rows, columns), dtype=torch.float64, device="cuda")
+    coefficients = torch.empty(count, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    # The first call may load the library's device code (and with it the scratch array).
+    status, message, _ = _call(image, canvas, coefficients, stream=stream)
+    assert status == 0, message
+    first = canvas.clone()
+    before = _device_memory()
+    for _ in range(2):
+        status, message, _ = _call(image, canvas, coefficients, stream=stream)
+        assert status == 0, message
+        assert _device_memory() == before
+    assert torch.equal(canvas, first)
 
 
 @pytest.mark.gpu
