@@ -187,9 +187,10 @@ unround_status unround_b200_model(const unround_input* input, const unround_sett
  * Its device scratch is one fixed array of 64 MiB on each device, reserved when this library's
  * device code is loaded there: an input whose levels, flat flags and constants need more (about
  * 33 million coefficients) is refused with UNROUND_ERROR_ARGUMENT and left to unround_solve. The
- * first call on a device looks up the array's address there (cudaGetSymbolAddress), once. Calls
- * share the array: calls that run at the same time on one device race on it, and the caller
- * serializes them. */
+ * first call on a device looks up the array's address there (cudaGetSymbolAddress, with that
+ * device current), and later calls keep it once a lookup has succeeded. Calls share the array:
+ * calls that run at the same time on one device race on it, and the caller serializes them.
+ * Every call waits for its own work on `stream` before it returns, on failure too. */
 unround_status unround_b200_decode_centres_noalloc(const unround_input* input, const unround_settings* settings,
                                                    double* canvas, uint64_t canvas_capacity, double* coefficients,
                                                    uint64_t coefficient_capacity, uint64_t* sizes, void* stream,
@@ -218,6 +219,16 @@ uint64_t unround_b200_strip_state(const unround_b200_strip* strip, float** plane
 unround_status unround_b200_strip_finish(unround_b200_strip* strip, unround_result** result, char* message,
                                          size_t message_size);
 void unround_b200_strip_free(unround_b200_strip* strip);
+
+/* The failure path of the bounded waits (no counterpart in the reference, whose solver has no
+ * device): every wait of a kernel on an mbarrier is bounded, and one that runs out sets an error
+ * word that the solve reports as UNROUND_ERROR_INTERNAL ("a bounded wait of the sweep ran out")
+ * after draining the loads still in flight. This sets the tries that the dual sweep's compute
+ * warps give a chunk of their ring, for the solves of this process from now on: `tries` >= 0
+ * sets it, a negative value puts back the full limit (2^22). It returns the limit before. With
+ * 0, every sweep gives up at its first chunk although its loads complete as usual: a test of
+ * the failure path that neither faults nor hangs the device. */
+int64_t unround_b200_set_ring_wait_limit(int64_t tries);
 
 #ifdef __cplusplus
 }

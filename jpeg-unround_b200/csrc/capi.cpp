@@ -1805,3 +1805,5 @@ void unround_jpegio_bytes_free(unround_jpegio_bytes* bytes) {
 }
 
 }  // extern "C"
+
+extern "C" int64_t unround_b200_set_ring_wait_limit(int64_t tries) { return urb::set_ring_wait_limit(tries); }

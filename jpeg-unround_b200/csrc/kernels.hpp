@@ -104,7 +104,18 @@ struct DualParams {
   float radius0 = 2.0f;  // alpha0
   int* error = nullptr;  // set to 1 where a bounded wait of the sweep ran out
   int strip_rows = 256;  // rows a CTA of the sweep walks, a multiple of 8 (set by its launcher)
+  // Tries of the compute warps' wait for a chunk of the ring (the drain of the loads in flight
+  // before a CTA leaves always has the full limit): the full limit but where a test of the
+  // failure path shortens it (ring_wait_limit()).
+  long long ring_wait_limit = 1LL << 22;
 };
+
+// The tries the dual sweep's compute warps give a chunk of its ring, for every solve of this
+// process from now on: `tries` >= 0 sets it, and a negative value puts back the full limit.
+// Returns the limit before. A test of the failure path sets 0, so that the waits give up on
+// loads that complete as usual.
+long long set_ring_wait_limit(long long tries);
+long long ring_wait_limit();
 
 // The primal step of iteration n+1 for one channel: v = x + tau gamma div p and its proximal
 // map x~ (docs/math.md 4.4, 5); with keep, the coefficients zeta, v, and each CTA's sum of

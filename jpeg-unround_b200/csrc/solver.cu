@@ -524,6 +524,7 @@ struct Solver::Impl {
     dp.radius = static_cast<float>(tgv ? plan.alpha1 : plan.alpha);
     dp.radius0 = static_cast<float>(plan.alpha0);
     dp.error = error_word;
+    dp.ring_wait_limit = ring_wait_limit();
     return dp;
   }
 

@@ -168,8 +168,8 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
   bool failed = false;
   int stopped = chunks;
   for (int k = 0; k < chunks; ++k) {
-    const bool ready = barrier_wait(&bars[k % kSlots], (k / kSlots) & 1) &&
-                       barrier_wait(&bars[(k + 1) % kSlots], ((k + 1) / kSlots) & 1);
+    const bool ready = barrier_wait(&bars[k % kSlots], (k / kSlots) & 1, P.ring_wait_limit) &&
+                       barrier_wait(&bars[(k + 1) % kSlots], ((k + 1) / kSlots) & 1, P.ring_wait_limit);
     if (__syncthreads_or(!ready)) {
       failed = true;
       stopped = k;
@@ -736,5 +736,16 @@ int batch_tile_rows(const std::vector<Geometry>& pictures, int slots) {
   }
   return best;
 }
+
+namespace {
+constexpr long long kFullRingLimit = 1LL << 22;
+std::atomic<long long> ring_limit{kFullRingLimit};
+}  // namespace
+
+long long set_ring_wait_limit(long long tries) {
+  return ring_limit.exchange(tries < 0 ? kFullRingLimit : tries);
+}
+
+long long ring_wait_limit() { return ring_limit.load(); }
 
 }  // namespace urb

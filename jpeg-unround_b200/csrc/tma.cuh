@@ -39,9 +39,9 @@ __device__ __forceinline__ bool barrier_try(std::uint64_t* bar, unsigned parity)
   return done != 0;
 }
 
-// Waits for a phase of a barrier, at most kWaitLimit tries; false where it ran out.
-__device__ __forceinline__ bool barrier_wait(std::uint64_t* bar, unsigned parity) {
-  for (long long k = 0; k < kWaitLimit; ++k) {
+// Waits for a phase of a barrier, at most `limit` tries; false where it ran out.
+__device__ __forceinline__ bool barrier_wait(std::uint64_t* bar, unsigned parity, long long limit = kWaitLimit) {
+  for (long long k = 0; k < limit; ++k) {
     if (barrier_try(bar, parity)) return true;
   }
   return false;

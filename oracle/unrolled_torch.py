@@ -99,25 +99,34 @@ class Reference:
         return self._canvas(back)
 
     def run(self, alpha0: torch.Tensor, alpha1: torch.Tensor, tau: torch.Tensor, sigma: torch.Tensor,
-            iterations: int) -> torch.Tensor:
-        """x~_N of the unrolled solve: P_1, D_1, ..., D_{N-1}, P_N from s_0 = (x0, 0, grad x0, 0)."""
+            iterations: int, checkpoint_every: int = 0) -> torch.Tensor:
+        """x~_N of the unrolled solve: P_1, D_1, ..., D_{N-1}, P_N from s_0 = (x0, 0, grad x0, 0).
+        checkpoint_every > 0 keeps autograd's tape of only one segment of that many iterations at
+        a time (torch.utils.checkpoint recomputes it in the backward pass): the same values and
+        gradients in a fraction of the memory, for pictures of 512 x 512 and more."""
         x = self.start.clone()
-        p1 = torch.zeros_like(x)
-        p2 = torch.zeros_like(x)
-        w1 = _forward_x(x)
-        w2 = _forward_y(x)
-        r11 = torch.zeros_like(x)
-        r22 = torch.zeros_like(x)
-        r12 = torch.zeros_like(x)
-        a0, a1 = alpha0[:, None, None], alpha1[:, None, None]
-        tt, ss = tau[:, None, None], sigma[:, None, None]
+        zero = torch.zeros_like(x)
+        state = (x, zero, zero.clone(), _forward_x(x), _forward_y(x), zero.clone(), zero.clone(), zero.clone())
+        params = (alpha0[:, None, None], alpha1[:, None, None], tau[:, None, None], sigma[:, None, None], tau)
+        done = 0
+        while done < iterations - 1:
+            count = iterations - 1 - done if checkpoint_every <= 0 else min(checkpoint_every, iterations - 1 - done)
+            if checkpoint_every > 0:
+                from torch.utils.checkpoint import checkpoint
+
+                state = checkpoint(self._segment, count, *params, *state, use_reentrant=False)
+            else:
+                state = self._segment(count, *params, *state)
+            done += count
+        x, p1, p2 = state[0], state[1], state[2]
+        return self.prox(x + params[2] * (_backward_y(p2) + _backward_x(p1)), tau)
+
+    def _segment(self, count: int, a0, a1, tt, ss, tau, x, p1, p2, w1, w2, r11, r22, r12):
+        """`count` iterations P_k, D_k from the state s_{k-1}: the state s_{k-1+count}."""
         rho = self.rho
-        xt = None
-        for k in range(1, iterations + 1):
+        for _ in range(count):
             v = x + tt * (_backward_y(p2) + _backward_x(p1))
             xt = self.prox(v, tau)
-            if k == iterations:
-                break
             bar = 2.0 * xt - x
             d1 = _forward_x(r11) + _forward_y(r12)
             d2 = _forward_x(r12) + _forward_y(r22)
@@ -140,4 +149,4 @@ class Reference:
             w1, w2 = rho * t1 + (1 - rho) * w1, rho * t2 + (1 - rho) * w2
             r11, r22, r12 = (rho * (s11 * fs) + (1 - rho) * r11, rho * (s22 * fs) + (1 - rho) * r22,
                              rho * (s12 * fs) + (1 - rho) * r12)
-        return xt
+        return x, p1, p2, w1, w2, r11, r22, r12

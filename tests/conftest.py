@@ -4,6 +4,8 @@ Tests marked gpu run on a B200 (`pytest -m gpu`); the others need no GPU (`-m "n
 The oracle (oracle/) is test infrastructure: the tests use it as the checker only.
 """
 
+import json
+import os
 import sys
 from pathlib import Path
 
@@ -20,6 +22,35 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 
 def pytest_configure(config: pytest.Config) -> None:
     config.addinivalue_line("markers", "gpu: needs a B200 (CUDA device)")
+
+
+# Parity figures of the GPU tests against the reference's solver: one dict per case, printed at
+# the end of the run and, where UNROUND_PARITY_REPORT names a file, written there as JSON.
+PARITY: list[dict] = []
+
+
+def report_parity(case: str, **figures) -> None:
+    PARITY.append({"case": case, **{k: (float(v) if hasattr(v, "__float__") else v) for k, v in figures.items()}})
+
+
+def canvas_figures(ours: np.ndarray, theirs: np.ndarray) -> dict[str, float]:
+    """Relative L2 and max |difference| of two canvases (0..255 scale)."""
+    difference = ours - theirs
+    return {"rel_l2": float(np.linalg.norm(difference) / np.linalg.norm(theirs)),
+            "max_abs": float(np.max(np.abs(difference)))}
+
+
+def pytest_terminal_summary(terminalreporter, exitstatus, config) -> None:
+    if not PARITY:
+        return
+    terminalreporter.section("parity against the reference's solver")
+    for entry in PARITY:
+        terminalreporter.write_line(
+            " ".join(f"{k}={v:.3g}" if isinstance(v, float) else f"{k}={v}" for k, v in entry.items()))
+    target = os.environ.get("UNROUND_PARITY_REPORT")
+    if target:
+        Path(target).parent.mkdir(parents=True, exist_ok=True)
+        Path(target).write_text(json.dumps(PARITY, indent=1))
 
 
 def golden_cases() -> list[Path]:

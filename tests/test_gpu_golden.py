@@ -2,13 +2,15 @@
 interface. The iterations compute in binary32, the cases in binary64 within tolerances of
 binary64 rounding; the bar here is the parity bar: relative L2 <= 1e-4 and max |difference|
 <= 2e-3 (0..255 scale) of the canvas, the same records and stop, every coefficient within its
-interval in binary64, and the decoder of the centres (binary64 end to end) within the case's
-own tolerance."""
+interval in binary64, every record (primal and dual values, TGV's scaling and partial gap)
+within 1e-4 of the case's relative to the record's scale, and the decoder of the centres
+(binary64 end to end) within the case's own tolerance."""
 
 import numpy as np
 import pytest
 
-from conftest import case_image, case_options, case_start, golden_cases
+from conftest import canvas_figures, case_image, case_options, case_start, golden_cases, report_parity
+from test_gpu_oracle import RECORDS, record_differences
 
 pytestmark = pytest.mark.gpu
 
@@ -42,13 +44,15 @@ def test_golden_case(path):
         assert np.linalg.norm(difference) <= float(case["tolerance_canvas"])
         assert decoded.result is None
         return
-    rel = np.linalg.norm(difference) / np.linalg.norm(expected)
-    assert rel <= REL_L2, rel
-    assert np.max(np.abs(difference)) <= MAX_ABS
-    # Records at the same iterations, primal values close, the same stop.
+    figures = canvas_figures(decoded.canvas, expected)
+    # Records at the same iterations: primal and dual values, TGV's scaling and partial gap.
     records = case["records"]
     history = decoded.result.history
-    assert list(history.iterations) == [int(r) for r in records[:, 0]]
+    worst = record_differences(history, [int(r) for r in records[:, 0]], records)
+    report_parity(f"golden {path.stem}", **figures, **{f"record_{k}": v for k, v in worst.items()})
+    assert figures["rel_l2"] <= REL_L2, figures
+    assert figures["max_abs"] <= MAX_ABS, figures
+    assert max(worst.values()) <= RECORDS, worst
     np.testing.assert_allclose(history.primal, records[:, 1], rtol=2e-5)
     assert decoded.result.iterations == int(case["stop_iterations"])
     assert decoded.result.stop.name.lower() == str(case["stop_reason"])
