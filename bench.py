@@ -11,6 +11,13 @@ A step is one full solve of it (500 iterations).
   e2e    the same metric through the drop-in call (unround.native.solve -> unround_solve) with
          host arrays: levels copied in, the binary64 result copied out, every step.
 
+Beside them, outside the timed regions: cpu_baseline (the reference's C++ solver on the host
+cores, run first: best of three bounded samples with every thread and with one, and one whole
+solve of the workload), parity (the device's result against that whole solve), records (the
+cost of a record every 10 iterations, the reference's default), mix (the batched 64-picture mix
+against the same pictures one at a time, with the ceiling the image-at-a-time path's share of
+the HBM peak leaves).
+
 With --gpus N (under torchrun) each rank solves its own picture (images are independent units,
 no data-path collective): weak scaling, value = all ranks' pixel-iterations / max time.
 --impl reference times the reference's own C++ solver (oracle/_ref) on the host cores instead.
@@ -130,6 +137,26 @@ def _workload(seed: int):
     return synthetic.colour(HEIGHT, WIDTH, quality=75, seed=seed, noise=3.0).image
 
 
+def _components(image):
+    return [(c.coefficients, c.quant_table.reshape(64), c.h_samp_factor, c.v_samp_factor) for c in image.components]
+
+
+def _reference_seconds(image, threads: int, sample: int, repeats: int) -> list[float]:
+    """Seconds of `sample` iterations of the reference's solver on the picture with `threads`
+    host threads, `repeats` times: each a solve of 1 + sample iterations less one of 1 iteration
+    (the host model, the start and the first iteration differenced out)."""
+    from oracle import reference
+
+    def run(iterations: int) -> float:
+        options = [*OPTIONS[:6], "--iterations", str(iterations), "--tolerance", "0", "--record-every", "0",
+                   "--threads", str(threads)]
+        began = time.perf_counter()
+        reference.solve(image.height, image.width, int(image.color_space), _components(image), options)
+        return time.perf_counter() - began
+
+    return [max(run(1 + sample) - run(1), 1e-9) for _ in range(repeats)]
+
+
 def _reference_arm(args: argparse.Namespace, rank: int) -> None:
     """The reference's own C++ solver on the host cores: each step a bounded sample of the
     workload (two iterations of the same picture, setup excluded by differencing)."""
@@ -141,24 +168,10 @@ def _reference_arm(args: argparse.Namespace, rank: int) -> None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libunround_ref.so is not built"}))
         return
     image = _workload(seed=0)
-    components = [(c.coefficients, c.quant_table.reshape(64), c.h_samp_factor, c.v_samp_factor)
-                  for c in image.components]
     threads = os.cpu_count() or 1
-
-    def run(iterations: int) -> float:
-        options = [*OPTIONS[:6], "--iterations", str(iterations), "--tolerance", "0", "--record-every", "0",
-                   "--threads", str(threads)]
-        began = time.perf_counter()
-        reference.solve(image.height, image.width, int(image.color_space), components, options)
-        return time.perf_counter() - began
-
     sample = 2
-    for _ in range(args.warmup):
-        run(1)
-    seconds = []
-    for _ in range(args.steps):
-        seconds.append(max(run(1 + sample) - run(1), 1e-9))
-    per_step = statistics.median(seconds)
+    _reference_seconds(image, threads, 1, args.warmup)
+    per_step = statistics.median(_reference_seconds(image, threads, sample, args.steps))
     pixels = HEIGHT * WIDTH
     value = pixels * sample / per_step / 1e6
     line = {
@@ -174,27 +187,55 @@ def _reference_arm(args: argparse.Namespace, rank: int) -> None:
     print(json.dumps(line))
 
 
-def _cpu_baseline(image) -> dict | None:
-    """The reference's solver on the host cores, a bounded sample (two iterations, differenced)."""
+def _cpu_baseline(image) -> tuple[dict | None, object]:
+    """The reference's solver on the host cores, a bounded sample: two iterations (setup
+    differenced out), the best of three, with every host thread and with one; then one whole
+    solve of the workload (500 iterations, every thread), timed, whose canvas is the checker of
+    the device's result (the line's parity). Run before the process touches the GPU, so that
+    nothing of the GPU's side (its driver threads, pinned host memory) competes with it.
+    Returns the baseline and the reference's solve (None where oracle/_ref is not built)."""
     from oracle import reference
 
     if not reference.available():
-        return None
-    components = [(c.coefficients, c.quant_table.reshape(64), c.h_samp_factor, c.v_samp_factor)
-                  for c in image.components]
+        return None, None
     threads = os.cpu_count() or 1
+    sample, repeats = 2, 3
+    _reference_seconds(image, threads, 1, 1)  # the library's pages and the picture's arrays warmed
+    best = min(_reference_seconds(image, threads, sample, repeats))
+    one = min(_reference_seconds(image, 1, sample, repeats))
+    began = time.perf_counter()
+    whole = reference.solve(image.height, image.width, int(image.color_space), _components(image),
+                            [*OPTIONS, "--threads", str(threads)])
+    whole_seconds = time.perf_counter() - began
+    pixels = HEIGHT * WIDTH
+    return {"value": pixels * sample / best / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{sample} iterations of the 4032x3024 4:2:0 TGV workload (setup differenced out), "
+                      f"best of {repeats}, {threads} threads",
+            "one_thread": {"value": pixels * sample / one / 1e6, "unit": UNIT, "cores": 1,
+                           "sample": f"{sample} iterations, best of {repeats}, 1 thread"},
+            "whole_solve": {"seconds": whole_seconds, "iterations": ITERATIONS, "cores": threads,
+                            "value": pixels * ITERATIONS / whole_seconds / 1e6, "unit": UNIT,
+                            "note": "one solve of 500 iterations with the host model and the start"}}, whole
 
-    def run(iterations: int) -> float:
-        options = [*OPTIONS[:6], "--iterations", str(iterations), "--tolerance", "0", "--record-every", "0",
-                   "--threads", str(threads)]
-        began = time.perf_counter()
-        reference.solve(image.height, image.width, int(image.color_space), components, options)
-        return time.perf_counter() - began
 
-    sample = 2
-    seconds = max(run(1 + sample) - run(1), 1e-9)
-    return {"value": HEIGHT * WIDTH * sample / seconds / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"{sample} iterations of the 4032x3024 4:2:0 TGV workload (setup differenced out), {threads} threads"}
+def _parity(decoded, theirs, image) -> dict:
+    """The device's result of the workload against the reference's solve of it (binary64):
+    canvas relative L2 and max |difference| (0..255), the share of 8-bit output samples that are
+    identical, and whether every coefficient lies inside its interval in binary64."""
+    import numpy as np
+
+    from unround import native
+
+    difference = decoded.canvas - theirs.canvas
+    rounded = lambda x: np.clip(np.sign(x) * np.floor(np.abs(x) + 0.5), 0, 255)  # noqa: E731
+    theirs_picture = native.to_rgb(theirs.canvas[:, : image.height, : image.width])
+    inside = all(bool(np.all(c >= p.lower) and np.all(c <= p.upper))
+                 for c, p in zip(decoded.coefficients, decoded.problems))
+    return {"against": "the reference's solver (oracle/_ref, binary64), same picture and options",
+            "rel_l2": float(np.linalg.norm(difference) / np.linalg.norm(theirs.canvas)),
+            "max_abs": float(np.abs(difference).max()),
+            "same_8bit": float(np.mean(rounded(decoded.picture) == rounded(theirs_picture))),
+            "inside_intervals": inside, "bar": {"rel_l2": 1e-4, "max_abs": 2e-3, "same_8bit": 0.999}}
 
 
 def _traffic() -> float | None:
@@ -379,21 +420,22 @@ def _call_batch(images, options) -> int:
         del kept
 
 
-def _mix_arm(args: argparse.Namespace, rank: int, world: int) -> None:
-    """The batched solve of a seeded mix of pictures (sides multiples of 16 in [256, 2048], grey
-    or 4:2:0 colour, quality 10..90, TV or TGV, alpha log-uniform in [0.3, 3], 300 iterations)
-    in one CUDA graph, against the same pictures solved one after another with plain launches.
-    value: all pictures' pixel-iterations over the batched iterations' device time (CUDA events
-    around the graph launch); image_at_a_time: the same over the sum of each picture's
-    iteration loop alone (unround_b200_measure, CUDA events); e2e: through the C interface's
-    batch call with host arrays (levels in, binary64 results out), wall clock. Each rank solves
-    its own mix (weak scaling); rank 0 prints."""
+# Algorithmic bytes per sample-iteration of a fused iteration: TV 3 fields, TGV 8, read and
+# written in binary32, and the int16 levels (2 B a sample in grey, 1 B in 4:2:0).
+def _picture_bytes(entry) -> float:
+    samples = entry.image.height * entry.image.width * (3 if entry.colour else 1)
+    fields = 8 if entry.method == "tgv" else 3
+    return samples * (fields * 8.0 + (1.0 if entry.colour else 2.0))
+
+
+def _mix_measure(pictures: int, warmup: int, seed: int) -> dict:
+    """The batched solve of a seeded mix against the same pictures solved one after another."""
     from unround import native, synthetic
 
-    mix = synthetic.mix(args.pictures, seed=3 + rank, iterations=MIX_ITERATIONS)
+    mix = synthetic.mix(pictures, seed=seed, iterations=MIX_ITERATIONS)
     images, options = [e.image for e in mix], [e.options for e in mix]
     pixels = sum(e.image.height * e.image.width for e in mix)
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         native.solve_batch(images[:2], options[:2])  # warm the call path and the kernels
     with Clocks(0) as clocks:
         _, timing = native.solve_batch(images, options)
@@ -407,24 +449,50 @@ def _mix_arm(args: argparse.Namespace, rank: int, world: int) -> None:
         measured, _ = native.measure(image, option, warmup=0, iterations=timing.iterations)
         alone_ms += measured.milliseconds
     alone = pixels * timing.iterations / (alone_ms / 1e3) / 1e6
-    h2d = sum(sum(c.coefficients.nbytes for c in e.image.components) for e in mix)
+    peak, peak_kind = _peaks()
+    moved = sum(_picture_bytes(e) for e in mix) * timing.iterations
+    alone_gbs, batched_gbs = moved / (alone_ms / 1e3) / 1e9, moved / (timing.milliseconds / 1e3) / 1e9
+    return {
+        "mix": mix, "timing": timing, "pixels": pixels, "batched": batched, "alone": alone, "alone_ms": alone_ms,
+        "e2e": pixels * MIX_ITERATIONS / e2e_seconds / 1e6, "d2h": d2h, "clocks": clocks.summary(),
+        "h2d": sum(sum(c.coefficients.nbytes for c in e.image.components) for e in mix),
+        # The image-at-a-time path's share of the peak bounds what batching can gain: at best
+        # the whole mix moves its bytes at the peak.
+        "roofline": {"algorithmic_bytes_per_iteration": moved / timing.iterations, "peak": peak,
+                     "peak_kind": peak_kind, "image_at_a_time_gbs": alone_gbs,
+                     "image_at_a_time_frac": alone_gbs / peak, "batched_gbs": batched_gbs,
+                     "batched_frac": batched_gbs / peak, "speedup_ceiling": peak / alone_gbs},
+    }
+
+
+def _mix_arm(args: argparse.Namespace, rank: int, world: int) -> None:
+    """The batched solve of a seeded mix of pictures (sides multiples of 16 in [256, 2048], grey
+    or 4:2:0 colour, quality 10..90, TV or TGV, alpha log-uniform in [0.3, 3], 300 iterations)
+    in one CUDA graph, against the same pictures solved one after another with plain launches.
+    value: all pictures' pixel-iterations over the batched iterations' device time (CUDA events
+    around the graph launch); image_at_a_time: the same over the sum of each picture's
+    iteration loop alone (unround_b200_measure, CUDA events); e2e: through the C interface's
+    batch call with host arrays (levels in, binary64 results out), wall clock. Each rank solves
+    its own mix (weak scaling); rank 0 prints."""
+    m = _mix_measure(args.pictures, args.warmup, 3 + rank)
+    mix, timing = m["mix"], m["timing"]
     if rank != 0:
         return
     line = {
         "metric": f"batched TV/TGV mix Mpx*iter/s on 1 B200 ({args.pictures} pictures, {MIX_ITERATIONS} iterations)",
-        "value": batched, "unit": "Mpx*iter/s", "n_gpus": world, "steps": 1, "warmup": args.warmup,
+        "value": m["batched"], "unit": "Mpx*iter/s", "n_gpus": world, "steps": 1, "warmup": args.warmup,
         "ms_per_step": timing.milliseconds, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded mix: sides 16k in [256, 2048], grey/4:2:0, Q 10..90, TV/TGV)",
-        "config": {"workload": f"mix-{args.pictures}", "pictures": args.pictures, "pixels": pixels,
+        "config": {"workload": f"mix-{args.pictures}", "pictures": args.pictures, "pixels": m["pixels"],
                    "samples": timing.samples, "iterations_timed": timing.iterations,
                    "tgv": sum(e.method == "tgv" for e in mix), "colour": sum(e.colour for e in mix),
                    "l2": "state larger than L2, no flush"},
-        "image_at_a_time": {"value": alone, "unit": "Mpx*iter/s", "ms": alone_ms},
-        "speedup_vs_image_at_a_time": batched / alone,
-        "e2e": {"value": pixels * MIX_ITERATIONS / e2e_seconds / 1e6, "unit": "Mpx*iter/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "image_at_a_time": {"value": m["alone"], "unit": "Mpx*iter/s", "ms": m["alone_ms"]},
+        "speedup_vs_image_at_a_time": m["batched"] / m["alone"],
+        "roofline": m["roofline"],
+        "e2e": {"value": m["e2e"], "unit": "Mpx*iter/s", "h2d_bytes_per_step": m["h2d"], "d2h_bytes_per_step": m["d2h"]},
         "gpu_launches": timing.launches_per_iteration * timing.iterations,
-        "clocks": clocks.summary(),
+        "clocks": m["clocks"],
     }
     print(json.dumps(line))
 
@@ -749,6 +817,8 @@ def main() -> None:
     from unround import native
 
     image = _workload(seed=rank)
+    # The CPU baseline first, before any GPU work in this process (rank 0, one GPU only).
+    cpu_baseline, theirs = _cpu_baseline(image) if (world == 1 and rank == 0) else (None, None)
     # Warm-up steps and timed steps of the device-resident loop.
     if group is not None:
         group.barrier()
@@ -785,6 +855,26 @@ def main() -> None:
         file_d2h = _call_file(jpeg)
     file_seconds = max_over_ranks(time.perf_counter() - began)
     e2e_file = world * pixels * args.steps * ITERATIONS / file_seconds / 1e6
+    # The records' cost at the reference's default (a record every 10 iterations, each with its
+    # host round trip): solves through the drop-in call with and without them.
+    recording = [*OPTIONS[:-1], "10"]
+    native.solve(image, recording)
+    plain_s, recorded_s = [], []
+    for _ in range(2):
+        began = time.perf_counter()
+        native.solve(image, OPTIONS)
+        plain_s.append(time.perf_counter() - began)
+        began = time.perf_counter()
+        recorded = native.solve(image, recording)
+        recorded_s.append(time.perf_counter() - began)
+    record_count = len(recorded.result.history.iterations)
+    records = {"record_every": 10, "records": record_count, "solve_ms": min(recorded_s) * 1e3,
+               "solve_ms_without": min(plain_s) * 1e3,
+               "ms_per_record": (min(recorded_s) - min(plain_s)) * 1e3 / max(record_count - 1, 1),
+               "value": pixels * ITERATIONS / min(recorded_s) / 1e6, "unit": UNIT}
+    parity = _parity(native.solve(image, OPTIONS), theirs, image) if theirs is not None else None
+    # The batched mix beside (the batching workload): batched against image at a time.
+    mixed = _mix_measure(64, 1, 3) if world == 1 else None
     peak, peak_kind = _peaks()
     copy = _copy_gbs()
     samples = timing.samples
@@ -821,9 +911,15 @@ def main() -> None:
                                  "workload's picture; coefficients read on the host"},
             "gpu_launches": timing.launches_per_iteration * args.steps * ITERATIONS,
             "clocks": clocks.summary(),
+            "records": records,
         }
         if world == 1:
-            line["cpu_baseline"] = _cpu_baseline(image)
+            line["cpu_baseline"] = cpu_baseline
+            line["parity"] = parity
+            line["mix"] = {"pictures": 64, "iterations_timed": mixed["timing"].iterations,
+                           "batched": mixed["batched"], "image_at_a_time": mixed["alone"],
+                           "speedup_vs_image_at_a_time": mixed["batched"] / mixed["alone"],
+                           "roofline": mixed["roofline"], "e2e": mixed["e2e"], "unit": UNIT}
         print(json.dumps(line))
     if group is not None:
         group.destroy_process_group()
