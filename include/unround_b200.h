@@ -201,7 +201,8 @@ unround_status unround_b200_decode_centres_noalloc(const unround_input* input, c
  * of its strip -- the picture's MCU bands it owns and two halo bands either side, given as an
  * unround_input of those bands -- and drives it iteration by iteration, exchanging between the
  * steps the halo rows of the state with its neighbours (the python package's strips module, over
- * NCCL). The plan must record at its last iteration only (--record-every 0 --tolerance 0).
+ * NCCL). A plan that records before its last iteration, or stops at a tolerance, is recorded
+ * across the ranks by the functions below.
  *   _new     the strip's solver, started (the start s_0 on the device);
  *   _step    `iterations` iterations keeping nothing, waited for; the last one is _finish's;
  *   _state   the device planes of the current state (x, p1, p2, and for TGV w1, w2, r11, r22,
@@ -219,6 +220,36 @@ uint64_t unround_b200_strip_state(const unround_b200_strip* strip, float** plane
 unround_status unround_b200_strip_finish(unround_b200_strip* strip, unround_result** result, char* message,
                                          size_t message_size);
 void unround_b200_strip_free(unround_b200_strip* strip);
+
+/* The records of a picture solved in row strips, added up across the ranks (the reference's
+ * records over all its strips, rust/unround/src/records.rs:154-186; here each rank's sums over
+ * its own bands, added in rank order):
+ *   _plan          the plan's {iterations, record_every, tolerance, relative tolerance, partial
+ *                  tolerance, partial radius (NaN: none), alpha, alpha1, alpha0, method (1 TV,
+ *                  2 TGV), iterations made}: returns 11, up to `most` written;
+ *   _rows          the strip's canvas rows [first, end) whose terms its records count: its own
+ *                  bands;
+ *   _record        one iteration keeping its tilde point (`advance` 0: none, the start's) and
+ *                  the record's first sums over those rows, waited for: {G at the kept
+ *                  coefficients, the first-order norms, the second-order norms (TGV), the
+ *                  largest |div2 r~| (TGV), the samples counted};
+ *   _record_duals  the second sums at the scaling theta (TGV: min(1, alpha1 / the largest
+ *                  |div2 r~| of all ranks); TV: 1): {the dual's G* over the channels (the dual
+ *                  value is minus the ranks' total), and with a partial radius the partial gap's
+ *                  G* and its residual};
+ *   _result        after the last iteration (made by _record), the result of the strip's canvas
+ *                  with the stop given (1 converged, 2 iterations, 3 observer), no more
+ *                  iterations. A strip whose plan records before its last iteration is finished
+ *                  by _result, not _finish. */
+uint64_t unround_b200_strip_plan(const unround_b200_strip* strip, double* values, uint64_t most);
+unround_status unround_b200_strip_rows(unround_b200_strip* strip, uint64_t first, uint64_t end, char* message,
+                                       size_t message_size);
+unround_status unround_b200_strip_record(unround_b200_strip* strip, int32_t advance, double* first, char* message,
+                                         size_t message_size);
+unround_status unround_b200_strip_record_duals(unround_b200_strip* strip, double theta, double* second,
+                                               char* message, size_t message_size);
+unround_status unround_b200_strip_result(unround_b200_strip* strip, int32_t stop, unround_result** result,
+                                         char* message, size_t message_size);
 
 /* The failure path of the bounded waits (no counterpart in the reference, whose solver has no
  * device): every wait of a kernel on an mbarrier is bounded, and one that runs out sets an error

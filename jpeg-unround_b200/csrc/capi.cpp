@@ -1673,12 +1673,6 @@ unround_status unround_b200_strip_new(const unround_input* input, const unround_
     if (!frame) return false;
     auto plan = urb::make_plan(s, frame->channels(), failure);
     if (!plan) return false;
-    if (plan->record_every != 0 || plan->tolerance > 0.0 || plan->relative_tolerance > 0.0 ||
-        plan->partial_tolerance > 0.0) {
-      failure = {urb::kOptions, "a picture solved in strips records at its last iteration only and stops there: "
-                                "give --record-every 0 and --tolerance 0"};
-      return false;
-    }
     if (!have_device(failure)) return false;
     auto made = std::make_unique<unround_b200_strip>();
     if (made->stream.error != cudaSuccess) {
@@ -1729,8 +1723,98 @@ unround_status unround_b200_strip_finish(unround_b200_strip* strip, unround_resu
       failure = {urb::kArgument, "the strip and the result are not null pointers"};
       return false;
     }
+    if (!strip->solver) {
+      failure = {urb::kArgument, "the strip is finished"};
+      return false;
+    }
+    const urb::Plan& plan = strip->plan;
+    if (plan.record_every != 0 || plan.tolerance > 0.0 || plan.relative_tolerance > 0.0 ||
+        plan.partial_tolerance > 0.0) {
+      failure = {urb::kOptions, "a strip whose plan records before its last iteration or stops at a tolerance is "
+                                "recorded across the ranks (unround_b200_strip_record) and finished by "
+                                "unround_b200_strip_result"};
+      return false;
+    }
     urb::Outcome outcome;
     if (!strip->solver->finish_batch(strip->done, outcome, failure)) return false;
+    strip->solver.reset();
+    *result = result_of(std::move(strip->frame), std::move(outcome));
+    return true;
+  });
+}
+
+uint64_t unround_b200_strip_plan(const unround_b200_strip* strip, double* values, uint64_t most) {
+  if (strip == nullptr) return 0;
+  const urb::Plan& p = strip->plan;
+  const double nan = std::numeric_limits<double>::quiet_NaN();
+  const double all[11] = {static_cast<double>(p.iterations), static_cast<double>(p.record_every), p.tolerance,
+                          p.relative_tolerance, p.partial_tolerance, p.partial_radius ? *p.partial_radius : nan,
+                          p.alpha, p.alpha1, p.alpha0, p.tgv ? 2.0 : 1.0, static_cast<double>(strip->done)};
+  const uint64_t count = std::min<uint64_t>(most, 11);
+  for (uint64_t k = 0; values != nullptr && k < count; ++k) values[k] = all[k];
+  return 11;
+}
+
+unround_status unround_b200_strip_rows(unround_b200_strip* strip, uint64_t first, uint64_t end, char* message,
+                                       size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (strip == nullptr || !strip->solver) {
+      failure = {urb::kArgument, "the strip is a null pointer or finished"};
+      return false;
+    }
+    const auto rows = static_cast<uint64_t>(strip->solver->geometry().rows);
+    if (first > end || end > rows) {
+      failure = {urb::kArgument, "the record rows [" + std::to_string(first) + ", " + std::to_string(end) +
+                                     ") do not lie within the strip's " + std::to_string(rows) + " canvas rows"};
+      return false;
+    }
+    strip->solver->set_record_rows(static_cast<int>(first), static_cast<int>(end));
+    return true;
+  });
+}
+
+unround_status unround_b200_strip_record(unround_b200_strip* strip, int32_t advance, double* first, char* message,
+                                         size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (strip == nullptr || !strip->solver || first == nullptr) {
+      failure = {urb::kArgument, "the strip (not finished) and the sums are not null pointers"};
+      return false;
+    }
+    if (advance != 0 && strip->done >= strip->plan.iterations) {
+      failure = {urb::kArgument, "the strip has made all of its plan's iterations"};
+      return false;
+    }
+    double sums[5] = {};
+    if (!strip->solver->record_step(advance != 0, sums, failure)) return false;
+    if (advance != 0) ++strip->done;
+    std::copy(sums, sums + 5, first);
+    return true;
+  });
+}
+
+unround_status unround_b200_strip_record_duals(unround_b200_strip* strip, double theta, double* second, char* message,
+                                               size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (strip == nullptr || !strip->solver || second == nullptr) {
+      failure = {urb::kArgument, "the strip (not finished) and the sums are not null pointers"};
+      return false;
+    }
+    double sums[3] = {};
+    if (!strip->solver->record_duals(theta, sums, failure)) return false;
+    std::copy(sums, sums + 3, second);
+    return true;
+  });
+}
+
+unround_status unround_b200_strip_result(unround_b200_strip* strip, int32_t stop, unround_result** result,
+                                         char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (strip == nullptr || !strip->solver || result == nullptr) {
+      failure = {urb::kArgument, "the strip (not finished) and the result are not null pointers"};
+      return false;
+    }
+    urb::Outcome outcome;
+    if (!strip->solver->finish_here(strip->done, stop, outcome, failure)) return false;
     strip->solver.reset();
     *result = result_of(std::move(strip->frame), std::move(outcome));
     return true;

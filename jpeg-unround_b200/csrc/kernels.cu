@@ -19,6 +19,8 @@
 #include <atomic>
 #include <cfloat>
 #include <cstdint>
+#include <cstdlib>
+#include <string_view>
 
 #include "colour.hpp"
 #include "dct.cuh"
@@ -426,7 +428,7 @@ __global__ void __launch_bounds__(256, 2) primal_kernel(const PrimalParams P) {
           const double absolute = k == 0 ? static_cast<double>(zeta[u]) +
                                                (static_cast<double>(levels[0]) * P.component.constants->step[0] + 1024.0)
                                          : static_cast<double>(zeta[u]);
-          sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
+          if (P.g.recorded_row(i0)) sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
         }
       }
     }
@@ -578,7 +580,7 @@ __device__ __forceinline__ void primal_block_row(const float* slot, const std::i
             k == 0 ? static_cast<double>(zeta[u]) +
                          (static_cast<double>(levels[0]) * P.component.constants->step[0] + 1024.0)
                    : static_cast<double>(zeta[u]);
-        sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
+        if (P.g.recorded_row(i0)) sum += value_term(absolute, levels[u], k, flat, *P.component.constants);
       }
     }
   }
@@ -713,6 +715,10 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  // Launched after the dual sweep it reads (programmatic stream serialization): the factors and
+  // barriers above were set up while the sweep finished; the state is read from here on.
+  grid_dependency_wait();
+  allow_dependents();
   const int items = (Q.items - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
                     static_cast<int>(gridDim.x);  // this CTA's
   // The levels of an item's blocks (NB block rows of B blocks), after the slots.
@@ -934,6 +940,8 @@ __global__ void __launch_bounds__(256) start_kernel(const StartParams P) {
   if (block < blocks) {
     const Constants64& K = *P.component.constants;
     const bool flat = P.component.flat[block] != 0;
+    const int canvas_row = (block / P.component.block_columns) * 8 * P.component.cell_rows;
+    const bool counted = canvas_row >= P.record_first && canvas_row < P.record_end;
     for (int u = 0; u < 8; ++u) {
       const int k = m * 8 + u;
       const std::size_t at = static_cast<std::size_t>(block) * 64 + k;
@@ -953,7 +961,7 @@ __global__ void __launch_bounds__(256) start_kernel(const StartParams P) {
       const double from = P.given != nullptr ? P.given[at] : centre;
       const double zeta = clamp_to(from, low, high);
       P.coefficients[at] = zeta;
-      sum += value_term(zeta, q, k, flat, K);
+      if (counted) sum += value_term(zeta, q, k, flat, K);
     }
   }
   cta_sum(sum, P.partials);
@@ -1165,6 +1173,7 @@ __global__ void __launch_bounds__(256) norms_kernel(const NormParams P) {
       if constexpr (COUPLED) most = fmax(most, sqrt(square));
     }
   }
+  if (!P.g.recorded_row(i)) first = second = most = 0.0;  // div2 is still made for every row
   const double sum_first = cta_reduce<false>(first);
   const double sum_second = cta_reduce<false>(second);
   const double largest = cta_reduce<true>(most);
@@ -1227,6 +1236,7 @@ __global__ void __launch_bounds__(256) conjugate_kernel(const ConjugateParams P)
   const bool active = vbx * BW < columns && vby * BH < rows;
   const bool in_blocks = active && vby < P.component.block_rows && vbx < P.component.block_columns;
   const int j0 = vbx * BW + m * CC, i0 = vby * BH;
+  const bool counted = P.g.recorded_row(i0);
   // xi = gamma div q at the lane's samples, q = scale (q1, q2).
   auto q_at = [&](const float* f, int i, int j) -> double { return P.scale * static_cast<double>(f[static_cast<std::size_t>(i) * pitch + j]); };
   double xi[BH][CC];
@@ -1291,13 +1301,13 @@ __global__ void __launch_bounds__(256) conjugate_kernel(const ConjugateParams P)
       total += conjugate_term(coef[u], P.component.levels[block * 64 + k], k, flat, *P.component.constants);
     }
   }
-  cta_sum(total, P.partials);
+  cta_sum(counted ? total : 0.0, P.partials);
 }
 
 __global__ void __launch_bounds__(256) residual_kernel(const ResidualParams P) {
   const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y;
   double value = 0.0;
-  if (i < P.g.rows && j < P.g.columns) {
+  if (i < P.g.rows && j < P.g.columns && P.g.recorded_row(i)) {
     const std::size_t at = static_cast<std::size_t>(i) * P.g.pitch + j;
     const double a = static_cast<double>(P.p1[at]) + 1.0 * P.d1[at];
     const double b = static_cast<double>(P.p2[at]) + 1.0 * P.d2[at];
@@ -1442,6 +1452,14 @@ int primal_grid_blocks(const Geometry& g, const ComponentDevice& c) {
 int conjugate_grid_blocks(const Geometry& g, const ComponentDevice& c) { return primal_grid_blocks(g, c); }
 int start_grid_blocks(const ComponentDevice& c) { return (c.block_rows * c.block_columns * 8 + 255) / 256; }
 
+bool dependent_launches() {
+  static const bool on = [] {
+    const char* value = std::getenv("UNROUND_B200_LAUNCH");
+    return value == nullptr || std::string_view(value) != "plain";
+  }();
+  return on;
+}
+
 cudaError_t launch_dual(const DualParams& p, bool tgv, bool coupled, bool keep, cudaStream_t stream) {
   return tgv ? dual_channels<true>(p, coupled, keep, stream) : dual_channels<false>(p, coupled, keep, stream);
 }
@@ -1483,8 +1501,7 @@ cudaError_t primal_tma_one(const CUtensorMap* maps, const PrimalParams* parts, i
   batch.items = count * batch.strips * batch.stages;
   *grid = std::min(batch.items, slots);
   if (*grid <= 0) return cudaSuccess;  // no block row
-  kernel<<<*grid, threads, bytes, s>>>(maps[0], maps[count > 1 ? 1 : 0], batch);
-  return cudaGetLastError();
+  return launch_after(kernel, dim3(*grid), dim3(threads), bytes, s, maps[0], maps[count > 1 ? 1 : 0], batch);
 }
 
 template <int CR, int CC>

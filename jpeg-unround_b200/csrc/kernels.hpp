@@ -16,6 +16,31 @@ namespace urb {
 
 constexpr int kMaxChannels = 3;
 
+// Whether the iteration's kernels are launched with programmatic stream serialization (on,
+// unless UNROUND_B200_LAUNCH=plain): each may then be scheduled while the one before it in the
+// stream finishes, its CTAs doing their set-up as SMs free up and waiting (griddepcontrol.wait)
+// before they touch what that kernel writes.
+bool dependent_launches();
+
+// Launches `kernel` on `stream` after the work before it, as dependent_launches() says. Only a
+// kernel that calls grid_dependency_wait (tma.cuh) before its first global access to what the
+// kernel before it writes may be launched so.
+template <typename... Params, typename... Args>
+cudaError_t launch_after(void (*kernel)(Params...), dim3 grid, dim3 block, std::size_t bytes, cudaStream_t stream,
+                         Args&&... args) {
+  cudaLaunchConfig_t config = {};
+  config.gridDim = grid;
+  config.blockDim = block;
+  config.dynamicSmemBytes = bytes;
+  config.stream = stream;
+  cudaLaunchAttribute attribute = {};
+  attribute.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attribute.val.programmaticStreamSerializationAllowed = 1;
+  config.attrs = &attribute;
+  config.numAttrs = dependent_launches() ? 1 : 0;
+  return cudaLaunchKernelEx(&config, kernel, static_cast<Args&&>(args)...);
+}
+
 // The per-frequency factors of a component's proximal map in binary32, for one step tau
 // (docs/math.md 4.1, 4.4; cpp/src/model.cpp:483-497), with t = (tau / n_c) m and
 // r = 1 / (1 + t): z = (e + t c) r = e r + (t r) c, clipped to q Q -+ (1/2 + s) Q. They are
@@ -74,6 +99,11 @@ struct Geometry {
   int pitch = 0;
   int channels = 1;
   std::size_t plane = 0;  // rows * pitch
+  // The rows whose terms the records add up: every row, but in a strip of a picture solved in
+  // row strips its own bands (whole blocks), so that the strips' sums make the picture's.
+  int record_first = 0;
+  int record_end = 1 << 30;
+  __host__ __device__ bool recorded_row(int i) const { return i >= record_first && i < record_end; }
 };
 
 // A state of the method (docs/math.md 5): x, p and for TGV w and r, each channels planes.
@@ -187,6 +217,8 @@ struct StartParams {
   const double* given = nullptr;  // null: the centres
   double* coefficients = nullptr;
   double* partials = nullptr;
+  int record_first = 0;  // the canvas rows whose blocks the data term adds up (Geometry's)
+  int record_end = 1 << 30;
 };
 
 int dual_grid_blocks(const Geometry& g);

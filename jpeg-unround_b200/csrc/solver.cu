@@ -359,6 +359,8 @@ struct Solver::Impl {
       sp.component = components[c];
       sp.coefficients = coefficients[c];
       sp.partials = value_slot(c);
+      sp.record_first = g.record_first;
+      sp.record_end = g.record_end;
       const double* given_coefficients = nullptr;
       if (given != nullptr && !given->coefficients.empty()) {
         given_coefficients = upload(given->coefficients[c].data(), given->coefficients[c].size());
@@ -622,13 +624,15 @@ struct Solver::Impl {
   // The channels of the data term: the components, or the samples' channels.
   std::size_t data_channels() const { return samples != nullptr ? samples->channels : components.size(); }
 
-  // The record of the tilde point (cpp/src/primal_dual.hpp:446-501).
-  Record record(std::uint64_t iteration) {
-    Record r;
-    r.iteration = iteration;
-    r.scaling = kNaN;
-    r.partial_gap = kNaN;
-    const double data = data_value();
+  // The first sums of a record, over the record rows (Geometry::record_first/end: the canvas,
+  // or a strip's own bands): G at the kept coefficients, the first-order norms, and for TGV the
+  // second-order norms and the largest |div2 r~| (cpp/src/primal_dual.hpp:446-501, 836-895).
+  struct FirstSums {
+    double data = 0.0, first = 0.0, second = 0.0, most = 0.0;
+  };
+  FirstSums first_sums() {
+    FirstSums f;
+    f.data = data_value();
     NormParams np;
     np.g = g;
     np.xt = xt;
@@ -638,31 +642,36 @@ struct Solver::Impl {
     np.partials = partials;
     if (error == cudaSuccess) error = launch_norms(np, tgv, plan.coupled, stream);
     const std::size_t count = norms_grid_blocks(g);
-    const double first = sum_of(partials, count, 0);
-    if (!tgv) {
-      r.primal = plan.alpha * first + data;
-      double conjugates = 0.0;
-      for (std::size_t c = 0; c < data_channels(); ++c) {
-        conjugates += conjugate(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0);
-      }
-      r.dual = -conjugates;
-      return r;
+    f.first = sum_of(partials, count, 0);
+    if (tgv) {
+      f.second = sum_of(partials, count, count);
+      f.most = max_of(partials, count, 2 * count);
     }
-    const double second = sum_of(partials, count, count);
-    const double most = max_of(partials, count, 2 * count);
-    r.primal = (plan.alpha1 * first + plan.alpha0 * second) + data;
-    const double theta = most > plan.alpha1 ? plan.alpha1 / most : 1.0;
-    r.scaling = theta;
-    double conjugates = 0.0;
+    return f;
+  }
+
+  // The second sums at the scaling theta: G*(-gamma div(theta div2 r~)) (TGV) or G*(gamma div
+  // p~) (TV) summed over the channels; with a partial radius (TGV), the partial gap's
+  // G*(gamma div p~) and its residual.
+  struct SecondSums {
+    double conjugates = 0.0, partial = 0.0, residual = 0.0;
+  };
+  SecondSums second_sums(double theta) {
+    SecondSums s;
+    if (!tgv) {
+      for (std::size_t c = 0; c < data_channels(); ++c) {
+        s.conjugates += conjugate(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0);
+      }
+      return s;
+    }
     for (std::size_t c = 0; c < data_channels(); ++c) {
       const std::size_t base = 2 * c * g.plane;
-      conjugates += conjugate(c, div2 + base, div2 + base + g.plane, -theta);
+      s.conjugates += conjugate(c, div2 + base, div2 + base + g.plane, -theta);
     }
-    r.dual = -conjugates;
     if (plan.partial_radius) {
-      double partial = 0.0, residual = 0.0;
+      const std::size_t count = norms_grid_blocks(g);
       for (std::size_t c = 0; c < data_channels(); ++c) {
-        partial += conjugate(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0);
+        s.partial += conjugate(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0);
         ResidualParams rp;
         rp.g = g;
         rp.p1 = tilde.p1 + c * g.plane;
@@ -671,10 +680,30 @@ struct Solver::Impl {
         rp.d2 = div2 + (2 * c + 1) * g.plane;
         rp.partials = partials;
         if (error == cudaSuccess) error = launch_residual(rp, stream);
-        residual += plan.channel_weights[c] * sum_of(partials, count);
+        s.residual += plan.channel_weights[c] * sum_of(partials, count);
       }
-      r.partial_gap = r.primal + partial + *plan.partial_radius * residual;
     }
+    return s;
+  }
+
+  // The record of the tilde point (cpp/src/primal_dual.hpp:446-501).
+  Record record(std::uint64_t iteration) {
+    Record r;
+    r.iteration = iteration;
+    r.scaling = kNaN;
+    r.partial_gap = kNaN;
+    const FirstSums f = first_sums();
+    if (!tgv) {
+      r.primal = plan.alpha * f.first + f.data;
+      r.dual = -second_sums(1.0).conjugates;
+      return r;
+    }
+    r.primal = (plan.alpha1 * f.first + plan.alpha0 * f.second) + f.data;
+    const double theta = f.most > plan.alpha1 ? plan.alpha1 / f.most : 1.0;
+    r.scaling = theta;
+    const SecondSums s = second_sums(theta);
+    r.dual = -s.conjugates;
+    if (plan.partial_radius) r.partial_gap = r.primal + s.partial + *plan.partial_radius * s.residual;
     return r;
   }
 
@@ -970,6 +999,54 @@ bool Solver::step(std::uint64_t iterations, Failure& failure) {
   }
   if (m.error == cudaSuccess) m.error = cudaStreamSynchronize(m.stream);
   return m.check(failure, "the strip's iterations");
+}
+
+void Solver::set_record_rows(int first, int end) {
+  impl_->g.record_first = first;
+  impl_->g.record_end = end;
+  geometry_ = impl_->g;
+}
+
+bool Solver::record_step(bool advance, double (&first)[5], Failure& failure) {
+  Impl& m = *impl_;
+  if (advance) {
+    m.primal(true);
+    m.dual(true);
+  }
+  if (m.error == cudaSuccess) m.error = cudaStreamSynchronize(m.stream);
+  const Impl::FirstSums f = m.first_sums();
+  const int counted = std::max(0, std::min(m.g.record_end, m.g.rows) - std::max(m.g.record_first, 0));
+  first[0] = f.data;
+  first[1] = f.first;
+  first[2] = f.second;
+  first[3] = f.most;
+  first[4] = static_cast<double>(m.g.channels) * counted * m.g.columns;
+  return m.check(failure, "the strip's record");
+}
+
+bool Solver::record_duals(double theta, double (&second)[3], Failure& failure) {
+  Impl& m = *impl_;
+  const Impl::SecondSums s = m.second_sums(theta);
+  second[0] = s.conjugates;
+  second[1] = s.partial;
+  second[2] = s.residual;
+  return m.check(failure, "the strip's record");
+}
+
+bool Solver::finish_here(std::uint64_t done, std::int32_t stop, Outcome& out, Failure& failure) {
+  Impl& m = *impl_;
+  if (!m.check(failure, "the strip's iterations")) return false;
+  out.tau = m.plan.tau;
+  out.sigma = m.plan.sigma;
+  out.iterations = done;
+  out.stop = stop;
+  out.solved = true;
+  if (done == 0) {
+    if (m.host_result) m.fetch(out);
+  } else {
+    m.result(out);
+  }
+  return m.check(failure, "the result");
 }
 
 int Solver::state_planes(float** planes, int most) const {

@@ -105,6 +105,17 @@ class Solver {
   // Returns how many planes there are (up to `most` written).
   bool step(std::uint64_t iterations, Failure& failure);
   int state_planes(float** planes, int most) const;
+  // A strip's records, which the ranks add up (strips.py): the canvas rows [first, end) whose
+  // terms its records count (its own bands); one iteration keeping its tilde point (none with
+  // `advance` false: the start's) and the record's first sums over those rows -- G at the kept
+  // coefficients, the first-order norms, the second-order norms and the largest |div2 r~| (TGV),
+  // the samples counted -- waited for; the second sums at the scaling theta -- the dual's G*
+  // over the channels, and with a partial radius the partial gap's G* and residual; and after
+  // the last iteration (made by record_step), the result with no more iterations.
+  void set_record_rows(int first, int end);
+  bool record_step(bool advance, double (&first)[5], Failure& failure);
+  bool record_duals(double theta, double (&second)[3], Failure& failure);
+  bool finish_here(std::uint64_t done, std::int32_t stop, Outcome& out, Failure& failure);
 
   // Before solve(): keep the result on the device (the Outcome gets the records and counts,
   // not the arrays); after it, the picture's 8- or 16-bit levels into host memory `out`

@@ -16,6 +16,7 @@ and the owned rows of the canvases make the picture's canvas.
   exchanges        the rows each neighbour pair swaps: (sender, sender's first row, receiver,
                    receiver's first row, rows)
   exchange         the swap over torch.distributed (NCCL for device tensors, gloo on the CPU)
+  combine          a record of the picture from every rank's sums
   solve_in_strips  the whole solve with the strips in one process on one GPU (the ranks
                    emulated, the swaps device copies between them), for tests and one device
   solve_strip      a rank's part of it under torch.distributed (one process per GPU)
@@ -24,6 +25,8 @@ and the owned rows of the canvases make the picture's canvas.
 from __future__ import annotations
 
 import ctypes
+import math
+from collections.abc import Callable, Sequence
 from dataclasses import dataclass
 from typing import Final
 
@@ -167,6 +170,48 @@ class StripSolver:
         return [torch.as_tensor(_DevicePlane(ctypes.cast(pointers[k], ctypes.c_void_p).value, rows.value,
                                              columns.value, pitch.value), device="cuda") for k in range(count)]
 
+    def plan(self) -> StripPlan:
+        values = (ctypes.c_double * 11)()
+        self._library.unround_b200_strip_plan(self._handle, values, 11)
+        return StripPlan.of(list(values))
+
+    def set_rows(self, first: int, end: int) -> None:
+        """The canvas rows [first, end) whose terms the strip's records count: its own bands."""
+        message = ctypes.create_string_buffer(self._native._MESSAGE)
+        status = self._library.unround_b200_strip_rows(self._handle, first, end, message, self._native._MESSAGE)
+        self._native._raise(status, message)
+
+    def record(self, advance: bool) -> list[float]:
+        """One iteration keeping its tilde point (none when not `advance`: the start's), and the
+        record's first sums over the strip's own rows."""
+        sums = (ctypes.c_double * 5)()
+        message = ctypes.create_string_buffer(self._native._MESSAGE)
+        status = self._library.unround_b200_strip_record(self._handle, 1 if advance else 0, sums, message,
+                                                         self._native._MESSAGE)
+        self._native._raise(status, message)
+        return list(sums)
+
+    def record_duals(self, theta: float) -> list[float]:
+        """The record's second sums at the scaling theta."""
+        sums = (ctypes.c_double * 3)()
+        message = ctypes.create_string_buffer(self._native._MESSAGE)
+        status = self._library.unround_b200_strip_record_duals(self._handle, theta, sums, message,
+                                                               self._native._MESSAGE)
+        self._native._raise(status, message)
+        return list(sums)
+
+    def result(self, stop: int) -> object:
+        """The result after the last iteration made (a Decoded of the strip's canvas)."""
+        result = ctypes.c_void_p()
+        message = ctypes.create_string_buffer(self._native._MESSAGE)
+        status = self._library.unround_b200_strip_result(self._handle, stop, ctypes.byref(result), message,
+                                                         self._native._MESSAGE)
+        self._native._raise(status, message)
+        try:
+            return self._native._decoded(self._library, result, problems=False)
+        finally:
+            self._library.unround_result_free(result)
+
     def finish(self) -> object:
         """The last iteration and the result (a Decoded of the strip's canvas)."""
         result = ctypes.c_void_p()
@@ -195,6 +240,11 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_b200_strip_state": (u64, handle, ctypes.c_void_p, u64, u64p, u64p, u64p),
         "unround_b200_strip_finish": (ctypes.c_int32, handle, ctypes.POINTER(handle), *text),
         "unround_b200_strip_free": (None, handle),
+        "unround_b200_strip_plan": (u64, handle, ctypes.c_void_p, u64),
+        "unround_b200_strip_rows": (ctypes.c_int32, handle, u64, u64, *text),
+        "unround_b200_strip_record": (ctypes.c_int32, handle, ctypes.c_int32, ctypes.c_void_p, *text),
+        "unround_b200_strip_record_duals": (ctypes.c_int32, handle, ctypes.c_double, ctypes.c_void_p, *text),
+        "unround_b200_strip_result": (ctypes.c_int32, handle, ctypes.c_int32, ctypes.POINTER(handle), *text),
     }
     for name, (result, *arguments) in table.items():
         function = getattr(library, name)
@@ -202,32 +252,137 @@ def _bind(library: ctypes.CDLL) -> None:
         function.argtypes = arguments
 
 
-def _iterations(options: list[str]) -> int:
-    """The options' iterations: a solve in strips is given them (it stops at its last only)."""
-    for k, option in enumerate(options):
-        if option == "--iterations" and k + 1 < len(options):
-            return int(options[k + 1])
-        if option.startswith("--iterations="):
-            return int(option.split("=", 1)[1])
-    raise ValueError("a solve in strips is given its --iterations")
+@dataclass(frozen=True)
+class StripPlan:
+    """What of a strip's plan the driver needs: its iterations, records and stops, weights."""
+
+    iterations: int
+    record_every: int
+    tolerance: float
+    relative_tolerance: float
+    partial_tolerance: float
+    partial_radius: float | None
+    alpha: float
+    alpha1: float
+    alpha0: float
+    tgv: bool
+
+    @staticmethod
+    def of(values: Sequence[float]) -> StripPlan:
+        return StripPlan(int(values[0]), int(values[1]), values[2], values[3], values[4],
+                         None if math.isnan(values[5]) else values[5], values[6], values[7], values[8],
+                         values[9] == 2.0)
+
+    def recorded(self, n: int) -> bool:
+        return (self.record_every > 0 and n % self.record_every == 0) or n == self.iterations
 
 
-def _own_rows(decoded: object, strip: Strip, rows: int) -> npt.NDArray[np.float64]:
-    canvas = decoded.canvas  # type: ignore[attr-defined]
-    start = (strip.first - strip.low) * rows
-    return canvas[:, start : start + (strip.end - strip.first) * rows]
+@dataclass(frozen=True)
+class StripSolution:
+    """A solve in strips: this rank's own rows of the canvas (all of it from solve_in_strips),
+    the picture's records (native.History), its iterations and why it stopped."""
+
+    canvas: npt.NDArray[np.float64]
+    history: object
+    iterations: int
+    stop: int
 
 
-def solve_in_strips(image: jpegio.Image, options: list[str], strips: int = 2) -> npt.NDArray[np.float64]:
+def combine(plan: StripPlan, firsts: Sequence[Sequence[float]],
+            second_of: Callable[[float], Sequence[Sequence[float]]]) -> tuple[tuple[float, ...], float]:
+    """A record of the picture from every rank's sums, in rank order: `firsts` each rank's
+    {G, first-order norms, second-order norms, largest |div2 r~|, samples}; `second_of(theta)`
+    each rank's {conjugates, partial gap's conjugates, its residual} at theta. Returns (primal,
+    dual, scaling, partial gap) and the samples, in the whole solve's binary64 arithmetic
+    (cpp/src/primal_dual.hpp:446-501)."""
+    data = first = second = samples = 0.0
+    most = 0.0
+    for f in firsts:
+        data += f[0]
+        first += f[1]
+        second += f[2]
+        most = max(most, f[3])
+        samples += f[4]
+    nan = float("nan")
+    if not plan.tgv:
+        primal = plan.alpha * first + data
+        conjugates = 0.0
+        for s in second_of(1.0):
+            conjugates += s[0]
+        return (primal, -conjugates, nan, nan), samples
+    primal = (plan.alpha1 * first + plan.alpha0 * second) + data
+    theta = plan.alpha1 / most if most > plan.alpha1 else 1.0
+    conjugates = partial = residual = 0.0
+    for s in second_of(theta):
+        conjugates += s[0]
+        partial += s[1]
+        residual += s[2]
+    partial_gap = primal + partial + plan.partial_radius * residual if plan.partial_radius is not None else nan
+    return (primal, -conjugates, theta, partial_gap), samples
+
+
+def _met(plan: StripPlan, values: tuple[float, ...], samples: float) -> bool:
+    """Whether a record meets a tolerance of the plan (the whole solve's stops)."""
+    primal, dual, _, partial_gap = values
+    gap = primal - dual
+    if plan.tolerance > 0.0 and gap / samples <= plan.tolerance:
+        return True
+    if plan.relative_tolerance > 0.0 and gap <= plan.relative_tolerance * primal:
+        return True
+    return plan.partial_tolerance > 0.0 and not math.isnan(partial_gap) and partial_gap / samples <= plan.partial_tolerance
+
+
+def _drive(plan: StripPlan, step: Callable[[], None], swap: Callable[[], None],
+           firsts_of: Callable[[bool], Sequence[Sequence[float]]],
+           seconds_of: Callable[[float], Sequence[Sequence[float]]]) -> tuple[list[tuple], int, int]:
+    """The method's loop over the strips, as the whole solve runs it: a record at 0 (where the plan
+    records) and at every recorded iteration, each the ranks' sums combined; the halos swapped
+    after the start and after every iteration; a tolerance met stops every rank there. Returns
+    the records (iteration, seconds 0, primal, dual, scaling, partial gap), the iterations made
+    and the stop (1 converged, 2 iterations)."""
+    records: list[tuple] = []
+    swap()  # the start's halos
+
+    def take(iteration: int, advance: bool) -> bool:
+        values, samples = combine(plan, firsts_of(advance), seconds_of)
+        records.append((iteration, 0.0, *values))
+        return _met(plan, values, samples)
+
+    if (plan.record_every > 0 or plan.iterations == 0) and take(0, False):
+        return records, 0, 1
+    for n in range(1, plan.iterations + 1):
+        if plan.recorded(n):
+            met = take(n, True)
+            swap()
+            if met:
+                return records, n, 1
+        else:
+            step()
+            swap()
+    return records, plan.iterations, 2
+
+
+def _history(records: list[tuple]) -> object:
+    from unround import native
+
+    columns = list(zip(*records)) if records else [()] * 6
+    arrays = [np.asarray(column, dtype=np.float64) for column in columns[1:]]
+    return native.History(np.asarray(columns[0], dtype=np.int64), *arrays)
+
+
+def solve_in_strips(image: jpegio.Image, options: list[str], strips: int = 2) -> StripSolution:
     """The whole solve of `image` with its bands in `strips` strips, each its own solver on the
-    current device, the halo swaps device copies: the canvas (channels x rows x columns), which
-    is the whole solve's. The options record at the last iteration only."""
+    current device, the halo swaps device copies between them and the records the strips' sums
+    added in strip order: the canvas (channels x rows x columns), the records and the stop,
+    which are the whole solve's."""
     import torch
 
     rows = band_rows(image)
     parts = partition(band_count(image), strips)
     solvers = [StripSolver(sub_image(image, part), options) for part in parts]
-    iterations = _iterations(options)
+    for solver, part in zip(solvers, parts):
+        solver.set_rows((part.first - part.low) * rows, (part.end - part.low) * rows)
+    plan = solvers[0].plan()
 
     def swap() -> None:
         planes = [solver.planes() for solver in solvers]
@@ -237,27 +392,60 @@ def solve_in_strips(image: jpegio.Image, options: list[str], strips: int = 2) ->
                 target[r_row : r_row + count].copy_(source[s_row : s_row + count])
         torch.cuda.synchronize()
 
-    swap()  # the start's halos
-    for _ in range(max(0, iterations - 1)):
+    def step() -> None:
         for solver in solvers:
             solver.step(1)
-        swap()
-    decoded = [solver.finish() for solver in solvers]
-    return np.concatenate([_own_rows(d, part, rows) for d, part in zip(decoded, parts)], axis=1)
+
+    records, iterations, stop = _drive(plan, step, swap, lambda advance: [s.record(advance) for s in solvers],
+                                       lambda theta: [s.record_duals(theta) for s in solvers])
+    decoded = [solver.result(stop) for solver in solvers]
+    canvas = np.concatenate([_own_rows(d, part, rows) for d, part in zip(decoded, parts)], axis=1)
+    return StripSolution(canvas, _history(records), iterations, stop)
 
 
-def solve_strip(image: jpegio.Image, options: list[str], group: object = None) -> npt.NDArray[np.float64]:
+def _gathered(values: Sequence[float], group: object) -> list[list[float]]:
+    """Every rank's values, in rank order (NCCL: through the device; gloo: the host)."""
+    import torch
+    import torch.distributed as dist
+
+    device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    mine = torch.tensor(list(values), dtype=torch.float64, device=device)
+    every = [torch.empty_like(mine) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(every, mine, group=group)
+    return [t.cpu().tolist() for t in every]
+
+
+def drive_rank(solver: object, parts: list[Strip], rank: int, rows: int, group: object = None) -> tuple:
+    """This rank's loop over its strip's `solver` (a StripSolver, or any object with its plan,
+    set_rows, step, planes, record, record_duals and result): the swaps with its neighbours and
+    the records gathered from every rank. Returns (the result of the strip, the records, the
+    iterations made, the stop)."""
+    part = parts[rank]
+    solver.set_rows((part.first - part.low) * rows, (part.end - part.low) * rows)
+    plan = solver.plan()
+    records, iterations, stop = _drive(
+        plan, lambda: solver.step(1), lambda: exchange(solver.planes(), parts, rank, rows, group),
+        lambda advance: _gathered(solver.record(advance), group),
+        lambda theta: _gathered(solver.record_duals(theta), group))
+    return solver.result(stop), records, iterations, stop
+
+
+def _own_rows(decoded: object, strip: Strip, rows: int) -> npt.NDArray[np.float64]:
+    canvas = decoded.canvas  # type: ignore[attr-defined]
+    start = (strip.first - strip.low) * rows
+    return canvas[:, start : start + (strip.end - strip.first) * rows]
+
+
+def solve_strip(image: jpegio.Image, options: list[str], group: object = None) -> StripSolution:
     """This rank's part of the solve of `image` in strips under torch.distributed (one rank a
-    GPU, the swaps NCCL sends and receives with its neighbours): the rows of the canvas it owns
-    (channels x rows x columns). Concatenated in rank order, they are the whole solve's canvas."""
+    GPU, the swaps NCCL sends and receives with its neighbours, the records' sums gathered from
+    every rank): the rows of the canvas it owns (channels x rows x columns), concatenated in rank
+    order the whole solve's canvas, and the picture's records and stop, alike on every rank."""
     import torch.distributed as dist
 
     rank, ranks = dist.get_rank(group), dist.get_world_size(group)
     rows = band_rows(image)
     parts = partition(band_count(image), ranks)
     solver = StripSolver(sub_image(image, parts[rank]), options)
-    exchange(solver.planes(), parts, rank, rows, group)
-    for _ in range(max(0, _iterations(options) - 1)):
-        solver.step(1)
-        exchange(solver.planes(), parts, rank, rows, group)
-    return _own_rows(solver.finish(), parts[rank], rows)
+    decoded, records, iterations, stop = drive_rank(solver, parts, rank, rows, group)
+    return StripSolution(_own_rows(decoded, parts[rank], rows), _history(records), iterations, stop)

@@ -1,7 +1,9 @@
 """One picture in row strips (unround.strips.solve_in_strips): the strips' solvers on one GPU with
 their halo rows swapped after every iteration, against the whole picture solved at once
 (unround_solve): the canvas to binary32 rounding (rel L2 <= 1e-5, max |difference| <= 1e-3 on
-0-255), grey and colour, TV and TGV, heights that are not whole bands, two to four strips."""
+0-255), grey and colour, TV and TGV, heights that are not whole bands, two to four strips; and
+the records the strips add up across the ranks (every 10 iterations, TGV's scaling and partial
+gap among them) within 1e-9 of the whole solve's, with the same stop at a tolerance."""
 
 import numpy as np
 import pytest
@@ -25,7 +27,7 @@ def test_strips_equal_the_whole_solve(name, kind, shape, options, strips):
     image = make(*shape, quality=60, seed=len(name), noise=2.0).image
     given = [*options, "--iterations", "60", "--tolerance", "0", "--record-every", "0"]
     whole = native.solve(image, given).canvas
-    parts = solve_in_strips(image, given, strips)
+    parts = solve_in_strips(image, given, strips).canvas
     assert parts.shape == whole.shape
     difference = parts - whole
     assert np.linalg.norm(difference) / np.linalg.norm(whole) <= 1e-5, name
@@ -52,9 +54,55 @@ def test_the_distributed_form_on_one_rank():
     given = ["--method", "tgv", "--iterations", "30", "--tolerance", "0", "--record-every", "0"]
     dist.init_process_group("nccl", rank=0, world_size=1)
     try:
-        mine = solve_strip(image, given)
+        mine = solve_strip(image, given).canvas
     finally:
         dist.destroy_process_group()
     whole = native.solve(image, given).canvas
     np.testing.assert_allclose(mine, whole, rtol=0, atol=1e-3)
     assert np.linalg.norm(mine - whole) / np.linalg.norm(whole) <= 1e-5
+
+
+RECORDED = [
+    ("grey-tgv-partial-2", "grey", (150, 96), ["--method", "tgv", "--partial-radius", "4"], 2),
+    ("colour420-tgv-3", "colour", (240, 88), ["--method", "tgv"], 3),
+    ("grey-tv-2", "grey", (130, 72), ["--method", "tv"], 2),
+]
+
+
+@pytest.mark.parametrize("name, kind, shape, options, strips", RECORDED, ids=[c[0] for c in RECORDED])
+def test_strips_records_equal_the_whole_solve(name, kind, shape, options, strips):
+    from unround import native, synthetic
+    from unround.strips import solve_in_strips
+
+    make = synthetic.grey if kind == "grey" else synthetic.colour
+    image = make(*shape, quality=50, seed=len(name), noise=2.0).image
+    given = [*options, "--iterations", "60", "--tolerance", "0", "--record-every", "10"]
+    whole = native.solve(image, given)
+    parts = solve_in_strips(image, given, strips)
+    mine, theirs = parts.history, whole.result.history
+    np.testing.assert_array_equal(mine.iterations, theirs.iterations)
+    for column in ("primal", "dual", "scaling", "partial_gap"):
+        np.testing.assert_allclose(getattr(mine, column), getattr(theirs, column), rtol=1e-9, atol=0,
+                                   err_msg=f"{name}: {column}")
+    assert parts.iterations == whole.result.iterations and parts.stop == int(whole.result.stop)
+    assert np.linalg.norm(parts.canvas - whole.canvas) / np.linalg.norm(whole.canvas) <= 1e-5
+
+
+def test_strips_stop_at_a_tolerance_with_the_whole_solve():
+    from unround import native, synthetic
+    from unround.strips import solve_in_strips
+
+    image = synthetic.grey(160, 120, quality=40, seed=71, noise=2.0).image
+    probe = ["--method", "tgv", "--iterations", "200", "--tolerance", "0", "--record-every", "10"]
+    history = native.solve(image, probe).result.history
+    per_sample = history.gap / (image.height * image.width)  # one channel, whole MCUs
+    # A tolerance between the records of iterations 50 and 60: the solve stops at 60.
+    assert per_sample[6] < per_sample[5] and np.all(per_sample[:6] > per_sample[6])
+    tolerance = float(np.sqrt(per_sample[6] * per_sample[5]))
+    given = ["--method", "tgv", "--iterations", "200", "--tolerance", repr(tolerance), "--record-every", "10"]
+    whole = native.solve(image, given)
+    parts = solve_in_strips(image, given, 2)
+    assert whole.result.stop is native.Stop.CONVERGED and whole.result.iterations == 60
+    assert parts.stop == 1 and parts.iterations == 60
+    np.testing.assert_allclose(parts.history.primal, whole.result.history.primal, rtol=1e-9, atol=0)
+    assert np.linalg.norm(parts.canvas - whole.canvas) / np.linalg.norm(whole.canvas) <= 1e-5

@@ -80,3 +80,105 @@ def test_gloo_ranks_swap_their_halos(world, bands):
         for k, plane in enumerate(results[rank]):
             expected = 1000.0 * k + part.low * rows + np.arange(plane.shape[0])
             np.testing.assert_array_equal(plane, np.repeat(expected[:, None], plane.shape[1], axis=1))
+
+
+class _FakeSolver:
+    """A strip's solver without a GPU: its record sums a function of the rank and the iteration
+    (the dual value nearing the primal as the iterations go), its planes CPU tensors."""
+
+    def __init__(self, rank: int, height: int) -> None:
+        import torch
+
+        self.rank, self.done, self.rows = rank, 0, None
+        self._planes = [torch.zeros((height, 4)) for _ in range(3)]
+
+    @staticmethod
+    def plan():
+        from unround.strips import StripPlan
+
+        return StripPlan(iterations=40, record_every=5, tolerance=0.005, relative_tolerance=0.0,
+                         partial_tolerance=0.0, partial_radius=3.0, alpha=1.0, alpha1=1.0, alpha0=2.0, tgv=True)
+
+    def set_rows(self, first: int, end: int) -> None:
+        self.rows = (first, end)
+
+    def step(self, iterations: int = 1) -> None:
+        self.done += iterations
+
+    def planes(self) -> list:
+        return self._planes
+
+    @staticmethod
+    def firsts(rank: int, done: int) -> list[float]:
+        # G, first-order norms, second-order norms, largest |div2 r~|, samples.
+        return [100.0 + rank, 50.0 * (rank + 1), 20.0 + rank, 1.5 + 0.5 * rank + done * 0.01, 64.0 * (rank + 1)]
+
+    @staticmethod
+    def seconds(rank: int, done: int, theta: float) -> list[float]:
+        # The dual's conjugates (the dual value nears the primal, 433, as the iterations go), the
+        # partial gap's conjugates, its residual.
+        return [-(216.5 - 10.0 / (1 + done)), -(200.0 + rank), 0.25 * (rank + 1) * theta]
+
+    def record(self, advance: bool) -> list[float]:
+        if advance:
+            self.done += 1
+        return self.firsts(self.rank, self.done)
+
+    def record_duals(self, theta: float) -> list[float]:
+        return self.seconds(self.rank, self.done, theta)
+
+    def result(self, stop: int) -> tuple[int, int]:
+        return self.done, stop
+
+
+def _records_rank(rank: int, world: int, port: int, bands: int, results) -> None:
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from unround.strips import drive_rank, partition
+
+        rows = 8
+        parts = partition(bands, world)
+        solver = _FakeSolver(rank, (parts[rank].high - parts[rank].low) * rows)
+        result, records, iterations, stop = drive_rank(solver, parts, rank, rows)
+        results[rank] = (result, records, iterations, stop, solver.rows)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_ranks_take_the_same_records_and_stop():
+    """Two gloo ranks gather their record sums: both take the records that the sums of every
+    rank make (combine, in rank order), count only their own rows, and stop together at the first
+    record whose gap per sample meets the tolerance."""
+    from unround.strips import _met, combine, partition
+
+    world, bands = 2, 6
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    manager = mp.get_context("spawn").Manager()
+    results = manager.dict()
+    mp.start_processes(_records_rank, args=(world, port, bands, results), nprocs=world, join=True,
+                       start_method="spawn")
+    plan = _FakeSolver.plan()
+    expected, stop_at = [], None
+    for n in [0, *range(5, plan.iterations + 1, 5)]:
+        firsts = [_FakeSolver.firsts(r, n) for r in range(world)]
+        values, samples = combine(plan, firsts, lambda theta: [_FakeSolver.seconds(r, n, theta) for r in range(world)])
+        expected.append((n, 0.0, *values))
+        if _met(plan, values, samples):
+            stop_at = n
+            break
+    assert stop_at is not None and 0 < stop_at < plan.iterations
+    parts = partition(bands, world)
+    for rank in range(world):
+        (done, stop), records, iterations, stop_reason, rows = results[rank]
+        assert records == expected
+        assert iterations == stop_at and done == stop_at and stop == 1 and stop_reason == 1
+        assert rows == ((parts[rank].first - parts[rank].low) * 8, (parts[rank].end - parts[rank].low) * 8)
+    # TGV's scaling is alpha1 over the largest |div2 r~| of every rank's, not of one.
+    largest = max(_FakeSolver.firsts(r, 5)[3] for r in range(world))
+    assert expected[1][4] == (plan.alpha1 / largest if largest > plan.alpha1 else 1.0)
