@@ -19,8 +19,6 @@
 #include <atomic>
 #include <cfloat>
 #include <cstdint>
-#include <cstdlib>
-#include <string_view>
 
 #include "colour.hpp"
 #include "dct.cuh"
@@ -715,10 +713,6 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // Launched after the dual sweep it reads (programmatic stream serialization): the factors and
-  // barriers above were set up while the sweep finished; the state is read from here on.
-  grid_dependency_wait();
-  allow_dependents();
   const int items = (Q.items - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
                     static_cast<int>(gridDim.x);  // this CTA's
   // The levels of an item's blocks (NB block rows of B blocks), after the slots.
@@ -1316,16 +1310,6 @@ __global__ void __launch_bounds__(256) residual_kernel(const ResidualParams P) {
   cta_sum(value, P.partials);
 }
 
-__global__ void widen_kernel(const float* from, double* to, Geometry g) {
-  const std::size_t n = static_cast<std::size_t>(g.rows) * g.columns * g.channels;
-  for (std::size_t k = blockIdx.x * 256ull + threadIdx.x; k < n; k += static_cast<std::size_t>(gridDim.x) * 256) {
-    const std::size_t c = k / (static_cast<std::size_t>(g.rows) * g.columns);
-    const std::size_t rest = k % (static_cast<std::size_t>(g.rows) * g.columns);
-    const std::size_t i = rest / g.columns, j = rest % g.columns;
-    to[k] = from[c * g.plane + i * g.pitch + j];
-  }
-}
-
 __global__ void narrow_kernel(const double* from, float* to, Geometry g) {
   const std::size_t n = static_cast<std::size_t>(g.rows) * g.columns * g.channels;
   for (std::size_t k = blockIdx.x * 256ull + threadIdx.x; k < n; k += static_cast<std::size_t>(gridDim.x) * 256) {
@@ -1449,16 +1433,13 @@ int primal_grid_blocks(const Geometry& g, const ComponentDevice& c) {
   const dim3 d = primal_grid(g, c.cell_rows, c.cell_columns);
   return static_cast<int>(d.x * d.y);
 }
-int conjugate_grid_blocks(const Geometry& g, const ComponentDevice& c) { return primal_grid_blocks(g, c); }
-int start_grid_blocks(const ComponentDevice& c) { return (c.block_rows * c.block_columns * 8 + 255) / 256; }
-
-bool dependent_launches() {
-  static const bool on = [] {
-    const char* value = std::getenv("UNROUND_B200_LAUNCH");
-    return value == nullptr || std::string_view(value) != "plain";
-  }();
-  return on;
+// The conjugate kernel's CTAs (one per block_grid cell: 4 block columns by kWarps block rows),
+// each of which writes one partial sum.
+int conjugate_grid_blocks(const Geometry& g, const ComponentDevice& c) {
+  const dim3 d = block_grid(g, c);
+  return static_cast<int>(d.x * d.y);
 }
+int start_grid_blocks(const ComponentDevice& c) { return (c.block_rows * c.block_columns * 8 + 255) / 256; }
 
 cudaError_t launch_dual(const DualParams& p, bool tgv, bool coupled, bool keep, cudaStream_t stream) {
   return tgv ? dual_channels<true>(p, coupled, keep, stream) : dual_channels<false>(p, coupled, keep, stream);
@@ -1501,7 +1482,8 @@ cudaError_t primal_tma_one(const CUtensorMap* maps, const PrimalParams* parts, i
   batch.items = count * batch.strips * batch.stages;
   *grid = std::min(batch.items, slots);
   if (*grid <= 0) return cudaSuccess;  // no block row
-  return launch_after(kernel, dim3(*grid), dim3(threads), bytes, s, maps[0], maps[count > 1 ? 1 : 0], batch);
+  kernel<<<*grid, threads, bytes, s>>>(maps[0], maps[count > 1 ? 1 : 0], batch);
+  return cudaGetLastError();
 }
 
 template <int CR, int CC>
@@ -1625,11 +1607,6 @@ cudaError_t launch_conjugate(const ConjugateParams& p, cudaStream_t stream) {
 
 cudaError_t launch_residual(const ResidualParams& p, cudaStream_t stream) {
   residual_kernel<<<pixel_grid(p.g), dim3(32, 8), 0, stream>>>(p);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_widen(const float* from, double* to, const Geometry& g, cudaStream_t stream) {
-  widen_kernel<<<1184, 256, 0, stream>>>(from, to, g);
   return cudaGetLastError();
 }
 

@@ -16,31 +16,6 @@ namespace urb {
 
 constexpr int kMaxChannels = 3;
 
-// Whether the iteration's kernels are launched with programmatic stream serialization (on,
-// unless UNROUND_B200_LAUNCH=plain): each may then be scheduled while the one before it in the
-// stream finishes, its CTAs doing their set-up as SMs free up and waiting (griddepcontrol.wait)
-// before they touch what that kernel writes.
-bool dependent_launches();
-
-// Launches `kernel` on `stream` after the work before it, as dependent_launches() says. Only a
-// kernel that calls grid_dependency_wait (tma.cuh) before its first global access to what the
-// kernel before it writes may be launched so.
-template <typename... Params, typename... Args>
-cudaError_t launch_after(void (*kernel)(Params...), dim3 grid, dim3 block, std::size_t bytes, cudaStream_t stream,
-                         Args&&... args) {
-  cudaLaunchConfig_t config = {};
-  config.gridDim = grid;
-  config.blockDim = block;
-  config.dynamicSmemBytes = bytes;
-  config.stream = stream;
-  cudaLaunchAttribute attribute = {};
-  attribute.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attribute.val.programmaticStreamSerializationAllowed = 1;
-  config.attrs = &attribute;
-  config.numAttrs = dependent_launches() ? 1 : 0;
-  return cudaLaunchKernelEx(&config, kernel, static_cast<Args&&>(args)...);
-}
-
 // The per-frequency factors of a component's proximal map in binary32, for one step tau
 // (docs/math.md 4.1, 4.4; cpp/src/model.cpp:483-497), with t = (tau / n_c) m and
 // r = 1 / (1 + t): z = (e + t c) r = e r + (t r) c, clipped to q Q -+ (1/2 + s) Q. They are
@@ -455,7 +430,6 @@ cudaError_t launch_dual_samples(const CUtensorMap& state, const CUtensorMap& til
 cudaError_t launch_samples_iteration(const CUtensorMap& state, const CUtensorMap& tilde,
                                      const SamplesIterationParams& p, bool tgv, bool coupled, cudaStream_t stream);
 
-cudaError_t launch_widen(const float* from, double* to, const Geometry& g, cudaStream_t stream);
 cudaError_t launch_narrow(const double* from, float* to, const Geometry& g, cudaStream_t stream);
 
 }  // namespace urb

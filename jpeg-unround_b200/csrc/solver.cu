@@ -710,6 +710,14 @@ struct Solver::Impl {
   // The binary64 result from the last kept coefficients (docs/math.md 5: the canvas whose
   // coefficients are zeta).
   void result(Outcome& out) {
+    make_canvas();
+    if (host_result) fetch(out);
+  }
+
+  // The binary64 canvas of the last kept tilde point into `canvas` (channels x rows x columns),
+  // as the result has it: the coefficients zeta restored to binary64 and clipped to their
+  // intervals, the canvas whose coefficients they are.
+  void make_canvas() {
     const std::size_t size = static_cast<std::size_t>(g.rows) * g.columns;
     if (samples != nullptr) {
       // The last tilde point in binary64, each sample clipped to its interval.
@@ -733,7 +741,6 @@ struct Solver::Impl {
       cp.mode = 1;
       if (error == cudaSuccess) error = launch_canvas(cp, stream);
     }
-    if (host_result) fetch(out);
   }
 
   // The picture's 8- or 16-bit levels into host memory `out` (height x width x its channels,
@@ -898,8 +905,9 @@ bool Solver::run(std::uint64_t first, const Observer& observer, Outcome& out, Fa
       return true;
     }
     if (observer && out.records.size() > 1) {
+      // The record's canvas as the result would have it, were the solve to stop here.
       const Geometry whole = m.g;
-      if (m.error == cudaSuccess) m.error = launch_widen(m.xt, m.canvas, whole, m.stream);
+      m.make_canvas();
       std::vector<double> host(static_cast<std::size_t>(whole.channels) * whole.rows * whole.columns);
       if (m.error == cudaSuccess) {
         m.error = cudaMemcpyAsync(host.data(), m.canvas, host.size() * sizeof(double), cudaMemcpyDeviceToHost, m.stream);

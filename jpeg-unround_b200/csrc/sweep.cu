@@ -82,10 +82,6 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // Launched after the primal step it reads (programmatic stream serialization): everything
-  // above ran while that step finished; from here on the state and x~ are read and written.
-  grid_dependency_wait();
-  allow_dependents();
   auto issue = [&](int k) {
     if (threadIdx.x == 0 && k <= chunks) {
       const int slot = k % kSlots;
@@ -515,7 +511,8 @@ cudaError_t launch_one(const CUtensorMap& state, const CUtensorMap& tilde, const
   DualParams q = p;
   q.strip_rows = strip_rows_for(p.g, slots);
   const dim3 grid((p.g.columns + 31) / 32, (p.g.rows + q.strip_rows - 1) / q.strip_rows, 1);
-  return launch_after(kernel, grid, dim3(kThreads), bytes, s, state, tilde, q);
+  kernel<<<grid, kThreads, bytes, s>>>(state, tilde, q);
+  return cudaGetLastError();
 }
 
 template <bool TGV, int C, bool COUPLED>

@@ -47,17 +47,6 @@ __device__ __forceinline__ bool barrier_wait(std::uint64_t* bar, unsigned parity
   return false;
 }
 
-// Programmatic dependent launch: a kernel launched with programmatic stream serialization may
-// start while the kernel before it in the stream is still running. It waits here, before its
-// first access to global memory that the kernel before it writes or reads, until that kernel
-// has completed and its writes are visible; launched without it, the wait returns at once.
-__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
-// Lets the kernel after this one in the stream (launched with programmatic stream
-// serialization) be scheduled once every CTA of this grid has said so or exited: its CTAs then
-// take SMs as this grid's leave, do their set-up, and wait in grid_dependency_wait.
-__device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
 __device__ __forceinline__ void load_box(float* to, const CUtensorMap* map, std::uint64_t* bar, int x, int y, int z) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "

@@ -65,19 +65,21 @@ def _dct_matrix() -> torch.Tensor:
 class Reference:
     """The unrolled map in float64 of a problem's constants (moved to the CPU)."""
 
-    def __init__(self, problem, relaxation: float | None = None) -> None:
-        # The problem's constants in binary64, as the host model made them.
+    def __init__(self, problem, relaxation: float | None = None, dtype: torch.dtype = torch.float64) -> None:
+        # The problem's constants as the host model made them (binary64), in `dtype`: float64 is
+        # the reference; float32 runs the same map in binary32, which measures how far that
+        # arithmetic alone moves the map and its gradient.
         host = {k: torch.from_numpy(v) for k, v in problem.host.items()}
-        self.lower = host["lower"].to(torch.float64)  # (B, by, bx, 64)
-        self.upper = host["upper"].to(torch.float64)
-        self.centre = host["centre"].to(torch.float64)
-        self.middle = host["middle"].to(torch.float64)  # (B, by, bx)
-        self.weight = host["weight"].to(torch.float64)  # (B, 64)
-        self.flat_weight = host["flat_weight"].to(torch.float64)
+        self.lower = host["lower"].to(dtype)  # (B, by, bx, 64)
+        self.upper = host["upper"].to(dtype)
+        self.centre = host["centre"].to(dtype)
+        self.middle = host["middle"].to(dtype)  # (B, by, bx)
+        self.weight = host["weight"].to(dtype)  # (B, 64)
+        self.flat_weight = host["flat_weight"].to(dtype)
         self.flat = host["flat"] != 0  # (B, by, bx)
-        self.start = host["start"].to(torch.float64)  # (B, H, W)
+        self.start = host["start"].to(dtype)  # (B, H, W)
         self.rho = problem.relaxation if relaxation is None else relaxation
-        self.c = _dct_matrix()
+        self.c = _dct_matrix().to(dtype)
 
     def _blocks(self, canvas: torch.Tensor) -> torch.Tensor:
         b, h, w = canvas.shape
