@@ -1232,7 +1232,8 @@ __global__ void __launch_bounds__(256) conjugate_kernel(const ConjugateParams P)
   const int j0 = vbx * BW + m * CC, i0 = vby * BH;
   const bool counted = P.g.recorded_row(i0);
   // xi = gamma div q at the lane's samples, q = scale (q1, q2).
-  auto q_at = [&](const float* f, int i, int j) -> double { return P.scale * static_cast<double>(f[static_cast<std::size_t>(i) * pitch + j]); };
+  const double scale = P.most_at != nullptr ? negative_theta(*P.most_at, P.alpha1) : P.scale;
+  auto q_at = [&](const float* f, int i, int j) -> double { return scale * static_cast<double>(f[static_cast<std::size_t>(i) * pitch + j]); };
   double xi[BH][CC];
   double sums[8], means[8];
   double total = 0.0;
@@ -1308,6 +1309,19 @@ __global__ void __launch_bounds__(256) residual_kernel(const ResidualParams P) {
     value = sqrt(a * a + b * b);
   }
   cta_sum(value, P.partials);
+}
+
+// One array of partials a CTA: the sum (or the largest) of its entries, each thread's strided
+// share in index order, then the CTA's fixed-order reduction.
+__global__ void __launch_bounds__(512) reduce_kernel(const __grid_constant__ Reductions R) {
+  const int k = blockIdx.x;
+  const double* in = R.in[k];
+  const int n = R.count[k];
+  const bool most = R.largest[k] != 0;
+  double value = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) value = most ? fmax(value, in[i]) : value + in[i];
+  const double total = most ? cta_reduce<true>(value) : cta_reduce<false>(value);
+  if (threadIdx.x == 0) R.out[k] = total;
 }
 
 __global__ void narrow_kernel(const double* from, float* to, Geometry g) {
@@ -1603,6 +1617,12 @@ cudaError_t launch_norms(const NormParams& p, bool tgv, bool coupled, cudaStream
 
 cudaError_t launch_conjugate(const ConjugateParams& p, cudaStream_t stream) {
   return by_cells<ConjugateLaunch>(p.component.cell_rows, p.component.cell_columns, p, stream);
+}
+
+cudaError_t launch_reductions(const Reductions& r, cudaStream_t stream) {
+  if (r.n == 0) return cudaSuccess;
+  reduce_kernel<<<r.n, 512, 0, stream>>>(r);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_residual(const ResidualParams& p, cudaStream_t stream) {

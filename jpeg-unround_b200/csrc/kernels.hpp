@@ -155,11 +155,39 @@ struct ConjugateParams {
   const float* q1 = nullptr;  // the field whose divergence xi is: p~, or div_2 r~ scaled
   const float* q2 = nullptr;
   double scale = 1.0;   // q = scale * (q1, q2): 1 for p~, -theta for div_2 r~
+  // Where given, the scale is -theta, theta = min(1, alpha1 / most) with `most` (the largest
+  // |div_2 r~| of a record) read from the device, so that no host round trip comes between a
+  // record's norms and its conjugates.
+  const double* most_at = nullptr;
+  double alpha1 = 1.0;
   double gamma = 1.0;   // xi = gamma div q
   double radius = 255.0;  // R of the free samples (docs/math.md 6.6)
   int free = 0;
   double* partials = nullptr;  // 1 per CTA
 };
+
+// -theta of a record from its largest |div_2 r~| (the host's formula, operation for operation).
+__host__ __device__ inline double negative_theta(double most, double alpha1) {
+  return -(most > alpha1 ? alpha1 / most : 1.0);
+}
+
+// Sums (or largest values) of arrays of per-CTA partials, each by one CTA in a fixed order:
+// out[k] of the k-th array. A record's sums, taken on the device and copied back at once.
+constexpr int kMaxReductions = 16;
+struct Reductions {
+  const double* in[kMaxReductions] = {};
+  int count[kMaxReductions] = {};
+  int largest[kMaxReductions] = {};
+  int n = 0;
+  double* out = nullptr;
+  int add(const double* array, int entries, bool most = false) {
+    in[n] = array;
+    count[n] = entries;
+    largest[n] = most ? 1 : 0;
+    return n++;
+  }
+};
+cudaError_t launch_reductions(const Reductions& r, cudaStream_t stream);
 
 struct ResidualParams {
   Geometry g;
@@ -277,6 +305,8 @@ struct SamplesConjugateParams {
   const float* q1 = nullptr;
   const float* q2 = nullptr;
   double scale = 1.0;
+  const double* most_at = nullptr;  // where given, the scale is negative_theta(*most_at, alpha1)
+  double alpha1 = 1.0;
   double gamma = 1.0;
   double mu = 0.0;
   const std::uint16_t* levels = nullptr;  // the channel's plane

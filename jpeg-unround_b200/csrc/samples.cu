@@ -117,8 +117,9 @@ __global__ void __launch_bounds__(256) samples_conjugate_kernel(const SamplesCon
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
   double term = 0.0;
   if (i < rows && j < columns) {
+    const double scale = P.most_at != nullptr ? negative_theta(*P.most_at, P.alpha1) : P.scale;
     auto q_at = [&](const float* f, int ii, int jj) -> double {
-      return P.scale * static_cast<double>(f[static_cast<std::size_t>(ii) * pitch + jj]);
+      return scale * static_cast<double>(f[static_cast<std::size_t>(ii) * pitch + jj]);
     };
     const double dy = (i + 1 < rows ? q_at(P.q2, i, j) : 0.0) - (i > 0 ? q_at(P.q2, i - 1, j) : 0.0);
     const double dx = (j + 1 < columns ? q_at(P.q1, i, j) : 0.0) - (j > 0 ? q_at(P.q1, i, j - 1) : 0.0);

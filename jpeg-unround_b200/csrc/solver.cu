@@ -59,6 +59,8 @@ struct Solver::Impl {
   float* div2 = nullptr;
   double* canvas = nullptr;
   double* partials = nullptr;        // record reductions
+  double* record_partials = nullptr;  // a record's conjugates and residuals, a region each
+  double* record_sums = nullptr;      // a record's sums (2 x kMaxReductions)
   double* value_partials = nullptr;  // the data term of the last kept primal step, per component
   std::size_t partial_count = 0;
   std::vector<int> value_counts;
@@ -267,6 +269,15 @@ struct Solver::Impl {
     }
     partial_count = most;
     partials = allocate<double>(most);
+    {
+      std::size_t regions = 0;
+      const std::size_t channels = samples != nullptr ? samples->channels : components.size();
+      for (std::size_t c = 0; c < channels; ++c) {
+        regions += 2 * static_cast<std::size_t>(conjugate_count(c)) + norms_grid_blocks(g);
+      }
+      record_partials = allocate<double>(std::max<std::size_t>(regions, 1));
+      record_sums = allocate<double>(2 * kMaxReductions);
+    }
     std::size_t values = 0;
     for (int count : value_counts) values += count;
     if (samples != nullptr) values += samples_grid_blocks(g, g.channels);
@@ -592,6 +603,21 @@ struct Solver::Impl {
 
   // G* of channel c at xi = gamma div(scale q) (cpp/src/frames.cpp:428-493).
   double conjugate(std::size_t c, const float* q1, const float* q2, double scale) {
+    return sum_of(partials, conjugate_into(c, q1, q2, scale, nullptr, partials));
+  }
+
+  // The per-CTA partials of G* of channel c into `out`; returns their count. With `most_at`,
+  // the scale is -theta of the largest |div_2 r~| read there (negative_theta).
+  int conjugate_count(std::size_t c) const {
+    if (samples != nullptr) {
+      Geometry one = g;
+      one.channels = 1;
+      return samples_grid_blocks(one, 1);
+    }
+    return conjugate_grid_blocks(g, components[c]);
+  }
+  int conjugate_into(std::size_t c, const float* q1, const float* q2, double scale, const double* most_at,
+                     double* out) {
     if (samples != nullptr) {
       SamplesConjugateParams sp;
       sp.g = g;
@@ -599,13 +625,15 @@ struct Solver::Impl {
       sp.q1 = q1;
       sp.q2 = q2;
       sp.scale = scale;
+      sp.most_at = most_at;
+      sp.alpha1 = plan.alpha1;
       sp.gamma = plan.channel_weights[c];
       sp.mu = samples->mu;
       sp.levels = s_levels + c * g.plane;
       sp.ends64 = s_ends64;
-      sp.partials = partials;
+      sp.partials = out;
       if (error == cudaSuccess) error = launch_samples_conjugate(sp, stream);
-      return sum_of(partials, samples_grid_blocks(sp.g, 1));
+      return conjugate_count(c);
     }
     ConjugateParams cp;
     cp.g = g;
@@ -613,12 +641,14 @@ struct Solver::Impl {
     cp.q1 = q1;
     cp.q2 = q2;
     cp.scale = scale;
+    cp.most_at = most_at;
+    cp.alpha1 = plan.alpha1;
     cp.gamma = plan.channel_weights[c];
     cp.radius = plan.free_radius;
     cp.free = frame.components[c].free ? 1 : 0;
-    cp.partials = partials;
+    cp.partials = out;
     if (error == cudaSuccess) error = launch_conjugate(cp, stream);
-    return sum_of(partials, conjugate_grid_blocks(g, components[c]));
+    return conjugate_count(c);
   }
 
   // The channels of the data term: the components, or the samples' channels.
@@ -686,24 +716,95 @@ struct Solver::Impl {
     return s;
   }
 
-  // The record of the tilde point (cpp/src/primal_dual.hpp:446-501).
+  // The record of the tilde point (cpp/src/primal_dual.hpp:446-501), its kernels back to back
+  // with no host round trip among them: the norms, then every sum reduced on the device (the
+  // norms, the largest |div_2 r~|, the data term of each component), the conjugates at the theta
+  // those give (read on the device), their sums, and one copy of the sums to the host.
   Record record(std::uint64_t iteration) {
     Record r;
     r.iteration = iteration;
     r.scaling = kNaN;
     r.partial_gap = kNaN;
-    const FirstSums f = first_sums();
+    NormParams np;
+    np.g = g;
+    np.xt = xt;
+    np.tilde = tilde;
+    np.div2 = div2;
+    for (int c = 0; c < g.channels; ++c) np.weight[c] = plan.channel_weights[c];
+    np.partials = partials;
+    if (error == cudaSuccess) error = launch_norms(np, tgv, plan.coupled, stream);
+    const int count = norms_grid_blocks(g);
+    Reductions first;
+    first.out = record_sums;
+    const int at_first = first.add(partials, count);
+    const int at_second = tgv ? first.add(partials + count, count) : -1;
+    const int at_most = tgv ? first.add(partials + 2 * count, count, true) : -1;
+    std::vector<int> at_data;
+    if (samples != nullptr) {
+      at_data.push_back(first.add(value_partials, static_cast<int>(samples_written)));
+    } else {
+      for (std::size_t c = 0; c < components.size(); ++c) {
+        at_data.push_back(first.add(value_slot(c), static_cast<int>(value_written[c])));
+      }
+    }
+    if (error == cudaSuccess) error = launch_reductions(first, stream);
+    // The conjugates of each channel into regions of their own, then their sums.
+    Reductions second;
+    second.out = record_sums + kMaxReductions;
+    double* region = record_partials;
+    std::vector<int> at_dual, at_partial, at_residual;
+    const double* most_at = tgv ? record_sums + at_most : nullptr;
+    for (std::size_t c = 0; c < data_channels(); ++c) {
+      const float* q1 = tgv ? div2 + 2 * c * g.plane : tilde.p1 + c * g.plane;
+      const float* q2 = tgv ? div2 + (2 * c + 1) * g.plane : tilde.p2 + c * g.plane;
+      const int n = conjugate_into(c, q1, q2, 1.0, most_at, region);
+      at_dual.push_back(second.add(region, n));
+      region += n;
+    }
+    if (tgv && plan.partial_radius) {
+      for (std::size_t c = 0; c < data_channels(); ++c) {
+        const int n = conjugate_into(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0, nullptr, region);
+        at_partial.push_back(second.add(region, n));
+        region += n;
+        ResidualParams rp;
+        rp.g = g;
+        rp.p1 = tilde.p1 + c * g.plane;
+        rp.p2 = tilde.p2 + c * g.plane;
+        rp.d1 = div2 + 2 * c * g.plane;
+        rp.d2 = div2 + (2 * c + 1) * g.plane;
+        rp.partials = region;
+        if (error == cudaSuccess) error = launch_residual(rp, stream);
+        at_residual.push_back(second.add(region, count));
+        region += count;
+      }
+    }
+    if (error == cudaSuccess) error = launch_reductions(second, stream);
+    double sums[2 * kMaxReductions] = {};
+    if (error == cudaSuccess) {
+      error = cudaMemcpyAsync(sums, record_sums, sizeof(sums), cudaMemcpyDeviceToHost, stream);
+    }
+    if (error == cudaSuccess) error = cudaStreamSynchronize(stream);
+    if (error != cudaSuccess) return r;
+    const double* second_sums = sums + kMaxReductions;
+    double data = 0.0;
+    for (int k : at_data) data += sums[k];
+    double conjugates = 0.0;
+    for (int k : at_dual) conjugates += second_sums[k];
+    r.dual = -conjugates;
     if (!tgv) {
-      r.primal = plan.alpha * f.first + f.data;
-      r.dual = -second_sums(1.0).conjugates;
+      r.primal = plan.alpha * sums[at_first] + data;
       return r;
     }
-    r.primal = (plan.alpha1 * f.first + plan.alpha0 * f.second) + f.data;
-    const double theta = f.most > plan.alpha1 ? plan.alpha1 / f.most : 1.0;
-    r.scaling = theta;
-    const SecondSums s = second_sums(theta);
-    r.dual = -s.conjugates;
-    if (plan.partial_radius) r.partial_gap = r.primal + s.partial + *plan.partial_radius * s.residual;
+    r.primal = (plan.alpha1 * sums[at_first] + plan.alpha0 * sums[at_second]) + data;
+    r.scaling = -negative_theta(sums[at_most], plan.alpha1);
+    if (plan.partial_radius) {
+      double partial = 0.0, residual = 0.0;
+      for (std::size_t c = 0; c < at_partial.size(); ++c) {
+        partial += second_sums[at_partial[c]];
+        residual += plan.channel_weights[c] * second_sums[at_residual[c]];
+      }
+      r.partial_gap = r.primal + partial + *plan.partial_radius * residual;
+    }
     return r;
   }
 
