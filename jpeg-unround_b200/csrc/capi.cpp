@@ -12,6 +12,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -44,9 +45,11 @@ struct unround_result {
   }
   std::vector<std::uint64_t> record_iterations;
   std::vector<double> record_values[5];
-  // What the model holds, made when first asked for (rust/capi/src/lib.rs:888-930).
+  // What the model holds, made when first asked for (rust/capi/src/lib.rs:888-930): each
+  // component's lower ends, upper ends and centres, coefficient by coefficient.
   mutable std::once_flag problem_once;
-  mutable std::vector<std::vector<double>> problem[3];
+  mutable std::vector<std::unique_ptr<double[]>> problem[3];
+  mutable std::vector<std::size_t> problem_sizes;
   std::vector<std::vector<double>> steps, weights;
   // What the file held besides its picture (unround_result_format and the rest).
   std::int32_t format = UNROUND_FORMAT_JPEG;
@@ -1012,26 +1015,41 @@ const double* unround_result_problem(const unround_result* result, uint64_t comp
   }
   try {
     std::call_once(result->problem_once, [result] {
+      // Blocks of coefficients shared out among the host's threads, each filling (and first
+      // touching) its own part of the three arrays.
+      const unsigned threads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
       for (const urb::Component& c : result->frame.components) {
         const std::size_t n = c.coefficient_count();
-        std::vector<double> lower(n), upper(n), centres(n);
-        for (std::size_t at = 0; at < n; ++at) {
-          const int k = static_cast<int>(at % 64);
-          lower[at] = c.lower(c.levels[at], k);
-          upper[at] = c.upper(c.levels[at], k);
-          centres[at] = c.centre(c.levels[at], k);
+        auto lower = std::make_unique_for_overwrite<double[]>(n);
+        auto upper = std::make_unique_for_overwrite<double[]>(n);
+        auto centres = std::make_unique_for_overwrite<double[]>(n);
+        auto fill = [&](std::size_t first, std::size_t end) {
+          for (std::size_t at = first; at < end; ++at) {
+            const int k = static_cast<int>(at % 64);
+            lower[at] = c.lower(c.levels[at], k);
+            upper[at] = c.upper(c.levels[at], k);
+            centres[at] = c.centre(c.levels[at], k);
+          }
+        };
+        const std::size_t blocks = n / 64;
+        const unsigned parts = static_cast<unsigned>(std::min<std::size_t>(threads, std::max<std::size_t>(blocks / 4096, 1)));
+        std::vector<std::thread> workers;
+        for (unsigned t = 1; t < parts; ++t) {
+          workers.emplace_back(fill, blocks * t / parts * 64, blocks * (t + 1) / parts * 64);
         }
+        fill(0, blocks / parts * 64);
+        for (std::thread& w : workers) w.join();
         result->problem[0].push_back(std::move(lower));
         result->problem[1].push_back(std::move(upper));
         result->problem[2].push_back(std::move(centres));
+        result->problem_sizes.push_back(n);
       }
     });
   } catch (...) {
     return nullptr;
   }
-  const std::vector<double>& values = result->problem[which][component];
-  put(count, values.size());
-  return values.data();
+  put(count, result->problem_sizes[component]);
+  return result->problem[which][component].get();
 }
 
 unround_status unround_result_component(const unround_result* result, uint64_t component, uint64_t* rows,

@@ -1099,75 +1099,144 @@ __global__ void project_kernel(Fields f, Geometry g, int tgv, int coupled, float
 // 791-895): the norms of the pixels, TGV's div2 r~ and its largest norm; G* of a field
 // (cpp/src/frames.cpp:428-487, model.cpp:74-111); the residual of the partial gap.
 
+// The records' norms as a sweep: a warp owns 32 columns and walks down kNormRows rows, so that
+// every plane is read once -- the row below one row ahead, the row above kept in registers, the
+// neighbours across by shuffles (lane 0 reads column x0 - 1, lane 31 column x0 + 32). At each
+// pixel, in binary64 from the binary32 tilde point: |grad x~ - w~| (the first-order term),
+// |E w~|_F (the second-order term) and div2 r~ (written, binary32) and its norm, each operation
+// as the per-pixel form of cpp/src/primal_dual.hpp:836-895 orders it. Rows outside the record
+// rows add nothing (div2 is still made for them).
+constexpr int kNormRows = 64;
+
 template <bool TGV, int C, bool COUPLED>
 __global__ void __launch_bounds__(256) norms_kernel(const NormParams P) {
-  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y;
+  const int lane = threadIdx.x;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
-  double first = 0.0, second = 0.0, most = 0.0;
-  if (i < rows && j < columns) {
-    const std::size_t at = static_cast<std::size_t>(i) * pitch + j;
-    double square = 0.0;
-    for (int c = 0; c < C; ++c) {
-      const std::size_t base = c * P.g.plane;
-      const double gamma = P.weight[c];
-      const double here = P.xt[base + at];
-      double gx = j + 1 < columns ? static_cast<double>(P.xt[base + at + 1]) - here : 0.0;
-      double gy = i + 1 < rows ? static_cast<double>(P.xt[base + at + pitch]) - here : 0.0;
+  const std::size_t plane = P.g.plane;
+  const int x0 = blockIdx.x * 32;
+  const int j = x0 + lane;
+  const bool valid = j < columns;
+  const int jc = valid ? j : columns - 1;
+  const bool has_left = j > 0, has_right = j + 1 < columns;
+  const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kNormRows;
+  const int i1 = min(i0 + kNormRows, rows);
+  constexpr unsigned kAll = 0xffffffffu;
+  auto at = [&](int c, int i, int col) -> std::size_t {
+    return c * plane + static_cast<std::size_t>(i) * pitch + col;
+  };
+  // The lane's values of the current row i (xt, r) and of the row above (w).
+  float xt[C], r11[C], r22[C], r12[C], w1_above[C], w2_above[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    xt[c] = r11[c] = r22[c] = r12[c] = w1_above[c] = w2_above[c] = 0.0f;
+    if (i0 < i1) {
+      xt[c] = P.xt[at(c, i0, jc)];
       if constexpr (TGV) {
-        gx = gx - static_cast<double>(P.tilde.w1[base + at]);
-        gy = gy - static_cast<double>(P.tilde.w2[base + at]);
+        r11[c] = P.tilde.r11[at(c, i0, jc)];
+        r22[c] = P.tilde.r22[at(c, i0, jc)];
+        r12[c] = P.tilde.r12[at(c, i0, jc)];
+        if (i0 > 0) {
+          w1_above[c] = P.tilde.w1[at(c, i0 - 1, jc)];
+          w2_above[c] = P.tilde.w2[at(c, i0 - 1, jc)];
+        }
+      }
+    }
+  }
+  double first = 0.0, second = 0.0, most = 0.0;
+  for (int i = i0; i < i1; ++i) {
+    const bool has_down = i + 1 < rows;
+    const bool counted = valid && P.g.recorded_row(i);
+    double square = 0.0, first_here = 0.0;
+    double square2 = 0.0, second_here = 0.0;
+    double square3 = 0.0, most_here = 0.0;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const double gamma = P.weight[c];
+      // The row below (one ahead), and the right neighbours across.
+      const float xt_down = has_down ? P.xt[at(c, i + 1, jc)] : 0.0f;
+      float xt_right = __shfl_down_sync(kAll, xt[c], 1);
+      if (lane == 31) xt_right = x0 + 32 < columns ? P.xt[at(c, i, x0 + 32)] : 0.0f;
+      float w1 = 0.0f, w2 = 0.0f, w1_left = 0.0f, w2_left = 0.0f;
+      if constexpr (TGV) {
+        w1 = P.tilde.w1[at(c, i, jc)];
+        w2 = P.tilde.w2[at(c, i, jc)];
+        w1_left = __shfl_up_sync(kAll, w1, 1);
+        w2_left = __shfl_up_sync(kAll, w2, 1);
+        if (lane == 0 && x0 > 0) {
+          w1_left = P.tilde.w1[at(c, i, x0 - 1)];
+          w2_left = P.tilde.w2[at(c, i, x0 - 1)];
+        }
+      }
+      const double here = xt[c];
+      double gx = has_right ? static_cast<double>(xt_right) - here : 0.0;
+      double gy = has_down ? static_cast<double>(xt_down) - here : 0.0;
+      if constexpr (TGV) {
+        gx = gx - static_cast<double>(w1);
+        gy = gy - static_cast<double>(w2);
       }
       square += (COUPLED ? gamma * gamma : 1.0) * (gx * gx + gy * gy);
       if constexpr (!COUPLED) {
-        first += gamma * sqrt(square);
+        first_here += gamma * sqrt(square);
         square = 0.0;
       }
-    }
-    if constexpr (COUPLED) first = sqrt(square);
-    if constexpr (TGV) {
-      square = 0.0;
-      for (int c = 0; c < C; ++c) {
-        const std::size_t base = c * P.g.plane;
-        const double gamma = P.weight[c];
-        const float* w1 = P.tilde.w1 + base;
-        const float* w2 = P.tilde.w2 + base;
+      if constexpr (TGV) {
         const bool last_c = j + 1 == columns, last_r = i + 1 == rows;
-        const double a1 = last_c ? 0.0 : w1[at], a2 = last_r ? 0.0 : w2[at];
-        const double b1 = last_r ? 0.0 : w1[at], b2 = last_c ? 0.0 : w2[at];
-        const double l1 = j > 0 ? w1[at - 1] : 0.0, l2 = j > 0 ? w2[at - 1] : 0.0;
-        const double u1 = i > 0 ? w1[at - pitch] : 0.0, u2 = i > 0 ? w2[at - pitch] : 0.0;
+        const double a1 = last_c ? 0.0 : w1, a2 = last_r ? 0.0 : w2;
+        const double b1 = last_r ? 0.0 : w1, b2 = last_c ? 0.0 : w2;
+        const double l1 = has_left ? w1_left : 0.0, l2 = has_left ? w2_left : 0.0;
+        const double u1 = i > 0 ? w1_above[c] : 0.0, u2 = i > 0 ? w2_above[c] : 0.0;
         const double exx = a1 - l1, eyy = a2 - u2, exy = 0.5 * ((b1 - u1) + (b2 - l2));
-        square += (COUPLED ? gamma * gamma : 1.0) * (exx * exx + eyy * eyy + 2.0 * (exy * exy));
+        square2 += (COUPLED ? gamma * gamma : 1.0) * (exx * exx + eyy * eyy + 2.0 * (exy * exy));
         if constexpr (!COUPLED) {
-          second += gamma * sqrt(square);
-          square = 0.0;
+          second_here += gamma * sqrt(square2);
+          square2 = 0.0;
         }
-      }
-      if constexpr (COUPLED) second = sqrt(square);
-      square = 0.0;
-      for (int c = 0; c < C; ++c) {
-        const std::size_t base = c * P.g.plane;
-        const float* r11 = P.tilde.r11 + base;
-        const float* r22 = P.tilde.r22 + base;
-        const float* r12 = P.tilde.r12 + base;
-        double d1 = j + 1 < columns ? static_cast<double>(r11[at + 1]) - r11[at] : 0.0;
-        double d2 = j + 1 < columns ? static_cast<double>(r12[at + 1]) - r12[at] : 0.0;
-        if (i + 1 < rows) {
-          d1 += static_cast<double>(r12[at + pitch]) - r12[at];
-          d2 += static_cast<double>(r22[at + pitch]) - r22[at];
+        w1_above[c] = w1;
+        w2_above[c] = w2;
+        // div2 r~ by forward differences.
+        float r11_right = __shfl_down_sync(kAll, r11[c], 1), r12_right = __shfl_down_sync(kAll, r12[c], 1);
+        if (lane == 31) {
+          const bool beyond = x0 + 32 < columns;
+          r11_right = beyond ? P.tilde.r11[at(c, i, x0 + 32)] : 0.0f;
+          r12_right = beyond ? P.tilde.r12[at(c, i, x0 + 32)] : 0.0f;
         }
-        P.div2[(2 * c) * P.g.plane + at] = static_cast<float>(d1);
-        P.div2[(2 * c + 1) * P.g.plane + at] = static_cast<float>(d2);
-        square += d1 * d1 + d2 * d2;
+        const float r12_down = has_down ? P.tilde.r12[at(c, i + 1, jc)] : 0.0f;
+        const float r22_down = has_down ? P.tilde.r22[at(c, i + 1, jc)] : 0.0f;
+        double d1 = has_right ? static_cast<double>(r11_right) - r11[c] : 0.0;
+        double d2 = has_right ? static_cast<double>(r12_right) - r12[c] : 0.0;
+        if (has_down) {
+          d1 += static_cast<double>(r12_down) - r12[c];
+          d2 += static_cast<double>(r22_down) - r22[c];
+        }
+        if (valid) {
+          P.div2[(2 * c) * plane + static_cast<std::size_t>(i) * pitch + j] = static_cast<float>(d1);
+          P.div2[(2 * c + 1) * plane + static_cast<std::size_t>(i) * pitch + j] = static_cast<float>(d2);
+        }
+        square3 += d1 * d1 + d2 * d2;
         if constexpr (!COUPLED) {
-          most = fmax(most, sqrt(square));
-          square = 0.0;
+          most_here = fmax(most_here, sqrt(square3));
+          square3 = 0.0;
         }
+        // The next row's r: the one below, with its r11.
+        r11[c] = has_down ? P.tilde.r11[at(c, i + 1, jc)] : 0.0f;
+        r12[c] = r12_down;
+        r22[c] = r22_down;
       }
-      if constexpr (COUPLED) most = fmax(most, sqrt(square));
+      xt[c] = xt_down;
+    }
+    if constexpr (COUPLED) {
+      first_here = sqrt(square);
+      if constexpr (TGV) {
+        second_here = sqrt(square2);
+        most_here = fmax(most_here, sqrt(square3));
+      }
+    }
+    if (counted) {
+      first += first_here;
+      second += second_here;
+      most = fmax(most, most_here);
     }
   }
-  if (!P.g.recorded_row(i)) first = second = most = 0.0;  // div2 is still made for every row
   const double sum_first = cta_reduce<false>(first);
   const double sum_second = cta_reduce<false>(second);
   const double largest = cta_reduce<true>(most);
@@ -1418,9 +1487,14 @@ cudaError_t dual_channels(const DualParams& p, bool coupled, bool keep, cudaStre
   }
 }
 
+dim3 norms_grid(const Geometry& g) {
+  const int segments = (g.rows + kNormRows - 1) / kNormRows;
+  return dim3((g.columns + 31) / 32, (segments + 7) / 8, 1);
+}
+
 template <bool TGV>
 cudaError_t norms_channels(const NormParams& p, bool coupled, cudaStream_t s) {
-  const dim3 grid = pixel_grid(p.g);
+  const dim3 grid = norms_grid(p.g);
   switch (p.g.channels) {
     case 1: norms_kernel<TGV, 1, false><<<grid, dim3(32, 8), 0, s>>>(p); break;
     case 2:
@@ -1442,7 +1516,11 @@ int dual_grid_blocks(const Geometry& g) {
   const dim3 d = pixel_grid(g);
   return static_cast<int>(d.x * d.y);
 }
-int norms_grid_blocks(const Geometry& g) { return dual_grid_blocks(g); }
+int norms_grid_blocks(const Geometry& g) {
+  const dim3 d = norms_grid(g);
+  return static_cast<int>(d.x * d.y);
+}
+int residual_grid_blocks(const Geometry& g) { return dual_grid_blocks(g); }
 int primal_grid_blocks(const Geometry& g, const ComponentDevice& c) {
   const dim3 d = primal_grid(g, c.cell_rows, c.cell_columns);
   return static_cast<int>(d.x * d.y);

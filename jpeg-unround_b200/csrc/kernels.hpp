@@ -228,6 +228,7 @@ int dual_grid_blocks(const Geometry& g);
 int primal_grid_blocks(const Geometry& g, const ComponentDevice& c);
 int conjugate_grid_blocks(const Geometry& g, const ComponentDevice& c);
 int norms_grid_blocks(const Geometry& g);
+int residual_grid_blocks(const Geometry& g);
 int start_grid_blocks(const ComponentDevice& c);
 
 cudaError_t launch_dual(const DualParams& p, bool tgv, bool coupled, bool keep, cudaStream_t stream);

@@ -258,7 +258,7 @@ struct Solver::Impl {
     v = allocate<float>(n);
     if (with_tgv) div2 = allocate<float>(2 * n);
     canvas = allocate<double>(static_cast<std::size_t>(g.channels) * g.rows * g.columns);
-    std::size_t most = 3u * norms_grid_blocks(g);
+    std::size_t most = std::max<std::size_t>(3u * norms_grid_blocks(g), residual_grid_blocks(g));
     if (samples != nullptr) most = std::max<std::size_t>(most, samples_grid_blocks(g, g.channels));
     for (const ComponentDevice& d : components) {
       most = std::max<std::size_t>(most, conjugate_grid_blocks(g, d));
@@ -273,7 +273,7 @@ struct Solver::Impl {
       std::size_t regions = 0;
       const std::size_t channels = samples != nullptr ? samples->channels : components.size();
       for (std::size_t c = 0; c < channels; ++c) {
-        regions += 2 * static_cast<std::size_t>(conjugate_count(c)) + norms_grid_blocks(g);
+        regions += 2 * static_cast<std::size_t>(conjugate_count(c)) + residual_grid_blocks(g);
       }
       record_partials = allocate<double>(std::max<std::size_t>(regions, 1));
       record_sums = allocate<double>(2 * kMaxReductions);
@@ -699,7 +699,7 @@ struct Solver::Impl {
       s.conjugates += conjugate(c, div2 + base, div2 + base + g.plane, -theta);
     }
     if (plan.partial_radius) {
-      const std::size_t count = norms_grid_blocks(g);
+      const std::size_t count = residual_grid_blocks(g);
       for (std::size_t c = 0; c < data_channels(); ++c) {
         s.partial += conjugate(c, tilde.p1 + c * g.plane, tilde.p2 + c * g.plane, 1.0);
         ResidualParams rp;
@@ -774,8 +774,9 @@ struct Solver::Impl {
         rp.d2 = div2 + (2 * c + 1) * g.plane;
         rp.partials = region;
         if (error == cudaSuccess) error = launch_residual(rp, stream);
-        at_residual.push_back(second.add(region, count));
-        region += count;
+        const int residuals = residual_grid_blocks(g);
+        at_residual.push_back(second.add(region, residuals));
+        region += residuals;
       }
     }
     if (error == cudaSuccess) error = launch_reductions(second, stream);

@@ -35,9 +35,7 @@ namespace {
 constexpr int kChunk = 8;    // rows of a chunk, one per warp
 constexpr int kHalo = 4;     // columns loaded left of the strip (16-byte aligned start)
 constexpr int kSpan = 40;    // columns loaded: 4 + 32 + 4
-// The ring's slots: 3 where a chunk holds three channels' planes; 6 for one channel, whose chunks
-// are a third the size, so that as many bytes are in flight per CTA.
-__host__ __device__ constexpr int ring_slots(int channels) { return channels == 1 ? 6 : 3; }
+constexpr int kSlots = 3;    // the ring
 constexpr int kStrip = 256;  // rows a CTA sweeps unless the launcher finds better
 constexpr int kThreads = 32 * (kChunk + 1);  // the row warps and the side warp
 constexpr unsigned kAll = 0xffffffffu;
@@ -58,7 +56,6 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
   constexpr int PLANE = kChunk * kSpan;
   constexpr int SLOT = (F + 1) * C * PLANE;  // floats: the state planes, then x~'s
   constexpr int W = TGV ? C : 1;
-  constexpr int kSlots = ring_slots(C);
   extern __shared__ __align__(128) float ring[];
   __shared__ __align__(8) std::uint64_t bars[kSlots];
   __shared__ float carry[2][W][2][32];      // w- of the row above a chunk, own columns
@@ -468,7 +465,7 @@ __global__ void __launch_bounds__(kThreads, 2) dual_batch_kernel(const DualTile*
 
 std::size_t dual_tma_shared_bytes(bool tgv, int channels) {
   const int fields = tgv ? 8 : 3;
-  return static_cast<std::size_t>(ring_slots(channels)) * (fields + 1) * channels * kChunk * kSpan * sizeof(float);
+  return static_cast<std::size_t>(kSlots) * (fields + 1) * channels * kChunk * kSpan * sizeof(float);
 }
 
 // The strip height that finishes a sweep soonest: its CTAs in waves of `slots`, each wave as long
