@@ -298,11 +298,12 @@ def _call_file(data: bytes) -> int:
         library.unround_result_free(result)
 
 
-def _call(image) -> int:
+def _call(image, options: list[str] | None = None) -> int:
     """One solve through the C interface, as a C or cgo caller makes it: unround_solve on host
     arrays (levels in; the binary64 canvas, coefficients and RGB picture out, into the result),
     then the canvas and the picture read on the host. Returns the result's bytes copied from the
-    device (the picture is made on the device and copied like the canvas)."""
+    device (the picture is made on the device and copied like the canvas). The options are the
+    workload's unless given."""
     import ctypes
 
     import numpy as np
@@ -310,7 +311,7 @@ def _call(image) -> int:
     from unround import native
 
     library = native._library()
-    settings = native._Settings(OPTIONS)
+    settings = native._Settings(OPTIONS if options is None else options)
     given, kept = native._input_of(image)
     result = ctypes.c_void_p()
     message = ctypes.create_string_buffer(4096)
@@ -597,6 +598,44 @@ LARGE_OPTIONS = ["--method", "tgv", "--alpha1", "1.5", "--alpha0", "3", "--itera
                  "--record-every", "50"]
 
 
+def _records_arm(args: argparse.Namespace, rank: int, world: int) -> None:
+    """The bench workload through unround_solve with a record every 10 iterations, the
+    reference's default (each record: the tilde point kept by the dual and primal steps, its
+    norms, conjugates and data term summed on the device, one copy back), against the same solve
+    recording at its last iteration only. value: Mpx*iter/s with the records; ms_per_record the
+    difference over the records taken. Each rank solves its own picture; rank 0 prints."""
+    from unround import native
+
+    image = _workload(seed=rank)
+    recording = [*OPTIONS[:-1], "10"]
+    for _ in range(max(1, args.warmup)):
+        _call(image)
+    plain_s, recorded_s = [], []
+    with Clocks(0) as clocks:
+        for _ in range(max(1, args.steps)):
+            began = time.perf_counter()
+            _call(image)
+            plain_s.append(time.perf_counter() - began)
+            began = time.perf_counter()
+            _call(image, recording)
+            recorded_s.append(time.perf_counter() - began)
+    records = ITERATIONS // 10 + 1
+    pixels = HEIGHT * WIDTH
+    if rank != 0:
+        return
+    value = pixels * ITERATIONS / min(recorded_s) / 1e6
+    print(json.dumps({
+        "metric": METRIC + ", a record every 10 iterations", "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": min(recorded_s) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (the bench workload)",
+        "config": {"workload": "tgv-colour-4032x3024-420-records", "record_every": 10, "records": records,
+                   "call": "unround_solve on host arrays"},
+        "without_records": {"value": pixels * ITERATIONS / min(plain_s) / 1e6, "ms_per_step": min(plain_s) * 1e3},
+        "ms_per_record": (min(recorded_s) - min(plain_s)) * 1e3 / (records - 1),
+        "clocks": clocks.summary(),
+    }))
+
+
 def _large_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     """The large single solve: 8192^2 TGV (alpha0 3, alpha1 1.5), 1000 iterations. value:
     the iteration loop's device time (CUDA events, no records); e2e: the drop-in solve with the
@@ -774,10 +813,13 @@ def main() -> None:
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--height", type=int, default=HEIGHT, help="a smaller picture for profiling")
     parser.add_argument("--width", type=int, default=WIDTH)
-    parser.add_argument("--workload", default="tgv-colour", choices=["tgv-colour", "mix", "unrolled", "large", "samples"],
+    parser.add_argument("--workload", default="tgv-colour",
+                        choices=["tgv-colour", "mix", "unrolled", "large", "samples", "records"],
                         help="mix: the batched solve of 64 uneven pictures against image-at-a-time launches; "
                              "unrolled: the differentiable unrolled TGV solve, forward and forward+adjoint")
     parser.add_argument("--pictures", type=int, default=64, help="pictures of the mix")
+    parser.add_argument("--mix-iterations", type=int, default=MIX_ITERATIONS,
+                        help="iterations of each picture of the mix (fewer for a launch list)")
     args = parser.parse_args()
     globals()["HEIGHT"], globals()["WIDTH"] = args.height, args.width
     rank, local_rank, world = _rank()
@@ -786,8 +828,12 @@ def main() -> None:
         os.environ["CUDA_VISIBLE_DEVICES"] = str(local_rank)
     for path in (ROOT / "jpeg-unround_b200", ROOT):
         sys.path.insert(0, str(path))
+    globals()["MIX_ITERATIONS"] = args.mix_iterations
     if args.workload == "mix":
         _mix_arm(args, rank, world)
+        return
+    if args.workload == "records":
+        _records_arm(args, rank, world)
         return
     if args.workload == "unrolled":
         _unrolled_arm(args, rank, world)
