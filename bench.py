@@ -637,7 +637,8 @@ def _records_arm(args: argparse.Namespace, rank: int, world: int) -> None:
 
 
 def _large_arm(args: argparse.Namespace, rank: int, world: int) -> None:
-    """The large single solve: 8192^2 TGV (alpha0 3, alpha1 1.5), 1000 iterations. value:
+    """The large single solve: 8192^2 TGV (alpha0 3, alpha1 1.5), 1000 iterations (--side: a
+    smaller square of the same generator and table, for a capture of its kernels). value:
     the iteration loop's device time (CUDA events, no records); e2e: the drop-in solve with the
     primal-dual gap recorded every 50 iterations, host arrays in and out; and the binary64 check
     that every coefficient of all 1,048,576 blocks lies in its interval."""
@@ -645,7 +646,7 @@ def _large_arm(args: argparse.Namespace, rank: int, world: int) -> None:
 
     from unround import native, synthetic
 
-    made = synthetic.large(seed=5 + rank)
+    made = synthetic.large(args.side, seed=5 + rank)
     image = made.image
     iterations = 1000
     timed_options = [*LARGE_OPTIONS[:-2], "--record-every", "0"]
@@ -665,12 +666,12 @@ def _large_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     if rank != 0:
         return
     line = {
-        "metric": "TGV PDHG Mpx*iter/s on 1 B200 (8192x8192 grey, custom table, 1000 iterations)",
+        "metric": f"TGV PDHG Mpx*iter/s on 1 B200 ({args.side}x{args.side} grey, custom table, 1000 iterations)",
         "value": value, "unit": "Mpx*iter/s", "n_gpus": world, "steps": 1, "warmup": max(3, args.warmup) * 10,
         "ms_per_step": timing.milliseconds, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded piecewise-smooth + noise sigma 2, table steps U{1..64})",
-        "config": {"workload": "tgv-grey-8192-custom", "alpha1": 1.5, "alpha0": 3.0, "iterations": iterations,
-                   "samples": timing.samples, "l2": "state 4.3 GB, larger than L2"},
+        "config": {"workload": f"tgv-grey-{args.side}-custom", "alpha1": 1.5, "alpha0": 3.0, "iterations": iterations,
+                   "samples": timing.samples, "l2": f"state {17 * 4 * timing.samples / 1e9:.2f} GB"},
         "roofline": {"bound": "hbm", "kernel": "dual_tma_kernel<tgv,1>", "achieved":
                      DUAL_BYTES * timing.samples / (timing.dual_milliseconds / 1e3) / 1e9, "peak": peak,
                      "unit": "GB/s", "peak_kind": peak_kind,
@@ -818,6 +819,7 @@ def main() -> None:
                         help="mix: the batched solve of 64 uneven pictures against image-at-a-time launches; "
                              "unrolled: the differentiable unrolled TGV solve, forward and forward+adjoint")
     parser.add_argument("--pictures", type=int, default=64, help="pictures of the mix")
+    parser.add_argument("--side", type=int, default=8192, help="side of the large workload's square picture")
     parser.add_argument("--mix-iterations", type=int, default=MIX_ITERATIONS,
                         help="iterations of each picture of the mix (fewer for a launch list)")
     args = parser.parse_args()

@@ -1100,16 +1100,55 @@ __global__ void project_kernel(Fields f, Geometry g, int tgv, int coupled, float
 // (cpp/src/frames.cpp:428-487, model.cpp:74-111); the residual of the partial gap.
 
 // The records' norms as a sweep: a warp owns 32 columns and walks down kNormRows rows, so that
-// every plane is read once -- the row below one row ahead, the row above kept in registers, the
-// neighbours across by shuffles (lane 0 reads column x0 - 1, lane 31 column x0 + 32). At each
+// every plane is read once. Each row's loads -- the row below, every channel, and the columns
+// beside the strip (x0 + 32 for lane 31, x0 - 1 for lane 0) -- are issued together at the top of
+// the row, before any of its stores (which the compiler may not move loads across), so a row
+// waits for memory once; the row itself and w~ of the row above are kept in registers from the
+// rows before, and the neighbours across come by shuffles. At each
 // pixel, in binary64 from the binary32 tilde point: |grad x~ - w~| (the first-order term),
 // |E w~|_F (the second-order term) and div2 r~ (written, binary32) and its norm, each operation
 // as the per-pixel form of cpp/src/primal_dual.hpp:836-895 orders it. Rows outside the record
 // rows add nothing (div2 is still made for them).
-constexpr int kNormRows = 64;
+constexpr int kNormRows = 16;
+
+// One row's loads of a channel for the norms sweep: the lane's column, and in `edge` the column
+// beside the strip that the lane's shuffle cannot give -- lane 31: x~, r11, r12 at column x0 + 32;
+// lane 0: w1, w2 at column x0 - 1.
+struct NormRow {
+  float xt = 0.0f, r11 = 0.0f, r22 = 0.0f, r12 = 0.0f;
+  float w1 = 0.0f, w2 = 0.0f;
+  float edge[3] = {0.0f, 0.0f, 0.0f};
+};
+
+template <bool TGV>
+__device__ __forceinline__ NormRow norm_row(const NormParams& P, int c, int i, int jc, int lane, int x0) {
+  NormRow v;
+  const int columns = P.g.columns;
+  if (i >= P.g.rows) return v;
+  const std::size_t row = c * P.g.plane + static_cast<std::size_t>(i) * P.g.pitch;
+  v.xt = P.xt[row + jc];
+  const bool right = lane == 31 && x0 + 32 < columns;
+  if (right) v.edge[0] = P.xt[row + x0 + 32];
+  if constexpr (TGV) {
+    v.r11 = P.tilde.r11[row + jc];
+    v.r22 = P.tilde.r22[row + jc];
+    v.r12 = P.tilde.r12[row + jc];
+    v.w1 = P.tilde.w1[row + jc];
+    v.w2 = P.tilde.w2[row + jc];
+    if (right) {
+      v.edge[1] = P.tilde.r11[row + x0 + 32];
+      v.edge[2] = P.tilde.r12[row + x0 + 32];
+    }
+    if (lane == 0 && x0 > 0) {
+      v.edge[0] = P.tilde.w1[row + x0 - 1];
+      v.edge[1] = P.tilde.w2[row + x0 - 1];
+    }
+  }
+  return v;
+}
 
 template <bool TGV, int C, bool COUPLED>
-__global__ void __launch_bounds__(256) norms_kernel(const NormParams P) {
+__global__ void __launch_bounds__(256, 3) norms_kernel(const NormParams P) {
   const int lane = threadIdx.x;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
   const std::size_t plane = P.g.plane;
@@ -1121,58 +1160,43 @@ __global__ void __launch_bounds__(256) norms_kernel(const NormParams P) {
   const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kNormRows;
   const int i1 = min(i0 + kNormRows, rows);
   constexpr unsigned kAll = 0xffffffffu;
-  auto at = [&](int c, int i, int col) -> std::size_t {
-    return c * plane + static_cast<std::size_t>(i) * pitch + col;
-  };
-  // The lane's values of the current row i (xt, r) and of the row above (w).
-  float xt[C], r11[C], r22[C], r12[C], w1_above[C], w2_above[C];
+  // Row i (cur) kept from the row before; w~ of row i - 1 kept.
+  NormRow cur[C];
+  float w1_above[C], w2_above[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) {
-    xt[c] = r11[c] = r22[c] = r12[c] = w1_above[c] = w2_above[c] = 0.0f;
+    w1_above[c] = w2_above[c] = 0.0f;
     if (i0 < i1) {
-      xt[c] = P.xt[at(c, i0, jc)];
-      if constexpr (TGV) {
-        r11[c] = P.tilde.r11[at(c, i0, jc)];
-        r22[c] = P.tilde.r22[at(c, i0, jc)];
-        r12[c] = P.tilde.r12[at(c, i0, jc)];
-        if (i0 > 0) {
-          w1_above[c] = P.tilde.w1[at(c, i0 - 1, jc)];
-          w2_above[c] = P.tilde.w2[at(c, i0 - 1, jc)];
-        }
+      cur[c] = norm_row<TGV>(P, c, i0, jc, lane, x0);
+      if (TGV && i0 > 0) {
+        const std::size_t above = c * plane + static_cast<std::size_t>(i0 - 1) * pitch + jc;
+        w1_above[c] = P.tilde.w1[above];
+        w2_above[c] = P.tilde.w2[above];
       }
     }
   }
   double first = 0.0, second = 0.0, most = 0.0;
   for (int i = i0; i < i1; ++i) {
+    // The row below, every channel, before this row's arithmetic and stores.
+    NormRow down[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) down[c] = norm_row<TGV>(P, c, i + 1, jc, lane, x0);
     const bool has_down = i + 1 < rows;
-    const bool counted = valid && P.g.recorded_row(i);
     double square = 0.0, first_here = 0.0;
     double square2 = 0.0, second_here = 0.0;
     double square3 = 0.0, most_here = 0.0;
 #pragma unroll
     for (int c = 0; c < C; ++c) {
+      const NormRow& v = cur[c];
       const double gamma = P.weight[c];
-      // The row below (one ahead), and the right neighbours across.
-      const float xt_down = has_down ? P.xt[at(c, i + 1, jc)] : 0.0f;
-      float xt_right = __shfl_down_sync(kAll, xt[c], 1);
-      if (lane == 31) xt_right = x0 + 32 < columns ? P.xt[at(c, i, x0 + 32)] : 0.0f;
-      float w1 = 0.0f, w2 = 0.0f, w1_left = 0.0f, w2_left = 0.0f;
-      if constexpr (TGV) {
-        w1 = P.tilde.w1[at(c, i, jc)];
-        w2 = P.tilde.w2[at(c, i, jc)];
-        w1_left = __shfl_up_sync(kAll, w1, 1);
-        w2_left = __shfl_up_sync(kAll, w2, 1);
-        if (lane == 0 && x0 > 0) {
-          w1_left = P.tilde.w1[at(c, i, x0 - 1)];
-          w2_left = P.tilde.w2[at(c, i, x0 - 1)];
-        }
-      }
-      const double here = xt[c];
+      float xt_right = __shfl_down_sync(kAll, v.xt, 1);
+      if (lane == 31) xt_right = v.edge[0];
+      const double here = v.xt;
       double gx = has_right ? static_cast<double>(xt_right) - here : 0.0;
-      double gy = has_down ? static_cast<double>(xt_down) - here : 0.0;
+      double gy = has_down ? static_cast<double>(down[c].xt) - here : 0.0;
       if constexpr (TGV) {
-        gx = gx - static_cast<double>(w1);
-        gy = gy - static_cast<double>(w2);
+        gx = gx - static_cast<double>(v.w1);
+        gy = gy - static_cast<double>(v.w2);
       }
       square += (COUPLED ? gamma * gamma : 1.0) * (gx * gx + gy * gy);
       if constexpr (!COUPLED) {
@@ -1180,9 +1204,14 @@ __global__ void __launch_bounds__(256) norms_kernel(const NormParams P) {
         square = 0.0;
       }
       if constexpr (TGV) {
+        float w1_left = __shfl_up_sync(kAll, v.w1, 1), w2_left = __shfl_up_sync(kAll, v.w2, 1);
+        if (lane == 0) {
+          w1_left = v.edge[0];
+          w2_left = v.edge[1];
+        }
         const bool last_c = j + 1 == columns, last_r = i + 1 == rows;
-        const double a1 = last_c ? 0.0 : w1, a2 = last_r ? 0.0 : w2;
-        const double b1 = last_r ? 0.0 : w1, b2 = last_c ? 0.0 : w2;
+        const double a1 = last_c ? 0.0 : v.w1, a2 = last_r ? 0.0 : v.w2;
+        const double b1 = last_r ? 0.0 : v.w1, b2 = last_c ? 0.0 : v.w2;
         const double l1 = has_left ? w1_left : 0.0, l2 = has_left ? w2_left : 0.0;
         const double u1 = i > 0 ? w1_above[c] : 0.0, u2 = i > 0 ? w2_above[c] : 0.0;
         const double exx = a1 - l1, eyy = a2 - u2, exy = 0.5 * ((b1 - u1) + (b2 - l2));
@@ -1191,22 +1220,19 @@ __global__ void __launch_bounds__(256) norms_kernel(const NormParams P) {
           second_here += gamma * sqrt(square2);
           square2 = 0.0;
         }
-        w1_above[c] = w1;
-        w2_above[c] = w2;
+        w1_above[c] = v.w1;
+        w2_above[c] = v.w2;
         // div2 r~ by forward differences.
-        float r11_right = __shfl_down_sync(kAll, r11[c], 1), r12_right = __shfl_down_sync(kAll, r12[c], 1);
+        float r11_right = __shfl_down_sync(kAll, v.r11, 1), r12_right = __shfl_down_sync(kAll, v.r12, 1);
         if (lane == 31) {
-          const bool beyond = x0 + 32 < columns;
-          r11_right = beyond ? P.tilde.r11[at(c, i, x0 + 32)] : 0.0f;
-          r12_right = beyond ? P.tilde.r12[at(c, i, x0 + 32)] : 0.0f;
+          r11_right = v.edge[1];
+          r12_right = v.edge[2];
         }
-        const float r12_down = has_down ? P.tilde.r12[at(c, i + 1, jc)] : 0.0f;
-        const float r22_down = has_down ? P.tilde.r22[at(c, i + 1, jc)] : 0.0f;
-        double d1 = has_right ? static_cast<double>(r11_right) - r11[c] : 0.0;
-        double d2 = has_right ? static_cast<double>(r12_right) - r12[c] : 0.0;
+        double d1 = has_right ? static_cast<double>(r11_right) - v.r11 : 0.0;
+        double d2 = has_right ? static_cast<double>(r12_right) - v.r12 : 0.0;
         if (has_down) {
-          d1 += static_cast<double>(r12_down) - r12[c];
-          d2 += static_cast<double>(r22_down) - r22[c];
+          d1 += static_cast<double>(down[c].r12) - v.r12;
+          d2 += static_cast<double>(down[c].r22) - v.r22;
         }
         if (valid) {
           P.div2[(2 * c) * plane + static_cast<std::size_t>(i) * pitch + j] = static_cast<float>(d1);
@@ -1217,12 +1243,7 @@ __global__ void __launch_bounds__(256) norms_kernel(const NormParams P) {
           most_here = fmax(most_here, sqrt(square3));
           square3 = 0.0;
         }
-        // The next row's r: the one below, with its r11.
-        r11[c] = has_down ? P.tilde.r11[at(c, i + 1, jc)] : 0.0f;
-        r12[c] = r12_down;
-        r22[c] = r22_down;
       }
-      xt[c] = xt_down;
     }
     if constexpr (COUPLED) {
       first_here = sqrt(square);
@@ -1231,11 +1252,13 @@ __global__ void __launch_bounds__(256) norms_kernel(const NormParams P) {
         most_here = fmax(most_here, sqrt(square3));
       }
     }
-    if (counted) {
+    if (valid && P.g.recorded_row(i)) {
       first += first_here;
       second += second_here;
       most = fmax(most, most_here);
     }
+#pragma unroll
+    for (int c = 0; c < C; ++c) cur[c] = down[c];
   }
   const double sum_first = cta_reduce<false>(first);
   const double sum_second = cta_reduce<false>(second);
