@@ -636,6 +636,69 @@ def _records_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     }))
 
 
+TV_GREY_OPTIONS = ["--method", "tv", "--alpha", "1", "--iterations", "200", "--tolerance", "0", "--record-every", "0",
+                   "--step-ratio", "1", "--step-product", "0.99", "--norm-squared", "7.92"]
+
+
+def _tv_grey_arm(args: argparse.Namespace, rank: int, world: int) -> None:
+    """The small TV solve: a 512 x 512 grey picture of the generator at quality 50, TV with
+    alpha 1, 200 iterations, tau = sigma = sqrt(1/8) (step ratio 1, product 0.99, norm squared
+    7.92). Its state (3 MB) lives in L2 and a launch is short, so the figure is absolute, not a
+    fraction of HBM. value: the iteration loop's device time (CUDA events), K solves of 200
+    iterations; e2e: the drop-in call with host arrays; cpu_baseline: the reference's solver on
+    the host cores, one whole solve with every thread and with one, run first."""
+    from unround import native, synthetic
+
+    image = synthetic.grey(512, 512, quality=50, seed=1 + rank).image
+    iterations = 200
+    cpu = None
+    if world == 1 and rank == 0:
+        from oracle import reference
+
+        if reference.available():
+            components = [(c.coefficients, c.quant_table.reshape(64), c.h_samp_factor, c.v_samp_factor)
+                          for c in image.components]
+            cpu = {}
+            for threads in (os.cpu_count() or 1, 1):
+                best = None
+                for _ in range(3):
+                    began = time.perf_counter()
+                    reference.solve(512, 512, 1, components, [*TV_GREY_OPTIONS, "--threads", str(threads)])
+                    seconds = time.perf_counter() - began
+                    best = seconds if best is None else min(best, seconds)
+                cpu[threads] = 512 * 512 * iterations / best / 1e6
+    with Clocks(0) as clocks:
+        timing, _ = native.measure(image, TV_GREY_OPTIONS, warmup=max(3, args.warmup) * iterations,
+                                   iterations=max(1, args.steps) * iterations)
+    value = 512 * 512 * max(1, args.steps) * iterations / (timing.milliseconds / 1e3) / 1e6
+    native.solve(image, TV_GREY_OPTIONS)  # warm the call path
+    began = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        native.solve(image, TV_GREY_OPTIONS)
+    e2e_seconds = (time.perf_counter() - began) / max(1, args.steps)
+    if rank != 0:
+        return
+    line = {
+        "metric": "TV PDHG Mpx*iter/s on 1 B200 (512x512 grey, quality 50, 200 iterations)", "value": value,
+        "unit": "Mpx*iter/s", "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+        "ms_per_step": timing.milliseconds / max(1, args.steps), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded piecewise-smooth, quality 50)",
+        "config": {"workload": "tv-grey-512", "iterations": iterations, "tau_sigma": "sqrt(1/8)",
+                   "l2": "state 3 MB: L2-resident, absolute figure"},
+        "e2e": {"value": 512 * 512 * iterations / e2e_seconds / 1e6, "unit": "Mpx*iter/s",
+                "h2d_bytes_per_step": int(image.components[0].coefficients.nbytes), "d2h_bytes_per_step": None,
+                "call": "unround.native.solve (the drop-in, with the model's arrays made and copied)"},
+        "gpu_launches": timing.launches_per_iteration * iterations * max(1, args.steps),
+        "clocks": clocks.summary(),
+    }
+    if cpu:
+        threads = os.cpu_count() or 1
+        line["cpu_baseline"] = {"value": cpu[threads], "unit": "Mpx*iter/s", "cores": threads, "kind": "reference",
+                                "sample": "one whole solve (200 iterations with its set-up), best of 3",
+                                "one_thread": {"value": cpu[1], "cores": 1}}
+    print(json.dumps(line))
+
+
 def _large_arm(args: argparse.Namespace, rank: int, world: int) -> None:
     """The large single solve: 8192^2 TGV (alpha0 3, alpha1 1.5), 1000 iterations (--side: a
     smaller square of the same generator and table, for a capture of its kernels). value:
@@ -815,7 +878,7 @@ def main() -> None:
     parser.add_argument("--height", type=int, default=HEIGHT, help="a smaller picture for profiling")
     parser.add_argument("--width", type=int, default=WIDTH)
     parser.add_argument("--workload", default="tgv-colour",
-                        choices=["tgv-colour", "mix", "unrolled", "large", "samples", "records"],
+                        choices=["tgv-colour", "mix", "unrolled", "large", "samples", "records", "tv-grey"],
                         help="mix: the batched solve of 64 uneven pictures against image-at-a-time launches; "
                              "unrolled: the differentiable unrolled TGV solve, forward and forward+adjoint")
     parser.add_argument("--pictures", type=int, default=64, help="pictures of the mix")
@@ -836,6 +899,9 @@ def main() -> None:
         return
     if args.workload == "records":
         _records_arm(args, rank, world)
+        return
+    if args.workload == "tv-grey":
+        _tv_grey_arm(args, rank, world)
         return
     if args.workload == "unrolled":
         _unrolled_arm(args, rank, world)
