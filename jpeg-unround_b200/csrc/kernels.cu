@@ -1099,167 +1099,110 @@ __global__ void project_kernel(Fields f, Geometry g, int tgv, int coupled, float
 // 791-895): the norms of the pixels, TGV's div2 r~ and its largest norm; G* of a field
 // (cpp/src/frames.cpp:428-487, model.cpp:74-111); the residual of the partial gap.
 
-// The records' norms as a sweep: a warp owns 32 columns and walks down kNormRows rows, so that
-// every plane is read once. Each row's loads -- the row below, every channel, and the columns
-// beside the strip (x0 + 32 for lane 31, x0 - 1 for lane 0) -- are issued together at the top of
-// the row, before any of its stores (which the compiler may not move loads across), so a row
-// waits for memory once; the row itself and w~ of the row above are kept in registers from the
-// rows before, and the neighbours across come by shuffles. At each
-// pixel, in binary64 from the binary32 tilde point: |grad x~ - w~| (the first-order term),
-// |E w~|_F (the second-order term) and div2 r~ (written, binary32) and its norm, each operation
-// as the per-pixel form of cpp/src/primal_dual.hpp:836-895 orders it. Rows outside the record
+// The records' norms, a thread per pixel: every value the pixel needs, of every channel, is
+// loaded first (the neighbours' from L1 and L2), before any arithmetic or store, so that a pixel
+// waits for memory once; then, in binary64 from the binary32 tilde point, |grad x~ - w~| (the
+// first-order term), |E w~|_F (the second-order term) and div2 r~ (written, binary32) and its
+// norm, each operation as cpp/src/primal_dual.hpp:836-895 orders it. Pixels outside the record
 // rows add nothing (div2 is still made for them).
-constexpr int kNormRows = 16;
-
-// One row's loads of a channel for the norms sweep: the lane's column, and in `edge` the column
-// beside the strip that the lane's shuffle cannot give -- lane 31: x~, r11, r12 at column x0 + 32;
-// lane 0: w1, w2 at column x0 - 1.
-struct NormRow {
-  float xt = 0.0f, r11 = 0.0f, r22 = 0.0f, r12 = 0.0f;
-  float w1 = 0.0f, w2 = 0.0f;
-  float edge[3] = {0.0f, 0.0f, 0.0f};
-};
-
-template <bool TGV>
-__device__ __forceinline__ NormRow norm_row(const NormParams& P, int c, int i, int jc, int lane, int x0) {
-  NormRow v;
-  const int columns = P.g.columns;
-  if (i >= P.g.rows) return v;
-  const std::size_t row = c * P.g.plane + static_cast<std::size_t>(i) * P.g.pitch;
-  v.xt = P.xt[row + jc];
-  const bool right = lane == 31 && x0 + 32 < columns;
-  if (right) v.edge[0] = P.xt[row + x0 + 32];
-  if constexpr (TGV) {
-    v.r11 = P.tilde.r11[row + jc];
-    v.r22 = P.tilde.r22[row + jc];
-    v.r12 = P.tilde.r12[row + jc];
-    v.w1 = P.tilde.w1[row + jc];
-    v.w2 = P.tilde.w2[row + jc];
-    if (right) {
-      v.edge[1] = P.tilde.r11[row + x0 + 32];
-      v.edge[2] = P.tilde.r12[row + x0 + 32];
-    }
-    if (lane == 0 && x0 > 0) {
-      v.edge[0] = P.tilde.w1[row + x0 - 1];
-      v.edge[1] = P.tilde.w2[row + x0 - 1];
-    }
-  }
-  return v;
-}
-
 template <bool TGV, int C, bool COUPLED>
 __global__ void __launch_bounds__(256, 3) norms_kernel(const NormParams P) {
-  const int lane = threadIdx.x;
+  const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y;
   const int rows = P.g.rows, columns = P.g.columns, pitch = P.g.pitch;
-  const std::size_t plane = P.g.plane;
-  const int x0 = blockIdx.x * 32;
-  const int j = x0 + lane;
-  const bool valid = j < columns;
-  const int jc = valid ? j : columns - 1;
-  const bool has_left = j > 0, has_right = j + 1 < columns;
-  const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kNormRows;
-  const int i1 = min(i0 + kNormRows, rows);
-  constexpr unsigned kAll = 0xffffffffu;
-  // Row i (cur) kept from the row before; w~ of row i - 1 kept.
-  NormRow cur[C];
-  float w1_above[C], w2_above[C];
-#pragma unroll
-  for (int c = 0; c < C; ++c) {
-    w1_above[c] = w2_above[c] = 0.0f;
-    if (i0 < i1) {
-      cur[c] = norm_row<TGV>(P, c, i0, jc, lane, x0);
-      if (TGV && i0 > 0) {
-        const std::size_t above = c * plane + static_cast<std::size_t>(i0 - 1) * pitch + jc;
-        w1_above[c] = P.tilde.w1[above];
-        w2_above[c] = P.tilde.w2[above];
-      }
-    }
-  }
   double first = 0.0, second = 0.0, most = 0.0;
-  for (int i = i0; i < i1; ++i) {
-    // The row below, every channel, before this row's arithmetic and stores.
-    NormRow down[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) down[c] = norm_row<TGV>(P, c, i + 1, jc, lane, x0);
-    const bool has_down = i + 1 < rows;
-    double square = 0.0, first_here = 0.0;
-    double square2 = 0.0, second_here = 0.0;
-    double square3 = 0.0, most_here = 0.0;
+  if (i < rows && j < columns) {
+    const std::size_t at = static_cast<std::size_t>(i) * pitch + j;
+    const bool right = j + 1 < columns, down = i + 1 < rows, left = j > 0, up = i > 0;
+    const std::size_t ar = right ? at + 1 : at, ad = down ? at + pitch : at;
+    const std::size_t al = left ? at - 1 : at, au = up ? at - pitch : at;
+    // The loads.
+    float xt[C], xt_r[C], xt_d[C];
+    float w1[C], w2[C], w1_l[C], w2_l[C], w1_u[C], w2_u[C];
+    float r11[C], r22[C], r12[C], r11_r[C], r12_r[C], r12_d[C], r22_d[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-      const NormRow& v = cur[c];
-      const double gamma = P.weight[c];
-      float xt_right = __shfl_down_sync(kAll, v.xt, 1);
-      if (lane == 31) xt_right = v.edge[0];
-      const double here = v.xt;
-      double gx = has_right ? static_cast<double>(xt_right) - here : 0.0;
-      double gy = has_down ? static_cast<double>(down[c].xt) - here : 0.0;
+      const std::size_t base = c * P.g.plane;
+      xt[c] = P.xt[base + at];
+      xt_r[c] = P.xt[base + ar];
+      xt_d[c] = P.xt[base + ad];
       if constexpr (TGV) {
-        gx = gx - static_cast<double>(v.w1);
-        gy = gy - static_cast<double>(v.w2);
+        w1[c] = P.tilde.w1[base + at];
+        w2[c] = P.tilde.w2[base + at];
+        w1_l[c] = P.tilde.w1[base + al];
+        w2_l[c] = P.tilde.w2[base + al];
+        w1_u[c] = P.tilde.w1[base + au];
+        w2_u[c] = P.tilde.w2[base + au];
+        r11[c] = P.tilde.r11[base + at];
+        r22[c] = P.tilde.r22[base + at];
+        r12[c] = P.tilde.r12[base + at];
+        r11_r[c] = P.tilde.r11[base + ar];
+        r12_r[c] = P.tilde.r12[base + ar];
+        r12_d[c] = P.tilde.r12[base + ad];
+        r22_d[c] = P.tilde.r22[base + ad];
+      }
+    }
+    // The arithmetic.
+    double square = 0.0;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const double gamma = P.weight[c];
+      const double here = xt[c];
+      double gx = right ? static_cast<double>(xt_r[c]) - here : 0.0;
+      double gy = down ? static_cast<double>(xt_d[c]) - here : 0.0;
+      if constexpr (TGV) {
+        gx = gx - static_cast<double>(w1[c]);
+        gy = gy - static_cast<double>(w2[c]);
       }
       square += (COUPLED ? gamma * gamma : 1.0) * (gx * gx + gy * gy);
       if constexpr (!COUPLED) {
-        first_here += gamma * sqrt(square);
+        first += gamma * sqrt(square);
         square = 0.0;
       }
-      if constexpr (TGV) {
-        float w1_left = __shfl_up_sync(kAll, v.w1, 1), w2_left = __shfl_up_sync(kAll, v.w2, 1);
-        if (lane == 0) {
-          w1_left = v.edge[0];
-          w2_left = v.edge[1];
-        }
-        const bool last_c = j + 1 == columns, last_r = i + 1 == rows;
-        const double a1 = last_c ? 0.0 : v.w1, a2 = last_r ? 0.0 : v.w2;
-        const double b1 = last_r ? 0.0 : v.w1, b2 = last_c ? 0.0 : v.w2;
-        const double l1 = has_left ? w1_left : 0.0, l2 = has_left ? w2_left : 0.0;
-        const double u1 = i > 0 ? w1_above[c] : 0.0, u2 = i > 0 ? w2_above[c] : 0.0;
-        const double exx = a1 - l1, eyy = a2 - u2, exy = 0.5 * ((b1 - u1) + (b2 - l2));
-        square2 += (COUPLED ? gamma * gamma : 1.0) * (exx * exx + eyy * eyy + 2.0 * (exy * exy));
-        if constexpr (!COUPLED) {
-          second_here += gamma * sqrt(square2);
-          square2 = 0.0;
-        }
-        w1_above[c] = v.w1;
-        w2_above[c] = v.w2;
-        // div2 r~ by forward differences.
-        float r11_right = __shfl_down_sync(kAll, v.r11, 1), r12_right = __shfl_down_sync(kAll, v.r12, 1);
-        if (lane == 31) {
-          r11_right = v.edge[1];
-          r12_right = v.edge[2];
-        }
-        double d1 = has_right ? static_cast<double>(r11_right) - v.r11 : 0.0;
-        double d2 = has_right ? static_cast<double>(r12_right) - v.r12 : 0.0;
-        if (has_down) {
-          d1 += static_cast<double>(down[c].r12) - v.r12;
-          d2 += static_cast<double>(down[c].r22) - v.r22;
-        }
-        if (valid) {
-          P.div2[(2 * c) * plane + static_cast<std::size_t>(i) * pitch + j] = static_cast<float>(d1);
-          P.div2[(2 * c + 1) * plane + static_cast<std::size_t>(i) * pitch + j] = static_cast<float>(d2);
-        }
-        square3 += d1 * d1 + d2 * d2;
-        if constexpr (!COUPLED) {
-          most_here = fmax(most_here, sqrt(square3));
-          square3 = 0.0;
-        }
-      }
     }
-    if constexpr (COUPLED) {
-      first_here = sqrt(square);
-      if constexpr (TGV) {
-        second_here = sqrt(square2);
-        most_here = fmax(most_here, sqrt(square3));
-      }
-    }
-    if (valid && P.g.recorded_row(i)) {
-      first += first_here;
-      second += second_here;
-      most = fmax(most, most_here);
-    }
+    if constexpr (COUPLED) first = sqrt(square);
+    if constexpr (TGV) {
+      square = 0.0;
 #pragma unroll
-    for (int c = 0; c < C; ++c) cur[c] = down[c];
+      for (int c = 0; c < C; ++c) {
+        const double gamma = P.weight[c];
+        const double a1 = right ? w1[c] : 0.0, a2 = down ? w2[c] : 0.0;
+        const double b1 = down ? w1[c] : 0.0, b2 = right ? w2[c] : 0.0;
+        const double l1 = left ? w1_l[c] : 0.0, l2 = left ? w2_l[c] : 0.0;
+        const double u1 = up ? w1_u[c] : 0.0, u2 = up ? w2_u[c] : 0.0;
+        const double exx = a1 - l1, eyy = a2 - u2, exy = 0.5 * ((b1 - u1) + (b2 - l2));
+        square += (COUPLED ? gamma * gamma : 1.0) * (exx * exx + eyy * eyy + 2.0 * (exy * exy));
+        if constexpr (!COUPLED) {
+          second += gamma * sqrt(square);
+          square = 0.0;
+        }
+      }
+      if constexpr (COUPLED) second = sqrt(square);
+      square = 0.0;
+      double d1[C], d2[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        d1[c] = right ? static_cast<double>(r11_r[c]) - r11[c] : 0.0;
+        d2[c] = right ? static_cast<double>(r12_r[c]) - r12[c] : 0.0;
+        if (down) {
+          d1[c] += static_cast<double>(r12_d[c]) - r12[c];
+          d2[c] += static_cast<double>(r22_d[c]) - r22[c];
+        }
+        square += d1[c] * d1[c] + d2[c] * d2[c];
+        if constexpr (!COUPLED) {
+          most = fmax(most, sqrt(square));
+          square = 0.0;
+        }
+      }
+      if constexpr (COUPLED) most = fmax(most, sqrt(square));
+      // The stores, last.
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        P.div2[(2 * c) * P.g.plane + at] = static_cast<float>(d1[c]);
+        P.div2[(2 * c + 1) * P.g.plane + at] = static_cast<float>(d2[c]);
+      }
+    }
   }
+  if (!P.g.recorded_row(i)) first = second = most = 0.0;  // div2 is still made for every row
   const double sum_first = cta_reduce<false>(first);
   const double sum_second = cta_reduce<false>(second);
   const double largest = cta_reduce<true>(most);
@@ -1323,48 +1266,48 @@ __global__ void __launch_bounds__(256) conjugate_kernel(const ConjugateParams P)
   const bool in_blocks = active && vby < P.component.block_rows && vbx < P.component.block_columns;
   const int j0 = vbx * BW + m * CC, i0 = vby * BH;
   const bool counted = P.g.recorded_row(i0);
-  // xi = gamma div q at the lane's samples, q = scale (q1, q2).
+  // xi = gamma div q at the lane's sample (row r of the block, sample c of its cell's row),
+  // q = scale (q1, q2); made where needed rather than kept (a block of 16 x 2 binary64 values a
+  // lane would hold the registers of half the CTAs an SM can run).
   const double scale = P.most_at != nullptr ? negative_theta(*P.most_at, P.alpha1) : P.scale;
-  auto q_at = [&](const float* f, int i, int j) -> double { return scale * static_cast<double>(f[static_cast<std::size_t>(i) * pitch + j]); };
-  double xi[BH][CC];
+  auto q_at = [&](const float* f, int i, int j) -> double {
+    return scale * static_cast<double>(f[static_cast<std::size_t>(i) * pitch + j]);
+  };
+  auto xi = [&](int r, int c) -> double {
+    const int i = i0 + r, j = j0 + c;
+    if (!active) return 0.0;
+    const double dy = (i + 1 < rows ? q_at(P.q2, i, j) : 0.0) - (i > 0 ? q_at(P.q2, i - 1, j) : 0.0);
+    const double dx = (j + 1 < columns ? q_at(P.q1, i, j) : 0.0) - (j > 0 ? q_at(P.q1, i, j - 1) : 0.0);
+    return P.gamma * (dy + dx);
+  };
   double sums[8], means[8];
   double total = 0.0;
-#pragma unroll
-  for (int r = 0; r < BH; ++r) {
-#pragma unroll
-    for (int c = 0; c < CC; ++c) {
-      const int i = i0 + r, j = j0 + c;
-      double value = 0.0;
-      if (active) {
-        const double dy = (i + 1 < rows ? q_at(P.q2, i, j) : 0.0) - (i > 0 ? q_at(P.q2, i - 1, j) : 0.0);
-        const double dx = (j + 1 < columns ? q_at(P.q1, i, j) : 0.0) - (j > 0 ? q_at(P.q1, i, j - 1) : 0.0);
-        value = P.gamma * (dy + dx);
-      }
-      xi[r][c] = value;
-    }
-  }
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     double sum = 0.0;
 #pragma unroll
     for (int c = 0; c < CC; ++c) {
-      double column = xi[CR * r][c];
+      double column = xi(CR * r, c);
 #pragma unroll
-      for (int a = 1; a < CR; ++a) column += xi[CR * r + a][c];
+      for (int a = 1; a < CR; ++a) column += xi(CR * r + a, c);
       sum = c == 0 ? column : sum + column;
     }
     sums[r] = sum;
     means[r] = sum / static_cast<double>(CR * CC);
   }
   if (P.free && active) {
-#pragma unroll
+    // A loop kept rolled, so that the compiler holds no value of the pass above for it.
+#pragma unroll 1
     for (int r = 0; r < 8; ++r) {
+      double mean = means[0];
+#pragma unroll
+      for (int k = 1; k < 8; ++k) mean = k == r ? means[k] : mean;
 #pragma unroll
       for (int a = 0; a < CR; ++a) {
 #pragma unroll
         for (int c = 0; c < CC; ++c) {
-          const double s = xi[CR * r + a][c];
-          total += in_blocks ? P.radius * fabs(s - means[r]) : 128.0 * s + P.radius * fabs(s);
+          const double s = xi(CR * r + a, c);
+          total += in_blocks ? P.radius * fabs(s - mean) : 128.0 * s + P.radius * fabs(s);
         }
       }
     }
@@ -1510,10 +1453,7 @@ cudaError_t dual_channels(const DualParams& p, bool coupled, bool keep, cudaStre
   }
 }
 
-dim3 norms_grid(const Geometry& g) {
-  const int segments = (g.rows + kNormRows - 1) / kNormRows;
-  return dim3((g.columns + 31) / 32, (segments + 7) / 8, 1);
-}
+dim3 norms_grid(const Geometry& g) { return pixel_grid(g); }
 
 template <bool TGV>
 cudaError_t norms_channels(const NormParams& p, bool coupled, cudaStream_t s) {
