@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(256) dual_stream_kernel(const DualParams P) {
       const float q1 = step_p1[c] * sp, q2 = step_p2[c] * sp;
       P.out.p1[base + here] = rho * q1 + rest * old_p1[c];
       P.out.p2[base + here] = rho * q2 + rest * old_p2[c];
-      if constexpr (KEEP) {
+      if (KEEP && P.tilde.p1 != nullptr) {  // p~: TV's records and the partial gap's
         P.tilde.p1[base + here] = q1;
         P.tilde.p2[base + here] = q2;
       }
@@ -477,11 +477,19 @@ constexpr int primal_warps() {
   return kStageRows / (8 * CR);
 }
 
-// Slots of the ring: the most that leave room for two CTAs of 256 threads on an SM (luma), or
-// for three of 128 (2x2 chroma cells).
+// Slots of the ring: two, which leave room for three CTAs on an SM (the loader warp fills one
+// slot while the compute warps work on the other).
 template <int CR>
 constexpr int primal_slots() {
-  return CR == 1 ? 3 : 2;
+  return 2;
+}
+
+// A compute warp's transpose tiles (4 blocks x 72 floats) inside its slot: the warp's own rows
+// of the x plane, which no other warp reads and which it has read into registers (v) before its
+// first transpose.
+template <int CR>
+__device__ __forceinline__ float* primal_tiles(float* slot, int warp) {
+  return slot + (1 + warp * 8 * CR) * kPrimalSpan;
 }
 
 // The dynamic shared memory of a primal CTA: the slots' boxes (x, p1, p2), then their levels.
@@ -680,7 +688,7 @@ __device__ __forceinline__ void primal_issue(float* box, std::int16_t* levels, c
 // when every compute warp is done with it, and only then is the slot loaded again, so the
 // compute warps never wait for one another.
 template <int CR, int CC, bool KEEP>
-__global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
+__global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1), 3)
     primal_tma_kernel(const __grid_constant__ CUtensorMap map0, const __grid_constant__ CUtensorMap map1,
                       const __grid_constant__ PrimalBatch Q) {
   constexpr unsigned kAll = 0xffffffffu;
@@ -695,7 +703,6 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
   __shared__ __align__(8) std::uint64_t full[S], empty[S];
   __shared__ ProxFactors factors[2];
   __shared__ PrimalParams parts[2];  // the components' parameters, read per item
-  __shared__ float tile[NB][4][72];
   __shared__ int failures;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int z = 0; z < Q.count; ++z) {
@@ -735,7 +742,6 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
     }
   } else {
     const int blk = lane / L, in_block = lane % L;
-    float* t = tile[warp][blk];
     // The flat flag of the lane's block in an item, read an item ahead of its use.
     auto flag_of = [&](const ItemWalk& w) -> std::uint8_t {
       const PrimalParams& P = parts[w.z];
@@ -768,8 +774,9 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
         if (lane == 0) atomicAdd(&failures, 1);
         break;
       }
-      const float* slot = ring + (s % S) * STRIDE;
+      float* const slot = ring + (s % S) * STRIDE;
       const std::int16_t* stage_levels = levels_ring + (s % S) * kStageLevels + (warp * B + blk) * 64;
+      float* const t = primal_tiles<CR>(slot, warp) + blk * 72;
       if (vby < vbr) {
         primal_block_row<CR, CC, KEEP>(slot, stage_levels, P, F, t, warp, lane, vby, j, column_in, in_blocks, flat,
                                        block, sum);
@@ -779,6 +786,8 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
       } else {
         sum1 += sum;
       }
+      // The warp's tile writes into the slot ordered before the next load's (async proxy) writes.
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) barrier_arrive(&empty[s % S]);  // the warp is done with the slot
     }
@@ -806,7 +815,7 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
 // factors are read from global memory. Nothing is kept (the batch's last primal step, which
 // keeps, runs per image).
 template <int CR, int CC>
-__global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
+__global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1), 3)
     primal_batch_kernel(const PrimalItem* __restrict__ list, int count, const PrimalBatchComponent* components,
                         int parity) {
   constexpr unsigned kAll = 0xffffffffu;
@@ -819,7 +828,6 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
   extern __shared__ __align__(128) float ring[];
   __shared__ __align__(8) std::uint64_t full[S], empty[S];
   __shared__ PrimalParams parts[S];  // of the items in the slots
-  __shared__ float tile[NB][4][72];
   __shared__ int failures;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int first = static_cast<int>(static_cast<long long>(blockIdx.x) * count / gridDim.x);
@@ -855,7 +863,6 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
     }
   } else {
     const int blk = lane / L, in_block = lane % L;
-    float* t = tile[warp][blk];
     double sum = 0.0;  // unused: nothing is kept
     for (int s = 0; s < items; ++s) {
       const PrimalItem item = list[first + s];
@@ -876,12 +883,15 @@ __global__ void __launch_bounds__(32 * (primal_warps<CR>() + 1))
       const std::size_t block =
           static_cast<std::size_t>(in_blocks ? vby : 0) * P.component.block_columns + (in_blocks ? vbx : 0);
       const bool flat = in_blocks && P.component.flat[block] != 0;
-      const float* slot = ring + (s % S) * STRIDE;
+      float* const slot = ring + (s % S) * STRIDE;
       const std::int16_t* stage_levels = levels_ring + (s % S) * kStageLevels + (warp * B + blk) * 64;
+      float* const t = primal_tiles<CR>(slot, warp) + blk * 72;
       if (vby < vbr) {
         primal_block_row<CR, CC, false>(slot, stage_levels, P, F, t, warp, lane, vby, j, column_in, in_blocks, flat,
                                         block, sum);
       }
+      // The warp's tile writes into the slot ordered before the next load's (async proxy) writes.
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) barrier_arrive(&empty[s % S]);  // the warp is done with the slot and its parameters
     }
@@ -1266,48 +1276,48 @@ __global__ void __launch_bounds__(256) conjugate_kernel(const ConjugateParams P)
   const bool in_blocks = active && vby < P.component.block_rows && vbx < P.component.block_columns;
   const int j0 = vbx * BW + m * CC, i0 = vby * BH;
   const bool counted = P.g.recorded_row(i0);
-  // xi = gamma div q at the lane's sample (row r of the block, sample c of its cell's row),
-  // q = scale (q1, q2); made where needed rather than kept (a block of 16 x 2 binary64 values a
-  // lane would hold the registers of half the CTAs an SM can run).
+  // xi = gamma div q at the lane's samples, q = scale (q1, q2).
   const double scale = P.most_at != nullptr ? negative_theta(*P.most_at, P.alpha1) : P.scale;
-  auto q_at = [&](const float* f, int i, int j) -> double {
-    return scale * static_cast<double>(f[static_cast<std::size_t>(i) * pitch + j]);
-  };
-  auto xi = [&](int r, int c) -> double {
-    const int i = i0 + r, j = j0 + c;
-    if (!active) return 0.0;
-    const double dy = (i + 1 < rows ? q_at(P.q2, i, j) : 0.0) - (i > 0 ? q_at(P.q2, i - 1, j) : 0.0);
-    const double dx = (j + 1 < columns ? q_at(P.q1, i, j) : 0.0) - (j > 0 ? q_at(P.q1, i, j - 1) : 0.0);
-    return P.gamma * (dy + dx);
-  };
+  auto q_at = [&](const float* f, int i, int j) -> double { return scale * static_cast<double>(f[static_cast<std::size_t>(i) * pitch + j]); };
+  double xi[BH][CC];
   double sums[8], means[8];
   double total = 0.0;
+#pragma unroll
+  for (int r = 0; r < BH; ++r) {
+#pragma unroll
+    for (int c = 0; c < CC; ++c) {
+      const int i = i0 + r, j = j0 + c;
+      double value = 0.0;
+      if (active) {
+        const double dy = (i + 1 < rows ? q_at(P.q2, i, j) : 0.0) - (i > 0 ? q_at(P.q2, i - 1, j) : 0.0);
+        const double dx = (j + 1 < columns ? q_at(P.q1, i, j) : 0.0) - (j > 0 ? q_at(P.q1, i, j - 1) : 0.0);
+        value = P.gamma * (dy + dx);
+      }
+      xi[r][c] = value;
+    }
+  }
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     double sum = 0.0;
 #pragma unroll
     for (int c = 0; c < CC; ++c) {
-      double column = xi(CR * r, c);
+      double column = xi[CR * r][c];
 #pragma unroll
-      for (int a = 1; a < CR; ++a) column += xi(CR * r + a, c);
+      for (int a = 1; a < CR; ++a) column += xi[CR * r + a][c];
       sum = c == 0 ? column : sum + column;
     }
     sums[r] = sum;
     means[r] = sum / static_cast<double>(CR * CC);
   }
   if (P.free && active) {
-    // A loop kept rolled, so that the compiler holds no value of the pass above for it.
-#pragma unroll 1
-    for (int r = 0; r < 8; ++r) {
-      double mean = means[0];
 #pragma unroll
-      for (int k = 1; k < 8; ++k) mean = k == r ? means[k] : mean;
+    for (int r = 0; r < 8; ++r) {
 #pragma unroll
       for (int a = 0; a < CR; ++a) {
 #pragma unroll
         for (int c = 0; c < CC; ++c) {
-          const double s = xi(CR * r + a, c);
-          total += in_blocks ? P.radius * fabs(s - mean) : 128.0 * s + P.radius * fabs(s);
+          const double s = xi[CR * r + a][c];
+          total += in_blocks ? P.radius * fabs(s - means[r]) : 128.0 * s + P.radius * fabs(s);
         }
       }
     }
@@ -1348,13 +1358,23 @@ __global__ void __launch_bounds__(256) residual_kernel(const ResidualParams P) {
 
 // One array of partials a CTA: the sum (or the largest) of its entries, each thread's strided
 // share in index order, then the CTA's fixed-order reduction.
-__global__ void __launch_bounds__(512) reduce_kernel(const __grid_constant__ Reductions R) {
+__global__ void __launch_bounds__(1024) reduce_kernel(const __grid_constant__ Reductions R) {
   const int k = blockIdx.x;
   const double* in = R.in[k];
   const int n = R.count[k];
   const bool most = R.largest[k] != 0;
-  double value = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) value = most ? fmax(value, in[i]) : value + in[i];
+  // Four accumulators a thread (entries i, i + T, i + 2T, i + 3T of each stretch of 4T), so that
+  // four loads are in flight; combined in a fixed order.
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  const int step = blockDim.x;
+  for (int i = threadIdx.x; i < n; i += 4 * step) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int at = i + u * step;
+      if (at < n) acc[u] = most ? fmax(acc[u], in[at]) : acc[u] + in[at];
+    }
+  }
+  const double value = most ? fmax(fmax(acc[0], acc[1]), fmax(acc[2], acc[3])) : (acc[0] + acc[1]) + (acc[2] + acc[3]);
   const double total = most ? cta_reduce<true>(value) : cta_reduce<false>(value);
   if (threadIdx.x == 0) R.out[k] = total;
 }
@@ -1662,7 +1682,7 @@ cudaError_t launch_conjugate(const ConjugateParams& p, cudaStream_t stream) {
 
 cudaError_t launch_reductions(const Reductions& r, cudaStream_t stream) {
   if (r.n == 0) return cudaSuccess;
-  reduce_kernel<<<r.n, 512, 0, stream>>>(r);
+  reduce_kernel<<<r.n, 1024, 0, stream>>>(r);
   return cudaGetLastError();
 }
 

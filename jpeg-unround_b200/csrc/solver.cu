@@ -528,6 +528,11 @@ struct Solver::Impl {
     dp.in = state[current];
     dp.out = state[1 - current];
     dp.tilde = tilde;
+    if (tgv && !plan.partial_radius) {
+      // TGV's records read p~ only for the partial gap: without it, the dual step keeps none.
+      dp.tilde.p1 = nullptr;
+      dp.tilde.p2 = nullptr;
+    }
     for (int c = 0; c < g.channels; ++c) {
       dp.sigma[c] = static_cast<float>(plan.sigma * plan.channel_weights[c]);
       dp.tau[c] = static_cast<float>(plan.tau * plan.channel_weights[c]);

@@ -291,7 +291,7 @@ __device__ __forceinline__ void dual_strip(const CUtensorMap* state_map, const C
           const float q1 = step_p1[c] * sp, q2 = step_p2[c] * sp;
           P.out.p1[base + here] = rho * q1 + rest * old_p1[c];
           P.out.p2[base + here] = rho * q2 + rest * old_p2[c];
-          if constexpr (KEEP) {
+          if (KEEP && P.tilde.p1 != nullptr) {  // p~: TV's records and the partial gap's
             P.tilde.p1[base + here] = q1;
             P.tilde.p2[base + here] = q2;
           }
