@@ -7,10 +7,25 @@
 #include <algorithm>
 #include <cmath>
 #include <limits>
+#include <thread>
 
 namespace urb {
 
 namespace {
+
+// body(first, end) over block rows [0, rows), shared out among the host's threads in contiguous
+// ranges (one thread for small pictures); returns once every range is done.
+template <typename Body>
+void in_parallel(std::uint32_t rows, const Body& body) {
+  const unsigned threads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const auto parts = static_cast<std::uint32_t>(std::min<std::uint32_t>(threads, std::max<std::uint32_t>(rows / 32, 1)));
+  std::vector<std::thread> workers;
+  for (std::uint32_t t = 1; t < parts; ++t) {
+    workers.emplace_back([&body, rows, t, parts] { body(rows * t / parts, rows * (t + 1) / parts); });
+  }
+  body(0, rows / parts);
+  for (std::thread& worker : workers) worker.join();
+}
 
 constexpr double kLevelShiftDc = 1024.0;  // 8 x 128 on DC (docs/math.md 1.1)
 constexpr std::uint32_t kBlock = 8;
@@ -160,11 +175,13 @@ bool make_component(const ComponentInput& input, std::uint32_t block_rows, std::
   // The kept blocks: the top-left block_rows x block_columns of the given ones.
   const std::size_t count = static_cast<std::size_t>(block_rows) * block_columns;
   out.levels.resize(count * 64);
-  for (std::uint32_t by = 0; by < block_rows; ++by) {
-    const std::int16_t* from = input.levels + (static_cast<std::size_t>(by) * input.columns) * 64;
-    std::copy(from, from + static_cast<std::size_t>(block_columns) * 64,
-              out.levels.begin() + static_cast<std::ptrdiff_t>(by) * block_columns * 64);
-  }
+  in_parallel(block_rows, [&](std::uint32_t first, std::uint32_t end) {
+    for (std::uint32_t by = first; by < end; ++by) {
+      const std::int16_t* from = input.levels + (static_cast<std::size_t>(by) * input.columns) * 64;
+      std::copy(from, from + static_cast<std::size_t>(block_columns) * 64,
+                out.levels.begin() + static_cast<std::ptrdiff_t>(by) * block_columns * 64);
+    }
+  });
   for (int k = 0; k < 64; ++k) {
     out.steps[k] = static_cast<double>(input.table[k]);
     out.weights[k] = mu / power_of(out.steps[k], data.power);
@@ -176,11 +193,12 @@ bool make_component(const ComponentInput& input, std::uint32_t block_rows, std::
   }
   // Flat blocks (docs/math.md 4.1): at most flat_levels AC levels not 0 and, with a bound,
   // a DC level within it of the blocks above, below, left and right.
-  out.flat.assign(count, 0);
+  out.flat.resize(count);  // every entry written below
   auto dc = [&](std::uint32_t by, std::uint32_t bx) {
     return static_cast<std::int32_t>(out.levels[(static_cast<std::size_t>(by) * block_columns + bx) * 64]);
   };
-  for (std::uint32_t by = 0; by < block_rows; ++by) {
+  in_parallel(block_rows, [&](std::uint32_t first, std::uint32_t end) {
+  for (std::uint32_t by = first; by < end; ++by) {
     for (std::uint32_t bx = 0; bx < block_columns; ++bx) {
       const std::int16_t* q = &out.levels[(static_cast<std::size_t>(by) * block_columns + bx) * 64];
       std::uint32_t nonzero = 0;
@@ -198,6 +216,7 @@ bool make_component(const ComponentInput& input, std::uint32_t block_rows, std::
       out.flat[static_cast<std::size_t>(by) * block_columns + bx] = flat ? 1 : 0;
     }
   }
+  });
   // MMSE centres: the Laplace scale of each AC frequency from the component's levels
   // (cpp/src/laplace.cpp:109-130), and delta / Q at rho = Q / beta.
   if (out.mmse) {

@@ -8,8 +8,11 @@
 
 #include <array>
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <optional>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "settings.hpp"
@@ -42,6 +45,27 @@ struct ComponentInput {
   std::array<std::uint16_t, 64> table{};
 };
 
+// An allocator whose resize leaves new elements uninitialised, so that a large array is first
+// touched by the threads that fill it rather than zeroed first by one.
+template <typename T>
+struct Uninitialised : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = Uninitialised<U>;
+  };
+  Uninitialised() = default;
+  template <typename U>
+  Uninitialised(const Uninitialised<U>&) noexcept {}
+  template <typename U>
+  void construct(U* at) noexcept {
+    ::new (static_cast<void*>(at)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* at, Args&&... args) {
+    ::new (static_cast<void*>(at)) U(std::forward<Args>(args)...);
+  }
+};
+
 // One component's problem on the canvas (cpp/src/model.cpp:124-256 and
 // rust/unround/src/model.rs Problem::new): the kept levels, the steps, the weights of
 // the data term in a block that is not flat and in one that is, which blocks are flat,
@@ -52,8 +76,8 @@ struct Component {
   std::uint32_t cell_rows = 1;     // canvas samples down per sample of the component
   std::uint32_t cell_columns = 1;  // and across
   bool free = false;               // some canvas samples are free (docs/math.md 1.3)
-  std::vector<std::int16_t> levels;  // [by][bx][64], natural order
-  std::vector<std::uint8_t> flat;    // [by][bx]
+  std::vector<std::int16_t, Uninitialised<std::int16_t>> levels;  // [by][bx][64], natural order
+  std::vector<std::uint8_t, Uninitialised<std::uint8_t>> flat;    // [by][bx]
   std::array<double, 64> steps{};
   std::array<double, 64> weights{};
   std::array<double, 64> flat_weights{};
