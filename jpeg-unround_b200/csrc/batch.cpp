@@ -93,12 +93,14 @@ struct Branches {
   }
 };
 
-// A class's tiles: strips of 32 columns of each of its pictures, cut into tiles of `rows` rows.
+// A class's tiles: strips of the sweep's width (sweep_width) of each of its pictures, cut into
+// tiles of `rows` rows.
 std::vector<DualTile> tiles_of(const DualClass& dual, int rows) {
   std::vector<DualTile> tiles;
+  const int width = sweep_width(dual.channels);
   for (std::size_t m = 0; m < dual.pictures.size(); ++m) {
     const Geometry& g = dual.geometry[m];
-    for (int x0 = 0; x0 < g.columns; x0 += 32) {
+    for (int x0 = 0; x0 < g.columns; x0 += width) {
       for (int i0 = 0; i0 < g.rows; i0 += rows) tiles.push_back({dual.pictures[m], x0, i0, std::min(i0 + rows, g.rows)});
     }
   }
@@ -252,7 +254,7 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
   PrimalBatchComponent* components_device = nullptr;
   cudaError_t error = owned.upload(images, &images_device);
   if (error == cudaSuccess) error = owned.upload(components, &components_device);
-  // Each class's tiles: strips of 32 columns cut into tiles of the height that finishes the
+  // Each class's tiles: strips of the sweep's width cut into tiles of the height that finishes the
   // class's pictures soonest in waves of the CTAs the device holds (the wave model), or, with
   // the autotuner (UNROUND_B200_AUTOTUNE=1), the height its measurement chose.
   int device = 0;

@@ -955,7 +955,7 @@ cudaError_t launch_one(const CUtensorMap& state, const CUtensorMap& tilde, const
     resident[device & 63].store(slots);
   }
   const int strips = (p.dual.g.columns + 31) / 32;
-  const int best = strip_rows_for(p.dual.g, slots);
+  const int best = strip_rows_for(p.dual.g, slots, 32);
   IterationParams q = p;
   q.strip_rows = best;
   const dim3 grid(strips, (p.dual.g.rows + best - 1) / best, 1);
@@ -1007,7 +1007,7 @@ cudaError_t launch_samples_one(const CUtensorMap& state, const CUtensorMap& tild
     resident[device & 63].store(slots);
   }
   const int strips = (p.dual.g.columns + 31) / 32;
-  const int best = strip_rows_for(p.dual.g, slots);
+  const int best = strip_rows_for(p.dual.g, slots, 32);
   SamplesIterationParams q = p;
   q.strip_rows = best;
   const dim3 grid(strips, (p.dual.g.rows + best - 1) / best, 1);

@@ -339,7 +339,11 @@ cudaError_t launch_conjugate(const ConjugateParams& p, cudaStream_t stream);
 cudaError_t launch_residual(const ResidualParams& p, cudaStream_t stream);
 // The dual step as a TMA-fed sweep (sweep.cu): `state` maps the input state's planes (fields x,
 // p1, p2 and for TGV w1, w2, r11, r22, r12, each channel after channel, one allocation), `tilde`
-// the planes of x~.
+// the planes of x~. A CTA sweeps a strip of sweep_width(channels) columns: with one channel each
+// lane takes two columns, so that a chunk's barriers and fixed work cover as many samples as
+// with more channels.
+__host__ __device__ constexpr int lane_columns(int channels) { return channels == 1 ? 2 : 1; }
+__host__ __device__ constexpr int sweep_width(int channels) { return 32 * lane_columns(channels); }
 std::size_t dual_tma_shared_bytes(bool tgv, int channels);
 bool make_sweep_map(CUtensorMap& map, const float* planes, const Geometry& g, int count);
 // The primal step fed by TMA, persistent CTAs over (component, strip, stage) items: `maps[z]`
@@ -361,8 +365,8 @@ int primal_tma_grid_blocks(const Geometry& g, const ComponentDevice& c);
 cudaError_t launch_primal_tma(const CUtensorMap* maps, const PrimalParams* parts, int count, bool keep,
                               cudaStream_t stream, int* grid);
 // The rows a CTA of a strip sweep walks (a multiple of 16) so that the sweep's CTAs, `slots`
-// of them resident at once, finish soonest (sweep.cu).
-int strip_rows_for(const Geometry& g, int slots);
+// of them resident at once, finish soonest (sweep.cu); strips of `width` columns.
+int strip_rows_for(const Geometry& g, int slots, int width);
 
 // The batched solve (batch.cu): one launch steps many images' states. A component's or an
 // image's entry holds its tensor maps and parameters for each state parity (the state the step
