@@ -204,7 +204,8 @@ unround_status unround_b200_decode_centres_noalloc(const unround_input* input, c
  * NCCL). A plan that records before its last iteration, or stops at a tolerance, is recorded
  * across the ranks by the functions below.
  *   _new     the strip's solver, started (the start s_0 on the device);
- *   _step    `iterations` iterations keeping nothing, waited for; the last one is _finish's;
+ *   _step    `iterations` iterations keeping nothing, waited for; the last one is _finish's
+ *            (_run below makes them with the exchanges, not waited for);
  *   _state   the device planes of the current state (x, p1, p2, and for TGV w1, w2, r11, r22,
  *            r12, each channel after channel), rows x columns each, rows `pitch` floats apart:
  *            returns the count, up to `most` written;
@@ -250,6 +251,37 @@ unround_status unround_b200_strip_record_duals(unround_b200_strip* strip, double
                                                char* message, size_t message_size);
 unround_status unround_b200_strip_result(unround_b200_strip* strip, int32_t stop, unround_result** result,
                                          char* message, size_t message_size);
+
+/* The halo swaps inside the library. An exchange copies `rows` canvas rows of every state plane
+ * (as _state lists them) from the strip `sender`, starting at its row `sender_row`, over the
+ * rows of the strip `receiver` starting at `receiver_row` (the python strips module's
+ * exchanges()).
+ *   _run             `iterations` iterations of the strip, each followed by the exchanges in
+ *                    which `rank` sends or receives (sender and receiver are ranks of the NCCL
+ *                    communicator `comm`, an ncclComm_t; a rank may exchange with itself): every
+ *                    plane's rows one ncclSend or ncclRecv, all of an iteration in one NCCL
+ *                    group, on the strip's stream after its kernels; the call returns without
+ *                    waiting for the device (the next _record or _result waits). `iterations` 0:
+ *                    the exchanges only. NCCL is the libnccl.so.2 already loaded in the process
+ *                    (the one torch.distributed uses), else the one the loader finds; the last
+ *                    iteration is _record's or _finish's.
+ *   _exchange_local  the exchanges among `count` strips of one process and device (sender and
+ *                    receiver index `strips`): device copies on each receiver's stream after the
+ *                    sender's work so far, and each sender's later work after the copies of its
+ *                    rows; not waited for. */
+typedef struct unround_b200_strip_exchange {
+  int32_t sender;
+  int32_t receiver;
+  uint64_t sender_row;
+  uint64_t receiver_row;
+  uint64_t rows;
+} unround_b200_strip_exchange;
+unround_status unround_b200_strip_run(unround_b200_strip* strip, uint64_t iterations, int32_t rank,
+                                      const unround_b200_strip_exchange* exchanges, uint64_t count, void* comm,
+                                      char* message, size_t message_size);
+unround_status unround_b200_strip_exchange_local(unround_b200_strip* const* strips, uint64_t count,
+                                                 const unround_b200_strip_exchange* exchanges,
+                                                 uint64_t exchange_count, char* message, size_t message_size);
 
 /* The failure path of the bounded waits (no counterpart in the reference, whose solver has no
  * device): every wait of a kernel on an mbarrier is bounded, and one that runs out sets an error

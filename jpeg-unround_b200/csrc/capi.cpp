@@ -16,6 +16,8 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 #include <zlib.h>
 
 #include "batch.hpp"
@@ -1840,6 +1842,206 @@ unround_status unround_b200_strip_result(unround_b200_strip* strip, int32_t stop
 }
 
 void unround_b200_strip_free(unround_b200_strip* strip) { delete strip; }
+
+extern "C++" {
+namespace {
+
+// The NCCL calls of the halo swaps, from the libnccl.so.2 the process has loaded (torch's, whose
+// communicators the callers hand over), else the one the loader finds; looked up once.
+struct NcclCalls {
+  decltype(&ncclSend) send = nullptr;
+  decltype(&ncclRecv) recv = nullptr;
+  decltype(&ncclGroupStart) group_start = nullptr;
+  decltype(&ncclGroupEnd) group_end = nullptr;
+  decltype(&ncclGetErrorString) text = nullptr;
+  bool found() const { return send && recv && group_start && group_end && text; }
+};
+
+const NcclCalls& nccl_calls() {
+  static const NcclCalls calls = [] {
+    NcclCalls c;
+    void* library = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+    if (library == nullptr) library = dlopen("libnccl.so.2", RTLD_NOW);
+    if (library == nullptr) return c;
+    c.send = reinterpret_cast<decltype(&ncclSend)>(dlsym(library, "ncclSend"));
+    c.recv = reinterpret_cast<decltype(&ncclRecv)>(dlsym(library, "ncclRecv"));
+    c.group_start = reinterpret_cast<decltype(&ncclGroupStart)>(dlsym(library, "ncclGroupStart"));
+    c.group_end = reinterpret_cast<decltype(&ncclGroupEnd)>(dlsym(library, "ncclGroupEnd"));
+    c.text = reinterpret_cast<decltype(&ncclGetErrorString)>(dlsym(library, "ncclGetErrorString"));
+    return c;
+  }();
+  return calls;
+}
+
+// Whether each exchange's rows lie within the canvases of the strips it names (`rows_of(strip)`
+// the canvas rows of a strip, -1 for a strip that this call does not hold).
+template <class RowsOf>
+bool exchanges_fit(const unround_b200_strip_exchange* exchanges, uint64_t count, RowsOf rows_of,
+                   urb::Failure& failure) {
+  for (uint64_t e = 0; e < count; ++e) {
+    const unround_b200_strip_exchange& x = exchanges[e];
+    const long long sender_rows = rows_of(x.sender), receiver_rows = rows_of(x.receiver);
+    const bool sender_fits = sender_rows < 0 || (x.sender_row <= static_cast<uint64_t>(sender_rows) &&
+                                                 x.rows <= static_cast<uint64_t>(sender_rows) - x.sender_row);
+    const bool receiver_fits = receiver_rows < 0 || (x.receiver_row <= static_cast<uint64_t>(receiver_rows) &&
+                                                     x.rows <= static_cast<uint64_t>(receiver_rows) - x.receiver_row);
+    if (x.sender < 0 || x.receiver < 0 || !sender_fits || !receiver_fits) {
+      failure = {urb::kArgument, "exchange " + std::to_string(e) + " names a strip that does not hold its rows"};
+      return false;
+    }
+  }
+  return true;
+}
+
+// This rank's part of the exchanges, one NCCL group on the strip's stream.
+bool exchange_nccl(unround_b200_strip* strip, int32_t rank, const unround_b200_strip_exchange* exchanges,
+                   uint64_t count, ncclComm_t comm, urb::Failure& failure) {
+  const NcclCalls& nccl = nccl_calls();
+  float* planes[64];
+  const int n = strip->solver->state_planes(planes, 64);
+  const std::size_t pitch = static_cast<std::size_t>(strip->solver->geometry().pitch);
+  const cudaStream_t on = strip->solver->stream();
+  ncclResult_t result = nccl.group_start();
+  for (uint64_t e = 0; e < count && result == ncclSuccess; ++e) {
+    const unround_b200_strip_exchange& x = exchanges[e];
+    const std::size_t floats = x.rows * pitch;  // a plane's rows are contiguous, `pitch` floats each
+    for (int k = 0; k < n && result == ncclSuccess && x.sender == rank; ++k) {
+      result = nccl.send(planes[k] + x.sender_row * pitch, floats, ncclFloat32, x.receiver, comm, on);
+    }
+    for (int k = 0; k < n && result == ncclSuccess && x.receiver == rank; ++k) {
+      result = nccl.recv(planes[k] + x.receiver_row * pitch, floats, ncclFloat32, x.sender, comm, on);
+    }
+  }
+  const ncclResult_t ended = nccl.group_end();
+  if (result == ncclSuccess) result = ended;
+  if (result == ncclSuccess) return true;
+  failure = {urb::kInternal, std::string("the halo exchange through NCCL: ") + nccl.text(result)};
+  return false;
+}
+
+bool involves(const unround_b200_strip_exchange* exchanges, uint64_t count, int32_t rank) {
+  for (uint64_t e = 0; e < count; ++e) {
+    if (exchanges[e].sender == rank || exchanges[e].receiver == rank) return true;
+  }
+  return false;
+}
+
+}  // namespace
+}  // extern "C++"
+
+unround_status unround_b200_strip_run(unround_b200_strip* strip, uint64_t iterations, int32_t rank,
+                                      const unround_b200_strip_exchange* exchanges, uint64_t count, void* comm,
+                                      char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (strip == nullptr || !strip->solver || (exchanges == nullptr && count > 0)) {
+      failure = {urb::kArgument, "the strip (not finished) and the exchanges are not null pointers"};
+      return false;
+    }
+    if (strip->done + iterations >= strip->plan.iterations && iterations > 0) {
+      failure = {urb::kArgument, "the strip's last iteration is made by unround_b200_strip_record or _finish"};
+      return false;
+    }
+    const long long rows = strip->solver->geometry().rows;
+    // The rows on this rank's side of each exchange; the other side's are its peer's to check.
+    auto rows_of = [&](int32_t who) { return who == rank ? rows : -1LL; };
+    if (!exchanges_fit(exchanges, count, rows_of, failure)) return false;
+    const bool swapping = involves(exchanges, count, rank);
+    if (swapping && comm == nullptr) {
+      failure = {urb::kArgument, "the NCCL communicator is not a null pointer"};
+      return false;
+    }
+    if (swapping && !nccl_calls().found()) {
+      failure = {urb::kInternal, "NCCL (libnccl.so.2) could not be loaded"};
+      return false;
+    }
+    const auto communicator = static_cast<ncclComm_t>(comm);
+    for (uint64_t n = 0; n < iterations; ++n) {
+      if (!strip->solver->advance(1, failure)) return false;
+      ++strip->done;
+      if (swapping && !exchange_nccl(strip, rank, exchanges, count, communicator, failure)) return false;
+    }
+    if (iterations == 0 && swapping) return exchange_nccl(strip, rank, exchanges, count, communicator, failure);
+    return true;
+  });
+}
+
+unround_status unround_b200_strip_exchange_local(unround_b200_strip* const* strips, uint64_t count,
+                                                 const unround_b200_strip_exchange* exchanges,
+                                                 uint64_t exchange_count, char* message, size_t message_size) {
+  return guarded(message, message_size, [&](urb::Failure& failure) {
+    if (strips == nullptr || (exchanges == nullptr && exchange_count > 0)) {
+      failure = {urb::kArgument, "the strips and the exchanges are not null pointers"};
+      return false;
+    }
+    for (uint64_t s = 0; s < count; ++s) {
+      if (strips[s] == nullptr || !strips[s]->solver) {
+        failure = {urb::kArgument, "strip " + std::to_string(s) + " is a null pointer or finished"};
+        return false;
+      }
+    }
+    auto rows_of = [&](int32_t who) {
+      return static_cast<uint64_t>(who) < count ? static_cast<long long>(strips[who]->solver->geometry().rows)
+                                                : -2LL;
+    };
+    for (uint64_t e = 0; e < exchange_count; ++e) {
+      if (rows_of(exchanges[e].sender) == -2 || rows_of(exchanges[e].receiver) == -2) {
+        failure = {urb::kArgument, "exchange " + std::to_string(e) + " names a strip beyond the " +
+                                       std::to_string(count) + " given"};
+        return false;
+      }
+    }
+    if (!exchanges_fit(exchanges, exchange_count, rows_of, failure)) return false;
+    for (uint64_t e = 0; e < exchange_count; ++e) {
+      const urb::Solver& from = *strips[exchanges[e].sender]->solver;
+      const urb::Solver& to = *strips[exchanges[e].receiver]->solver;
+      if (from.state_planes(nullptr, 0) != to.state_planes(nullptr, 0) ||
+          from.geometry().columns != to.geometry().columns) {
+        failure = {urb::kArgument, "exchange " + std::to_string(e) + " joins strips of different widths or fields"};
+        return false;
+      }
+    }
+    // Events: each strip's work so far (the senders' rows are ready), then each receiver's copies
+    // (the senders' later steps overwrite nothing still being read).
+    std::vector<cudaEvent_t> ready(count, nullptr), copied(count, nullptr);
+    cudaError_t error = cudaSuccess;
+    for (uint64_t s = 0; s < count && error == cudaSuccess; ++s) {
+      error = cudaEventCreateWithFlags(&ready[s], cudaEventDisableTiming);
+      if (error == cudaSuccess) error = cudaEventCreateWithFlags(&copied[s], cudaEventDisableTiming);
+      if (error == cudaSuccess) error = cudaEventRecord(ready[s], strips[s]->solver->stream());
+    }
+    for (uint64_t e = 0; e < exchange_count && error == cudaSuccess; ++e) {
+      const unround_b200_strip_exchange& x = exchanges[e];
+      urb::Solver& from = *strips[x.sender]->solver;
+      urb::Solver& to = *strips[x.receiver]->solver;
+      float* sent[64];
+      float* received[64];
+      const int n = from.state_planes(sent, 64);
+      to.state_planes(received, 64);
+      const std::size_t from_pitch = static_cast<std::size_t>(from.geometry().pitch);
+      const std::size_t to_pitch = static_cast<std::size_t>(to.geometry().pitch);
+      const std::size_t width = static_cast<std::size_t>(from.geometry().columns) * sizeof(float);
+      error = cudaStreamWaitEvent(to.stream(), ready[x.sender], 0);
+      for (int k = 0; k < n && error == cudaSuccess; ++k) {
+        error = cudaMemcpy2DAsync(received[k] + x.receiver_row * to_pitch, to_pitch * sizeof(float),
+                                  sent[k] + x.sender_row * from_pitch, from_pitch * sizeof(float), width, x.rows,
+                                  cudaMemcpyDeviceToDevice, to.stream());
+      }
+    }
+    for (uint64_t s = 0; s < count && error == cudaSuccess; ++s) {
+      error = cudaEventRecord(copied[s], strips[s]->solver->stream());
+    }
+    for (uint64_t e = 0; e < exchange_count && error == cudaSuccess; ++e) {
+      error = cudaStreamWaitEvent(strips[exchanges[e].sender]->solver->stream(), copied[exchanges[e].receiver], 0);
+    }
+    for (uint64_t s = 0; s < count; ++s) {
+      if (ready[s] != nullptr) cudaEventDestroy(ready[s]);
+      if (copied[s] != nullptr) cudaEventDestroy(copied[s]);
+    }
+    if (error == cudaSuccess) return true;
+    failure = {urb::kInternal, std::string("the halo exchange between strips: ") + cudaGetErrorString(error)};
+    return false;
+  });
+}
 
 // The C layer's PNG reading and writing (c/jpegio/include/unround/jpegio.h:225-256), by png_io.hpp.
 unround_jpegio_status unround_jpegio_read_png(const uint8_t* data, size_t size, uint64_t max_pixels,

@@ -1116,6 +1116,21 @@ bool Solver::step(std::uint64_t iterations, Failure& failure) {
   return m.check(failure, "the strip's iterations");
 }
 
+bool Solver::advance(std::uint64_t iterations, Failure& failure) {
+  Impl& m = *impl_;
+  for (std::uint64_t n = 0; n < iterations && m.error == cudaSuccess; ++n) {
+    m.primal(false);
+    m.dual(false);
+  }
+  if (m.error == cudaSuccess) m.error = cudaGetLastError();
+  if (m.error == cudaSuccess) return true;
+  failure.status = kInternal;
+  failure.message = std::string("the device failed in the strip's iterations: ") + describe(m.error);
+  return false;
+}
+
+cudaStream_t Solver::stream() const { return impl_->stream; }
+
 void Solver::set_record_rows(int first, int end) {
   impl_->g.record_first = first;
   impl_->g.record_end = end;

@@ -104,6 +104,10 @@ class Solver {
   // p2, and for TGV w1, w2, r11, r22, r12), each channel after channel, rows `pitch` floats apart.
   // Returns how many planes there are (up to `most` written).
   bool step(std::uint64_t iterations, Failure& failure);
+  // The same iterations launched on the stream and not waited for (the next record or result
+  // checks the device).
+  bool advance(std::uint64_t iterations, Failure& failure);
+  cudaStream_t stream() const;
   int state_planes(float** planes, int most) const;
   // A strip's records, which the ranks add up (strips.py): the canvas rows [first, end) whose
   // terms its records count (its own bands); one iteration keeping its tilde point (none with

@@ -15,11 +15,15 @@ and the owned rows of the canvases make the picture's canvas.
   sub_image        a strip's bands of a JPEG file's components, as an Image
   exchanges        the rows each neighbour pair swaps: (sender, sender's first row, receiver,
                    receiver's first row, rows)
-  exchange         the swap over torch.distributed (NCCL for device tensors, gloo on the CPU)
+  exchange         the swap over torch.distributed from Python (gloo on the CPU; NCCL where the
+                   library's own swap cannot be used)
   combine          a record of the picture from every rank's sums
   solve_in_strips  the whole solve with the strips in one process on one GPU (the ranks
-                   emulated, the swaps device copies between them), for tests and one device
-  solve_strip      a rank's part of it under torch.distributed (one process per GPU)
+                   emulated, the swaps device copies between them inside the library), for tests
+                   and one device
+  solve_strip      a rank's part of it under torch.distributed (one process per GPU; the
+                   iterations between records and their swaps one library call, NCCL sends and
+                   receives on the strip's stream with no host wait)
 """
 
 from __future__ import annotations
@@ -159,6 +163,17 @@ class StripSolver:
         status = self._library.unround_b200_strip_step(self._handle, iterations, message, self._native._MESSAGE)
         self._native._raise(status, message)
 
+    def run(self, iterations: int, rank: int = 0, swaps: Sequence[tuple[int, int, int, int, int]] = (),
+            comm: int | None = None) -> None:
+        """`iterations` iterations (0: none), each followed by the exchanges of `swaps` (as
+        exchanges() gives them) in which `rank` takes part, through the NCCL communicator `comm`
+        (an ncclComm_t's address) on the strip's stream; not waited for."""
+        table, count = _exchange_table(swaps)
+        message = ctypes.create_string_buffer(self._native._MESSAGE)
+        status = self._library.unround_b200_strip_run(self._handle, iterations, rank, table, count, comm, message,
+                                                      self._native._MESSAGE)
+        self._native._raise(status, message)
+
     def planes(self) -> list:
         """The current state's planes as device tensors that alias the solver's memory."""
         import torch
@@ -231,6 +246,32 @@ class StripSolver:
             self._handle = None
 
 
+class _Exchange(ctypes.Structure):
+    _fields_ = [("sender", ctypes.c_int32), ("receiver", ctypes.c_int32), ("sender_row", ctypes.c_uint64),
+                ("receiver_row", ctypes.c_uint64), ("rows", ctypes.c_uint64)]
+
+
+def _exchange_table(swaps: Sequence[tuple[int, int, int, int, int]]) -> tuple[object, int]:
+    table = (_Exchange * max(1, len(swaps)))()
+    for k, (sender, s_row, receiver, r_row, count) in enumerate(swaps):
+        table[k] = _Exchange(sender, receiver, s_row, r_row, count)
+    return table, len(swaps)
+
+
+def exchange_local(solvers: Sequence[StripSolver], swaps: Sequence[tuple[int, int, int, int, int]]) -> None:
+    """The swaps among strips of one process (sender and receiver index `solvers`): device copies
+    ordered after each sender's work so far and before its next, not waited for."""
+    if not solvers:
+        return
+    first = solvers[0]
+    handles = (ctypes.c_void_p * len(solvers))(*[s._handle.value for s in solvers])
+    table, count = _exchange_table(swaps)
+    message = ctypes.create_string_buffer(first._native._MESSAGE)
+    status = first._library.unround_b200_strip_exchange_local(handles, len(solvers), table, count, message,
+                                                              first._native._MESSAGE)
+    first._native._raise(status, message)
+
+
 def _bind(library: ctypes.CDLL) -> None:
     text = (ctypes.c_char_p, ctypes.c_size_t)
     u64, u64p, handle = ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p
@@ -245,6 +286,9 @@ def _bind(library: ctypes.CDLL) -> None:
         "unround_b200_strip_record": (ctypes.c_int32, handle, ctypes.c_int32, ctypes.c_void_p, *text),
         "unround_b200_strip_record_duals": (ctypes.c_int32, handle, ctypes.c_double, ctypes.c_void_p, *text),
         "unround_b200_strip_result": (ctypes.c_int32, handle, ctypes.c_int32, ctypes.POINTER(handle), *text),
+        "unround_b200_strip_run": (ctypes.c_int32, handle, u64, ctypes.c_int32, ctypes.c_void_p, u64, ctypes.c_void_p,
+                                   *text),
+        "unround_b200_strip_exchange_local": (ctypes.c_int32, ctypes.c_void_p, u64, ctypes.c_void_p, u64, *text),
     }
     for name, (result, *arguments) in table.items():
         function = getattr(library, name)
@@ -332,16 +376,16 @@ def _met(plan: StripPlan, values: tuple[float, ...], samples: float) -> bool:
     return plan.partial_tolerance > 0.0 and not math.isnan(partial_gap) and partial_gap / samples <= plan.partial_tolerance
 
 
-def _drive(plan: StripPlan, step: Callable[[], None], swap: Callable[[], None],
-           firsts_of: Callable[[bool], Sequence[Sequence[float]]],
+def _drive(plan: StripPlan, run: Callable[[int], None], firsts_of: Callable[[bool], Sequence[Sequence[float]]],
            seconds_of: Callable[[float], Sequence[Sequence[float]]]) -> tuple[list[tuple], int, int]:
     """The method's loop over the strips, as the whole solve runs it: a record at 0 (where the plan
     records) and at every recorded iteration, each the ranks' sums combined; the halos swapped
-    after the start and after every iteration; a tolerance met stops every rank there. Returns
-    the records (iteration, seconds 0, primal, dual, scaling, partial gap), the iterations made
-    and the stop (1 converged, 2 iterations)."""
+    after the start and after every iteration; a tolerance met stops every rank there. `run(k)`
+    makes k iterations, each followed by the swap (k = 0: the swap alone); the iterations between
+    two records are one call. Returns the records (iteration, seconds 0, primal, dual, scaling,
+    partial gap), the iterations made and the stop (1 converged, 2 iterations)."""
     records: list[tuple] = []
-    swap()  # the start's halos
+    run(0)  # the start's halos
 
     def take(iteration: int, advance: bool) -> bool:
         values, samples = combine(plan, firsts_of(advance), seconds_of)
@@ -350,15 +394,19 @@ def _drive(plan: StripPlan, step: Callable[[], None], swap: Callable[[], None],
 
     if (plan.record_every > 0 or plan.iterations == 0) and take(0, False):
         return records, 0, 1
-    for n in range(1, plan.iterations + 1):
-        if plan.recorded(n):
-            met = take(n, True)
-            swap()
-            if met:
-                return records, n, 1
-        else:
-            step()
-            swap()
+    n = 0
+    while n < plan.iterations:
+        # The next recorded iteration (the last one always is).
+        recorded = plan.iterations
+        if plan.record_every > 0:
+            recorded = min(plan.iterations, (n // plan.record_every + 1) * plan.record_every)
+        if recorded - 1 > n:
+            run(recorded - 1 - n)
+        n = recorded
+        met = take(n, True)
+        run(0)
+        if met:
+            return records, n, 1
     return records, plan.iterations, 2
 
 
@@ -384,19 +432,17 @@ def solve_in_strips(image: jpegio.Image, options: list[str], strips: int = 2) ->
         solver.set_rows((part.first - part.low) * rows, (part.end - part.low) * rows)
     plan = solvers[0].plan()
 
-    def swap() -> None:
-        planes = [solver.planes() for solver in solvers]
-        torch.cuda.synchronize()
-        for sender, s_row, receiver, r_row, count in exchanges(parts, rows):
-            for source, target in zip(planes[sender], planes[receiver]):
-                target[r_row : r_row + count].copy_(source[s_row : s_row + count])
-        torch.cuda.synchronize()
+    swaps = exchanges(parts, rows)
 
-    def step() -> None:
-        for solver in solvers:
-            solver.step(1)
+    def run(count: int) -> None:
+        for _ in range(count):
+            for solver in solvers:
+                solver.run(1)
+            exchange_local(solvers, swaps)
+        if count == 0:
+            exchange_local(solvers, swaps)
 
-    records, iterations, stop = _drive(plan, step, swap, lambda advance: [s.record(advance) for s in solvers],
+    records, iterations, stop = _drive(plan, run, lambda advance: [s.record(advance) for s in solvers],
                                        lambda theta: [s.record_duals(theta) for s in solvers])
     decoded = [solver.result(stop) for solver in solvers]
     canvas = np.concatenate([_own_rows(d, part, rows) for d, part in zip(decoded, parts)], axis=1)
@@ -415,18 +461,51 @@ def _gathered(values: Sequence[float], group: object) -> list[list[float]]:
     return [t.cpu().tolist() for t in every]
 
 
+def _communicator(group: object) -> int | None:
+    """The address of `group`'s NCCL communicator on this rank's device (torch's
+    ProcessGroupNCCL), made by a first collective; None where the backend is not NCCL or torch does
+    not expose it."""
+    import torch
+    import torch.distributed as dist
+
+    if dist.get_backend(group) != "nccl":
+        return None
+    owner = group if group is not None else dist.distributed_c10d._get_default_group()
+    try:
+        dist.all_reduce(torch.zeros(1, device="cuda"), group=group)
+        backend = owner._get_backend(torch.device("cuda", torch.cuda.current_device()))
+        return int(backend._comm_ptr())
+    except (AttributeError, RuntimeError):
+        return None
+
+
 def drive_rank(solver: object, parts: list[Strip], rank: int, rows: int, group: object = None) -> tuple:
     """This rank's loop over its strip's `solver` (a StripSolver, or any object with its plan,
     set_rows, step, planes, record, record_duals and result): the swaps with its neighbours and
-    the records gathered from every rank. Returns (the result of the strip, the records, the
+    the records gathered from every rank. With NCCL and a StripSolver the iterations between two
+    records and their swaps are one library call (StripSolver.run: NCCL sends and receives of
+    torch's communicator on the strip's stream, no host wait); otherwise each iteration is a step
+    and a swap through torch.distributed. Returns (the result of the strip, the records, the
     iterations made, the stop)."""
     part = parts[rank]
     solver.set_rows((part.first - part.low) * rows, (part.end - part.low) * rows)
     plan = solver.plan()
-    records, iterations, stop = _drive(
-        plan, lambda: solver.step(1), lambda: exchange(solver.planes(), parts, rank, rows, group),
-        lambda advance: _gathered(solver.record(advance), group),
-        lambda theta: _gathered(solver.record_duals(theta), group))
+    comm = _communicator(group) if isinstance(solver, StripSolver) else None
+    if comm is not None:
+        swaps = exchanges(parts, rows)
+
+        def run(count: int) -> None:
+            solver.run(count, rank, swaps, comm)
+    else:
+        def run(count: int) -> None:
+            for _ in range(count):
+                solver.step(1)
+                exchange(solver.planes(), parts, rank, rows, group)
+            if count == 0:
+                exchange(solver.planes(), parts, rank, rows, group)
+
+    records, iterations, stop = _drive(plan, run, lambda advance: _gathered(solver.record(advance), group),
+                                       lambda theta: _gathered(solver.record_duals(theta), group))
     return solver.result(stop), records, iterations, stop
 
 

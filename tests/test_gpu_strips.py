@@ -106,3 +106,46 @@ def test_strips_stop_at_a_tolerance_with_the_whole_solve():
     assert parts.stop == 1 and parts.iterations == 60
     np.testing.assert_allclose(parts.history.primal, whole.result.history.primal, rtol=1e-9, atol=0)
     assert np.linalg.norm(parts.canvas - whole.canvas) / np.linalg.norm(whole.canvas) <= 1e-5
+
+
+def test_nccl_exchange_equals_the_local_one():
+    """The library's swap through NCCL (unround_b200_strip_run, torch's communicator at one rank,
+    a strip exchanging rows with itself) against its swap of device copies
+    (unround_b200_strip_exchange_local): after each of five iterations, every state plane bit for
+    bit, and the exchanged rows equal to their sources."""
+    import os
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from unround import synthetic
+    from unround.strips import StripSolver, _communicator, exchange_local
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    image = synthetic.colour(161, 120, quality=60, seed=5, noise=2.0).image
+    given = ["--method", "tgv", "--iterations", "20", "--tolerance", "0", "--record-every", "0"]
+    # (sender, its first row, receiver, its first row, rows): disjoint sources and targets.
+    swaps = [(0, 0, 0, 48, 16), (0, 96, 0, 16, 8)]
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        comm = _communicator(None)
+        assert comm is not None, "torch exposes no NCCL communicator"
+        through_nccl, local = StripSolver(image, given), StripSolver(image, given)
+        through_nccl.run(5, 0, swaps, comm)
+        for _ in range(5):
+            local.run(1)
+            exchange_local([local], swaps)
+        torch.cuda.synchronize()
+        mine = [t.clone() for t in through_nccl.planes()]
+        theirs = [t.clone() for t in local.planes()]
+    finally:
+        dist.destroy_process_group()
+    assert len(mine) == len(theirs) == 8 * 3
+    for k, (a, b) in enumerate(zip(mine, theirs)):
+        assert torch.equal(a, b), f"plane {k}"
+        assert torch.equal(a[48:64], a[0:16]) and torch.equal(a[16:24], a[96:104]), f"plane {k}"
