@@ -769,15 +769,12 @@ def _unrolled_backward_launches(iterations: int, every: int) -> int:
     return launches + (iterations - 1) + iterations
 
 
-def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
-    """The differentiable unrolled TGV solve of 16 greyscale 512x512 pictures (quality 30),
-    100 iterations, checkpoints every 10: a step is one forward pass with the loss
-    (MSE against the clean pictures) and its backward pass (the adjoint) to the gradients of
-    every picture's alpha0, alpha1, tau and sigma. value: pixel-iterations of the forward and
-    backward pass per second (device time by CUDA events); forward: the same of the forward
-    pass alone; ratio: (forward + backward) / forward. every_iterate_kept: the forward and
-    backward pass with a checkpoint every iteration (no state recomputed; 9 planes an iteration
-    in HBM)."""
+def _unrolled_measure(steps: int, warmup: int, rank: int) -> dict:
+    """The differentiable unrolled TGV solve of 16 greyscale 512x512 pictures (quality 30), 100
+    iterations: per step one forward pass with the loss (MSE against the clean pictures), one
+    forward and backward pass (the adjoint) to the gradients of every picture's alpha0, alpha1, tau
+    and sigma with checkpoints every 10 iterations, and the same with a checkpoint every iteration
+    (no state recomputed; 9 planes an iteration in HBM); device times by CUDA events."""
     import numpy as np
     import torch
 
@@ -786,12 +783,11 @@ def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
 
     pictures, side, iterations, every = 16, 512, 100, 10
     made = [synthetic.grey(side, side, quality=30, seed=100 * rank + s, noise=2) for s in range(pictures)]
-    problem = UnrolledProblem([m.image for m in made], ["--method", "tgv", "--alpha1", "1", "--alpha0", "2"],
-                              iterations=iterations, checkpoint_every=every)
+    options = ["--method", "tgv", "--alpha1", "1", "--alpha0", "2"]
+    problem = UnrolledProblem([m.image for m in made], options, iterations=iterations, checkpoint_every=every)
     clean = torch.tensor(np.stack([m.samples for m in made]), dtype=torch.float32, device="cuda")
     base = [torch.full((pictures,), v, dtype=torch.float32, device="cuda")
             for v in (2.0, 1.0, problem.tau, problem.sigma)]
-    h2d = sum(m.image.components[0].coefficients.nbytes for m in made)
 
     def forward_only():
         with torch.no_grad():
@@ -802,71 +798,78 @@ def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
         leaves = [b.clone().requires_grad_(True) for b in base]
         loss = torch.mean((unrolled_tgv(problem, *leaves) - clean) ** 2)
         loss.backward()
-        return loss, leaves
+        return leaves
 
-    # The same with every iterate kept (a checkpoint every iteration: no recomputation).
-    kept = UnrolledProblem([m.image for m in made], ["--method", "tgv", "--alpha1", "1", "--alpha0", "2"],
-                           iterations=iterations, checkpoint_every=1)
+    kept = UnrolledProblem([m.image for m in made], options, iterations=iterations, checkpoint_every=1)
 
     def forward_backward_kept():
         leaves = [b.clone().requires_grad_(True) for b in base]
         torch.mean((unrolled_tgv(kept, *leaves) - clean) ** 2).backward()
 
-    for _ in range(max(3, args.warmup)):
+    for _ in range(max(3, warmup)):
         forward_only()
         forward_backward()
         forward_backward_kept()
     torch.cuda.synchronize()
     start, mid, end, last = (torch.cuda.Event(enable_timing=True) for _ in range(4))
-    steps = max(1, args.steps)
+    steps = max(1, steps)
     with Clocks(0) as clocks:
         start.record()
         for _ in range(steps):
             forward_only()
         mid.record()
         for _ in range(steps):
-            loss, leaves = forward_backward()
+            leaves = forward_backward()
         end.record()
         for _ in range(steps):
             forward_backward_kept()
         last.record()
         torch.cuda.synchronize()
-    forward_ms = start.elapsed_time(mid) / steps
-    both_ms = mid.elapsed_time(end) / steps
-    kept_ms = end.elapsed_time(last) / steps
     grads = torch.stack([leaf.grad for leaf in leaves]).cpu()  # the step's result read on the host
-    pixels = pictures * side * side
     # End to end: levels in from the host (the problem made from the files' levels), gradients out.
     began = time.perf_counter()
-    problem_e2e = UnrolledProblem([m.image for m in made], ["--method", "tgv", "--alpha1", "1", "--alpha0", "2"],
-                                  iterations=iterations, checkpoint_every=every)
+    problem_e2e = UnrolledProblem([m.image for m in made], options, iterations=iterations, checkpoint_every=every)
     leaves = [b.clone().requires_grad_(True) for b in base]
     torch.mean((unrolled_tgv(problem_e2e, *leaves) - clean) ** 2).backward()
     e2e_grads = torch.stack([leaf.grad for leaf in leaves]).cpu()
-    e2e_seconds = time.perf_counter() - began
+    return {"pictures": pictures, "side": side, "iterations": iterations, "every": every, "steps": steps,
+            "forward_ms": start.elapsed_time(mid) / steps, "both_ms": mid.elapsed_time(end) / steps,
+            "kept_ms": end.elapsed_time(last) / steps, "kept_bytes": kept.checkpoint_floats * 4,
+            "grad_finite": bool(torch.isfinite(grads).all()) and bool(torch.isfinite(e2e_grads).all()),
+            "e2e_seconds": time.perf_counter() - began, "e2e_d2h": int(e2e_grads.numel() * 4),
+            "h2d": sum(m.image.components[0].coefficients.nbytes for m in made), "clocks": clocks.summary()}
+
+
+def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
+    """The unrolled solve's line (_unrolled_measure). value: pixel-iterations of the forward and
+    backward pass per second; forward: the same of the forward pass alone; ratio: (forward +
+    backward) / forward; every_iterate_kept: the same with a checkpoint every iteration."""
+    m = _unrolled_measure(args.steps, args.warmup, rank)
     if rank != 0:
         return
+    pixels, iterations, every, steps = m["pictures"] * m["side"] ** 2, m["iterations"], m["every"], m["steps"]
     line = {
         "metric": "unrolled TGV forward+adjoint Mpx*iter/s on 1 B200 (16 x 512x512, 100 iterations, checkpoints 10)",
-        "value": pixels * iterations / (both_ms / 1e3) / 1e6, "unit": "Mpx*iter/s", "n_gpus": world, "steps": steps,
-        "warmup": max(3, args.warmup), "ms_per_step": both_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded piecewise-smooth + noise sigma 2, quality 30)",
-        "config": {"workload": "unrolled-tgv-16x512", "pictures": pictures, "iterations": iterations,
+        "value": pixels * iterations / (m["both_ms"] / 1e3) / 1e6, "unit": "Mpx*iter/s", "n_gpus": world,
+        "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": m["both_ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded piecewise-smooth + noise sigma 2, quality 30)",
+        "config": {"workload": "unrolled-tgv-16x512", "pictures": m["pictures"], "iterations": iterations,
                    "checkpoint_every": every, "loss": "MSE against the clean pictures",
                    "l2": "state 16 x 512^2 x 9 fields = 151 MB, larger than L2"},
-        "forward": {"value": pixels * iterations / (forward_ms / 1e3) / 1e6, "ms": forward_ms},
-        "forward_backward_over_forward": both_ms / forward_ms,
-        "every_iterate_kept": {"checkpoint_every": 1, "ms": kept_ms, "forward_backward_over_forward": kept_ms / forward_ms,
-                               "checkpoint_bytes": kept.checkpoint_floats * 4},
-        "grad_finite": bool(torch.isfinite(grads).all()) and bool(torch.isfinite(e2e_grads).all()),
-        "e2e": {"value": pixels * iterations / e2e_seconds / 1e6, "unit": "Mpx*iter/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": int(e2e_grads.numel() * 4)},
+        "forward": {"value": pixels * iterations / (m["forward_ms"] / 1e3) / 1e6, "ms": m["forward_ms"]},
+        "forward_backward_over_forward": m["both_ms"] / m["forward_ms"],
+        "every_iterate_kept": {"checkpoint_every": 1, "ms": m["kept_ms"],
+                               "forward_backward_over_forward": m["kept_ms"] / m["forward_ms"],
+                               "checkpoint_bytes": m["kept_bytes"]},
+        "grad_finite": m["grad_finite"],
+        "e2e": {"value": pixels * iterations / m["e2e_seconds"] / 1e6, "unit": "Mpx*iter/s",
+                "h2d_bytes_per_step": m["h2d"], "d2h_bytes_per_step": m["e2e_d2h"]},
         "gpu_launches": steps * (2 * _unrolled_forward_launches(iterations) + _unrolled_backward_launches(iterations, every)
                                  + _unrolled_forward_launches(iterations) + _unrolled_backward_launches(iterations, 1)),
-        "clocks": clocks.summary(),
+        "clocks": m["clocks"],
     }
     print(json.dumps(line))
-    del loss
 
 
 def main() -> None:
@@ -989,6 +992,8 @@ def main() -> None:
     parity = _parity(native.solve(image, OPTIONS), theirs, image) if theirs is not None else None
     # The batched mix beside (the batching workload): batched against image at a time.
     mixed = _mix_measure(64, 1, 3) if world == 1 else None
+    # The unrolled solve beside (the differentiation workload): forward+backward against forward.
+    unrolled = _unrolled_measure(3, 3, 0) if world == 1 else None
     peak, peak_kind = _peaks()
     copy = _copy_gbs()
     samples = timing.samples
@@ -1034,6 +1039,12 @@ def main() -> None:
                            "batched": mixed["batched"], "image_at_a_time": mixed["alone"],
                            "speedup_vs_image_at_a_time": mixed["batched"] / mixed["alone"],
                            "roofline": mixed["roofline"], "e2e": mixed["e2e"], "unit": UNIT}
+            line["unrolled"] = {"workload": "unrolled-tgv-16x512, 100 iterations", "forward_ms": unrolled["forward_ms"],
+                                "forward_backward_ms": unrolled["both_ms"], "checkpoint_every": unrolled["every"],
+                                "forward_backward_over_forward": unrolled["both_ms"] / unrolled["forward_ms"],
+                                "every_iterate_kept_over_forward": unrolled["kept_ms"] / unrolled["forward_ms"],
+                                "every_iterate_kept_checkpoint_bytes": unrolled["kept_bytes"],
+                                "grad_finite": unrolled["grad_finite"]}
         print(json.dumps(line))
     if group is not None:
         group.destroy_process_group()
