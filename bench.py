@@ -189,7 +189,10 @@ def _reference_arm(args: argparse.Namespace, rank: int) -> None:
 
 def _cpu_baseline(image) -> tuple[dict | None, object]:
     """The reference's solver on the host cores, a bounded sample: two iterations (setup
-    differenced out), the best of three, with every host thread and with one; then one whole
+    differenced out), the median of five -- the reference arm's estimator, since a solve's setup
+    (the host model, the first touch of its arrays) varies by more than two iterations take, so
+    that the best of a few samples overstates the rate -- with every host thread and with one
+    (median of three); then one whole
     solve of the workload (500 iterations, every thread), timed, whose canvas is the checker of
     the device's result (the line's parity). Run before the process touches the GPU, so that
     nothing of the GPU's side (its driver threads, pinned host memory) competes with it.
@@ -199,20 +202,22 @@ def _cpu_baseline(image) -> tuple[dict | None, object]:
     if not reference.available():
         return None, None
     threads = os.cpu_count() or 1
-    sample, repeats = 2, 3
+    sample, repeats = 2, 5
     _reference_seconds(image, threads, 1, 1)  # the library's pages and the picture's arrays warmed
-    best = min(_reference_seconds(image, threads, sample, repeats))
-    one = min(_reference_seconds(image, 1, sample, repeats))
+    samples = _reference_seconds(image, threads, sample, repeats)
+    middle = statistics.median(samples)
+    one = statistics.median(_reference_seconds(image, 1, sample, 3))
     began = time.perf_counter()
     whole = reference.solve(image.height, image.width, int(image.color_space), _components(image),
                             [*OPTIONS, "--threads", str(threads)])
     whole_seconds = time.perf_counter() - began
     pixels = HEIGHT * WIDTH
-    return {"value": pixels * sample / best / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
+    return {"value": pixels * sample / middle / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"{sample} iterations of the 4032x3024 4:2:0 TGV workload (setup differenced out), "
-                      f"best of {repeats}, {threads} threads",
+                      f"median of {repeats}, {threads} threads",
+            "best_of_samples": pixels * sample / min(samples) / 1e6,
             "one_thread": {"value": pixels * sample / one / 1e6, "unit": UNIT, "cores": 1,
-                           "sample": f"{sample} iterations, best of {repeats}, 1 thread"},
+                           "sample": f"{sample} iterations, median of 3, 1 thread"},
             "whole_solve": {"seconds": whole_seconds, "iterations": ITERATIONS, "cores": threads,
                             "value": pixels * ITERATIONS / whole_seconds / 1e6, "unit": UNIT,
                             "note": "one solve of 500 iterations with the host model and the start"}}, whole
