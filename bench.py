@@ -864,6 +864,7 @@ def _unrolled_arm(args: argparse.Namespace, rank: int, world: int) -> None:
                    "l2": "state 16 x 512^2 x 9 fields = 151 MB, larger than L2"},
         "forward": {"value": pixels * iterations / (m["forward_ms"] / 1e3) / 1e6, "ms": m["forward_ms"]},
         "forward_backward_over_forward": m["both_ms"] / m["forward_ms"],
+        "backward_over_forward": (m["both_ms"] - m["forward_ms"]) / m["forward_ms"],
         "every_iterate_kept": {"checkpoint_every": 1, "ms": m["kept_ms"],
                                "forward_backward_over_forward": m["kept_ms"] / m["forward_ms"],
                                "checkpoint_bytes": m["kept_bytes"]},
@@ -1047,6 +1048,8 @@ def main() -> None:
             line["unrolled"] = {"workload": "unrolled-tgv-16x512, 100 iterations", "forward_ms": unrolled["forward_ms"],
                                 "forward_backward_ms": unrolled["both_ms"], "checkpoint_every": unrolled["every"],
                                 "forward_backward_over_forward": unrolled["both_ms"] / unrolled["forward_ms"],
+                                "backward_over_forward": (unrolled["both_ms"] - unrolled["forward_ms"])
+                                                         / unrolled["forward_ms"],
                                 "every_iterate_kept_over_forward": unrolled["kept_ms"] / unrolled["forward_ms"],
                                 "every_iterate_kept_checkpoint_bytes": unrolled["kept_bytes"],
                                 "grad_finite": unrolled["grad_finite"]}
