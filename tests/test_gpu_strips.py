@@ -149,3 +149,25 @@ def test_nccl_exchange_equals_the_local_one():
     for k, (a, b) in enumerate(zip(mine, theirs)):
         assert torch.equal(a, b), f"plane {k}"
         assert torch.equal(a[48:64], a[0:16]) and torch.equal(a[16:24], a[96:104]), f"plane {k}"
+
+
+def test_exchanges_refused():
+    """The library's swaps refuse what they cannot do, before touching the device: rows beyond a
+    strip's canvas, a strip index beyond those given, an exchange of this rank with no NCCL
+    communicator, and the strip's last iteration (its record's or _finish's)."""
+    from unround import native, synthetic
+    from unround.strips import StripSolver, exchange_local
+
+    image = synthetic.grey(96, 64, quality=50, seed=3, noise=2.0).image
+    given = ["--method", "tgv", "--iterations", "10", "--tolerance", "0", "--record-every", "0"]
+    solver = StripSolver(image, given)
+    with pytest.raises(native.UnroundError, match="does not hold its rows") as caught:
+        solver.run(0, 0, [(0, 0, 0, 90, 16)], None)
+    assert caught.value.status is native.Status.ARGUMENT
+    with pytest.raises(native.UnroundError, match="beyond the 1 given"):
+        exchange_local([solver], [(0, 0, 1, 16, 8)])
+    with pytest.raises(native.UnroundError, match="NCCL communicator"):
+        solver.run(1, 0, [(0, 0, 1, 16, 8)], None)
+    with pytest.raises(native.UnroundError, match="last iteration"):
+        solver.run(10)
+    solver.run(9)  # the rest is allowed: iterations 1 .. 9, no exchanges
