@@ -108,6 +108,12 @@ class Clocks:
             self._thread.start()
         except OSError:
             self._process = None
+        # nvidia-smi takes a moment to start: the timed region begins once it samples (3 s at
+        # most), so that a short region is sampled too.
+        for _ in range(60):
+            if self.samples or self._process is None or self._process.poll() is not None:
+                break
+            time.sleep(0.05)
         return self
 
     def _read(self) -> None:
