@@ -171,3 +171,37 @@ def test_exchanges_refused():
     with pytest.raises(native.UnroundError, match="last iteration"):
         solver.run(10)
     solver.run(9)  # the rest is allowed: iterations 1 .. 9, no exchanges
+
+
+def test_the_distributed_form_records_on_one_rank():
+    """solve_strip at one NCCL rank with records every 10 iterations: the iterations between
+    records as one library call each (StripSolver.run on torch's communicator), the records
+    gathered, and the history and stop of the whole solve."""
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from unround import native, synthetic
+    from unround.strips import solve_strip
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    image = synthetic.colour(144, 96, quality=50, seed=11, noise=2.0).image
+    given = ["--method", "tgv", "--iterations", "45", "--tolerance", "0", "--record-every", "10"]
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        mine = solve_strip(image, given)
+    finally:
+        dist.destroy_process_group()
+    whole = native.solve(image, given)
+    theirs = whole.result.history
+    np.testing.assert_array_equal(mine.history.iterations, theirs.iterations)
+    for column in ("primal", "dual", "scaling"):
+        np.testing.assert_allclose(getattr(mine.history, column), getattr(theirs, column), rtol=1e-9, atol=0,
+                                   err_msg=column)
+    assert mine.iterations == 45 and mine.stop == int(whole.result.stop)
+    assert np.linalg.norm(mine.canvas - whole.canvas) / np.linalg.norm(whole.canvas) <= 1e-5
