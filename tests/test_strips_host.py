@@ -182,3 +182,32 @@ def test_gloo_ranks_take_the_same_records_and_stop():
     # TGV's scaling is alpha1 over the largest |div2 r~| of every rank's, not of one.
     largest = max(_FakeSolver.firsts(r, 5)[3] for r in range(world))
     assert expected[1][4] == (plan.alpha1 / largest if largest > plan.alpha1 else 1.0)
+
+
+def test_drive_makes_the_iterations_between_records_in_one_run():
+    """The loop's calls: the start's swap, a record at 0, then each stretch of iterations between
+    two records as one run(k) (each iteration followed by its swap inside), the recorded iteration
+    (made by the record) and its swap; the last iteration is always recorded."""
+    from unround.strips import StripPlan, _drive
+
+    plan = StripPlan(iterations=25, record_every=10, tolerance=0.0, relative_tolerance=0.0, partial_tolerance=0.0,
+                     partial_radius=None, alpha=1.0, alpha1=1.0, alpha0=2.0, tgv=False)
+    calls = []
+
+    def firsts_of(advance):
+        calls.append(("record", advance))
+        return [[1.0, 2.0, 0.0, 0.0, 4.0]]
+
+    records, iterations, stop = _drive(plan, lambda k: calls.append(("run", k)), firsts_of,
+                                       lambda theta: [[-1.0, 0.0, 0.0]])
+    assert calls == [("run", 0), ("record", False), ("run", 9), ("record", True), ("run", 0), ("run", 9),
+                     ("record", True), ("run", 0), ("run", 4), ("record", True), ("run", 0)]
+    assert [r[0] for r in records] == [0, 10, 20, 25] and iterations == 25 and stop == 2
+    # Without records between: one stretch, then the last iteration's record.
+    plan = StripPlan(iterations=7, record_every=0, tolerance=0.0, relative_tolerance=0.0, partial_tolerance=0.0,
+                     partial_radius=None, alpha=1.0, alpha1=1.0, alpha0=2.0, tgv=False)
+    calls.clear()
+    records, iterations, stop = _drive(plan, lambda k: calls.append(("run", k)), firsts_of,
+                                       lambda theta: [[-1.0, 0.0, 0.0]])
+    assert calls == [("run", 0), ("run", 6), ("record", True), ("run", 0)]
+    assert [r[0] for r in records] == [7] and iterations == 7 and stop == 2
