@@ -57,12 +57,13 @@ unround_status unround_b200_measure(const unround_input* input, const unround_se
 /* Many pictures solved together (no counterpart in the reference, whose callers solve one
  * picture a call): `count` inputs, each with its settings (tv or tgv, the same number of
  * iterations, --record-every 0), into `count` results, each freed by unround_result_free and
- * each the result unround_solve gives that picture alone to binary32 rounding. The iterations but the
- * last run for all pictures at once -- one launch per kernel class an iteration (the dual sweep
- * of each method and channel count, the primal step of each cell layout) over tables of tiles
- * of all pictures, captured in one CUDA graph launched once. `timing` (may be null) gets that
- * part's device milliseconds (CUDA events), its iterations and launches per iteration, and the
- * samples and pixels of all pictures. On failure no result is made. */
+ * each the result unround_solve gives that picture alone to binary32 rounding. The iterations
+ * but the last run for all pictures at once -- one launch per kernel class an iteration (the
+ * dual sweep of each method and channel count, the primal step of each cell layout) over tables
+ * of tiles of all pictures, two iterations captured in one CUDA graph launched for every pair.
+ * `timing` (may be null) gets that part's device milliseconds (CUDA events), its iterations and
+ * launches per iteration, and the samples and pixels of all pictures. On failure no result is
+ * made. */
 typedef struct unround_b200_batch_timing {
   double milliseconds;
   uint64_t iterations;

@@ -335,7 +335,7 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
   cudaEvent_t began = nullptr, ended = nullptr;
   if (error == cudaSuccess) error = cudaEventCreate(&began);
   if (error == cudaSuccess) error = cudaEventCreate(&ended);
-  if (batched > 1 && error == cudaSuccess) {
+  if (batched > 2 && error == cudaSuccess) {
     // Set up every launcher (shared memory, occupancy) before the capture: a launch of no work.
     for (auto& [key, primal] : primals) {
       if (error == cudaSuccess) {
@@ -348,9 +348,12 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
         error = launch_dual_batch(dual.device, 0, images_device, 0, dual.tgv, dual.channels, dual.coupled, stream);
       }
     }
+    // Two iterations, one of each parity (an iteration's launches depend on k only through the
+    // parity of the state it reads): the graph of a pair, launched for every pair of 2 .. N - 1.
     if (error == cudaSuccess) error = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
     if (error == cudaSuccess) {
-      for (std::uint64_t k = 2; k <= batched; ++k) iteration(k, stream);
+      iteration(2, stream);
+      iteration(3, stream);
       const cudaError_t ended_capture = cudaStreamEndCapture(stream, &graph);
       if (error == cudaSuccess) error = ended_capture;
     }
@@ -358,7 +361,12 @@ bool solve_batch(const std::vector<BatchEntry>& entries, cudaStream_t stream, st
   }
   if (error == cudaSuccess) error = cudaEventRecord(began, stream);
   if (batched > 0) iteration(1, stream);
-  if (exec != nullptr && error == cudaSuccess) error = cudaGraphLaunch(exec, stream);
+  const std::uint64_t pairs = batched > 1 ? (batched - 1) / 2 : 0;
+  for (std::uint64_t n = 0; n < pairs && exec != nullptr && error == cudaSuccess; ++n) {
+    error = cudaGraphLaunch(exec, stream);
+  }
+  // With an even count the last iteration (k = N - 1, of the pairs' first parity) is left.
+  if (batched > 1 && (batched - 1) % 2 == 1) iteration(batched, stream);
   if (error == cudaSuccess) error = cudaEventRecord(ended, stream);
   if (error == cudaSuccess) error = cudaEventSynchronize(ended);
   float milliseconds = 0.0f;

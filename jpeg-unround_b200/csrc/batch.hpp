@@ -3,7 +3,8 @@
 // record and result (Solver); the iterations between run for all pictures at once, one launch
 // per kernel class an iteration -- the dual sweep of each (method, channels) class over a table
 // of tiles of all its pictures, the primal step of each cell layout over a table of items of
-// all its components -- captured in one CUDA graph. The kernels make each pixel and block by
+// all its components -- two iterations (one of each parity of the state) captured in one CUDA
+// graph, launched once for every pair of iterations. The kernels make each pixel and block by
 // the single-picture kernels' device functions, so each result is the one unround_solve gives
 // the picture alone to binary32 rounding (the compiler may fuse a multiply-add differently in
 // the two kernels).
