@@ -16,6 +16,8 @@ solver's (tgv, relaxation rho); a slack's cost (--slack-cost) is not taken.
 from __future__ import annotations
 
 import ctypes
+import os
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import numpy.typing as npt
@@ -82,38 +84,36 @@ class UnrolledProblem:
         if not images:
             raise ValueError("a problem has at least one picture")
         c = dct_matrix()
-        lowers, uppers, centres, middles, weights, flat_weights, flats, starts = [], [], [], [], [], [], [], []
-        shape = None
         for image in images:
             if image.color_space != jpegio.ColorSpace.GRAYSCALE or len(image.components) != 1:
                 raise ValueError("the unrolled solve takes greyscale pictures")
-            levels = image.components[0].coefficients
-            by, bx = levels.shape[:2]
-            if shape is None:
-                shape = (by, bx)
-            elif shape != (by, bx):
-                raise ValueError("the pictures of a problem have one canvas size")
+        shapes = {image.components[0].coefficients.shape[:2] for image in images}
+        if len(shapes) != 1:
+            raise ValueError("the pictures of a problem have one canvas size")
+        shape = next(iter(shapes))
+        by, bx = shape
+
+        def constants(image: jpegio.Image) -> tuple:
+            # One picture's constants from the host model (the library's calls release the
+            # interpreter, so pictures are made on the host's threads at once).
             lower = native.model(image, options, 0, 0).reshape(by, bx, 64)
             upper = native.model(image, options, 0, 1).reshape(by, bx, 64)
             centre = native.model(image, options, 0, 2).reshape(by, bx, 64)
             # The start: the clipped centres' canvas (absolute coefficients).
             zeta = np.clip(centre, lower, upper).reshape(by, bx, 8, 8)
-            starts.append(_blocks_to_canvas(np.einsum("vi,abvu,un->abin", c, zeta, c, optimize=True)))
+            start = _blocks_to_canvas(np.einsum("vi,abvu,un->abin", c, zeta, c, optimize=True))
             # DC centred on the middle of its interval.
             middle = 0.5 * (lower[..., 0] + upper[..., 0])
-            lower = lower.copy()
-            upper = upper.copy()
-            centre = centre.copy()
+            lower, upper, centre = lower.copy(), upper.copy(), centre.copy()
             lower[..., 0] -= middle
             upper[..., 0] -= middle
             centre[..., 0] -= middle
-            lowers.append(lower)
-            uppers.append(upper)
-            centres.append(centre)
-            middles.append(middle / 8.0)
-            weights.append(native.model(image, options, 0, 4))
-            flat_weights.append(native.model(image, options, 0, 5))
-            flats.append(native.model(image, options, 0, 6).reshape(by, bx))
+            return (lower, upper, centre, middle / 8.0, native.model(image, options, 0, 4),
+                    native.model(image, options, 0, 5), native.model(image, options, 0, 6).reshape(by, bx), start)
+
+        with ThreadPoolExecutor(max_workers=max(1, min(len(images), os.cpu_count() or 1, 16))) as pool:
+            made = list(pool.map(constants, images))
+        lowers, uppers, centres, middles, weights, flat_weights, flats, starts = (list(x) for x in zip(*made))
         assert shape is not None
         self.images = len(images)
         self.rows, self.columns = shape[0] * 8, shape[1] * 8
