@@ -75,3 +75,19 @@ def test_refusals_of_inputs():
         native.model(jpegio.image_of(32, 32, 2, [(good.components[0].coefficients, good.components[0].quant_table, 1, 1)]),
                      ["--method", "tv"])
     assert raised.value.status == native.Status.UNSUPPORTED
+
+
+@pytest.mark.parametrize("height, width, rows", [(0, 32, 4), (32, 0, 4), (32, 32, 2), (40, 32, 4), (32, 32, 0)],
+                         ids=["no-rows", "no-columns", "blocks-short", "picture-taller", "no-blocks"])
+def test_refusals_of_empty_and_ragged_inputs(height, width, rows):
+    """A picture without samples, or blocks that do not cover it, is refused before any device
+    work, as the reference's solver refuses it."""
+    good = synthetic.grey(32, 32, quality=50, seed=6).image
+    c = good.components[0]
+    blocks = np.ascontiguousarray(c.coefficients[:rows]) if rows else np.zeros((0, 4, 8, 8), np.int16)
+    image = jpegio.image_of(height, width, 1, [(blocks, c.quant_table, 1, 1)])
+    with pytest.raises(native.UnroundError) as raised:
+        native.model(image, ["--method", "tv"])
+    assert raised.value.status == native.Status.UNSUPPORTED
+    with pytest.raises(Exception):
+        _theirs(image, ["--method", "tv", "--iterations", "0"])
