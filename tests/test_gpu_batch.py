@@ -75,8 +75,11 @@ def test_other_layouts_and_channels_apart():
         _same(b, a, f"picture {n}")
 
 
-@pytest.mark.parametrize("iterations", [1, 2])
+@pytest.mark.parametrize("iterations", [1, 2, 3, 4, 5])
 def test_few_iterations(iterations):
+    # 1 and 2: no iteration batched or one, eagerly; 3: two, eagerly; 4: the first eagerly and one
+    # launch of the graph of a pair; 5: the first, a pair, and the last of the pairs' first parity
+    # eagerly.
     from unround import synthetic
 
     entries = synthetic.mix(3, seed=7, smallest=32, largest=96, iterations=iterations)
