@@ -608,7 +608,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
 }  // namespace
 
 // A 3D tiled map of `count` float planes `stride` floats apart, each the canvas's rows x columns
-// (rows `pitch` apart), boxes of 40 columns x `box_rows` rows x every plane.
+// (rows `pitch` apart), boxes of `box_columns` columns x `box_rows` rows x every plane.
 bool make_box_map(CUtensorMap& map, const float* planes, const Geometry& g, int count, std::size_t stride,
                   unsigned box_rows, unsigned box_columns) {
   PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
