@@ -6,10 +6,68 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <limits>
+#include <map>
+#include <mutex>
 #include <thread>
 
 namespace urb {
+
+namespace {
+
+// The reused blocks: each starts with a header of its size; idle ones are kept up to kKeep bytes
+// in all, a request taking the smallest idle block that holds it and is at most twice its size.
+constexpr std::size_t kHeader = 64;
+constexpr std::size_t kKeep = std::size_t{1} << 30;
+
+struct Blocks {
+  std::mutex lock;
+  std::multimap<std::size_t, void*> idle;  // bytes -> block
+  std::size_t idle_bytes = 0;
+};
+
+Blocks& blocks() {
+  static Blocks* made = new Blocks;  // never destroyed: blocks may be returned during exit
+  return *made;
+}
+
+}  // namespace
+
+void* reused_block(std::size_t bytes) {
+  Blocks& b = blocks();
+  {
+    std::lock_guard<std::mutex> hold(b.lock);
+    auto it = b.idle.lower_bound(bytes + kHeader);
+    if (it != b.idle.end() && it->first <= 2 * (bytes + kHeader)) {
+      void* block = it->second;
+      b.idle_bytes -= it->first;
+      b.idle.erase(it);
+      return static_cast<char*>(block) + kHeader;
+    }
+  }
+  const std::size_t size = bytes + kHeader;
+  void* block = std::malloc(size);
+  if (block == nullptr) throw std::bad_alloc();
+  *static_cast<std::size_t*>(block) = size;
+  return static_cast<char*>(block) + kHeader;
+}
+
+void return_block(void* at) {
+  if (at == nullptr) return;
+  void* block = static_cast<char*>(at) - kHeader;
+  const std::size_t size = *static_cast<std::size_t*>(block);
+  Blocks& b = blocks();
+  {
+    std::lock_guard<std::mutex> hold(b.lock);
+    if (b.idle_bytes + size <= kKeep) {
+      b.idle.emplace(size, block);
+      b.idle_bytes += size;
+      return;
+    }
+  }
+  std::free(block);
+}
 
 namespace {
 

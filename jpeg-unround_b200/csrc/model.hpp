@@ -45,10 +45,17 @@ struct ComponentInput {
   std::array<std::uint16_t, 64> table{};
 };
 
-// An allocator whose resize leaves new elements uninitialised, so that a large array is first
-// touched by the threads that fill it rather than zeroed first by one.
+// Host blocks of the model's large arrays, kept for the next solve when freed (up to a limit),
+// so that a solve writes into memory whose pages the process already holds instead of faulting in
+// fresh pages (model.cpp).
+void* reused_block(std::size_t bytes);
+void return_block(void* block);
+
+// An allocator whose resize leaves new elements uninitialised (the threads that fill a large array
+// touch it first, not one thread zeroing it), from the reused host blocks.
 template <typename T>
 struct Uninitialised : std::allocator<T> {
+  using is_always_equal = std::true_type;
   template <typename U>
   struct rebind {
     using other = Uninitialised<U>;
@@ -56,6 +63,8 @@ struct Uninitialised : std::allocator<T> {
   Uninitialised() = default;
   template <typename U>
   Uninitialised(const Uninitialised<U>&) noexcept {}
+  T* allocate(std::size_t n) { return static_cast<T*>(reused_block(n * sizeof(T))); }
+  void deallocate(T* at, std::size_t) noexcept { return_block(at); }
   template <typename U>
   void construct(U* at) noexcept {
     ::new (static_cast<void*>(at)) U;
