@@ -12,8 +12,8 @@ A step is one full solve of it (500 iterations).
          host arrays: levels copied in, the binary64 result copied out, every step.
 
 Beside them, outside the timed regions: cpu_baseline (the reference's C++ solver on the host
-cores, run first: best of three bounded samples with every thread and with one, and one whole
-solve of the workload), parity (the device's result against that whole solve), records (the
+cores, run first: the median of five bounded samples with every thread and of three with one,
+and one whole solve of the workload), parity (the device's result against that whole solve), records (the
 cost of a record every 10 iterations, the reference's default), mix (the batched 64-picture mix
 against the same pictures one at a time, with the ceiling the image-at-a-time path's share of
 the HBM peak leaves).
@@ -129,12 +129,26 @@ class Clocks:
             self._thread.join(timeout=2)
 
     def summary(self) -> dict:
-        mhz = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
-        top = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        """The median SM clock under load -- over the samples drawing at least half the most
+        power drawn in the region, so that the idle moments around a short timed region (the
+        host's set-up, the sampler's start) do not count -- the highest clock, and the throttle
+        reasons seen in any sample."""
+        def number(text: str) -> float | None:
+            try:
+                return float(text)
+            except ValueError:
+                return None
+
+        rows = [s for s in self.samples if len(s) >= 9]
+        readings = [(number(s[1]), number(s[3])) for s in rows]
+        most = max((w for _, w in readings if w is not None), default=None)
+        loaded = [m for m, w in readings if m is not None and (most is None or (w is not None and w >= 0.5 * most))]
+        top = [t for t in (number(s[2]) for s in rows) if t is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples if len(s) >= 9 for k in range(4) if s[5 + k] == "Active"})
-        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": max(top) if top else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        reasons = sorted({names[k] for s in rows for k in range(4) if s[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(top) if top else None,
+                "reasons": reasons, "samples": len(self.samples), "samples_under_load": len(loaded),
+                "power_w_max": most}
 
 
 def _workload(seed: int):
