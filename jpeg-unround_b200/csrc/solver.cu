@@ -39,6 +39,13 @@ int samples_kernels() {
   return 0;
 }
 
+// UNROUND_B200_GRAPHS=0 launches every iteration's kernels one by one; otherwise the iterations
+// that keep nothing go two at a time as one CUDA graph (Impl::pair).
+bool pair_graphs() {
+  const char* value = std::getenv("UNROUND_B200_GRAPHS");
+  return value == nullptr || std::strcmp(value, "0") != 0;
+}
+
 }  // namespace
 
 struct Solver::Impl {
@@ -95,10 +102,17 @@ struct Solver::Impl {
   SampleEnds32* s_ends = nullptr;       // per level: binary32 ends rounded inward, the centre
   SampleEnds64* s_ends64 = nullptr;     // per level: binary64 ends and centre
   int samples_written = 0;  // the CTAs of the last kept primal step's sums of G
+  // Two iterations that keep nothing (the dual step and the next primal step, twice) captured as
+  // one CUDA graph from the state of parity `pair_parity`; made at the first pair after both
+  // launches have run eagerly (which sets up their launchers), made again for the other parity.
+  cudaGraphExec_t pair_exec = nullptr;
+  int pair_parity = -1;
+  bool plain_dual = false, plain_primal = false;  // a dual(false) and a primal(false) have run
 
   Impl(const Frame& f, cudaStream_t s) : frame(f), stream(s) {}
 
   ~Impl() {
+    if (pair_exec != nullptr) cudaGraphExecDestroy(pair_exec);
     for (void* p : owned) cudaFreeAsync(p, stream);
     cudaStreamSynchronize(stream);
   }
@@ -476,6 +490,7 @@ struct Solver::Impl {
   // The primal step of every component; the TMA path takes two components of the same cells
   // (Cb and Cr) in one launch.
   void primal(bool keep) {
+    plain_primal = plain_primal || !keep;
     if (samples != nullptr) {
       const Fields& st = state[current];
       SamplesPrimalParams sp;
@@ -547,6 +562,7 @@ struct Solver::Impl {
   }
 
   void dual(bool keep) {
+    plain_dual = plain_dual || !keep;
     const DualParams dp = dual_params();
     if (error == cudaSuccess) {
       error = swept ? launch_dual_tma(state_maps[current], tilde_maps[xt_id], dp, tgv, plan.coupled, keep, stream)
@@ -557,6 +573,39 @@ struct Solver::Impl {
 
   // The dual step of iteration n and the primal step of iteration n + 1 as one sweep
   // (iteration.cu), keeping nothing: from x~_n and s_{n-1} to s_n and x~_{n+1}.
+  // Launches two iterations that keep nothing -- dual(false), primal(false), twice -- as one
+  // graph; false (nothing launched) where the solve does not take graphs. The launches depend on
+  // the iteration only through the parity of the state, which the pair leaves as it found it.
+  bool pair() {
+    if (!plain_dual || !plain_primal || fusable || samples != nullptr || error != cudaSuccess || !pair_graphs()) {
+      return false;
+    }
+    if (pair_exec == nullptr || pair_parity != current) {
+      if (pair_exec != nullptr) {
+        cudaGraphExecDestroy(pair_exec);
+        pair_exec = nullptr;
+      }
+      const int parity = current;
+      cudaGraph_t graph = nullptr;
+      if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+      dual(false);
+      primal(false);
+      dual(false);
+      primal(false);
+      const cudaError_t ended = cudaStreamEndCapture(stream, &graph);
+      if (error == cudaSuccess) error = ended;
+      if (error == cudaSuccess) error = cudaGraphInstantiate(&pair_exec, graph, 0);
+      if (graph != nullptr) cudaGraphDestroy(graph);
+      if (error != cudaSuccess) return false;
+      pair_parity = parity;
+    }
+    error = cudaGraphLaunch(pair_exec, stream);
+    return error == cudaSuccess;
+  }
+
   void fused() {
     if (samples != nullptr && samples_layout == 2) {
       SamplesStep q;
@@ -1041,6 +1090,12 @@ bool Solver::run(std::uint64_t first, const Observer& observer, Outcome& out, Fa
       iteration = next;
       continue;
     }
+    // D_next, P_{next+1}, D_{next+1}, P_{next+2} as one graph when none of them keeps anything.
+    if (next + 1 < most && !recorded(next) && !recorded(next + 1) && !recorded(next + 2) && m.pair()) {
+      iteration = next + 1;
+      continue;
+    }
+    if (m.error != cudaSuccess) break;
     m.dual(recorded(next));
     iteration = next;
     if (recorded(iteration)) stopped = take(iteration);
@@ -1206,14 +1261,23 @@ bool Solver::prepare(const Plan& plan, Failure& failure) {
 
 bool Solver::iterate(std::uint64_t iterations, Failure& failure) {
   Impl& m = *impl_;
-  for (std::uint64_t n = 0; n < iterations && m.error == cudaSuccess; ++n) {
+  std::uint64_t n = 0;
+  while (n < iterations && m.error == cudaSuccess) {
     const bool last = n + 1 == iterations;
     if (m.fusable && !last) {
       m.fused();
-    } else {
-      m.dual(false);
-      m.primal(last);
+      ++n;
+      continue;
     }
+    // Two iterations as one graph while at least one more (the last, which keeps) follows.
+    if (iterations - n >= 3 && m.pair()) {
+      n += 2;
+      continue;
+    }
+    if (m.error != cudaSuccess) break;
+    m.dual(false);
+    m.primal(last);
+    ++n;
   }
   return m.check(failure, "the iterations");
 }
