@@ -39,9 +39,12 @@ int samples_kernels() {
   return 0;
 }
 
-// UNROUND_B200_GRAPHS=0 launches every iteration's kernels one by one; otherwise the iterations
-// that keep nothing go two at a time as one CUDA graph (Impl::pair).
-bool pair_graphs() {
+// Iterations that keep nothing are launched kGraphIterations at a time as one CUDA graph
+// (Impl::group; an even count, so that a group leaves the state's parity as it found it);
+// UNROUND_B200_GRAPHS=0 launches every iteration's kernels one by one.
+constexpr std::uint64_t kGraphIterations = 8;
+
+bool group_graphs() {
   const char* value = std::getenv("UNROUND_B200_GRAPHS");
   return value == nullptr || std::strcmp(value, "0") != 0;
 }
@@ -102,17 +105,18 @@ struct Solver::Impl {
   SampleEnds32* s_ends = nullptr;       // per level: binary32 ends rounded inward, the centre
   SampleEnds64* s_ends64 = nullptr;     // per level: binary64 ends and centre
   int samples_written = 0;  // the CTAs of the last kept primal step's sums of G
-  // Two iterations that keep nothing (the dual step and the next primal step, twice) captured as
-  // one CUDA graph from the state of parity `pair_parity`; made at the first pair after both
-  // launches have run eagerly (which sets up their launchers), made again for the other parity.
-  cudaGraphExec_t pair_exec = nullptr;
-  int pair_parity = -1;
+  // kGraphIterations iterations that keep nothing (the dual step and the next primal step, each
+  // time) captured as one CUDA graph from the state of parity `group_parity`; made at the first
+  // group after both launches have run eagerly (which sets up their launchers), made again for
+  // the other parity.
+  cudaGraphExec_t group_exec = nullptr;
+  int group_parity = -1;
   bool plain_dual = false, plain_primal = false;  // a dual(false) and a primal(false) have run
 
   Impl(const Frame& f, cudaStream_t s) : frame(f), stream(s) {}
 
   ~Impl() {
-    if (pair_exec != nullptr) cudaGraphExecDestroy(pair_exec);
+    if (group_exec != nullptr) cudaGraphExecDestroy(group_exec);
     for (void* p : owned) cudaFreeAsync(p, stream);
     cudaStreamSynchronize(stream);
   }
@@ -573,17 +577,18 @@ struct Solver::Impl {
 
   // The dual step of iteration n and the primal step of iteration n + 1 as one sweep
   // (iteration.cu), keeping nothing: from x~_n and s_{n-1} to s_n and x~_{n+1}.
-  // Launches two iterations that keep nothing -- dual(false), primal(false), twice -- as one
-  // graph; false (nothing launched) where the solve does not take graphs. The launches depend on
-  // the iteration only through the parity of the state, which the pair leaves as it found it.
-  bool pair() {
-    if (!plain_dual || !plain_primal || fusable || samples != nullptr || error != cudaSuccess || !pair_graphs()) {
+  // Launches kGraphIterations iterations that keep nothing -- dual(false), primal(false), each
+  // time -- as one graph; false (nothing launched) where the solve does not take graphs. The
+  // launches depend on the iteration only through the parity of the state, which an even count
+  // of iterations leaves as it found it.
+  bool group() {
+    if (!plain_dual || !plain_primal || fusable || samples != nullptr || error != cudaSuccess || !group_graphs()) {
       return false;
     }
-    if (pair_exec == nullptr || pair_parity != current) {
-      if (pair_exec != nullptr) {
-        cudaGraphExecDestroy(pair_exec);
-        pair_exec = nullptr;
+    if (group_exec == nullptr || group_parity != current) {
+      if (group_exec != nullptr) {
+        cudaGraphExecDestroy(group_exec);
+        group_exec = nullptr;
       }
       const int parity = current;
       cudaGraph_t graph = nullptr;
@@ -591,18 +596,18 @@ struct Solver::Impl {
         cudaGetLastError();
         return false;
       }
-      dual(false);
-      primal(false);
-      dual(false);
-      primal(false);
+      for (std::uint64_t k = 0; k < kGraphIterations; ++k) {
+        dual(false);
+        primal(false);
+      }
       const cudaError_t ended = cudaStreamEndCapture(stream, &graph);
       if (error == cudaSuccess) error = ended;
-      if (error == cudaSuccess) error = cudaGraphInstantiate(&pair_exec, graph, 0);
+      if (error == cudaSuccess) error = cudaGraphInstantiate(&group_exec, graph, 0);
       if (graph != nullptr) cudaGraphDestroy(graph);
       if (error != cudaSuccess) return false;
-      pair_parity = parity;
+      group_parity = parity;
     }
-    error = cudaGraphLaunch(pair_exec, stream);
+    error = cudaGraphLaunch(group_exec, stream);
     return error == cudaSuccess;
   }
 
@@ -1077,6 +1082,12 @@ bool Solver::run(std::uint64_t first, const Observer& observer, Outcome& out, Fa
     return false;
   };
   auto recorded = [&](std::uint64_t n) { return (every > 0 && n % every == 0) || n == most; };
+  auto none_recorded = [&](std::uint64_t from, std::uint64_t to) {
+    for (std::uint64_t n = from; n <= to; ++n) {
+      if (recorded(n)) return false;
+    }
+    return true;
+  };
   bool stopped = false;
   if (first == 0 && (every > 0 || most == 0)) stopped = take(0);
   std::uint64_t iteration = first;
@@ -1090,9 +1101,10 @@ bool Solver::run(std::uint64_t first, const Observer& observer, Outcome& out, Fa
       iteration = next;
       continue;
     }
-    // D_next, P_{next+1}, D_{next+1}, P_{next+2} as one graph when none of them keeps anything.
-    if (next + 1 < most && !recorded(next) && !recorded(next + 1) && !recorded(next + 2) && m.pair()) {
-      iteration = next + 1;
+    // D_next, P_{next+1}, ..., D_{next+G-1}, P_{next+G} (G = kGraphIterations) as one graph when
+    // none of them keeps anything.
+    if (next + kGraphIterations - 1 < most && none_recorded(next, next + kGraphIterations) && m.group()) {
+      iteration = next + kGraphIterations - 1;
       continue;
     }
     if (m.error != cudaSuccess) break;
@@ -1269,9 +1281,10 @@ bool Solver::iterate(std::uint64_t iterations, Failure& failure) {
       ++n;
       continue;
     }
-    // Two iterations as one graph while at least one more (the last, which keeps) follows.
-    if (iterations - n >= 3 && m.pair()) {
-      n += 2;
+    // kGraphIterations iterations as one graph while at least one more (the last, which keeps)
+    // follows.
+    if (iterations - n > kGraphIterations && m.group()) {
+      n += kGraphIterations;
       continue;
     }
     if (m.error != cudaSuccess) break;
