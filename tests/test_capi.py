@@ -143,3 +143,27 @@ def test_the_c_layer_s_metadata_and_the_profile_check():
 
 def test_the_command_line_is_outside_this_build():
     assert native.main(["--help"]) == 3
+
+
+def _copy_in_child(out) -> None:
+    data = np.arange(3_000_000, dtype=np.float64)
+    copied = native._copy(data.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), (1000, 3000))
+    out.put(bool(np.array_equal(copied.reshape(-1), data)))
+
+
+@pytest.mark.filterwarnings("ignore:This process .* is multi-threaded:DeprecationWarning")
+def test_large_copies_in_parts_and_after_fork():
+    """A result's large arrays are copied on the host's threads, in parts, exactly; a process forked
+    after the copying threads exist makes its own (the parent's do not exist in the child)."""
+    import multiprocessing as mp
+
+    data = np.arange(5_000_000, dtype=np.float64)  # 40 MB: copied in parts
+    copied = native._copy(data.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), (5000, 1000))
+    assert copied.shape == (5000, 1000) and np.array_equal(copied.reshape(-1), data)
+    assert copied.ctypes.data != data.ctypes.data
+    context = mp.get_context("fork")
+    out = context.Queue()
+    child = context.Process(target=_copy_in_child, args=(out,))
+    child.start()
+    child.join(timeout=60)
+    assert child.exitcode == 0 and out.get(timeout=5) is True
