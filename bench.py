@@ -1054,6 +1054,9 @@ def main() -> None:
                          "d2h_bytes_per_step": file_d2h,
                          "call": "unround_decode of a JPEG file (quality 75, 4:2:0, Pillow-written) of the "
                                  "workload's picture; coefficients read on the host"},
+            "e2e_python": {"value": pixels * ITERATIONS / min(plain_s) / 1e6, "unit": UNIT,
+                           "call": "unround.native.solve, the Python drop-in: the result's arrays and the "
+                                   "model's copied into NumPy (best of 2)"},
             "gpu_launches": timing.launches_per_iteration * args.steps * ITERATIONS,
             "clocks": clocks.summary(),
             "records": records,
