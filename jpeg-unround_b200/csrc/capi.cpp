@@ -1034,7 +1034,9 @@ const double* unround_result_problem(const unround_result* result, uint64_t comp
           }
         };
         const std::size_t blocks = n / 64;
-        const unsigned parts = static_cast<unsigned>(std::min<std::size_t>(threads, std::max<std::size_t>(blocks / 4096, 1)));
+        // A thread a part of at least 512 blocks (about 0.2 ms of work), so that small pictures
+        // are shared out too.
+        const unsigned parts = static_cast<unsigned>(std::min<std::size_t>(threads, std::max<std::size_t>(blocks / 512, 1)));
         std::vector<std::thread> workers;
         for (unsigned t = 1; t < parts; ++t) {
           workers.emplace_back(fill, blocks * t / parts * 64, blocks * (t + 1) / parts * 64);
