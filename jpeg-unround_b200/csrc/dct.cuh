@@ -42,6 +42,7 @@ __host__ __device__ constexpr T basis_as(int k, int n) {
   return static_cast<T>(basis(k, n));
 }
 
+#ifdef __CUDACC__
 // y = C x: the forward 8-point transform, even outputs from the sums, odd from the
 // differences.
 template <typename T>
@@ -70,5 +71,6 @@ __device__ __forceinline__ void inverse8(const T (&y)[8], T (&x)[8]) {
     x[7 - n] = even - odd;
   }
 }
+#endif  // __CUDACC__: the transforms are device code; host code takes the basis alone
 
 }  // namespace urb
