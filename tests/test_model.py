@@ -91,3 +91,16 @@ def test_refusals_of_empty_and_ragged_inputs(height, width, rows):
     assert raised.value.status == native.Status.UNSUPPORTED
     with pytest.raises(Exception):
         _theirs(image, ["--method", "tv", "--iterations", "0"])
+
+
+def test_reused_host_blocks_leave_no_trace():
+    """The model's levels and flat flags come from host blocks that earlier calls have used: the
+    same picture gives the same arrays before and after others, larger and smaller."""
+    options = ["--method", "tgv", "--flat-levels", "2", "--flat-dc", "3", "--iterations", "0"]
+    first = synthetic.grey(96, 80, quality=40, seed=31).image
+    before = [native.model(first, options, 0, which) for which in (0, 1, 2, 6)]
+    for seed, size in ((32, (200, 160)), (33, (24, 40)), (34, (120, 136))):
+        native.model(synthetic.grey(*size, quality=70, seed=seed).image, options, 0, 6)
+    after = [native.model(first, options, 0, which) for which in (0, 1, 2, 6)]
+    for a, b in zip(before, after):
+        np.testing.assert_array_equal(a, b)
